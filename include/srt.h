@@ -1,0 +1,349 @@
+/*
+ * srt.h — C ABI of the B200-native spectral path tracer.
+ *
+ * This is the drop-in boundary for the per-frame spectral path-tracing path of
+ * wgpu-spectral-rt.  Each entry point names the reference interface it
+ * replaces (path:line inside the reference project).  All signatures use
+ * plain C types, pointers and sizes; no CUDA or torch type appears here.
+ *
+ * Ownership: the library owns every device allocation.  Host arrays passed in
+ * are copied before the call returns.  Handles are destroyed in reverse order
+ * of creation (renderer, scene, context).  A handle is not thread-safe; use
+ * one context per host thread.
+ *
+ * Errors: every call returns an srt_status.  No exception or abort crosses
+ * the ABI.  srt_get_error_string(ctx) returns the last error text of a
+ * context (NULL ctx: the last error of a failed srt_ctx_create).
+ */
+#ifndef SRT_H
+#define SRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SRT_ABI_VERSION 1u
+
+/* Status codes.  Replaces unwrap()/panic! and wgpu::SurfaceError
+ * (src/app.rs:70-77, src/wgpu_ctx.rs:36-42). */
+typedef enum srt_status {
+    SRT_OK = 0,
+    SRT_ERR_INVALID_ARG = 1,
+    SRT_ERR_OOM = 2,
+    SRT_ERR_CUDA = 3,
+    SRT_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+    SRT_ERR_DEVICE_ASSERT = 5, /* a device-side check recorded an error */
+    SRT_ERR_NO_DEVICE = 6,
+    SRT_ERR_UNSUPPORTED = 7
+} srt_status;
+
+/* ------------------------------------------------------------------------ */
+/* Record layouts.  Byte-compatible with the reference's #[repr(C)] types.  */
+/* ------------------------------------------------------------------------ */
+
+/* src/scene/geometry.rs:4-9 (32 B). pos.w = 1, normal.w = 0. */
+typedef struct srt_vertex {
+    float pos[4];
+    float normal[4];
+} srt_vertex;
+
+/* src/scene/builder.rs:5-10 (32 B).
+ * extra.x = material type:
+ *   0 Lambert (color.rgb reflectance)
+ *   1 GGX metal (extra.y roughness alpha, clamped >= 0.001)
+ *   2 Cauchy dielectric (extra.z = A, extra.w = B in um^2)
+ *   3 blackbody emitter (color.r = temperature K, color.g = intensity,
+ *     extra.y > 0: emit from both faces)
+ *   4 Airy thin film (extra.y = thickness nm (>= 50), extra.z = n2, extra.w = n3)
+ *   5 thin-film-coated GGX (no reference counterpart): color.w = roughness
+ *     alpha, extra.y = film thickness nm, extra.z = n2 film, extra.w = n3
+ *     substrate; reflection only. */
+typedef struct srt_material {
+    float color[4];
+    float extra[4];
+} srt_material;
+
+/* src/scene/builder.rs:13-20 (64 B). World-space light triangle.
+ * params = (type, temperature K, intensity, pad). */
+typedef struct srt_light {
+    float v0[4];
+    float v1[4];
+    float v2[4];
+    float params[4];
+} srt_light;
+
+/* src/scene/builder.rs:22-28 (16 B). */
+typedef struct srt_mesh_info {
+    uint32_t vertex_offset;
+    uint32_t index_offset;
+    uint32_t pad[2];
+} srt_mesh_info;
+
+/* One instance: src/scene/builder.rs:41-45 (InstanceData).  transform is a
+ * column-major 4x4 object-to-world matrix (glam Mat4 memory order). */
+typedef struct srt_instance {
+    uint32_t mesh_id;
+    uint32_t mat_id;
+    uint32_t pad[2];
+    float transform[16];
+} srt_instance;
+
+/* src/scene/camera.rs:4-13 (272 B).  Matrices are column-major. */
+typedef struct srt_camera_uniform {
+    float view_inverse[16];
+    float proj_inverse[16];
+    float view[16];
+    float proj[16];
+    uint32_t frame_count;
+    uint32_t pad[3];
+} srt_camera_uniform;
+
+/* src/renderer/shaders/photon_emit.wgsl:19-24 (32 B). */
+typedef struct srt_photon {
+    float position[3];
+    float wavelength;
+    float direction[3];
+    float energy;
+} srt_photon;
+
+/* A ray for the batch trace entry points (32 B):
+ * origin.xyz, tmin, direction.xyz, tmax. */
+typedef struct srt_ray {
+    float origin[3];
+    float tmin;
+    float dir[3];
+    float tmax;
+} srt_ray;
+
+/* Closest-hit record (16 B).  prim = flattened triangle id (instance-major:
+ * instance i's triangles follow instance i-1's), 0xFFFFFFFF on a miss.
+ * u, v = barycentric weights of vertices 1 and 2 (the ray-query
+ * "barycentrics", src/renderer/shaders/shader.wgsl:541-544). */
+typedef struct srt_hit {
+    float t;
+    uint32_t prim;
+    float u;
+    float v;
+} srt_hit;
+
+/* Per-renderer parameters.  Defaults (srt_params_default) reproduce the
+ * reference's hard-coded constants. */
+typedef struct srt_params {
+    uint32_t max_depth;          /* MAX_DEPTH override 12: renderer/compute_pass.rs:26 */
+    uint32_t photons_per_frame;  /* MAX_PHOTONS 2^20: renderer/mod.rs:18; 0 disables the photon pass */
+    uint32_t hash_bits;          /* log2 HASH_SIZE = 22: renderer/mod.rs:19 */
+    uint32_t photon_max_bounces; /* 5: photon_emit.wgsl:219 */
+    uint32_t gather_cap;         /* 64: shader.wgsl:312 */
+    uint32_t flags;              /* SRT_FLAG_* */
+    float cell_size;             /* CELL_SIZE 0.02: shader.wgsl:275, build_grid.wgsl:23 */
+    float gather_radius0;        /* initial radius 0.02: shader.wgsl:302 */
+    float radius_exponent;       /* -0.15: shader.wgsl:303 */
+    float spectral_radius;       /* 20 nm: shader.wgsl:279 */
+    float photon_norm_count;     /* count in the density estimate; 0 = photons_per_frame
+                                    (the reference divides by MAX_PHOTON: shader.wgsl:339) */
+    uint32_t block_size;         /* trace/shade block size; 0 = autotuned default */
+} srt_params;
+
+#define SRT_FLAG_FP64_ACCUM   0x1u  /* keep an FP64 accumulation buffer beside the FP32 one */
+#define SRT_FLAG_NO_GRAPH     0x2u  /* launch kernels directly instead of a CUDA graph */
+#define SRT_FLAG_STAGE_TIMING 0x4u  /* record per-stage CUDA events (srt_renderer_get_stats) */
+#define SRT_FLAG_COUNT_VISITS 0x8u  /* traversal counts visited nodes and tested triangles */
+
+/* Per-renderer statistics of the frames rendered since the last reset. */
+typedef struct srt_stats {
+    uint64_t frames;
+    uint64_t paths;             /* camera paths started */
+    uint64_t rays_closest;      /* closest-hit rays traced (camera + photon) */
+    uint64_t rays_shadow;       /* any-hit rays traced */
+    uint64_t photons_emitted;
+    uint64_t photons_stored;
+    uint64_t nodes_visited;     /* SRT_FLAG_COUNT_VISITS only */
+    uint64_t tris_tested;       /* SRT_FLAG_COUNT_VISITS only */
+    double ms_photon_trace;     /* SRT_FLAG_STAGE_TIMING only: summed stage times */
+    double ms_photon_grid;
+    double ms_trace_closest;
+    double ms_shade;
+    double ms_trace_shadow;
+    double ms_finalize;
+    double ms_raygen;
+    uint64_t launches_trace_closest;
+    uint64_t kernel_launches;   /* kernels launched by the library in these frames */
+} srt_stats;
+
+typedef struct srt_ctx srt_ctx;
+typedef struct srt_scene srt_scene;
+typedef struct srt_scene_builder srt_scene_builder;
+typedef struct srt_renderer srt_renderer;
+
+/* ------------------------------------------------------------------------ */
+/* Context: replaces WgpuContext::new / resize (src/wgpu_ctx.rs:13-81).       */
+/* ------------------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  `stream` is a cudaStream_t to
+ * launch on (NULL: the library creates a non-blocking stream). */
+srt_status srt_ctx_create(int device, void* stream, srt_ctx** out);
+srt_status srt_ctx_destroy(srt_ctx* ctx);
+const char* srt_get_error_string(const srt_ctx* ctx);
+/* The cudaStream_t the context launches on. */
+void* srt_ctx_stream(srt_ctx* ctx);
+/* Wait for the context's stream; returns a pending device error, if any. */
+srt_status srt_ctx_synchronize(srt_ctx* ctx);
+uint32_t srt_abi_version(void);
+/* Number of SMs of the context's device. */
+int srt_ctx_sm_count(const srt_ctx* ctx);
+
+/* ------------------------------------------------------------------------ */
+/* Scene API: SceneBuilder (src/scene/builder.rs:47-267).                     */
+/* The builder is host-only; srt_scene_builder_build uploads it and builds    */
+/* the acceleration structure on the GPU (builder.rs:131-266).                */
+/* ------------------------------------------------------------------------ */
+
+srt_status srt_scene_builder_create(srt_scene_builder** out);
+srt_status srt_scene_builder_destroy(srt_scene_builder* b);
+/* builder.rs:70-74 */
+uint32_t srt_scene_builder_add_material(srt_scene_builder* b, const srt_material* m);
+/* builder.rs:76-91 */
+uint32_t srt_scene_builder_add_mesh(srt_scene_builder* b, const srt_vertex* v, uint32_t n_vertices,
+                                    const uint32_t* indices, uint32_t n_indices);
+/* builder.rs:93-99; transform column-major 4x4 */
+srt_status srt_scene_builder_add_instance(srt_scene_builder* b, uint32_t mesh_id, uint32_t mat_id,
+                                          const float transform[16]);
+/* builder.rs:101-129: adds the instance and one world-space srt_light per triangle */
+srt_status srt_scene_builder_add_light_instance(srt_scene_builder* b, uint32_t mesh_id, uint32_t mat_id,
+                                                const float transform[16], const float params[4]);
+/* Counts and read-only views of the builder's host arrays (for checkers and
+ * for srt_scene_build).  Pointers stay valid until the builder changes. */
+typedef struct srt_scene_arrays {
+    const srt_vertex* vertices;     uint32_t n_vertices;
+    const uint32_t* indices;        uint32_t n_indices;
+    const srt_mesh_info* mesh_infos; uint32_t n_meshes;
+    const srt_material* materials;  uint32_t n_materials;
+    const srt_instance* instances;  uint32_t n_instances;
+    const srt_light* lights;        uint32_t n_lights;
+} srt_scene_arrays;
+srt_status srt_scene_builder_arrays(const srt_scene_builder* b, srt_scene_arrays* out);
+srt_status srt_scene_builder_build(srt_ctx* ctx, const srt_scene_builder* b, srt_scene** out);
+
+/* Flat form of SceneBuilder::build: uploads already-assembled arrays.
+ * n_lights may be 0 (no light sampling, no photons). */
+srt_status srt_scene_build(srt_ctx* ctx, const srt_scene_arrays* arrays, srt_scene** out);
+srt_status srt_scene_destroy(srt_scene* s);
+/* Flattened triangle count and BVH node count of a built scene. */
+srt_status srt_scene_info(const srt_scene* s, uint64_t* n_triangles, uint64_t* n_nodes, uint32_t* bvh_depth);
+
+/* Procedural geometry (src/scene/geometry.rs:12-232).  Call with NULL
+ * outputs to query counts, then with arrays of at least that size. */
+srt_status srt_geometry_plane(srt_vertex* v, uint32_t* n_v, uint32_t* idx, uint32_t* n_i);
+srt_status srt_geometry_cube(srt_vertex* v, uint32_t* n_v, uint32_t* idx, uint32_t* n_i);
+srt_status srt_geometry_icosphere(uint32_t subdivisions, srt_vertex* v, uint32_t* n_v, uint32_t* idx, uint32_t* n_i);
+/* UV sphere, radius 0.5: `slices` around, `stacks` from pole to pole. */
+srt_status srt_geometry_uv_sphere(uint32_t slices, uint32_t stacks, srt_vertex* v, uint32_t* n_v, uint32_t* idx, uint32_t* n_i);
+
+/* Scene presets (src/scene/cornell_box.rs:6-110, src/scene/custom.rs:6-116)
+ * and the benchmark scenes.  Each fills an empty builder and returns the
+ * preset's default camera (position xyz, yaw, pitch in radians). */
+typedef enum srt_preset {
+    SRT_PRESET_CORNELL_BOX = 0,   /* cornell_box.rs:6-110 */
+    SRT_PRESET_CUSTOM_PRISM = 1,  /* custom.rs:6-116 */
+    SRT_PRESET_CONFIG1 = 2,       /* Cornell walls + 2-tri light + dispersive UV sphere */
+    SRT_PRESET_CONFIG2 = 3,       /* displaced level-8 icosphere + 64 coated GGX spheres */
+    SRT_PRESET_CAUSTIC_SLAB = 4   /* dispersive slab under a slit light + floor + config-1 mesh */
+} srt_preset;
+srt_status srt_scene_builder_add_preset(srt_scene_builder* b, int preset, uint32_t seed, float camera_out[5]);
+
+/* CameraController::build_uniform (src/scene/camera.rs:178-194):
+ * look_at_rh + perspective_rh(45 deg, aspect, 0.1, 100). */
+srt_status srt_camera_build_uniform(const float position[3], float yaw, float pitch, float aspect,
+                                    uint32_t frame_count, srt_camera_uniform* out);
+
+/* ------------------------------------------------------------------------ */
+/* Renderer API: Renderer::new / render (src/renderer/mod.rs:45-207).         */
+/* ------------------------------------------------------------------------ */
+
+srt_params srt_params_default(void);
+srt_status srt_renderer_create(srt_ctx* ctx, srt_scene* scene, uint32_t width, uint32_t height,
+                               const srt_params* params, srt_renderer** out);
+srt_status srt_renderer_destroy(srt_renderer* r);
+/* One frame = one sample per pixel: photon emit -> grid build -> camera
+ * paths -> accumulate + tonemap (renderer/mod.rs:168-207).  cam->frame_count
+ * seeds the RNG and resets the accumulation when 0 (engine.rs:154-166,
+ * shader.wgsl:803-805).  Asynchronous on the context's stream. */
+srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform* cam);
+/* Renderer.frame_count (renderer/mod.rs:30, incremented at :204). */
+uint32_t srt_renderer_frame_count(const srt_renderer* r);
+srt_status srt_renderer_set_frame_count(srt_renderer* r, uint32_t frame_count);
+/* Zero the accumulation buffers and set frame_count to 0 (engine.rs:154-156). */
+srt_status srt_reset_accumulation(srt_renderer* r);
+/* Linear accumulation (shader.wgsl:801-808): width*height float4
+ * (sum r, sum g, sum b, sample count), row 0 = bottom row. */
+srt_status srt_read_accum_f32(srt_renderer* r, float* rgba);
+/* FP64 accumulation (SRT_FLAG_FP64_ACCUM): width*height double4. */
+srt_status srt_read_accum_f64(srt_renderer* r, double* rgba);
+/* Tonemapped RGBA8 storage texture (shader.wgsl:809-822), row 0 = bottom
+ * row, `pitch` bytes per row (>= 4*width). */
+srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t pitch);
+/* Engine::save_screenshot + ScreenshotSaver (engine.rs:191-244,
+ * screenshot.rs:27-103): row flip, sRGB OETF of the 8-bit values, PNG file. */
+srt_status srt_save_screenshot(srt_renderer* r, const char* path);
+/* ScreenshotSaver::process_and_save (screenshot.rs:27-103) on host memory:
+ * `rgba` holds h rows of `pitch` bytes, row 0 = bottom row; writes a PNG
+ * with the rows flipped and the sRGB OETF applied to the 8-bit values. */
+srt_status srt_screenshot_write(const char* path, const uint8_t* rgba, uint32_t width, uint32_t height,
+                                uint32_t pitch);
+srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out);
+srt_status srt_renderer_reset_stats(srt_renderer* r);
+/* The photon set of the last frame in emission order (photon_emit.wgsl
+ * storage): copies min(count, capacity) photons to `out` (may be NULL) and
+ * the stored count to *count. */
+srt_status srt_renderer_read_photons(srt_renderer* r, srt_photon* out, uint32_t capacity, uint32_t* count);
+
+/* ------------------------------------------------------------------------ */
+/* Path kernels exposed on their own (parity checks and batch users).        */
+/* ------------------------------------------------------------------------ */
+
+/* Closest-hit (any_hit = 0) or any-hit (any_hit = 1, terminate on first hit)
+ * queries for a batch of rays in host memory: the ray queries of
+ * shader.wgsl:561-566, :654-659 and photon_emit.wgsl:222-227.  Any-hit
+ * writes prim = 0 for a hit and 0xFFFFFFFF for a miss. */
+srt_status srt_trace_rays(srt_scene* s, const srt_ray* rays, uint32_t n, srt_hit* hits, int any_hit);
+
+/* Photon hash grid over a given photon set (build_grid.wgsl:25-73), built
+ * by a stable radix sort of cell keys instead of linked lists.
+ * keys_out[i]  = (hash << 32) | photon index, ascending (n entries);
+ *                photons with energy == 0 get hash = 2^hash_bits.
+ * ranges_out   = 2^hash_bits pairs (start, end) into keys_out, (0,0) empty.
+ * Any output may be NULL. */
+srt_status srt_photon_grid_build(srt_ctx* ctx, const srt_photon* photons, uint32_t n, uint32_t frame_count,
+                                 float cell_size, uint32_t hash_bits, uint64_t* keys_out, uint32_t* ranges_out);
+
+/* Density estimate at query points (gather_photons, shader.wgsl:297-342)
+ * against a photon set: builds the grid then gathers.  query = n_q records
+ * of (position.xyz, normal.xyz, wavelengths[4]) = 10 floats; out = 4 floats
+ * per query. */
+srt_status srt_photon_gather(srt_ctx* ctx, const srt_photon* photons, uint32_t n, const float* queries,
+                             uint32_t n_q, uint32_t frame_count, const srt_params* params, float* out);
+
+/* Device unit kernels over the shading math, for parity checks.  op:
+ *  0 pcg_hash(u32 in[i]) -> u32 out[i]
+ *  1 sample_cie_xyz(lambda)                       in f32[1] -> out f32[3]
+ *  2 blackbody_radiance(lambda, T)                in f32[2] -> out f32[1]
+ *  3 rgb_to_spectrum(rgb[3], lambda[4])           in f32[7] -> out f32[4]
+ *  4 fresnel_thin_film(cos, n1, n2, n3, d, lambda[4]) in f32[9] -> out f32[4]
+ *  5 hero wavelengths from rng seed               in u32[1] -> out f32[5] (4 lambdas, sum pdf)
+ *  6 sample_bsdf: in f32[24] = r_dir[3], ffnormal[3], material[8], front(0/1),
+ *    wavelengths[4], throughput[4], rng seed (bits) -> out f32[10] =
+ *    scatter_dir[3], attenuation[4], absorbed(0/1), rng out (bits), pad
+ *  7 grid hash(position[3], frame bits, cell)     in f32[5] -> out u32[1]
+ *  8 camera ray(cam uniform from `aux`, pixel x, y, width, height as bits, rng seed) in u32[5]
+ *    -> out f32[7] origin[3] dir[3] rng out (bits)
+ * in/out strides are the per-op sizes above; n records. */
+srt_status srt_test_device_math(srt_ctx* ctx, int op, uint32_t n, const void* in, void* out, const void* aux);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SRT_H */

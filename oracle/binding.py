@@ -1,0 +1,137 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker.  The product package never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    """Compiles the oracle with its Makefile (g++ -fopenmp)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        P = C.c_void_p
+        U32 = C.c_uint32
+        L.orc_scene_create.restype = P
+        L.orc_scene_create.argtypes = [P]
+        L.orc_scene_destroy.argtypes = [P]
+        L.orc_scene_num_tris.restype = C.c_uint64
+        L.orc_scene_num_tris.argtypes = [P]
+        L.orc_trace.argtypes = [P, P, U32, C.c_int, C.c_int, P, P, P, P, P]
+        L.orc_device_math.restype = C.c_int
+        L.orc_device_math.argtypes = [C.c_int, U32, P, P, P]
+        L.orc_photon_emit.restype = U32
+        L.orc_photon_emit.argtypes = [P, U32, U32, U32, P, P, C.c_int]
+        L.orc_photon_grid_build.argtypes = [P, U32, U32, C.c_float, U32, P, P]
+        L.orc_photon_gather.argtypes = [P, U32, P, U32, U32, P, P]
+        L.orc_render_frame.argtypes = [P, P, U32, U32, P, U32, U32, P, P, P, P, C.c_int]
+        L.orc_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class OracleScene:
+    """FP64 ray queries + FP32 shading restatement over one scene's arrays."""
+
+    def __init__(self, arrays):
+        # arrays: a wgpu_spectral_rt_b200.SceneArrays (pointers into host memory)
+        self.h = lib().orc_scene_create(C.byref(arrays))
+
+    @property
+    def n_tris(self) -> int:
+        return int(lib().orc_scene_num_tris(self.h))
+
+    def trace(self, rays: np.ndarray, any_hit=False, brute=True):
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = len(r)
+        t = np.zeros(n, np.float64)
+        prim = np.zeros(n, np.uint32)
+        u = np.zeros(n, np.float64)
+        v = np.zeros(n, np.float64)
+        t2 = np.zeros(n, np.float64)
+        lib().orc_trace(self.h, _p(r), n, int(any_hit), int(brute), _p(t), _p(prim), _p(u), _p(v), _p(t2))
+        return t, prim, u, v, t2
+
+    def photon_emit(self, n_photons: int, frame: int, max_bounces: int = 5, threads: int = 0):
+        out = np.zeros((n_photons, 8), np.float32)
+        em = np.zeros(n_photons, np.uint32)
+        c = lib().orc_photon_emit(self.h, n_photons, frame, max_bounces, _p(out), _p(em), threads)
+        return out[:c].copy(), em[:c].copy()
+
+    def render_frame(self, cam, w: int, h: int, params, accum: np.ndarray | None = None, row_stride=1, row_phase=0,
+                     want_ldr=True, want_radiance=False, threads: int = 0):
+        if accum is None:
+            accum = np.zeros((h, w, 4), np.float32)
+        ldr = np.zeros((h, w, 4), np.uint8) if want_ldr else None
+        rad = np.zeros((h, w, 4), np.float32) if want_radiance else None
+        stats = np.zeros(5, np.uint64)
+        lib().orc_render_frame(self.h, C.byref(cam), w, h, C.byref(params), row_stride, row_phase, _p(accum),
+                               _p(ldr), _p(rad), _p(stats), threads)
+        return accum, ldr, rad, stats
+
+    def close(self):
+        if self.h:
+            lib().orc_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_math(op: int, inp: np.ndarray, aux=None) -> np.ndarray:
+    sizes = {0: (4, 4), 1: (4, 12), 2: (8, 4), 3: (28, 16), 4: (36, 16), 5: (4, 20), 6: (96, 40), 7: (20, 4),
+             8: (20, 28)}
+    isz, osz = sizes[op]
+    a = np.ascontiguousarray(inp)
+    n = a.nbytes // isz
+    out = np.zeros(n * osz // 4, np.uint32 if op in (0, 7) else np.float32)
+    rc = lib().orc_device_math(op, n, _p(a), _p(out), C.byref(aux) if aux is not None else None)
+    assert rc == 0
+    return out.reshape(n, osz // 4)
+
+
+def photon_grid_build(photons: np.ndarray, frame: int, cell: float = 0.02, hash_bits: int = 22):
+    p = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+    keys = np.zeros(len(p), np.uint64)
+    ranges = np.zeros((1 << hash_bits, 2), np.uint32)
+    lib().orc_photon_grid_build(_p(p), len(p), frame, cell, hash_bits, _p(keys), _p(ranges))
+    return keys, ranges
+
+
+def photon_gather(photons: np.ndarray, queries: np.ndarray, frame: int, params) -> np.ndarray:
+    p = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 10)
+    out = np.zeros((len(q), 4), np.float32)
+    lib().orc_photon_gather(_p(p), len(p), _p(q), len(q), frame, C.byref(params), _p(out))
+    return out
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())

@@ -1,0 +1,79 @@
+/*
+ * oracle.h — CPU oracle for the spectral path-tracing path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
+ * calls this code; only the tests, the smoke check and the benchmark's CPU
+ * baseline leg do, as the checker.
+ *
+ * The oracle restates the reference's WGSL hot path in C++ FP32 (same
+ * operation order, same RNG consumption order), with closest-hit / any-hit
+ * queries answered by an FP64 ray-triangle test in place of the Vulkan
+ * driver's ray queries.  Each function cites the reference line it follows.
+ *
+ * Parity status: the reference has no tests, golden vectors or fixtures, and
+ * its code path (wgpu -> Vulkan ray query) cannot run on this machine.  The
+ * oracle is pinned by known-answer tests derived from closed forms (PCG
+ * values, Planck peak, Fresnel limits, Airy film at zero thickness, hero
+ * wavelength pdf normalisation) and by the golden vectors under
+ * tests/golden/.  Where a value depends on the driver (traversal order,
+ * intersection rounding), parity is unpinned.
+ */
+#ifndef SRT_ORACLE_H
+#define SRT_ORACLE_H
+
+#include <stdint.h>
+#include "../include/srt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_scene orc_scene;
+
+orc_scene* orc_scene_create(const srt_scene_arrays* arrays);
+void orc_scene_destroy(orc_scene* s);
+uint64_t orc_scene_num_tris(const orc_scene* s);
+
+/* FP64 queries.  brute = 1 tests every triangle, otherwise an FP64 BVH.
+ * Closest: (t, prim, u, v) lexicographic min over (t, prim); t_second is the
+ * smallest t of any OTHER triangle hit (inf if none), used to detect ties.
+ * Any-hit (any_hit = 1): prim = 0 hit / 0xFFFFFFFF miss. */
+void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit, int brute,
+               double* t_out, uint32_t* prim_out, double* u_out, double* v_out, double* t_second);
+
+/* Same op codes and record layouts as srt_test_device_math. */
+int orc_device_math(int op, uint32_t n, const void* in, void* out, const void* aux);
+
+/* Photon emission for emitter ids [0, n_photons) (photon_emit.wgsl:154-331).
+ * Writes the stored photons in emitter order (the order a sequential run of
+ * the reference's atomicAdd would produce) and returns how many. */
+uint32_t orc_photon_emit(const orc_scene* s, uint32_t n_photons, uint32_t frame, uint32_t max_bounces,
+                         srt_photon* out, uint32_t* emitter_out, int n_threads);
+
+/* Grid over a photon set (build_grid.wgsl:25-73, sort form): same outputs
+ * as srt_photon_grid_build. */
+void orc_photon_grid_build(const srt_photon* photons, uint32_t n, uint32_t frame, float cell,
+                           uint32_t hash_bits, uint64_t* keys_out, uint32_t* ranges_out);
+
+/* gather_photons (shader.wgsl:297-342) for n_q queries of 10 floats. */
+void orc_photon_gather(const srt_photon* photons, uint32_t n, const float* queries, uint32_t n_q,
+                       uint32_t frame, const srt_params* params, float* out);
+
+/* One full frame (renderer/mod.rs:168-207): photon pass, grid, camera paths
+ * for rows y with y % row_stride == row_phase (all rows: 1, 0), accumulate
+ * and tonemap.  accum (w*h*4 floats) is read when cam->frame_count > 0 and
+ * written for the rendered rows; ldr (w*h*4 bytes, may be NULL) likewise.
+ * radiance_out (may be NULL): w*h*4 spectral radiance of the hero tuple
+ * before XYZ conversion, for per-path comparisons.  stats_out (may be NULL):
+ * [paths, closest rays, shadow rays, photons emitted, photons stored]. */
+void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
+                      const srt_params* params, uint32_t row_stride, uint32_t row_phase,
+                      float* accum, uint8_t* ldr, float* radiance_out, uint64_t* stats_out, int n_threads);
+
+int orc_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

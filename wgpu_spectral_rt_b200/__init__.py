@@ -1,0 +1,493 @@
+"""B200-native spectral path tracer: Python mirror of the reference's
+scene / renderer API over the C ABI of libsrt_b200.so (include/srt.h).
+
+The classes keep the reference's names and call order:
+
+    builder = SceneBuilder()                       # src/scene/builder.rs:47
+    builder.add_material(...); builder.add_mesh(...); builder.add_instance(...)
+    scene = builder.build(ctx)                     # builder.rs:131
+    renderer = Renderer(ctx, scene, w, h)          # src/renderer/mod.rs:45
+    cam = CameraController().build_uniform(w / h, renderer.frame_count)
+    renderer.render(cam)                           # renderer/mod.rs:168
+
+Every call goes through the native library; there is no Python or CPU
+fallback.  A missing library raises at import of `lib()`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libsrt_b200.so"
+
+# --------------------------------------------------------------------------- records
+
+
+class Vertex(C.Structure):
+    _fields_ = [("pos", C.c_float * 4), ("normal", C.c_float * 4)]
+
+
+class Material(C.Structure):
+    _fields_ = [("color", C.c_float * 4), ("extra", C.c_float * 4)]
+
+
+class Light(C.Structure):
+    _fields_ = [("v0", C.c_float * 4), ("v1", C.c_float * 4), ("v2", C.c_float * 4), ("params", C.c_float * 4)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("vertex_offset", C.c_uint32), ("index_offset", C.c_uint32), ("pad", C.c_uint32 * 2)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("mesh_id", C.c_uint32), ("mat_id", C.c_uint32), ("pad", C.c_uint32 * 2),
+                ("transform", C.c_float * 16)]
+
+
+class CameraUniform(C.Structure):
+    _fields_ = [("view_inverse", C.c_float * 16), ("proj_inverse", C.c_float * 16), ("view", C.c_float * 16),
+                ("proj", C.c_float * 16), ("frame_count", C.c_uint32), ("pad", C.c_uint32 * 3)]
+
+
+class Photon(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("wavelength", C.c_float), ("direction", C.c_float * 3),
+                ("energy", C.c_float)]
+
+
+class Ray(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("tmin", C.c_float), ("dir", C.c_float * 3), ("tmax", C.c_float)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("t", C.c_float), ("prim", C.c_uint32), ("u", C.c_float), ("v", C.c_float)]
+
+
+class Params(C.Structure):
+    _fields_ = [("max_depth", C.c_uint32), ("photons_per_frame", C.c_uint32), ("hash_bits", C.c_uint32),
+                ("photon_max_bounces", C.c_uint32), ("gather_cap", C.c_uint32), ("flags", C.c_uint32),
+                ("cell_size", C.c_float), ("gather_radius0", C.c_float), ("radius_exponent", C.c_float),
+                ("spectral_radius", C.c_float), ("photon_norm_count", C.c_float), ("block_size", C.c_uint32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("frames", C.c_uint64), ("paths", C.c_uint64), ("rays_closest", C.c_uint64),
+                ("rays_shadow", C.c_uint64), ("photons_emitted", C.c_uint64), ("photons_stored", C.c_uint64),
+                ("nodes_visited", C.c_uint64), ("tris_tested", C.c_uint64), ("ms_photon_trace", C.c_double),
+                ("ms_photon_grid", C.c_double), ("ms_trace_closest", C.c_double), ("ms_shade", C.c_double),
+                ("ms_trace_shadow", C.c_double), ("ms_finalize", C.c_double), ("ms_raygen", C.c_double),
+                ("launches_trace_closest", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+
+class SceneArrays(C.Structure):
+    _fields_ = [("vertices", C.POINTER(Vertex)), ("n_vertices", C.c_uint32),
+                ("indices", C.POINTER(C.c_uint32)), ("n_indices", C.c_uint32),
+                ("mesh_infos", C.POINTER(MeshInfo)), ("n_meshes", C.c_uint32),
+                ("materials", C.POINTER(Material)), ("n_materials", C.c_uint32),
+                ("instances", C.POINTER(Instance)), ("n_instances", C.c_uint32),
+                ("lights", C.POINTER(Light)), ("n_lights", C.c_uint32)]
+
+
+for _t, _n in ((Vertex, 32), (Material, 32), (Light, 64), (MeshInfo, 16), (Instance, 80), (CameraUniform, 272),
+               (Photon, 32), (Ray, 32), (Hit, 16), (Params, 48)):
+    assert C.sizeof(_t) == _n, (_t, C.sizeof(_t))
+
+FLAG_FP64_ACCUM = 0x1
+FLAG_NO_GRAPH = 0x2
+FLAG_STAGE_TIMING = 0x4
+FLAG_COUNT_VISITS = 0x8
+
+PRESET_CORNELL_BOX = 0
+PRESET_CUSTOM_PRISM = 1
+PRESET_CONFIG1 = 2
+PRESET_CONFIG2 = 3
+PRESET_CAUSTIC_SLAB = 4
+
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
+          7: "UNSUPPORTED"}
+
+# Every exported entry point with (restype, argtypes).
+_P = C.c_void_p
+_U32 = C.c_uint32
+_F = C.c_float
+_I = C.c_int
+SIGNATURES = {
+    "srt_abi_version": (_U32, []),
+    "srt_ctx_create": (_I, [_I, _P, C.POINTER(_P)]),
+    "srt_ctx_destroy": (_I, [_P]),
+    "srt_get_error_string": (C.c_char_p, [_P]),
+    "srt_ctx_stream": (_P, [_P]),
+    "srt_ctx_synchronize": (_I, [_P]),
+    "srt_ctx_sm_count": (_I, [_P]),
+    "srt_scene_builder_create": (_I, [C.POINTER(_P)]),
+    "srt_scene_builder_destroy": (_I, [_P]),
+    "srt_scene_builder_add_material": (_U32, [_P, C.POINTER(Material)]),
+    "srt_scene_builder_add_mesh": (_U32, [_P, C.POINTER(Vertex), _U32, C.POINTER(_U32), _U32]),
+    "srt_scene_builder_add_instance": (_I, [_P, _U32, _U32, C.POINTER(_F)]),
+    "srt_scene_builder_add_light_instance": (_I, [_P, _U32, _U32, C.POINTER(_F), C.POINTER(_F)]),
+    "srt_scene_builder_arrays": (_I, [_P, C.POINTER(SceneArrays)]),
+    "srt_scene_builder_build": (_I, [_P, _P, C.POINTER(_P)]),
+    "srt_scene_build": (_I, [_P, C.POINTER(SceneArrays), C.POINTER(_P)]),
+    "srt_scene_destroy": (_I, [_P]),
+    "srt_scene_info": (_I, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(_U32)]),
+    "srt_geometry_plane": (_I, [C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
+    "srt_geometry_cube": (_I, [C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
+    "srt_geometry_icosphere": (_I, [_U32, C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
+    "srt_geometry_uv_sphere": (_I, [_U32, _U32, C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32),
+                                    C.POINTER(_U32)]),
+    "srt_scene_builder_add_preset": (_I, [_P, _I, _U32, C.POINTER(_F)]),
+    "srt_camera_build_uniform": (_I, [C.POINTER(_F), _F, _F, _F, _U32, C.POINTER(CameraUniform)]),
+    "srt_params_default": (Params, []),
+    "srt_renderer_create": (_I, [_P, _P, _U32, _U32, C.POINTER(Params), C.POINTER(_P)]),
+    "srt_renderer_destroy": (_I, [_P]),
+    "srt_render_frame": (_I, [_P, C.POINTER(CameraUniform)]),
+    "srt_renderer_frame_count": (_U32, [_P]),
+    "srt_renderer_set_frame_count": (_I, [_P, _U32]),
+    "srt_reset_accumulation": (_I, [_P]),
+    "srt_read_accum_f32": (_I, [_P, _P]),
+    "srt_read_accum_f64": (_I, [_P, _P]),
+    "srt_read_ldr_rgba8": (_I, [_P, _P, _U32]),
+    "srt_save_screenshot": (_I, [_P, C.c_char_p]),
+    "srt_screenshot_write": (_I, [C.c_char_p, _P, _U32, _U32, _U32]),
+    "srt_renderer_get_stats": (_I, [_P, C.POINTER(Stats)]),
+    "srt_renderer_reset_stats": (_I, [_P]),
+    "srt_renderer_read_photons": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
+    "srt_trace_rays": (_I, [_P, _P, _U32, _P, _I]),
+    "srt_photon_grid_build": (_I, [_P, _P, _U32, _U32, _F, _U32, _P, _P]),
+    "srt_photon_gather": (_I, [_P, _P, _U32, _P, _U32, _U32, C.POINTER(Params), _P]),
+    "srt_test_device_math": (_I, [_P, _I, _U32, _P, _P, _P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"native library missing: {LIB_PATH} (run python -m wgpu_spectral_rt_b200.build)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class SrtError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _check(status: int, ctx=None):
+    if status != 0:
+        m = lib().srt_get_error_string(ctx)
+        raise SrtError(status, m.decode() if m else "")
+
+
+def ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def default_params(**kw) -> Params:
+    p = lib().srt_params_default()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def params_dict(p: Params) -> dict:
+    return {f: getattr(p, f) for f, _ in Params._fields_}
+
+
+# --------------------------------------------------------------------------- context
+
+
+class Context:
+    """WgpuContext replacement (src/wgpu_ctx.rs:3-82): one CUDA device + stream."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = C.c_void_p()
+        _check(lib().srt_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)), None)
+        self.h = h
+
+    @property
+    def stream(self) -> int:
+        return lib().srt_ctx_stream(self.h) or 0
+
+    @property
+    def sm_count(self) -> int:
+        return lib().srt_ctx_sm_count(self.h)
+
+    def synchronize(self):
+        _check(lib().srt_ctx_synchronize(self.h), self.h)
+
+    def close(self):
+        if self.h:
+            lib().srt_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- scene
+
+
+def _vertices(v) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(v, dtype=np.float32).reshape(-1, 8))
+    return a
+
+
+def geometry(kind: str, *args) -> tuple[np.ndarray, np.ndarray]:
+    """Procedural meshes (src/scene/geometry.rs): 'plane', 'cube', 'icosphere' (subdivisions),
+    'uv_sphere' (slices, stacks).  Returns (vertices float32 [n, 8], indices uint32)."""
+    fn = {"plane": lib().srt_geometry_plane, "cube": lib().srt_geometry_cube,
+          "icosphere": lib().srt_geometry_icosphere, "uv_sphere": lib().srt_geometry_uv_sphere}[kind]
+    nv, ni = C.c_uint32(0), C.c_uint32(0)
+    _check(fn(*args, None, C.byref(nv), None, C.byref(ni)))
+    v = np.zeros((nv.value, 8), np.float32)
+    i = np.zeros(ni.value, np.uint32)
+    _check(fn(*args, v.ctypes.data_as(C.POINTER(Vertex)), C.byref(nv), i.ctypes.data_as(C.POINTER(C.c_uint32)),
+              C.byref(ni)))
+    return v, i
+
+
+def material(color, extra) -> Material:
+    m = Material()
+    m.color[:] = [float(x) for x in color]
+    m.extra[:] = [float(x) for x in extra]
+    return m
+
+
+class SceneBuilder:
+    """SceneBuilder (src/scene/builder.rs:47-267) on the native host builder."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(lib().srt_scene_builder_create(C.byref(h)))
+        self.h = h
+
+    def add_material(self, color, extra) -> int:
+        m = color if isinstance(color, Material) else material(color, extra)
+        return int(lib().srt_scene_builder_add_material(self.h, C.byref(m)))
+
+    def add_mesh(self, vertices, indices) -> int:
+        v = _vertices(vertices)
+        i = np.ascontiguousarray(np.asarray(indices, np.uint32))
+        r = lib().srt_scene_builder_add_mesh(self.h, v.ctypes.data_as(C.POINTER(Vertex)), len(v),
+                                             i.ctypes.data_as(C.POINTER(C.c_uint32)), len(i))
+        if r == 0xFFFFFFFF:
+            raise SrtError(1, "invalid mesh")
+        return int(r)
+
+    def add_instance(self, mesh_id: int, mat_id: int, transform) -> None:
+        t = np.ascontiguousarray(np.asarray(transform, np.float32).reshape(4, 4).T.reshape(16))  # -> column-major
+        _check(lib().srt_scene_builder_add_instance(self.h, mesh_id, mat_id, t.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def add_light_instance(self, mesh_id: int, mat_id: int, transform, params) -> None:
+        t = np.ascontiguousarray(np.asarray(transform, np.float32).reshape(4, 4).T.reshape(16))
+        p = np.ascontiguousarray(np.asarray(params, np.float32).reshape(4))
+        _check(lib().srt_scene_builder_add_light_instance(self.h, mesh_id, mat_id, t.ctypes.data_as(C.POINTER(C.c_float)),
+                                                          p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def add_preset(self, preset: int, seed: int = 0) -> tuple[list[float], float, float]:
+        """Fills the builder with a preset scene; returns (camera position, yaw, pitch)."""
+        cam = (C.c_float * 5)()
+        _check(lib().srt_scene_builder_add_preset(self.h, preset, seed, cam))
+        return [cam[0], cam[1], cam[2]], cam[3], cam[4]
+
+    def arrays(self) -> SceneArrays:
+        a = SceneArrays()
+        _check(lib().srt_scene_builder_arrays(self.h, C.byref(a)))
+        return a
+
+    def build(self, ctx: Context) -> "Scene":
+        h = C.c_void_p()
+        _check(lib().srt_scene_builder_build(ctx.h, self.h, C.byref(h)), ctx.h)
+        return Scene(ctx, h)
+
+    def close(self):
+        if self.h:
+            lib().srt_scene_builder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """SceneResources (builder.rs:30-39): device buffers + the GPU-built BVH8."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx, self.h = ctx, h
+
+    def info(self) -> dict:
+        t, n, d = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(lib().srt_scene_info(self.h, C.byref(t), C.byref(n), C.byref(d)), self.ctx.h)
+        return {"triangles": t.value, "nodes": n.value, "depth": d.value}
+
+    def trace(self, rays: np.ndarray, any_hit: bool = False) -> np.ndarray:
+        """rays: float32 [n, 8] (origin, tmin, dir, tmax) -> hits structured (t, prim, u, v)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.zeros(len(r), dtype=[("t", np.float32), ("prim", np.uint32), ("u", np.float32), ("v", np.float32)])
+        _check(lib().srt_trace_rays(self.h, ptr(r), len(r), ptr(out), 1 if any_hit else 0), self.ctx.h)
+        return out
+
+    def close(self):
+        if self.h:
+            lib().srt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def camera_uniform(position, yaw: float, pitch: float, aspect: float, frame_count: int) -> CameraUniform:
+    """CameraController::build_uniform (src/scene/camera.rs:178-194)."""
+    u = CameraUniform()
+    p = (C.c_float * 3)(*[float(x) for x in position])
+    _check(lib().srt_camera_build_uniform(p, yaw, pitch, aspect, frame_count, C.byref(u)))
+    return u
+
+
+class CameraController:
+    """Camera state of src/scene/camera.rs:15-52 (keyboard handling left out)."""
+
+    def __init__(self, position=(0.0, 0.0, 3.0), yaw: float = -math.pi / 2, pitch: float = 0.0):
+        self.position = list(position)
+        self.yaw = yaw
+        self.pitch = pitch
+
+    def build_uniform(self, aspect: float, frame_count: int) -> CameraUniform:
+        return camera_uniform(self.position, self.yaw, self.pitch, aspect, frame_count)
+
+
+# --------------------------------------------------------------------------- renderer
+
+
+class Renderer:
+    """Renderer (src/renderer/mod.rs:21-208): per-frame photon pass, grid, wavefront camera paths."""
+
+    def __init__(self, ctx: Context, scene: Scene, width: int, height: int, params: Params | None = None):
+        self.ctx, self.scene = ctx, scene
+        self.target_width, self.target_height = int(width), int(height)
+        self.params = params if params is not None else default_params()
+        h = C.c_void_p()
+        _check(lib().srt_renderer_create(ctx.h, scene.h, width, height, C.byref(self.params), C.byref(h)), ctx.h)
+        self.h = h
+
+    @property
+    def frame_count(self) -> int:
+        return int(lib().srt_renderer_frame_count(self.h))
+
+    @frame_count.setter
+    def frame_count(self, v: int):
+        _check(lib().srt_renderer_set_frame_count(self.h, v), self.ctx.h)
+
+    def render(self, camera: CameraUniform) -> None:
+        _check(lib().srt_render_frame(self.h, C.byref(camera)), self.ctx.h)
+
+    def reset_accumulation(self):
+        _check(lib().srt_reset_accumulation(self.h), self.ctx.h)
+
+    def read_accum(self) -> np.ndarray:
+        out = np.zeros((self.target_height, self.target_width, 4), np.float32)
+        _check(lib().srt_read_accum_f32(self.h, ptr(out)), self.ctx.h)
+        return out
+
+    def read_accum64(self) -> np.ndarray:
+        out = np.zeros((self.target_height, self.target_width, 4), np.float64)
+        _check(lib().srt_read_accum_f64(self.h, ptr(out)), self.ctx.h)
+        return out
+
+    def read_ldr(self) -> np.ndarray:
+        out = np.zeros((self.target_height, self.target_width, 4), np.uint8)
+        _check(lib().srt_read_ldr_rgba8(self.h, ptr(out), 4 * self.target_width), self.ctx.h)
+        return out
+
+    def save_screenshot(self, path: str | os.PathLike):
+        _check(lib().srt_save_screenshot(self.h, str(path).encode()), self.ctx.h)
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().srt_renderer_get_stats(self.h, C.byref(s)), self.ctx.h)
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def reset_stats(self):
+        _check(lib().srt_renderer_reset_stats(self.h), self.ctx.h)
+
+    def read_photons(self) -> np.ndarray:
+        n = C.c_uint32()
+        _check(lib().srt_renderer_read_photons(self.h, None, 0, C.byref(n)), self.ctx.h)
+        out = np.zeros((n.value, 8), np.float32)
+        _check(lib().srt_renderer_read_photons(self.h, ptr(out), n.value, C.byref(n)), self.ctx.h)
+        return out
+
+    def close(self):
+        if self.h:
+            lib().srt_renderer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- standalone kernels
+
+
+def screenshot_write(path, rgba: np.ndarray) -> None:
+    """ScreenshotSaver (src/screenshot.rs:27-103): rgba uint8 [h, w, 4], row 0 = bottom."""
+    a = np.ascontiguousarray(rgba, np.uint8)
+    h, w = a.shape[:2]
+    _check(lib().srt_screenshot_write(str(path).encode(), ptr(a), w, h, 4 * w))
+
+
+def photon_grid_build(ctx: Context, photons: np.ndarray, frame: int, cell: float = 0.02, hash_bits: int = 22):
+    """Cell keys (sorted, u64) and ranges ([2^bits, 2] u32) for a photon set float32 [n, 8]."""
+    p = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+    keys = np.zeros(len(p), np.uint64)
+    ranges = np.zeros((1 << hash_bits, 2), np.uint32)
+    _check(lib().srt_photon_grid_build(ctx.h, ptr(p), len(p), frame, cell, hash_bits, ptr(keys), ptr(ranges)), ctx.h)
+    return keys, ranges
+
+
+def photon_gather(ctx: Context, photons: np.ndarray, queries: np.ndarray, frame: int, params: Params) -> np.ndarray:
+    p = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 10)
+    out = np.zeros((len(q), 4), np.float32)
+    _check(lib().srt_photon_gather(ctx.h, ptr(p), len(p), ptr(q), len(q), frame, C.byref(params), ptr(out)), ctx.h)
+    return out
+
+
+MATH_SIZES = {0: (4, 4), 1: (4, 12), 2: (8, 4), 3: (28, 16), 4: (36, 16), 5: (4, 20), 6: (96, 40), 7: (20, 4),
+              8: (20, 28)}
+
+
+def device_math(ctx: Context, op: int, inp: np.ndarray, aux: CameraUniform | None = None) -> np.ndarray:
+    """Runs one device unit kernel (srt_test_device_math); inp rows are op records."""
+    isz, osz = MATH_SIZES[op]
+    a = np.ascontiguousarray(inp)
+    n = a.nbytes // isz
+    out = np.zeros(n * osz // 4, np.uint32 if op in (0, 7) else np.float32)
+    _check(lib().srt_test_device_math(ctx.h, op, n, ptr(a), ptr(out), C.byref(aux) if aux is not None else None), ctx.h)
+    return out.reshape(n, osz // 4)

@@ -1,0 +1,99 @@
+"""Build script for the native library libsrt_b200.so (sm_100a).
+
+Compiles every CUDA source with nvcc for sm_100a (`-gencode
+arch=compute_100a,code=sm_100a -lineinfo`), the host C++ sources with g++,
+and links them into wgpu_spectral_rt_b200/libsrt_b200.so.  Objects go to
+wgpu_spectral_rt_b200/_build/.  Rebuilds only what changed (by mtime,
+headers included).
+
+Usage:  python -m wgpu_spectral_rt_b200.build [-v] [--force]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+INCLUDE = PKG.parent / "include"
+LIB = PKG / "libsrt_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+                     "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
+             f"-I{INCLUDE}", f"-I{CSRC}", "-I/usr/local/cuda/include"]
+
+
+def _nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _cxx() -> str:
+    # the system g++ (an exported CXX may point at a toolchain without the runtime libs)
+    return shutil.which("g++") or "g++"
+
+
+def _headers() -> list[Path]:
+    return list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+
+
+def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return src.stat().st_mtime > t or any(d.stat().st_mtime > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    deps = _headers()
+    jobs = []
+    for src in sorted(CSRC.glob("*.cu")):
+        obj = BUILD / (src.stem + ".o")
+        if force or _stale(obj, src, deps):
+            jobs.append([_nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+    for src in sorted(CSRC.glob("*.cpp")):
+        obj = BUILD / (src.stem + ".o")
+        if force or _stale(obj, src, deps):
+            jobs.append([_cxx(), *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
+        if verbose and (p.stdout or p.stderr):
+            print(p.stdout + p.stderr, flush=True)
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        list(ex.map(run, jobs))
+    objs = sorted(BUILD.glob("*.o"))
+    if jobs or force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        run([_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(a.verbose, a.force))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,502 @@
+// bvh_build.cu — GPU build of the compressed 8-wide BVH over the scene's
+// flattened world-space triangles.
+//
+// Replaces the driver's BLAS/TLAS build (src/scene/builder.rs:131-266).
+// Instances are flattened (their triangles transformed to world space) so a
+// single tree serves every ray; shading still uses the instance's object
+// space data.  Steps, all on the device:
+//   1. flatten: world-space triangle slots + per-triangle instance id
+//   2. centroid bounds and 30-bit Morton codes
+//   3. radix sort of (code, triangle) pairs
+//   4. binary radix tree over the sorted codes (Karras, HPG 2012)
+//   5. bottom-up bounding boxes (one thread per leaf, atomic visit flags)
+//   6. collapse into 8-wide nodes, level by level: expand the child of
+//      largest surface area until 8 children; subtrees of <= 3 triangles
+//      become leaves; children are placed in slots by ray octant; child
+//      boxes are quantised to 8 bits against the node's box.
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "radix_sort.cuh"
+
+namespace srt {
+
+namespace {
+
+constexpr uint32_t LEAF = 0x80000000u;
+
+__device__ __forceinline__ uint32_t float_flip(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float float_unflip(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+__global__ void k_flatten(const float4* __restrict__ vtx, const uint32_t* __restrict__ indices,
+                          const uint4* __restrict__ mesh_infos, const InstDev* __restrict__ inst,
+                          const InstFwd* __restrict__ fwd, uint32_t n_inst, uint32_t n_tris,
+                          TriSlot* __restrict__ flat, uint32_t* __restrict__ tri_inst, float4* __restrict__ cen,
+                          uint32_t* __restrict__ bounds /* 6 flipped: min xyz, max xyz */) {
+    __shared__ uint32_t sb[6];
+    if (threadIdx.x < 3) sb[threadIdx.x] = 0xFFFFFFFFu;
+    else if (threadIdx.x < 6) sb[threadIdx.x] = 0u;
+    __syncthreads();
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_tris) {
+        uint32_t lo = 0, hi = n_inst;  // last instance with tri_offset <= t
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (inst[mid].tri_offset <= t) lo = mid;
+            else hi = mid;
+        }
+        const InstDev& in = inst[lo];
+        InstFwd f = fwd[lo];
+        uint4 mi = mesh_infos[in.mesh_id];
+        uint32_t io = mi.y + (t - in.tri_offset) * 3u;
+        float3 w[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float4 p = vtx[2 * (indices[io + k] + mi.x)];
+            w[k] = f3(f.r0.x * p.x + f.r0.y * p.y + f.r0.z * p.z + f.r0.w,
+                      f.r1.x * p.x + f.r1.y * p.y + f.r1.z * p.z + f.r1.w,
+                      f.r2.x * p.x + f.r2.y * p.y + f.r2.z * p.z + f.r2.w);
+        }
+        TriSlot s;
+        s.v0 = make_float4(w[0].x, w[0].y, w[0].z, __uint_as_float(t));
+        s.v1 = make_float4(w[1].x, w[1].y, w[1].z, 0.f);
+        s.v2 = make_float4(w[2].x, w[2].y, w[2].z, 0.f);
+        flat[t] = s;
+        tri_inst[t] = lo;
+        float3 c = (w[0] + w[1] + w[2]) * (1.0f / 3.0f);
+        cen[t] = make_float4(c.x, c.y, c.z, 0.f);
+        atomicMin(&sb[0], float_flip(c.x));
+        atomicMin(&sb[1], float_flip(c.y));
+        atomicMin(&sb[2], float_flip(c.z));
+        atomicMax(&sb[3], float_flip(c.x));
+        atomicMax(&sb[4], float_flip(c.y));
+        atomicMax(&sb[5], float_flip(c.z));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&bounds[threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&bounds[threadIdx.x], sb[threadIdx.x]);
+}
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__global__ void k_morton(const float4* __restrict__ cen, const uint32_t* __restrict__ bounds, uint32_t n,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    float3 lo = f3(float_unflip(bounds[0]), float_unflip(bounds[1]), float_unflip(bounds[2]));
+    float3 hi = f3(float_unflip(bounds[3]), float_unflip(bounds[4]), float_unflip(bounds[5]));
+    float4 c = cen[t];
+    float ex = fmaxf(hi.x - lo.x, 1e-30f), ey = fmaxf(hi.y - lo.y, 1e-30f), ez = fmaxf(hi.z - lo.z, 1e-30f);
+    uint32_t x = (uint32_t)fminf(fmaxf((c.x - lo.x) / ex * 1024.0f, 0.0f), 1023.0f);
+    uint32_t y = (uint32_t)fminf(fmaxf((c.y - lo.y) / ey * 1024.0f, 0.0f), 1023.0f);
+    uint32_t z = (uint32_t)fminf(fmaxf((c.z - lo.z) / ez * 1024.0f, 0.0f), 1023.0f);
+    keys[t] = (expand_bits(x) << 2) | (expand_bits(y) << 1) | expand_bits(z);
+    vals[t] = t;
+}
+
+// delta(i, j): common prefix length of (key, index) pairs; -1 out of range.
+__device__ __forceinline__ int delta(const uint32_t* keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = keys[i], b = keys[j];
+    if (a == b) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+    return __clz(a ^ b);
+}
+
+struct Bvh2 {
+    uint4* inode;      // internal: left ref, right ref, first, last
+    float4* ibox;      // internal: lo, hi (2 per node)
+    float4* lbox;      // leaf: lo, hi
+    uint32_t* iparent; // parent of internal node
+    uint32_t* lparent; // parent of leaf
+    uint32_t* flags;   // refit visit counters
+};
+
+__global__ void k_karras(const uint32_t* __restrict__ keys, int n, Bvh2 b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int len = l;
+    for (int t = (len + 1) >> 1;; t = (t + 1) >> 1) {
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    uint32_t left = (first == gamma) ? (LEAF | (uint32_t)gamma) : (uint32_t)gamma;
+    uint32_t right = (last == gamma + 1) ? (LEAF | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
+    b.inode[i] = make_uint4(left, right, (uint32_t)first, (uint32_t)last);
+    if (left & LEAF) b.lparent[left & ~LEAF] = (uint32_t)i;
+    else b.iparent[left] = (uint32_t)i;
+    if (right & LEAF) b.lparent[right & ~LEAF] = (uint32_t)i;
+    else b.iparent[right] = (uint32_t)i;
+}
+
+__global__ void k_refit(const TriSlot* __restrict__ flat, const uint32_t* __restrict__ sorted_tri, int n, Bvh2 b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    TriSlot s = flat[sorted_tri[i]];
+    float3 lo = f3(fminf(fminf(s.v0.x, s.v1.x), s.v2.x), fminf(fminf(s.v0.y, s.v1.y), s.v2.y),
+                   fminf(fminf(s.v0.z, s.v1.z), s.v2.z));
+    float3 hi = f3(fmaxf(fmaxf(s.v0.x, s.v1.x), s.v2.x), fmaxf(fmaxf(s.v0.y, s.v1.y), s.v2.y),
+                   fmaxf(fmaxf(s.v0.z, s.v1.z), s.v2.z));
+    b.lbox[2 * i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    b.lbox[2 * i + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    if (n == 1) return;
+    uint32_t node = b.lparent[i];
+    while (true) {
+        __threadfence();
+        if (atomicAdd(&b.flags[node], 1u) == 0u) return;  // the sibling finishes this node
+        __threadfence();
+        uint4 nd = b.inode[node];
+        float4 a0, a1, c0, c1;
+        if (nd.x & LEAF) {
+            a0 = __ldcg(&b.lbox[2 * (nd.x & ~LEAF)]);
+            a1 = __ldcg(&b.lbox[2 * (nd.x & ~LEAF) + 1]);
+        } else {
+            a0 = __ldcg(&b.ibox[2 * nd.x]);
+            a1 = __ldcg(&b.ibox[2 * nd.x + 1]);
+        }
+        if (nd.y & LEAF) {
+            c0 = __ldcg(&b.lbox[2 * (nd.y & ~LEAF)]);
+            c1 = __ldcg(&b.lbox[2 * (nd.y & ~LEAF) + 1]);
+        } else {
+            c0 = __ldcg(&b.ibox[2 * nd.y]);
+            c1 = __ldcg(&b.ibox[2 * nd.y + 1]);
+        }
+        b.ibox[2 * node] = make_float4(fminf(a0.x, c0.x), fminf(a0.y, c0.y), fminf(a0.z, c0.z), 0.f);
+        b.ibox[2 * node + 1] = make_float4(fmaxf(a1.x, c1.x), fmaxf(a1.y, c1.y), fmaxf(a1.z, c1.z), 0.f);
+        if (node == 0u) return;
+        node = b.iparent[node];
+    }
+}
+
+__device__ __forceinline__ void ref_box(const Bvh2& b, uint32_t r, float3& lo, float3& hi) {
+    float4 a, c;
+    if (r & LEAF) {
+        a = b.lbox[2 * (r & ~LEAF)];
+        c = b.lbox[2 * (r & ~LEAF) + 1];
+    } else {
+        a = b.ibox[2 * r];
+        c = b.ibox[2 * r + 1];
+    }
+    lo = xyz(a);
+    hi = xyz(c);
+}
+__device__ __forceinline__ void ref_range(const Bvh2& b, uint32_t r, uint32_t& first, uint32_t& count) {
+    if (r & LEAF) {
+        first = r & ~LEAF;
+        count = 1;
+    } else {
+        uint4 nd = b.inode[r];
+        first = nd.z;
+        count = nd.w - nd.z + 1;
+    }
+}
+
+// One thread per 8-wide node of this level: queue entries (bvh2 ref, node).
+__global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in, uint2* __restrict__ qout,
+                           uint32_t* __restrict__ n_out, Node8* __restrict__ nodes, uint32_t* __restrict__ node_alloc,
+                           uint32_t node_cap, TriSlot* __restrict__ tris_out, uint32_t* __restrict__ tri_alloc,
+                           uint32_t tri_cap, const TriSlot* __restrict__ flat, const uint32_t* __restrict__ sorted_tri,
+                           uint32_t* __restrict__ err) {
+    uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_in) return;
+    uint2 q = qin[e];
+    uint32_t refs[8];
+    int nc;
+    if (q.x & LEAF) {
+        refs[0] = q.x;
+        nc = 1;
+    } else {
+        uint4 nd = b.inode[q.x];
+        refs[0] = nd.x;
+        refs[1] = nd.y;
+        nc = 2;
+    }
+    while (nc < 8) {
+        int best = -1;
+        float best_area = -1.0f;
+        for (int c = 0; c < nc; ++c) {
+            if (refs[c] & LEAF) continue;
+            float3 lo, hi;
+            ref_box(b, refs[c], lo, hi);
+            float3 ext = hi - lo;
+            float area = ext.x * ext.y + ext.y * ext.z + ext.z * ext.x;
+            if (area > best_area) {
+                best_area = area;
+                best = c;
+            }
+        }
+        if (best < 0) break;
+        uint4 nd = b.inode[refs[best]];
+        refs[best] = nd.x;
+        refs[nc++] = nd.y;
+    }
+    // children boxes, counts and node box
+    float3 clo[8], chi[8];
+    uint32_t cfirst[8], ccount[8];
+    float3 nlo = f3(3.4e38f, 3.4e38f, 3.4e38f), nhi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+    uint32_t n_int = 0, n_tri = 0;
+    for (int c = 0; c < nc; ++c) {
+        ref_box(b, refs[c], clo[c], chi[c]);
+        ref_range(b, refs[c], cfirst[c], ccount[c]);
+        nlo = f3(fminf(nlo.x, clo[c].x), fminf(nlo.y, clo[c].y), fminf(nlo.z, clo[c].z));
+        nhi = f3(fmaxf(nhi.x, chi[c].x), fmaxf(nhi.y, chi[c].y), fmaxf(nhi.z, chi[c].z));
+        if (ccount[c] <= 3u) n_tri += ccount[c];
+        else ++n_int;
+    }
+    uint32_t child_base = n_int ? atomicAdd(node_alloc, n_int) : 0u;
+    uint32_t tri_base = n_tri ? atomicAdd(tri_alloc, n_tri) : 0u;
+    if (child_base + n_int > node_cap || tri_base + n_tri > tri_cap) {
+        atomicOr(err, ERR_QUEUE_OVERFLOW);
+        return;
+    }
+    // slot assignment: slot s is visited first by rays whose octant is s
+    // (bit set = negative direction), which want the child lying farthest
+    // along +x/+y/+z for set bits; greedy on the best (child, slot) score.
+    float3 pc = (nlo + nhi) * 0.5f;
+    int slot_of[8];
+    int child_in[8];
+    for (int s = 0; s < 8; ++s) child_in[s] = -1;
+    for (int c = 0; c < nc; ++c) slot_of[c] = -1;
+    for (int it = 0; it < nc; ++it) {
+        float bs = -3.4e38f;
+        int bc = -1, bsl = -1;
+        for (int c = 0; c < nc; ++c) {
+            if (slot_of[c] >= 0) continue;
+            float3 d = (clo[c] + chi[c]) * 0.5f - pc;
+            for (int s = 0; s < 8; ++s) {
+                if (child_in[s] >= 0) continue;
+                float sc = ((s & 1) ? d.x : -d.x) + ((s & 2) ? d.y : -d.y) + ((s & 4) ? d.z : -d.z);
+                if (sc > bs) {
+                    bs = sc;
+                    bc = c;
+                    bsl = s;
+                }
+            }
+        }
+        slot_of[bc] = bsl;
+        child_in[bsl] = bc;
+    }
+    // quantisation frame
+    uint32_t ebyte[3];
+    float scale[3];
+    float nlov[3] = {nlo.x, nlo.y, nlo.z}, nhiv[3] = {nhi.x, nhi.y, nhi.z};
+    for (int a = 0; a < 3; ++a) {
+        double ext = (double)nhiv[a] - (double)nlov[a];
+        int ex = -126;
+        if (ext > 0.0) {
+            ex = (int)ceil(log2(ext / 255.0));
+            if (ldexp(255.0, ex) < ext) ++ex;
+            ex = max(ex, -126);
+            ex = min(ex, 127);
+        }
+        ebyte[a] = (uint32_t)(ex + 127);
+        scale[a] = __uint_as_float(ebyte[a] << 23);
+    }
+    uint32_t meta[2] = {0u, 0u}, qlo[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}}, qhi[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}};
+    uint32_t imask = 0u, int_rank = 0u, tri_off = 0u;
+    for (int s = 0; s < 8; ++s) {
+        int c = child_in[s];
+        if (c < 0) continue;
+        float lo3[3] = {clo[c].x, clo[c].y, clo[c].z}, hi3[3] = {chi[c].x, chi[c].y, chi[c].z};
+        for (int a = 0; a < 3; ++a) {
+            double sc = (double)scale[a];
+            int ql = (int)floor(((double)lo3[a] - (double)nlov[a]) / sc);
+            int qh = (int)ceil(((double)hi3[a] - (double)nlov[a]) / sc);
+            ql = min(max(ql, 0), 255);
+            qh = min(max(qh, 0), 255);
+            while (ql > 0 && nlov[a] + (float)ql * scale[a] > lo3[a]) --ql;
+            while (qh < 255 && nlov[a] + (float)qh * scale[a] < hi3[a]) ++qh;
+            qlo[a][s >> 2] |= (uint32_t)ql << (8 * (s & 3));
+            qhi[a][s >> 2] |= (uint32_t)qh << (8 * (s & 3));
+        }
+        uint32_t m;
+        if (ccount[c] <= 3u) {
+            m = (ccount[c] << 5) | tri_off;
+            for (uint32_t k = 0; k < ccount[c]; ++k) tris_out[tri_base + tri_off + k] = flat[sorted_tri[cfirst[c] + k]];
+            tri_off += ccount[c];
+        } else {
+            m = 7u << 5;
+            imask |= 1u << s;
+            uint32_t slot = atomicAdd(n_out, 1u);
+            qout[slot] = make_uint2(refs[c], child_base + int_rank);
+            ++int_rank;
+        }
+        meta[s >> 2] |= m << (8 * (s & 3));
+    }
+    Node8 nd;
+    nd.a = make_uint4(__float_as_uint(nlo.x), __float_as_uint(nlo.y), __float_as_uint(nlo.z),
+                      ebyte[0] | (ebyte[1] << 8) | (ebyte[2] << 16) | (imask << 24));
+    nd.b = make_uint4(child_base, tri_base, meta[0], meta[1]);
+    nd.c = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
+    nd.d = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
+    nd.e = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
+    nodes[q.y] = nd;
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+}  // namespace
+
+cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, std::string* msg) {
+    uint32_t n = in.n_tris;
+    out->nodes = nullptr;
+    out->tris = nullptr;
+    out->tri_inst = nullptr;
+    out->n_nodes = 0;
+    out->depth = 0;
+    out->kernel_launches = 0;
+    cudaError_t e = cudaSuccess;
+#define CK(x)                                         \
+    do {                                              \
+        e = (x);                                      \
+        if (e != cudaSuccess) {                       \
+            if (msg) *msg = std::string(#x) + ": " + cudaGetErrorString(e); \
+            goto done;                                \
+        }                                             \
+    } while (0)
+    TriSlot* flat = nullptr;
+    float4* cen = nullptr;
+    uint32_t *bounds = nullptr, *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr,
+             *scratch = nullptr, *counters = nullptr, *err = nullptr;
+    uint2 *qa = nullptr, *qb = nullptr;
+    Bvh2 b{};
+    if (n == 0) return cudaSuccess;
+    {
+        CK(dalloc(&out->tri_inst, n));
+        CK(dalloc(&out->tris, n));
+        uint32_t node_cap = n > 1 ? n - 1 : 1;
+        CK(dalloc(&out->nodes, node_cap));
+        CK(dalloc(&flat, n));
+        CK(dalloc(&cen, n));
+        CK(dalloc(&bounds, 6));
+        CK(dalloc(&keys, n));
+        CK(dalloc(&vals, n));
+        CK(dalloc(&keys2, n));
+        CK(dalloc(&vals2, n));
+        CK(dalloc(&scratch, radix_scratch_words(n)));
+        CK(dalloc(&counters, 4));
+        CK(dalloc(&err, 1));
+        CK(dalloc(&qa, node_cap));
+        CK(dalloc(&qb, node_cap));
+        CK(dalloc(&b.inode, node_cap));
+        CK(dalloc(&b.ibox, 2 * (size_t)node_cap));
+        CK(dalloc(&b.lbox, 2 * (size_t)n));
+        CK(dalloc(&b.iparent, node_cap));
+        CK(dalloc(&b.lparent, n));
+        CK(dalloc(&b.flags, node_cap));
+        uint32_t init_bounds[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+        CK(cudaMemcpyAsync(bounds, init_bounds, sizeof(init_bounds), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t) * node_cap, st));
+        CK(cudaMemsetAsync(err, 0, 4, st));
+        const int B = 256;
+        uint32_t grid = (n + B - 1) / B;
+        k_flatten<<<grid, B, 0, st>>>(in.vtx, in.indices, in.mesh_infos, in.inst, in.fwd, in.n_inst, n, flat,
+                                      out->tri_inst, cen, bounds);
+        k_morton<<<grid, B, 0, st>>>(cen, bounds, n, keys, vals);
+        out->kernel_launches += 2;
+        uint32_t *sk, *sv;
+        out->kernel_launches += sort_pairs(keys, vals, keys2, vals2, n, nullptr, 0, 30, scratch, st, &sk, &sv);
+        if (n > 1) {
+            k_karras<<<(n - 1 + B - 1) / B, B, 0, st>>>(sk, (int)n, b);
+            ++out->kernel_launches;
+        }
+        k_refit<<<grid, B, 0, st>>>(flat, sv, (int)n, b);
+        ++out->kernel_launches;
+        CK(cudaGetLastError());
+        // collapse, level by level; node 0 is the root
+        uint2 root = make_uint2(n > 1 ? 0u : LEAF, 0u);
+        uint32_t init_counts[4] = {1u, 0u, 0u, 0u};  // node alloc, tri alloc, queue out count, pad
+        CK(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(counters, init_counts, sizeof(init_counts), cudaMemcpyHostToDevice, st));
+        uint32_t n_in = 1;
+        uint32_t depth = 0;
+        while (n_in > 0) {
+            CK(cudaMemsetAsync(counters + 2, 0, 4, st));
+            k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(b, qa, n_in, qb, counters + 2, out->nodes, counters,
+                                                           node_cap, out->tris, counters + 1, n, flat, sv, err);
+            ++out->kernel_launches;
+            ++depth;
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(&n_in, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            uint2* t = qa;
+            qa = qb;
+            qb = t;
+            if (depth > 64) {
+                if (msg) *msg = "BVH8 collapse exceeded 64 levels";
+                e = cudaErrorUnknown;
+                goto done;
+            }
+        }
+        uint32_t hc[4], herr = 0;
+        CK(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr != 0u || hc[1] != n) {
+            if (msg) *msg = "BVH8 collapse produced an inconsistent tree";
+            e = cudaErrorUnknown;
+            goto done;
+        }
+        out->n_nodes = hc[0];
+        out->depth = depth;
+    }
+done:
+    cudaFree(flat);
+    cudaFree(cen);
+    cudaFree(bounds);
+    cudaFree(keys);
+    cudaFree(vals);
+    cudaFree(keys2);
+    cudaFree(vals2);
+    cudaFree(scratch);
+    cudaFree(counters);
+    cudaFree(err);
+    cudaFree(qa);
+    cudaFree(qb);
+    cudaFree(b.inode);
+    cudaFree(b.ibox);
+    cudaFree(b.lbox);
+    cudaFree(b.iparent);
+    cudaFree(b.lparent);
+    cudaFree(b.flags);
+    if (e != cudaSuccess) {
+        cudaFree(out->nodes);
+        cudaFree(out->tris);
+        cudaFree(out->tri_inst);
+        out->nodes = nullptr;
+        out->tris = nullptr;
+        out->tri_inst = nullptr;
+    }
+#undef CK
+    return e;
+}
+
+}  // namespace srt

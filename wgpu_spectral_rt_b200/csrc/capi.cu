@@ -1,0 +1,912 @@
+// capi.cu — implementation of the C ABI declared in include/srt.h.
+//
+// Host side of the path: the CUDA context that replaces WgpuContext
+// (src/wgpu_ctx.rs), scene upload + GPU BVH build that replace
+// SceneBuilder::build (src/scene/builder.rs:131-266), and the renderer that
+// replaces Renderer::new / render (src/renderer/mod.rs:45-207) and the
+// engine's screenshot readback (src/engine.rs:191-244).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "host_scene.h"
+#include "radix_sort.cuh"
+#include "render_kernels.h"
+
+using namespace srt;
+
+namespace {
+std::string g_last_create_error;
+
+bool env_fault(const char* what) {
+    // Host-side fault injection for the error paths: SRT_FAULT=alloc|launch
+    const char* f = std::getenv("SRT_FAULT");
+    return f && std::strcmp(f, what) == 0;
+}
+}  // namespace
+
+struct srt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 0;
+    std::string err;
+    uint32_t* d_err = nullptr;  // device error word for batch entry points
+};
+
+namespace {
+
+srt_status fail(srt_ctx* c, srt_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+srt_status cuda_fail(srt_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(ctx, expr)                                \
+    do {                                                   \
+        cudaError_t _e = (expr);                           \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #expr); \
+    } while (0)
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t count) {
+    if (env_fault("alloc")) return cudaErrorMemoryAllocation;
+    return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+// Reads and clears a device error word.
+srt_status check_device_error(srt_ctx* c, uint32_t* d_err) {
+    uint32_t h = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&h, d_err, 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (h != 0u) {
+        CUDA_TRY(c, cudaMemsetAsync(d_err, 0, 4, c->stream));
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "device check failed (error word 0x%x)", h);
+        return fail(c, SRT_ERR_DEVICE_ASSERT, buf);
+    }
+    return SRT_OK;
+}
+
+}  // namespace
+
+// ====================================================================== context
+extern "C" {
+
+uint32_t srt_abi_version(void) { return SRT_ABI_VERSION; }
+
+srt_status srt_ctx_create(int device, void* stream, srt_ctx** out) {
+    if (!out) return SRT_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        g_last_create_error = "no CUDA device";
+        return SRT_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) {
+        g_last_create_error = "device index out of range";
+        return SRT_ERR_INVALID_ARG;
+    }
+    std::unique_ptr<srt_ctx> c(new (std::nothrow) srt_ctx());
+    if (!c) return SRT_ERR_OOM;
+    c->device = device;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) {
+        g_last_create_error = cudaGetErrorString(e);
+        return SRT_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+            g_last_create_error = cudaGetErrorString(e);
+            return SRT_ERR_CUDA;
+        }
+        c->own_stream = true;
+    }
+    if ((e = dev_alloc(&c->d_err, 1)) != cudaSuccess || (e = cudaMemset(c->d_err, 0, 4)) != cudaSuccess) {
+        g_last_create_error = cudaGetErrorString(e);
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        return e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA;
+    }
+    *out = c.release();
+    return SRT_OK;
+}
+
+srt_status srt_ctx_destroy(srt_ctx* c) {
+    if (!c) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_err);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SRT_OK;
+}
+
+const char* srt_get_error_string(const srt_ctx* c) { return c ? c->err.c_str() : g_last_create_error.c_str(); }
+void* srt_ctx_stream(srt_ctx* c) { return c ? (void*)c->stream : nullptr; }
+int srt_ctx_sm_count(const srt_ctx* c) { return c ? c->sm_count : 0; }
+
+srt_status srt_ctx_synchronize(srt_ctx* c) {
+    if (!c) return SRT_ERR_INVALID_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, cudaGetLastError());
+    return SRT_OK;
+}
+
+// ====================================================================== scene builder (host)
+srt_status srt_scene_builder_create(srt_scene_builder** out) {
+    if (!out) return SRT_ERR_INVALID_ARG;
+    *out = new (std::nothrow) srt_scene_builder();
+    return *out ? SRT_OK : SRT_ERR_OOM;
+}
+srt_status srt_scene_builder_destroy(srt_scene_builder* b) {
+    delete b;
+    return SRT_OK;
+}
+uint32_t srt_scene_builder_add_material(srt_scene_builder* b, const srt_material* m) {
+    return (b && m) ? b->add_material(*m) : 0xFFFFFFFFu;
+}
+uint32_t srt_scene_builder_add_mesh(srt_scene_builder* b, const srt_vertex* v, uint32_t nv, const uint32_t* idx,
+                                    uint32_t ni) {
+    if (!b || (!v && nv) || (!idx && ni) || ni % 3u) return 0xFFFFFFFFu;
+    for (uint32_t i = 0; i < ni; ++i)
+        if (idx[i] >= nv) return 0xFFFFFFFFu;
+    return b->add_mesh(v, nv, idx, ni);
+}
+srt_status srt_scene_builder_add_instance(srt_scene_builder* b, uint32_t mesh, uint32_t mat, const float t[16]) {
+    if (!b || !t || mesh >= b->mesh_infos.size()) return SRT_ERR_INVALID_ARG;
+    Mat4 m;
+    std::memcpy(m.m, t, 64);
+    b->add_instance(mesh, mat, m);
+    return SRT_OK;
+}
+srt_status srt_scene_builder_add_light_instance(srt_scene_builder* b, uint32_t mesh, uint32_t mat, const float t[16],
+                                                const float params[4]) {
+    if (!b || !t || !params || mesh >= b->mesh_infos.size()) return SRT_ERR_INVALID_ARG;
+    Mat4 m;
+    std::memcpy(m.m, t, 64);
+    b->add_light_instance(mesh, mat, m, params);
+    return SRT_OK;
+}
+srt_status srt_scene_builder_arrays(const srt_scene_builder* b, srt_scene_arrays* o) {
+    if (!b || !o) return SRT_ERR_INVALID_ARG;
+    o->vertices = b->vertices.data();
+    o->n_vertices = (uint32_t)b->vertices.size();
+    o->indices = b->indices.data();
+    o->n_indices = (uint32_t)b->indices.size();
+    o->mesh_infos = b->mesh_infos.data();
+    o->n_meshes = (uint32_t)b->mesh_infos.size();
+    o->materials = b->materials.data();
+    o->n_materials = (uint32_t)b->materials.size();
+    o->instances = b->instances.data();
+    o->n_instances = (uint32_t)b->instances.size();
+    o->lights = b->lights.data();
+    o->n_lights = (uint32_t)b->lights.size();
+    return SRT_OK;
+}
+srt_status srt_scene_builder_add_preset(srt_scene_builder* b, int preset, uint32_t seed, float camera_out[5]) {
+    if (!b) return SRT_ERR_INVALID_ARG;
+    float cam[5];
+    if (!preset_fill(b, preset, seed, cam)) return SRT_ERR_INVALID_ARG;
+    if (camera_out) std::memcpy(camera_out, cam, sizeof cam);
+    return SRT_OK;
+}
+
+static srt_status geom_out(const std::vector<srt_vertex>& v, const std::vector<uint32_t>& i, srt_vertex* vo,
+                           uint32_t* nv, uint32_t* io, uint32_t* ni) {
+    if (!nv || !ni) return SRT_ERR_INVALID_ARG;
+    if (vo) {
+        if (*nv < v.size()) return SRT_ERR_INVALID_ARG;
+        std::memcpy(vo, v.data(), v.size() * sizeof(srt_vertex));
+    }
+    if (io) {
+        if (*ni < i.size()) return SRT_ERR_INVALID_ARG;
+        std::memcpy(io, i.data(), i.size() * 4);
+    }
+    *nv = (uint32_t)v.size();
+    *ni = (uint32_t)i.size();
+    return SRT_OK;
+}
+srt_status srt_geometry_plane(srt_vertex* v, uint32_t* nv, uint32_t* i, uint32_t* ni) {
+    std::vector<srt_vertex> vv;
+    std::vector<uint32_t> ii;
+    geom_plane(vv, ii);
+    return geom_out(vv, ii, v, nv, i, ni);
+}
+srt_status srt_geometry_cube(srt_vertex* v, uint32_t* nv, uint32_t* i, uint32_t* ni) {
+    std::vector<srt_vertex> vv;
+    std::vector<uint32_t> ii;
+    geom_cube(vv, ii);
+    return geom_out(vv, ii, v, nv, i, ni);
+}
+srt_status srt_geometry_icosphere(uint32_t sub, srt_vertex* v, uint32_t* nv, uint32_t* i, uint32_t* ni) {
+    if (sub > 10) return SRT_ERR_INVALID_ARG;
+    std::vector<srt_vertex> vv;
+    std::vector<uint32_t> ii;
+    geom_icosphere(sub, vv, ii);
+    return geom_out(vv, ii, v, nv, i, ni);
+}
+srt_status srt_geometry_uv_sphere(uint32_t slices, uint32_t stacks, srt_vertex* v, uint32_t* nv, uint32_t* i,
+                                  uint32_t* ni) {
+    if (slices < 3 || stacks < 2 || slices > 4096 || stacks > 4096) return SRT_ERR_INVALID_ARG;
+    std::vector<srt_vertex> vv;
+    std::vector<uint32_t> ii;
+    geom_uv_sphere(slices, stacks, vv, ii);
+    return geom_out(vv, ii, v, nv, i, ni);
+}
+
+srt_status srt_camera_build_uniform(const float position[3], float yaw, float pitch, float aspect, uint32_t frame,
+                                    srt_camera_uniform* out) {
+    if (!position || !out || !(aspect > 0.0f)) return SRT_ERR_INVALID_ARG;
+    camera_build_uniform(position, yaw, pitch, aspect, frame, out);
+    return SRT_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== scene (device)
+struct srt_scene {
+    srt_ctx* ctx = nullptr;
+    float4* vtx = nullptr;
+    uint32_t* idx = nullptr;
+    uint4* mesh_infos = nullptr;
+    float4* materials = nullptr;
+    float4* lights = nullptr;
+    InstDev* inst = nullptr;
+    InstFwd* fwd = nullptr;
+    BvhOutputs bvh{};
+    DevScene dev{};
+    uint64_t n_tris = 0;
+    uint32_t n_lights = 0;
+    ~srt_scene() {
+        cudaFree(vtx);
+        cudaFree(idx);
+        cudaFree(mesh_infos);
+        cudaFree(materials);
+        cudaFree(lights);
+        cudaFree(inst);
+        cudaFree(fwd);
+        cudaFree(bvh.nodes);
+        cudaFree(bvh.tris);
+        cudaFree(bvh.tri_inst);
+    }
+};
+
+namespace {
+template <typename T>
+cudaError_t upload(T** dst, const void* src, size_t bytes, size_t alloc_bytes, cudaStream_t st) {
+    cudaError_t e = dev_alloc((char**)dst, alloc_bytes ? alloc_bytes : 16);
+    if (e != cudaSuccess) return e;
+    if (bytes) e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st);
+    return e;
+}
+}  // namespace
+
+extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt_scene** out) {
+    if (!c || !a || !out) return SRT_ERR_INVALID_ARG;
+    *out = nullptr;
+    cudaSetDevice(c->device);
+    // ---- validation on the host: every device index is checked here
+    if ((a->n_vertices && !a->vertices) || (a->n_indices && !a->indices) || (a->n_meshes && !a->mesh_infos) ||
+        (a->n_materials && !a->materials) || (a->n_instances && !a->instances) || (a->n_lights && !a->lights))
+        return fail(c, SRT_ERR_INVALID_ARG, "null array with nonzero count");
+    std::vector<uint32_t> mesh_tris(a->n_meshes);
+    for (uint32_t m = 0; m < a->n_meshes; ++m) {
+        uint32_t io = a->mesh_infos[m].index_offset;
+        uint32_t end = m + 1 < a->n_meshes ? a->mesh_infos[m + 1].index_offset : a->n_indices;
+        if (io > end || end > a->n_indices || (end - io) % 3u)
+            return fail(c, SRT_ERR_INVALID_ARG, "mesh index ranges must be consecutive multiples of 3");
+        mesh_tris[m] = (end - io) / 3u;
+        uint32_t vend = m + 1 < a->n_meshes ? a->mesh_infos[m + 1].vertex_offset : a->n_vertices;
+        uint32_t vo = a->mesh_infos[m].vertex_offset;
+        for (uint32_t i = io; i < end; ++i)
+            if ((uint64_t)a->indices[i] + vo >= a->n_vertices || a->indices[i] + vo >= vend)
+                return fail(c, SRT_ERR_INVALID_ARG, "vertex index out of range");
+    }
+    std::vector<InstDev> inst(a->n_instances);
+    std::vector<InstFwd> fwd(a->n_instances);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < a->n_instances; ++i) {
+        const srt_instance& in = a->instances[i];
+        if (in.mesh_id >= a->n_meshes || in.mat_id >= a->n_materials)
+            return fail(c, SRT_ERR_INVALID_ARG, "instance mesh/material id out of range");
+        const float* M = in.transform;
+        double r[9] = {M[0], M[4], M[8], M[1], M[5], M[9], M[2], M[6], M[10]};  // row-major 3x3
+        double det = r[0] * (r[4] * r[8] - r[5] * r[7]) - r[1] * (r[3] * r[8] - r[5] * r[6]) +
+                     r[2] * (r[3] * r[7] - r[4] * r[6]);
+        if (!(std::fabs(det) > 0.0) || !std::isfinite(det))
+            return fail(c, SRT_ERR_INVALID_ARG, "instance transform is singular");
+        double iv[9] = {(r[4] * r[8] - r[5] * r[7]) / det, (r[2] * r[7] - r[1] * r[8]) / det,
+                        (r[1] * r[5] - r[2] * r[4]) / det, (r[5] * r[6] - r[3] * r[8]) / det,
+                        (r[0] * r[8] - r[2] * r[6]) / det, (r[2] * r[3] - r[0] * r[5]) / det,
+                        (r[3] * r[7] - r[4] * r[6]) / det, (r[1] * r[6] - r[0] * r[7]) / det,
+                        (r[0] * r[4] - r[1] * r[3]) / det};
+        InstDev d{};
+        d.mesh_id = in.mesh_id;
+        d.mat_id = in.mat_id;
+        d.tri_offset = (uint32_t)total;
+        d.tri_count = mesh_tris[in.mesh_id];
+        d.w2o0 = make_float4((float)iv[0], (float)iv[1], (float)iv[2], 0.f);
+        d.w2o1 = make_float4((float)iv[3], (float)iv[4], (float)iv[5], 0.f);
+        d.w2o2 = make_float4((float)iv[6], (float)iv[7], (float)iv[8], 0.f);
+        inst[i] = d;
+        fwd[i].r0 = make_float4(M[0], M[4], M[8], M[12]);
+        fwd[i].r1 = make_float4(M[1], M[5], M[9], M[13]);
+        fwd[i].r2 = make_float4(M[2], M[6], M[10], M[14]);
+        total += mesh_tris[in.mesh_id];
+    }
+    if (total >= 0x7FFFFFFFull) return fail(c, SRT_ERR_INVALID_ARG, "too many triangles");
+    std::unique_ptr<srt_scene> s(new (std::nothrow) srt_scene());
+    if (!s) return SRT_ERR_OOM;
+    s->ctx = c;
+    cudaStream_t st = c->stream;
+    CUDA_TRY(c, upload(&s->vtx, a->vertices, sizeof(srt_vertex) * a->n_vertices, sizeof(srt_vertex) * a->n_vertices, st));
+    CUDA_TRY(c, upload(&s->idx, a->indices, 4ull * a->n_indices, 4ull * a->n_indices, st));
+    CUDA_TRY(c, upload(&s->mesh_infos, a->mesh_infos, 16ull * a->n_meshes, 16ull * a->n_meshes, st));
+    CUDA_TRY(c, upload(&s->materials, a->materials, 32ull * a->n_materials, 32ull * a->n_materials, st));
+    CUDA_TRY(c, upload(&s->lights, a->lights, 64ull * a->n_lights, 64ull * a->n_lights, st));
+    CUDA_TRY(c, upload(&s->inst, inst.data(), sizeof(InstDev) * inst.size(), sizeof(InstDev) * inst.size(), st));
+    CUDA_TRY(c, upload(&s->fwd, fwd.data(), sizeof(InstFwd) * fwd.size(), sizeof(InstFwd) * fwd.size(), st));
+    BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total};
+    std::string msg;
+    cudaError_t e = build_bvh8(bi, st, &s->bvh, &msg);
+    if (e != cudaSuccess) return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, "BVH build: " + msg);
+    if (s->bvh.depth > (uint32_t)TRAV_STACK)
+        return fail(c, SRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+    s->n_tris = total;
+    s->n_lights = a->n_lights;
+    DevScene& d = s->dev;
+    d.vtx = s->vtx;
+    d.indices = s->idx;
+    d.mesh_infos = s->mesh_infos;
+    d.materials = s->materials;
+    d.lights = s->lights;
+    d.n_lights = a->n_lights;
+    d.inst = s->inst;
+    d.tri_inst = s->bvh.tri_inst;
+    d.nodes = s->bvh.nodes;
+    d.tris = s->bvh.tris;
+    d.n_nodes = s->bvh.n_nodes;
+    d.n_tris = (uint32_t)total;
+    *out = s.release();
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_scene_builder_build(srt_ctx* c, const srt_scene_builder* b, srt_scene** out) {
+    srt_scene_arrays a;
+    srt_status st = srt_scene_builder_arrays(b, &a);
+    if (st != SRT_OK) return st;
+    return srt_scene_build(c, &a, out);
+}
+
+extern "C" srt_status srt_scene_destroy(srt_scene* s) {
+    if (!s) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    delete s;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_scene_info(const srt_scene* s, uint64_t* n_tris, uint64_t* n_nodes, uint32_t* depth) {
+    if (!s) return SRT_ERR_INVALID_ARG;
+    if (n_tris) *n_tris = s->n_tris;
+    if (n_nodes) *n_nodes = s->bvh.n_nodes;
+    if (depth) *depth = s->bvh.depth;
+    return SRT_OK;
+}
+
+// ====================================================================== renderer
+struct srt_renderer {
+    srt_ctx* ctx = nullptr;
+    srt_scene* scene = nullptr;
+    uint32_t w = 0, h = 0;
+    srt_params p{};
+    FrameArgs args{};
+    srt_camera_uniform* cam_dev = nullptr;
+    srt_camera_uniform* cam_ring = nullptr;  // pinned staging
+    cudaEvent_t ring_ev[4] = {};
+    int ring_i = 0;
+    FrameCounters* counters = nullptr;
+    DevStats* stats = nullptr;
+    uint32_t* err = nullptr;
+    PathBuffers pb{};
+    PhotonBuffers ph{};
+    float4* accum = nullptr;
+    double4* accum64 = nullptr;
+    uchar4* ldr = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int launches_per_frame = 0;
+    uint32_t frame_count = 0;
+    uint64_t frames = 0, launches = 0, photons_emitted = 0, trace_launches = 0;
+    double ms[7] = {0, 0, 0, 0, 0, 0, 0};  // photon trace, grid, closest, shade, shadow, finalize, raygen
+    std::vector<cudaEvent_t> ev;
+
+    ~srt_renderer() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        for (auto& e : ring_ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : ev) cudaEventDestroy(e);
+        cudaFree(cam_dev);
+        cudaFreeHost(cam_ring);
+        cudaFree(counters);
+        cudaFree(stats);
+        cudaFree(err);
+        void* bufs[] = {pb.ray_o, pb.ray_d, pb.hit, pb.thr, pb.wl, pb.rad, pb.misc, pb.queue[0], pb.queue[1],
+                        pb.sh_o, pb.sh_d, pb.sh_c, pb.sh_id, ph.staging, ph.block_counts, ph.photons, ph.sorted,
+                        ph.keys, ph.vals, ph.keys2, ph.vals2, ph.sort_scratch, ph.ranges, accum, accum64, ldr};
+        for (void* b : bufs) cudaFree(b);
+    }
+
+    // Enqueues one frame (after the camera upload).  stage timing: events
+    // between stages (only when `timed`).
+    int record(cudaStream_t st, bool timed) {
+        int n = 0;
+        size_t e = 0;
+        auto mark = [&]() {
+            if (timed) cudaEventRecord(ev[e++], st);
+        };
+        cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
+        mark();  // 0
+        if (p.photons_per_frame > 0) {
+            // the trace kernel is the first launch of the photon pass
+            FrameArgs& a = args;
+            n += launch_photon_pass(a, st);
+        }
+        mark();  // 1 (photon pass total)
+        n += launch_raygen(args, st);
+        mark();  // 2
+        for (uint32_t b = 0; b < p.max_depth; ++b) {
+            n += launch_bounce(args, b, st, 1);
+            mark();
+            n += launch_bounce(args, b, st, 2);
+            mark();
+            n += launch_bounce(args, b, st, 3);
+            mark();
+        }
+        n += launch_finalize(args, st);
+        n += launch_frame_stats(args, st);
+        mark();
+        return n;
+    }
+};
+
+extern "C" srt_params srt_params_default(void) {
+    srt_params p{};
+    p.max_depth = 12;
+    p.photons_per_frame = 1u << 20;
+    p.hash_bits = 22;
+    p.photon_max_bounces = 5;
+    p.gather_cap = 64;
+    p.flags = 0;
+    p.cell_size = 0.02f;
+    p.gather_radius0 = 0.02f;
+    p.radius_exponent = -0.15f;
+    p.spectral_radius = 20.0f;
+    p.photon_norm_count = 0.0f;
+    p.block_size = 0;
+    return p;
+}
+
+extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, uint32_t h, const srt_params* prm,
+                                          srt_renderer** out) {
+    if (!c || !s || !out || w == 0 || h == 0) return SRT_ERR_INVALID_ARG;
+    *out = nullptr;
+    srt_params p = prm ? *prm : srt_params_default();
+    if (p.max_depth == 0 || p.max_depth > (uint32_t)MAX_BOUNCES) return fail(c, SRT_ERR_INVALID_ARG, "max_depth must be 1..31");
+    if (p.hash_bits < 4 || p.hash_bits > 26) return fail(c, SRT_ERR_INVALID_ARG, "hash_bits must be 4..26");
+    if (p.photons_per_frame > (1u << 26)) return fail(c, SRT_ERR_INVALID_ARG, "photons_per_frame above 2^26");
+    if (!(p.cell_size > 0.f) || !(p.gather_radius0 > 0.f) || !(p.spectral_radius > 0.f) || p.photon_max_bounces > 64)
+        return fail(c, SRT_ERR_INVALID_ARG, "invalid photon parameters");
+    if ((uint64_t)w * h > (1ull << 28)) return fail(c, SRT_ERR_INVALID_ARG, "viewport too large");
+    cudaSetDevice(c->device);
+    std::unique_ptr<srt_renderer> r(new (std::nothrow) srt_renderer());
+    if (!r) return SRT_ERR_OOM;
+    r->ctx = c;
+    r->scene = s;
+    r->w = w;
+    r->h = h;
+    r->p = p;
+    size_t np = (size_t)w * h;
+    CUDA_TRY(c, dev_alloc(&r->cam_dev, 1));
+    CUDA_TRY(c, cudaMallocHost((void**)&r->cam_ring, 4 * sizeof(srt_camera_uniform)));
+    for (auto& e : r->ring_ev) CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CUDA_TRY(c, dev_alloc(&r->counters, 1));
+    CUDA_TRY(c, dev_alloc(&r->stats, 1));
+    CUDA_TRY(c, dev_alloc(&r->err, 1));
+    CUDA_TRY(c, cudaMemset(r->stats, 0, sizeof(DevStats)));
+    CUDA_TRY(c, cudaMemset(r->err, 0, 4));
+    PathBuffers& pb = r->pb;
+    CUDA_TRY(c, dev_alloc(&pb.ray_o, np));
+    CUDA_TRY(c, dev_alloc(&pb.ray_d, np));
+    CUDA_TRY(c, dev_alloc(&pb.hit, np));
+    CUDA_TRY(c, dev_alloc(&pb.thr, np));
+    CUDA_TRY(c, dev_alloc(&pb.wl, np));
+    CUDA_TRY(c, dev_alloc(&pb.rad, np));
+    CUDA_TRY(c, dev_alloc(&pb.misc, np));
+    CUDA_TRY(c, dev_alloc(&pb.queue[0], np));
+    CUDA_TRY(c, dev_alloc(&pb.queue[1], np));
+    CUDA_TRY(c, dev_alloc(&pb.sh_o, np));
+    CUDA_TRY(c, dev_alloc(&pb.sh_d, np));
+    CUDA_TRY(c, dev_alloc(&pb.sh_c, np));
+    CUDA_TRY(c, dev_alloc(&pb.sh_id, np));
+    CUDA_TRY(c, dev_alloc(&r->accum, np));
+    CUDA_TRY(c, cudaMemset(r->accum, 0, np * sizeof(float4)));
+    if (p.flags & SRT_FLAG_FP64_ACCUM) {
+        CUDA_TRY(c, dev_alloc(&r->accum64, np));
+        CUDA_TRY(c, cudaMemset(r->accum64, 0, np * sizeof(double4)));
+    }
+    CUDA_TRY(c, dev_alloc(&r->ldr, np));
+    CUDA_TRY(c, cudaMemset(r->ldr, 0, np * 4));
+    PhotonBuffers& ph = r->ph;
+    uint32_t cap = p.photons_per_frame;
+    ph.capacity = cap;
+    ph.n_blocks = (cap + PHOTON_BLOCK - 1) / PHOTON_BLOCK;
+    if (cap > 0) {
+        CUDA_TRY(c, dev_alloc(&ph.staging, 2ull * ph.n_blocks * PHOTON_BLOCK));
+        CUDA_TRY(c, dev_alloc(&ph.block_counts, ph.n_blocks));
+        CUDA_TRY(c, dev_alloc(&ph.photons, 2ull * cap));
+        CUDA_TRY(c, dev_alloc(&ph.sorted, 2ull * cap));
+        CUDA_TRY(c, dev_alloc(&ph.keys, cap));
+        CUDA_TRY(c, dev_alloc(&ph.vals, cap));
+        CUDA_TRY(c, dev_alloc(&ph.keys2, cap));
+        CUDA_TRY(c, dev_alloc(&ph.vals2, cap));
+        CUDA_TRY(c, dev_alloc(&ph.sort_scratch, radix_scratch_words(cap)));
+        CUDA_TRY(c, dev_alloc(&ph.ranges, (size_t)1 << p.hash_bits));
+        CUDA_TRY(c, cudaMemset(ph.ranges, 0, sizeof(uint2) << p.hash_bits));
+    }
+    FrameArgs& a = r->args;
+    a.scene = s->dev;
+    a.cam = r->cam_dev;
+    a.width = w;
+    a.height = h;
+    a.max_depth = p.max_depth;
+    a.photons_per_frame = p.photons_per_frame;
+    a.photon_max_bounces = p.photon_max_bounces;
+    a.counters = r->counters;
+    a.stats = r->stats;
+    a.err = r->err;
+    a.pb = pb;
+    a.ph = ph;
+    a.gather.photons = ph.sorted;
+    a.gather.ranges = ph.ranges;
+    a.gather.hash_bits = p.hash_bits;
+    a.gather.cap = p.gather_cap;
+    a.gather.cell = p.cell_size;
+    a.gather.r0 = p.gather_radius0;
+    a.gather.rexp = p.radius_exponent;
+    a.gather.spectral_radius = p.spectral_radius;
+    a.gather.inv_norm_count = 1.0f / (p.photon_norm_count > 0.f ? p.photon_norm_count : (float)(cap ? cap : 1u));
+    a.gather.enabled = cap > 0;
+    a.accum = r->accum;
+    a.accum64 = r->accum64;
+    a.ldr = r->ldr;
+    a.count_visits = (p.flags & SRT_FLAG_COUNT_VISITS) ? 1 : 0;
+    a.block_size = (int)p.block_size;
+    size_t n_events = 4 + 3 * (size_t)p.max_depth;
+    r->ev.resize(n_events);
+    for (auto& e : r->ev) CUDA_TRY(c, cudaEventCreate(&e));
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
+    if (env_fault("launch")) return fail(c, SRT_ERR_CUDA, "injected launch failure");
+    *out = r.release();
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_destroy(srt_renderer* r) {
+    if (!r) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(r->ctx->device);
+    cudaStreamSynchronize(r->ctx->stream);
+    delete r;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform* cam) {
+    if (!r || !cam) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    int slot = r->ring_i++ & 3;
+    CUDA_TRY(c, cudaEventSynchronize(r->ring_ev[slot]));
+    r->cam_ring[slot] = *cam;
+    CUDA_TRY(c, cudaMemcpyAsync(r->cam_dev, &r->cam_ring[slot], sizeof(srt_camera_uniform), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaEventRecord(r->ring_ev[slot], st));
+    bool timed = (r->p.flags & SRT_FLAG_STAGE_TIMING) != 0;
+    bool use_graph = !timed && !(r->p.flags & SRT_FLAG_NO_GRAPH);
+    if (use_graph) {
+        if (!r->graph) {
+            cudaGraph_t g;
+            CUDA_TRY(c, cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal));
+            r->launches_per_frame = r->record(r->cap_stream, false);
+            CUDA_TRY(c, cudaStreamEndCapture(r->cap_stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&r->graph, g, 0);
+            cudaGraphDestroy(g);
+            CUDA_TRY(c, e);
+        }
+        CUDA_TRY(c, cudaGraphLaunch(r->graph, st));
+        r->launches += (uint64_t)r->launches_per_frame;
+    } else {
+        int n = r->record(st, timed);
+        r->launches += (uint64_t)n;
+        CUDA_TRY(c, cudaGetLastError());
+        if (timed) {
+            CUDA_TRY(c, cudaEventSynchronize(r->ev[3 + 3 * r->p.max_depth]));
+            float t;
+            auto el = [&](size_t a, size_t b) {
+                cudaEventElapsedTime(&t, r->ev[a], r->ev[b]);
+                return (double)t;
+            };
+            r->ms[0] += el(0, 1);
+            r->ms[6] += el(1, 2);
+            for (uint32_t b = 0; b < r->p.max_depth; ++b) {
+                size_t base = 2 + 3 * b;
+                r->ms[2] += el(base, base + 1);
+                r->ms[3] += el(base + 1, base + 2);
+                r->ms[4] += el(base + 2, base + 3);
+            }
+            r->ms[5] += el(2 + 3 * r->p.max_depth, 3 + 3 * r->p.max_depth);
+        }
+    }
+    r->trace_launches += r->p.max_depth;
+    r->frames += 1;
+    r->photons_emitted += r->p.photons_per_frame;
+    r->frame_count += 1;  // renderer/mod.rs:204
+    return SRT_OK;
+}
+
+extern "C" uint32_t srt_renderer_frame_count(const srt_renderer* r) { return r ? r->frame_count : 0u; }
+extern "C" srt_status srt_renderer_set_frame_count(srt_renderer* r, uint32_t f) {
+    if (!r) return SRT_ERR_INVALID_ARG;
+    r->frame_count = f;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_reset_accumulation(srt_renderer* r) {
+    if (!r) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    size_t np = (size_t)r->w * r->h;
+    CUDA_TRY(c, cudaMemsetAsync(r->accum, 0, np * sizeof(float4), c->stream));
+    if (r->accum64) CUDA_TRY(c, cudaMemsetAsync(r->accum64, 0, np * sizeof(double4), c->stream));
+    r->frame_count = 0;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_read_accum_f32(srt_renderer* r, float* rgba) {
+    if (!r || !rgba) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    CUDA_TRY(c, cudaMemcpyAsync(rgba, r->accum, (size_t)r->w * r->h * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_read_accum_f64(srt_renderer* r, double* rgba) {
+    if (!r || !rgba) return SRT_ERR_INVALID_ARG;
+    if (!r->accum64) return fail(r->ctx, SRT_ERR_INVALID_ARG, "renderer created without SRT_FLAG_FP64_ACCUM");
+    srt_ctx* c = r->ctx;
+    CUDA_TRY(c, cudaMemcpyAsync(rgba, r->accum64, (size_t)r->w * r->h * sizeof(double4), cudaMemcpyDeviceToHost,
+                                c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t pitch) {
+    if (!r || !out || pitch < 4 * r->w) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    CUDA_TRY(c, cudaMemcpy2DAsync(out, pitch, r->ldr, 4 * r->w, 4 * r->w, r->h, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_save_screenshot(srt_renderer* r, const char* path) {
+    if (!r || !path) return SRT_ERR_INVALID_ARG;
+    uint32_t pitch = (4 * r->w + 255u) & ~255u;  // utils/wgpu.rs:53-58
+    std::vector<uint8_t> buf((size_t)pitch * r->h);
+    srt_status s = srt_read_ldr_rgba8(r, buf.data(), pitch);
+    if (s != SRT_OK) return s;
+    if (!write_screenshot_png(path, buf.data(), r->w, r->h, pitch))
+        return fail(r->ctx, SRT_ERR_INVALID_ARG, std::string("cannot write ") + path);
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_screenshot_write(const char* path, const uint8_t* rgba, uint32_t w, uint32_t h,
+                                           uint32_t pitch) {
+    if (!path || !rgba || w == 0 || h == 0 || pitch < 4 * w) return SRT_ERR_INVALID_ARG;
+    return write_screenshot_png(path, rgba, w, h, pitch) ? SRT_OK : SRT_ERR_INVALID_ARG;
+}
+
+extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
+    if (!r || !out) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    DevStats d;
+    CUDA_TRY(c, cudaMemcpyAsync(&d, r->stats, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    std::memset(out, 0, sizeof *out);
+    out->frames = r->frames;
+    out->paths = d.paths;
+    out->rays_closest = d.closest_rays;
+    out->rays_shadow = d.shadow_rays;
+    out->photons_emitted = r->photons_emitted;
+    out->photons_stored = d.photons_stored;
+    out->nodes_visited = d.nodes_visited;
+    out->tris_tested = d.tris_tested;
+    out->ms_photon_trace = r->ms[0];
+    out->ms_photon_grid = 0.0;
+    out->ms_trace_closest = r->ms[2];
+    out->ms_shade = r->ms[3];
+    out->ms_trace_shadow = r->ms[4];
+    out->ms_finalize = r->ms[5];
+    out->ms_raygen = r->ms[6];
+    out->launches_trace_closest = r->trace_launches;
+    out->kernel_launches = r->launches;
+    return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_renderer_reset_stats(srt_renderer* r) {
+    if (!r) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    CUDA_TRY(c, cudaMemsetAsync(r->stats, 0, sizeof(DevStats), c->stream));
+    r->frames = r->launches = r->photons_emitted = r->trace_launches = 0;
+    for (double& m : r->ms) m = 0.0;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_read_photons(srt_renderer* r, srt_photon* out, uint32_t capacity, uint32_t* count) {
+    if (!r || !count) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    FrameCounters fc;
+    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->counters, sizeof fc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    *count = r->p.photons_per_frame ? fc.photons_stored : 0u;
+    uint32_t n = std::min(*count, capacity);
+    if (out && n) {
+        CUDA_TRY(c, cudaMemcpyAsync(out, r->ph.photons, (size_t)n * sizeof(srt_photon), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    return check_device_error(c, r->err);
+}
+
+// ====================================================================== standalone kernels
+namespace {
+struct TempPhotons {
+    PhotonBuffers ph{};
+    float4* src = nullptr;
+    ~TempPhotons() {
+        void* bufs[] = {ph.sorted, ph.keys, ph.vals, ph.keys2, ph.vals2, ph.sort_scratch, ph.ranges, src};
+        for (void* b : bufs) cudaFree(b);
+    }
+};
+
+srt_status temp_grid(srt_ctx* c, const srt_photon* photons, uint32_t n, uint32_t frame, float cell, uint32_t bits,
+                     TempPhotons& t) {
+    CUDA_TRY(c, dev_alloc(&t.src, 2ull * n));
+    CUDA_TRY(c, dev_alloc(&t.ph.sorted, 2ull * n));
+    CUDA_TRY(c, dev_alloc(&t.ph.keys, n));
+    CUDA_TRY(c, dev_alloc(&t.ph.vals, n));
+    CUDA_TRY(c, dev_alloc(&t.ph.keys2, n));
+    CUDA_TRY(c, dev_alloc(&t.ph.vals2, n));
+    CUDA_TRY(c, dev_alloc(&t.ph.sort_scratch, radix_scratch_words(n)));
+    CUDA_TRY(c, dev_alloc(&t.ph.ranges, (size_t)1 << bits));
+    if (n) CUDA_TRY(c, cudaMemcpyAsync(t.src, photons, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    t.ph.capacity = n;
+    launch_grid_build(t.src, n, frame, cell, bits, t.ph, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    return SRT_OK;
+}
+}  // namespace
+
+extern "C" srt_status srt_photon_grid_build(srt_ctx* c, const srt_photon* photons, uint32_t n, uint32_t frame,
+                                            float cell, uint32_t bits, uint64_t* keys_out, uint32_t* ranges_out) {
+    if (!c || (!photons && n) || bits < 4 || bits > 26 || !(cell > 0.f) || n >= (1u << 30)) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    TempPhotons t;
+    srt_status s = temp_grid(c, photons, n, frame, cell, bits, t);
+    if (s != SRT_OK) return s;
+    if (keys_out && n) {
+        std::vector<uint32_t> k(n), v(n);
+        CUDA_TRY(c, cudaMemcpyAsync(k.data(), t.ph.sorted_keys, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(v.data(), t.ph.sorted_vals, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        for (uint32_t i = 0; i < n; ++i) keys_out[i] = ((uint64_t)k[i] << 32) | v[i];
+    }
+    if (ranges_out)
+        CUDA_TRY(c, cudaMemcpyAsync(ranges_out, t.ph.ranges, sizeof(uint2) << bits, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_photon_gather(srt_ctx* c, const srt_photon* photons, uint32_t n, const float* queries,
+                                        uint32_t n_q, uint32_t frame, const srt_params* p, float* out) {
+    if (!c || !p || (!photons && n) || (!queries && n_q) || (!out && n_q)) return SRT_ERR_INVALID_ARG;
+    if (p->hash_bits < 4 || p->hash_bits > 26 || !(p->cell_size > 0.f) || n >= (1u << 30)) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    TempPhotons t;
+    srt_status s = temp_grid(c, photons, n, frame, p->cell_size, p->hash_bits, t);
+    if (s != SRT_OK) return s;
+    float* dq = nullptr;
+    float4* dout = nullptr;
+    CUDA_TRY(c, dev_alloc(&dq, 10ull * n_q));
+    cudaError_t e = dev_alloc(&dout, n_q);
+    if (e != cudaSuccess) {
+        cudaFree(dq);
+        return cuda_fail(c, e, "alloc");
+    }
+    GatherArgs g{};
+    g.photons = t.ph.sorted;
+    g.ranges = t.ph.ranges;
+    g.hash_bits = p->hash_bits;
+    g.cap = p->gather_cap;
+    g.cell = p->cell_size;
+    g.r0 = p->gather_radius0;
+    g.rexp = p->radius_exponent;
+    g.spectral_radius = p->spectral_radius;
+    float nc = p->photon_norm_count > 0.f ? p->photon_norm_count : (float)(p->photons_per_frame ? p->photons_per_frame : 1u);
+    g.inv_norm_count = 1.0f / nc;
+    g.enabled = 1;
+    if (n_q) cudaMemcpyAsync(dq, queries, 40ull * n_q, cudaMemcpyHostToDevice, c->stream);
+    launch_gather_queries(g, frame, dq, n_q, dout, c->stream);
+    if (n_q) cudaMemcpyAsync(out, dout, 16ull * n_q, cudaMemcpyDeviceToHost, c->stream);
+    e = cudaStreamSynchronize(c->stream);
+    cudaFree(dq);
+    cudaFree(dout);
+    if (e != cudaSuccess) return cuda_fail(c, e, "gather");
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_trace_rays(srt_scene* s, const srt_ray* rays, uint32_t n, srt_hit* hits, int any_hit) {
+    if (!s || (n && (!rays || !hits))) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    if (n == 0) return SRT_OK;
+    float4 *dr = nullptr, *dh = nullptr;
+    CUDA_TRY(c, dev_alloc(&dr, 2ull * n));
+    cudaError_t e = dev_alloc(&dh, n);
+    if (e != cudaSuccess) {
+        cudaFree(dr);
+        return cuda_fail(c, e, "alloc");
+    }
+    cudaMemcpyAsync(dr, rays, 32ull * n, cudaMemcpyHostToDevice, c->stream);
+    launch_trace_batch(s->dev, dr, n, dh, any_hit, c->d_err, c->stream);
+    cudaMemcpyAsync(hits, dh, 16ull * n, cudaMemcpyDeviceToHost, c->stream);
+    e = cudaStreamSynchronize(c->stream);
+    cudaFree(dr);
+    cudaFree(dh);
+    if (e != cudaSuccess) return cuda_fail(c, e, "trace");
+    return check_device_error(c, c->d_err);
+}
+
+extern "C" srt_status srt_test_device_math(srt_ctx* c, int op, uint32_t n, const void* in, void* out, const void* aux) {
+    static const size_t in_sz[9] = {4, 4, 8, 28, 36, 4, 96, 20, 20};
+    static const size_t out_sz[9] = {4, 12, 4, 16, 16, 20, 40, 4, 28};
+    if (!c || op < 0 || op > 8 || (n && (!in || !out)) || (op == 8 && !aux)) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (n == 0) return SRT_OK;
+    void *din = nullptr, *dout = nullptr, *daux = nullptr;
+    CUDA_TRY(c, dev_alloc((char**)&din, in_sz[op] * n));
+    cudaError_t e = dev_alloc((char**)&dout, out_sz[op] * n);
+    if (e == cudaSuccess && op == 8) e = dev_alloc((char**)&daux, sizeof(srt_camera_uniform));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(din, in, in_sz[op] * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && op == 8)
+        e = cudaMemcpyAsync(daux, aux, sizeof(srt_camera_uniform), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        launch_test_math(op, n, din, dout, daux, c->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, out_sz[op] * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(din);
+    cudaFree(dout);
+    cudaFree(daux);
+    if (e != cudaSuccess) return cuda_fail(c, e, "test_device_math");
+    return SRT_OK;
+}

@@ -1,0 +1,632 @@
+// device_common.cuh — device data layouts and shading math of the spectral
+// path tracer (sm_100a).
+//
+// The shading functions follow the reference WGSL (path:line cited at each
+// one) in FP32; they are written for the GPU (float4 SIMD-style helpers,
+// register-resident state) and checked against the CPU oracle.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/srt.h"
+
+#define SRT_DEV __device__ __forceinline__
+
+namespace srt {
+
+constexpr float PI = 3.14159265359f;  // shader.wgsl:6
+constexpr float LAMBDA_MIN = 380.0f;  // shader.wgsl:81-83
+constexpr float LAMBDA_MAX = 780.0f;
+constexpr float LAMBDA_RANGE = LAMBDA_MAX - LAMBDA_MIN;
+constexpr uint32_t MISS = 0xFFFFFFFFu;
+constexpr int TRAV_STACK = 32;  // BVH8 traversal stack entries per thread
+
+// Device error word bits (read back by the host after synchronising).
+constexpr uint32_t ERR_STACK_OVERFLOW = 0x1u;
+constexpr uint32_t ERR_QUEUE_OVERFLOW = 0x2u;
+constexpr uint32_t ERR_BAD_INDEX = 0x4u;
+
+// ------------------------------------------------------------------ layouts
+// Per instance (64 B): mesh/material ids, first flattened triangle and the
+// rows of world_to_object (inverse of the instance's linear part).
+struct InstDev {
+    uint32_t mesh_id, mat_id, tri_offset, tri_count;
+    float4 w2o0, w2o1, w2o2;  // rows; .w unused
+};
+
+// Compressed 8-wide BVH node, 80 B = 5 x uint4 (layout of Ylitie, Karras and
+// Laine, HPG 2017):
+//  w0..2  origin p (float x3)     w3  exponent bytes ex, ey, ez, imask
+//  w4     first child node index  w5  first triangle slot index
+//  w6..7  meta[8]: 0 empty; (7 << 5) internal child; (count << 5) | offset
+//         for a leaf of `count` (1..3) triangles starting at
+//         first triangle slot + offset
+//  w8..19 qlo.x[8] qlo.y[8] qlo.z[8] qhi.x[8] qhi.y[8] qhi.z[8]
+// Child bounds = p + 2^(e-127) * q.
+struct Node8 {
+    uint4 a, b, c, d, e;
+};
+static_assert(sizeof(Node8) == 80, "Node8 must be 80 bytes");
+
+// A leaf triangle slot (48 B): world-space v0.xyz + flattened triangle id
+// (bits in .w), v1.xyz, v2.xyz.
+struct TriSlot {
+    float4 v0, v1, v2;
+};
+
+struct DevScene {
+    const float4* vtx;          // srt_vertex: pos, normal
+    const uint32_t* indices;
+    const uint4* mesh_infos;    // srt_mesh_info
+    const float4* materials;    // srt_material: color, extra
+    const float4* lights;       // srt_light: v0, v1, v2, params
+    uint32_t n_lights;
+    const InstDev* inst;
+    const uint32_t* tri_inst;   // flattened triangle -> instance
+    const Node8* nodes;
+    const TriSlot* tris;
+    uint32_t n_nodes;
+    uint32_t n_tris;
+};
+
+// ------------------------------------------------------------------ vector helpers
+SRT_DEV float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+SRT_DEV float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+SRT_DEV float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+SRT_DEV float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+SRT_DEV float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+SRT_DEV float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+SRT_DEV float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+SRT_DEV float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+SRT_DEV float3 cross(float3 a, float3 b) {
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+SRT_DEV float length(float3 a) { return sqrtf(dot(a, a)); }
+SRT_DEV float3 normalize(float3 a) { return a / length(a); }
+SRT_DEV float3 reflect(float3 i, float3 n) { return i - n * (2.0f * dot(n, i)); }
+SRT_DEV float3 refract(float3 i, float3 n, float eta) {
+    float ni = dot(n, i);
+    float k = 1.0f - eta * eta * (1.0f - ni * ni);
+    if (k < 0.0f) return f3(0.f, 0.f, 0.f);
+    return i * eta - n * (eta * ni + sqrtf(k));
+}
+SRT_DEV float4 f4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
+SRT_DEV float4 splat4(float s) { return make_float4(s, s, s, s); }
+SRT_DEV float4 operator+(float4 a, float4 b) { return f4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+SRT_DEV float4 operator-(float4 a, float4 b) { return f4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+SRT_DEV float4 operator*(float4 a, float4 b) { return f4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+SRT_DEV float4 operator/(float4 a, float4 b) { return f4(a.x / b.x, a.y / b.y, a.z / b.z, a.w / b.w); }
+SRT_DEV float4 operator*(float4 a, float s) { return f4(a.x * s, a.y * s, a.z * s, a.w * s); }
+SRT_DEV float4 operator/(float4 a, float s) { return f4(a.x / s, a.y / s, a.z / s, a.w / s); }
+SRT_DEV float max4(float4 a) { return fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)); }
+SRT_DEV float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+SRT_DEV float sq(float x) { return x * x; }
+SRT_DEV float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
+// ------------------------------------------------------------------ RNG (shader.wgsl:144-169)
+SRT_DEV uint32_t pcg_hash(uint32_t input) {
+    uint32_t state = input * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+// rand(): f32(u32) / 4294967295.0 — the f32 constant is 2^32, so the
+// quotient is an exact scaling of the rounded u32.
+SRT_DEV float rng_next(uint32_t& s) {
+    s = pcg_hash(s);
+    return __fdiv_rn(__uint2float_rn(s), 4294967296.0f);
+}
+SRT_DEV float3 random_unit_vector(uint32_t& s) {
+    float u1 = rng_next(s);
+    float u2 = rng_next(s);
+    float z = 1.0f - 2.0f * u1;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float phi = 2.0f * PI * u2;
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    return f3(r * cp, r * sp, z);
+}
+
+// ------------------------------------------------------------------ spectra
+// sample_cie_xyz: shader.wgsl:85-97 (pow(x, 2.0) read as x*x)
+SRT_DEV float3 sample_cie_xyz(float l) {
+    float x = expf(-sq((l - 599.8f) / 37.9f)) * 1.056f + expf(-sq((l - 442.0f) / 16.0f)) * 0.362f -
+              expf(-sq((l - 501.1f) / 26.7f)) * 0.065f;
+    float y = expf(-sq((l - 568.8f) / 46.9f)) * 0.821f + expf(-sq((l - 530.9f) / 16.3f)) * 0.286f;
+    float z = expf(-sq((l - 437.0f) / 11.8f)) * 1.217f + expf(-sq((l - 459.0f) / 26.0f)) * 0.681f;
+    return f3(fmaxf(0.0f, x), fmaxf(0.0f, y), fmaxf(0.0f, z));
+}
+// XYZ_TO_SRGB: shader.wgsl:100-104
+SRT_DEV float3 xyz_to_srgb(float3 c) {
+    return f3(3.2404542f * c.x - 1.5371385f * c.y - 0.4985314f * c.z,
+              -0.9692660f * c.x + 1.8760108f * c.y + 0.0415560f * c.z,
+              0.0556434f * c.x - 0.2040259f * c.y + 1.0572252f * c.z);
+}
+// rgb_to_spectrum_eval: shader.wgsl:106-117
+SRT_DEV float rgb_to_spectrum(float3 rgb, float l) {
+    float white = fminf(rgb.x, fminf(rgb.y, rgb.z));
+    float cr = fmaxf(rgb.x - white, 0.f), cg = fmaxf(rgb.y - white, 0.f), cb = fmaxf(rgb.z - white, 0.f);
+    float r = cr * expf(-sq((l - 630.0f) / 20.0f));
+    float g = cg * expf(-sq((l - 525.0f) / 20.0f));
+    float b = cb * expf(-sq((l - 460.0f) / 20.0f));
+    return clampf(white + r + g + b, 0.0f, 0.99f);
+}
+SRT_DEV float4 rgb_to_spectrum4(float3 rgb, float4 wl) {
+    return f4(rgb_to_spectrum(rgb, wl.x), rgb_to_spectrum(rgb, wl.y), rgb_to_spectrum(rgb, wl.z),
+              rgb_to_spectrum(rgb, wl.w));
+}
+// blackbody_radiance: shader.wgsl:128-139
+SRT_DEV float blackbody(float lambda_nm, float temp_k) {
+    float lm = lambda_nm * 1e-9f;
+    const float h = 6.62607015e-34f, c = 299792458.0f, k = 1.380649e-23f;
+    float c1 = 2.0f * h * c * c;
+    float c2 = (h * c) / (k * temp_k);
+    return c1 / (powf(lm, 5.0f) * (expf(c2 / lm) - 1.0f)) * 1e-13f;
+}
+SRT_DEV float4 blackbody4(float4 wl, float t) {
+    return f4(blackbody(wl.x, t), blackbody(wl.y, t), blackbody(wl.z, t), blackbody(wl.w, t));
+}
+
+// ------------------------------------------------------------------ BSDF math
+// Airy reflectance of a film, one wavelength (photon_emit.wgsl:107-132;
+// the vec4 form shader.wgsl:233-262 runs the same per component).
+// Returns 1 and sets tir on total internal reflection.
+SRT_DEV float thin_film1(float cos1, float n1, float n2, float n3, float d, float lambda, bool& tir) {
+    float s1 = fmaxf(0.0f, 1.0f - cos1 * cos1);
+    float s2 = (n1 / n2) * (n1 / n2) * s1;
+    tir = true;
+    if (s2 >= 1.0f) return 1.0f;
+    float c2 = sqrtf(1.0f - s2);
+    float s3 = (n1 / n3) * (n1 / n3) * s1;
+    if (s3 >= 1.0f) return 1.0f;
+    tir = false;
+    float c3 = sqrtf(1.0f - s3);
+    float r12 = (n1 * cos1 - n2 * c2) / (n1 * cos1 + n2 * c2);
+    float r23 = (n2 * c2 - n3 * c3) / (n2 * c2 + n3 * c3);
+    float a = r12 * r12, b = r23 * r23;
+    float cd = cosf((4.0f * PI * n2 * d * c2) / lambda);
+    float num = a + b + 2.0f * r12 * r23 * cd;
+    float den = 1.0f + a * b + 2.0f * r12 * r23 * cd;
+    return clampf(num / den, 0.0f, 1.0f);
+}
+SRT_DEV float4 thin_film4(float cos1, float n1, float n2, float n3, float d, float4 wl) {
+    bool tir;
+    float x = thin_film1(cos1, n1, n2, n3, d, wl.x, tir);
+    if (tir) return splat4(1.0f);
+    return f4(x, thin_film1(cos1, n1, n2, n3, d, wl.y, tir), thin_film1(cos1, n1, n2, n3, d, wl.z, tir),
+              thin_film1(cos1, n1, n2, n3, d, wl.w, tir));
+}
+// reflectance (Schlick): shader.wgsl:264-268
+SRT_DEV float schlick(float cosine, float ri) {
+    float r0 = (1.0f - ri) / (1.0f + ri);
+    r0 = r0 * r0;
+    return r0 + (1.0f - r0) * powf(1.0f - cosine, 5.0f);
+}
+SRT_DEV float g1_schlick_ggx(float nv, float r) {  // shader.wgsl:207-213
+    float k = (r * r) / 2.0f;
+    return nv / (nv * (1.0f - k) + k);
+}
+// GGX half vector in the frame of n (shader.wgsl:171-205; the basis keeps
+// the reference's division by sign(n.z) + n.z).
+SRT_DEV float3 ggx_half_vector(float3 n, float alpha, uint32_t& s) {
+    float a2 = alpha * alpha;
+    float r1 = rng_next(s);
+    float r2 = rng_next(s);
+    float phi = 2.0f * PI * r1;
+    float ct = sqrtf((1.0f - r2) / (1.0f + (a2 - 1.0f) * r2));
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    float3 h = f3(cp * st, sp * st, ct);
+    float sg = signf(n.z);
+    float a = -1.0f / (sg + n.z);
+    float b = n.x * n.y * a;
+    float3 right = f3(1.0f + sg * n.x * n.x * a, sg * b, -sg * n.x);
+    float3 up = f3(b, sg + n.y * n.y * a, -n.y);
+    return normalize(right * h.x + up * h.y + n * h.z);
+}
+
+struct Scatter {
+    float3 dir;
+    float4 att;
+    bool absorbed;
+};
+
+// sample_bsdf: shader.wgsl:347-471.  Type 5 (no reference counterpart):
+// GGX sampling as type 1 with the film's Airy reflectance in place of
+// Schlick's F; roughness in color.w, film d/n2/n3 in extra.yzw.
+SRT_DEV Scatter sample_bsdf(float3 r_dir, float3 ffn, float4 color, float4 extra, bool front, float4 wl,
+                            float4 thr, uint32_t& s) {
+    Scatter rec;
+    rec.absorbed = false;
+    rec.dir = f3(0.f, 0.f, 0.f);
+    rec.att = splat4(0.f);
+    uint32_t type = (uint32_t)extra.x;
+    float4 spec = rgb_to_spectrum4(xyz(color), wl);
+    if (type == 1u || type == 5u) {
+        float alpha = fmaxf(type == 1u ? extra.y : color.w, 0.001f);
+        float3 v = normalize(-r_dir);
+        float3 h = ggx_half_vector(ffn, alpha, s);
+        float3 l = reflect(-v, h);
+        float nl = dot(ffn, l), nv = dot(ffn, v);
+        if (nl > 0.0f && nv > 0.0f) {
+            float nh = fmaxf(dot(ffn, h), 0.0f);
+            float vh = fmaxf(dot(v, h), 0.0f);
+            float4 F;
+            if (type == 1u) {
+                float p = powf(clampf(1.0f - vh, 0.0f, 1.0f), 5.0f);
+                F = spec + (splat4(1.0f) - spec) * p;
+            } else {
+                F = thin_film4(vh, 1.0f, extra.z, extra.w, fmaxf(extra.y, 50.0f), wl);
+            }
+            float G = g1_schlick_ggx(nl, alpha) * g1_schlick_ggx(nv, alpha);
+            rec.att = (F * G * vh) / fmaxf(nv * nh, 0.0001f);
+            rec.dir = l;
+        } else {
+            rec.absorbed = true;
+        }
+    } else if (type == 2u) {
+        float lum = wl.x / 1000.0f;
+        float ir = extra.z + (extra.w / (lum * lum));
+        float ratio = front ? 1.0f / ir : ir;
+        float3 u = normalize(r_dir);
+        float ct = fminf(dot(-u, ffn), 1.0f);
+        float si2 = fmaxf(0.0f, 1.0f - ct * ct);
+        float st2 = ratio * ratio * si2;
+        if (st2 >= 1.0f) {
+            rec.dir = reflect(u, ffn);
+            rec.att = splat4(1.0f);
+        } else {
+            float ctt = sqrtf(1.0f - st2);
+            if (schlick(front ? ct : ctt, ratio) > rng_next(s)) {
+                rec.dir = reflect(u, ffn);
+                rec.att = splat4(1.0f);
+            } else {
+                rec.dir = refract(u, ffn, ratio);
+                float4 base = spec * (ratio * ratio);
+                if (extra.w > 0.0f) {
+                    bool collapsed = thr.y < 0.0001f && thr.z < 0.0001f && thr.w < 0.0001f;
+                    rec.att = f4(base.x * (collapsed ? 1.0f : 4.0f), 0.f, 0.f, 0.f);
+                } else {
+                    rec.att = base;
+                }
+            }
+        }
+    } else if (type == 4u) {
+        float3 u = normalize(r_dir);
+        float c1 = fminf(dot(-u, ffn), 1.0f);
+        float4 F = thin_film4(c1, 1.0f, extra.z, extra.w, fmaxf(extra.y, 50.0f), wl);
+        float p = F.x;
+        if (rng_next(s) < p) {
+            rec.dir = reflect(u, ffn);
+            rec.att = F / p;
+        } else {
+            rec.dir = u;
+            rec.att = (splat4(1.0f) - F) / (1.0f - p);
+        }
+    } else {
+        float3 d = ffn + random_unit_vector(s);
+        if (length(d) < 0.001f) d = ffn;
+        rec.dir = normalize(d);
+        rec.att = spec;
+    }
+    return rec;
+}
+
+// Hero wavelengths (shader.wgsl:734-767) and the sum of their pdfs (:782-797).
+SRT_DEV float cauchy_cdf(float x) { return (1.0f / PI) * atanf((x - 555.0f) / 40.0f) + 0.5f; }
+SRT_DEV float lambda_wrap(float x) {  // WGSL float %: e1 - e2 * trunc(e1 / e2)
+    float a = x - LAMBDA_MIN;
+    return LAMBDA_MIN + (a - LAMBDA_RANGE * truncf(a / LAMBDA_RANGE));
+}
+SRT_DEV float4 sample_hero(uint32_t& s) {
+    float cmin = cauchy_cdf(LAMBDA_MIN), cmax = cauchy_cdf(LAMBDA_MAX);
+    float u = cmin + rng_next(s) * (cmax - cmin);
+    float hero = clampf(555.0f + 40.0f * tanf(PI * (u - 0.5f)), LAMBDA_MIN, LAMBDA_MAX);
+    const float q = LAMBDA_RANGE / 4.0f;
+    float4 w = f4(lambda_wrap(hero), lambda_wrap(hero + q), lambda_wrap(hero + q * 2.0f), lambda_wrap(hero + q * 3.0f));
+    float rot = rng_next(s);
+    if (rot < 0.25f) {
+    } else if (rot < 0.5f) {
+        w = f4(w.y, w.z, w.w, w.x);
+    } else if (rot < 0.75f) {
+        w = f4(w.z, w.w, w.x, w.y);
+    } else {
+        w = f4(w.w, w.x, w.y, w.z);
+    }
+    return w;
+}
+SRT_DEV float hero_pdf_sum(float4 w) {
+    float cmin = cauchy_cdf(LAMBDA_MIN), cmax = cauchy_cdf(LAMBDA_MAX);
+    float norm = 1.0f / ((cmax - cmin) * PI * 40.0f);
+    float a = (w.x - 555.0f) / 40.0f, b = (w.y - 555.0f) / 40.0f, c = (w.z - 555.0f) / 40.0f,
+          d = (w.w - 555.0f) / 40.0f;
+    return norm / (1.0f + a * a) + norm / (1.0f + b * b) + norm / (1.0f + c * c) + norm / (1.0f + d * d);
+}
+
+// ------------------------------------------------------------------ photon grid hashing
+// get_grid_jitter + hash_position: build_grid.wgsl:25-52.  Written with
+// explicitly rounded intrinsics so that no multiply-add is contracted: the
+// cell keys are compared bit for bit.
+SRT_DEV float3 grid_jitter(uint32_t frame, float cell) {
+    uint32_t seed = pcg_hash(frame * 114514u);
+    float rx = __fdiv_rn(__uint2float_rn(seed & 0xFFu), 255.0f);
+    float ry = __fdiv_rn(__uint2float_rn((seed >> 8u) & 0xFFu), 255.0f);
+    float rz = __fdiv_rn(__uint2float_rn((seed >> 16u) & 0xFFu), 255.0f);
+    return f3(__fmul_rn(__fsub_rn(rx, 0.5f), cell), __fmul_rn(__fsub_rn(ry, 0.5f), cell),
+              __fmul_rn(__fsub_rn(rz, 0.5f), cell));
+}
+SRT_DEV uint32_t grid_hash(float3 p, float3 j, float cell, uint32_t hash_bits) {
+    // f32 -> i32 conversion saturates as in WGSL (cvt.rzi.s32.f32 does)
+    int gx = __float2int_rz(floorf(__fdiv_rn(__fadd_rn(p.x, j.x), cell)));
+    int gy = __float2int_rz(floorf(__fdiv_rn(__fadd_rn(p.y, j.y), cell)));
+    int gz = __float2int_rz(floorf(__fdiv_rn(__fadd_rn(p.z, j.z), cell)));
+    uint32_t h = ((uint32_t)gx * 73856093u) ^ ((uint32_t)gy * 19349663u) ^ ((uint32_t)gz * 83492791u);
+    return h & ((1u << hash_bits) - 1u);
+}
+
+// ------------------------------------------------------------------ camera ray (shader.wgsl:713-728)
+SRT_DEV void camera_ray(const srt_camera_uniform& cam, uint32_t x, uint32_t y, uint32_t w, uint32_t h,
+                        uint32_t& s, float3& o, float3& d) {
+    const float* vi = cam.view_inverse;
+    const float* pi = cam.proj_inverse;
+    float jx = rng_next(s);
+    float jy = rng_next(s);
+    float nx = ((float)x + jx) / (float)w * 2.0f - 1.0f;
+    float ny = ((float)y + jy) / (float)h * 2.0f - 1.0f;
+    float t[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        // row r of (view_inv * proj_inv), then times (nx, ny, 1, 1)
+        float m0 = vi[r] * pi[0] + vi[4 + r] * pi[1] + vi[8 + r] * pi[2] + vi[12 + r] * pi[3];
+        float m1 = vi[r] * pi[4] + vi[4 + r] * pi[5] + vi[8 + r] * pi[6] + vi[12 + r] * pi[7];
+        float m2 = vi[r] * pi[8] + vi[4 + r] * pi[9] + vi[8 + r] * pi[10] + vi[12 + r] * pi[11];
+        float m3 = vi[r] * pi[12] + vi[4 + r] * pi[13] + vi[8 + r] * pi[14] + vi[12 + r] * pi[15];
+        t[r] = m0 * nx + m1 * ny + m2 + m3;
+    }
+    o = f3(vi[12], vi[13], vi[14]);
+    d = normalize(f3(t[0] / t[3], t[1] / t[3], t[2] / t[3]) - o);
+}
+
+// ------------------------------------------------------------------ traversal
+struct Ray {
+    float3 o, d;
+    float tmin, tmax;
+};
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013) with the
+// FP64 fallback for edge functions that evaluate to exactly zero.
+struct RayShear {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+SRT_DEV float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+SRT_DEV RayShear make_shear(float3 d) {
+    RayShear r;
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    r.kx = r.kz == 2 ? 0 : r.kz + 1;
+    r.ky = r.kx == 2 ? 0 : r.kx + 1;
+    float dz = comp(d, r.kz);
+    if (dz < 0.0f) {
+        int t = r.kx;
+        r.kx = r.ky;
+        r.ky = t;
+    }
+    r.sx = comp(d, r.kx) / dz;
+    r.sy = comp(d, r.ky) / dz;
+    r.sz = 1.0f / dz;
+    return r;
+}
+// Returns true on a hit with tmin <= t <= tmax; u, v = weights of v1, v2.
+SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3 v1, float3 v2, float& t,
+                           float& u, float& v) {
+    float3 A = v0 - ray.o, B = v1 - ray.o, C = v2 - ray.o;
+    float Az = comp(A, sh.kz), Bz = comp(B, sh.kz), Cz = comp(C, sh.kz);
+    float Ax = comp(A, sh.kx) - sh.sx * Az, Ay = comp(A, sh.ky) - sh.sy * Az;
+    float Bx = comp(B, sh.kx) - sh.sx * Bz, By = comp(B, sh.ky) - sh.sy * Bz;
+    float Cx = comp(C, sh.kx) - sh.sx * Cz, Cy = comp(C, sh.ky) - sh.sy * Cz;
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = U + V + W;
+    if (det == 0.0f) return false;
+    float T = U * (sh.sz * Az) + V * (sh.sz * Bz) + W * (sh.sz * Cz);
+    float inv = 1.0f / det;
+    float tt = T * inv;
+    if (!(tt >= ray.tmin && tt <= ray.tmax)) return false;
+    t = tt;
+    u = V * inv;
+    v = W * inv;
+    return true;
+}
+
+SRT_DEV uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xFFu; }
+
+struct TravCounters {
+    unsigned long long* nodes;
+    unsigned long long* tris;
+};
+
+// Stack-based traversal of the compressed BVH8.  A node group holds the
+// hit internal children of one node (bits 24..31 of .y, ordered so that the
+// highest bit is the nearest child for this ray octant) plus the node's
+// imask (bits 0..7); triangle hits go straight to the triangle loop.
+// ANY: return at the first hit in [tmin, tmax].  Closest: lexicographic
+// minimum of (t, flattened triangle id), independent of traversal order.
+// `stack` is this thread's slice of shared memory, stride `stride` entries.
+template <bool ANY, bool COUNT>
+SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, float& t_out, uint32_t& prim_out,
+                      float& u_out, float& v_out, uint32_t* err, TravCounters cnt) {
+    prim_out = MISS;
+    if (S.n_nodes == 0u) return false;
+    if (!(ray.d.x != 0.0f || ray.d.y != 0.0f || ray.d.z != 0.0f)) return false;
+    if (!(ray.tmin <= ray.tmax)) return false;
+    RayShear sh = make_shear(ray.d);
+    const float eps = 1e-12f;
+    float3 idir = f3(1.0f / (fabsf(ray.d.x) > eps ? ray.d.x : copysignf(eps, ray.d.x)),
+                     1.0f / (fabsf(ray.d.y) > eps ? ray.d.y : copysignf(eps, ray.d.y)),
+                     1.0f / (fabsf(ray.d.z) > eps ? ray.d.z : copysignf(eps, ray.d.z)));
+    uint32_t oct = (ray.d.x < 0.f ? 1u : 0u) | (ray.d.y < 0.f ? 2u : 0u) | (ray.d.z < 0.f ? 4u : 0u);
+    const float robust = 1.0000004f;  // conservative far-plane scaling of the slab test
+    float tbest = ray.tmax;
+    uint32_t best = MISS;
+    float bu = 0.f, bv = 0.f;
+    int sp = 0;
+    uint32_t n_nodes = 0, n_tris = 0;
+    // virtual group holding the root as child slot 0
+    uint2 g = make_uint2(0u, (1u << (24 + (0u ^ (oct ^ 7u)))) | 1u);
+    uint2 tg = make_uint2(0u, 0u);
+    while (true) {
+        // ---- triangles of the last node
+        while (tg.y != 0u) {
+            int b = __ffs(tg.y) - 1;
+            tg.y &= tg.y - 1u;
+            const TriSlot* ts = S.tris + tg.x + (uint32_t)b;
+            float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
+            if (COUNT) ++n_tris;
+            float t, u, v;
+            Ray r = ray;
+            r.tmax = tbest;
+            if (intersect_tri(r, sh, xyz(a0), xyz(a1), xyz(a2), t, u, v)) {
+                uint32_t id = __float_as_uint(a0.w);
+                if (ANY) {
+                    t_out = t;
+                    prim_out = id;
+                    if (COUNT) {
+                        atomicAdd(cnt.nodes, (unsigned long long)n_nodes);
+                        atomicAdd(cnt.tris, (unsigned long long)n_tris);
+                    }
+                    return true;
+                }
+                if (t < tbest || id < best) {  // (t, id) lexicographic; t <= tbest holds here
+                    if (t < tbest || (t == tbest && id < best)) {
+                        tbest = t;
+                        best = id;
+                        bu = u;
+                        bv = v;
+                    }
+                }
+            }
+        }
+        // ---- next node
+        if ((g.y & 0xFF000000u) == 0u) {
+            if (sp == 0) break;
+            --sp;
+            g = stack[sp * stride];
+        }
+        int bit = 31 - __clz(g.y & 0xFF000000u);
+        g.y &= ~(1u << bit);
+        uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
+        uint32_t idx = g.x + __popc(g.y & ((1u << slot) - 1u) & 0xFFu);
+        if (g.y & 0xFF000000u) {
+            if (sp >= TRAV_STACK) {
+                atomicOr(err, ERR_STACK_OVERFLOW);
+                break;
+            }
+            stack[sp * stride] = g;
+            ++sp;
+        }
+        if (idx >= S.n_nodes) {
+            atomicOr(err, ERR_BAD_INDEX);
+            break;
+        }
+        const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
+        uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+        if (COUNT) ++n_nodes;
+        float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+        float sx = __uint_as_float((w0.w & 0xFFu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
+              sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+        uint32_t imask = w0.w >> 24;
+        float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;
+        float bx = (px - ray.o.x) * idir.x, by = (py - ray.o.y) * idir.y, bz = (pz - ray.o.z) * idir.z;
+        // near/far quantised planes per axis by ray octant
+        uint32_t lx0 = w2.x, lx1 = w2.y, ly0 = w2.z, ly1 = w2.w, lz0 = w3.x, lz1 = w3.y;
+        uint32_t hx0 = w3.z, hx1 = w3.w, hy0 = w4.x, hy1 = w4.y, hz0 = w4.z, hz1 = w4.w;
+        uint32_t nx0 = (oct & 1u) ? hx0 : lx0, nx1 = (oct & 1u) ? hx1 : lx1;
+        uint32_t fx0 = (oct & 1u) ? lx0 : hx0, fx1 = (oct & 1u) ? lx1 : hx1;
+        uint32_t ny0 = (oct & 2u) ? hy0 : ly0, ny1 = (oct & 2u) ? hy1 : ly1;
+        uint32_t fy0 = (oct & 2u) ? ly0 : hy0, fy1 = (oct & 2u) ? ly1 : hy1;
+        uint32_t nz0 = (oct & 4u) ? hz0 : lz0, nz1 = (oct & 4u) ? hz1 : lz1;
+        uint32_t fz0 = (oct & 4u) ? lz0 : hz0, fz1 = (oct & 4u) ? lz1 : hz1;
+        uint32_t meta0 = w1.z, meta1 = w1.w;
+        uint32_t hits = 0u;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            int k = i & 3;
+            uint32_t m = byte_of(i < 4 ? meta0 : meta1, k);
+            float tnx = (float)byte_of(i < 4 ? nx0 : nx1, k) * ax + bx;
+            float tny = (float)byte_of(i < 4 ? ny0 : ny1, k) * ay + by;
+            float tnz = (float)byte_of(i < 4 ? nz0 : nz1, k) * az + bz;
+            float tfx = (float)byte_of(i < 4 ? fx0 : fx1, k) * ax + bx;
+            float tfy = (float)byte_of(i < 4 ? fy0 : fy1, k) * ay + by;
+            float tfz = (float)byte_of(i < 4 ? fz0 : fz1, k) * az + bz;
+            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
+            float tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest)) * robust;
+            if (m != 0u && tn <= tf) {
+                uint32_t c = m >> 5;
+                if (c == 7u)
+                    hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
+                else
+                    hits |= ((1u << c) - 1u) << (m & 31u);
+            }
+        }
+        g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
+        tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+    }
+    if (COUNT) {
+        atomicAdd(cnt.nodes, (unsigned long long)n_nodes);
+        atomicAdd(cnt.tris, (unsigned long long)n_tris);
+    }
+    if (ANY) return false;
+    if (best == MISS) return false;
+    t_out = tbest;
+    prim_out = best;
+    u_out = bu;
+    v_out = bv;
+    return true;
+}
+
+// ------------------------------------------------------------------ surface data at a hit
+struct Surface {
+    uint32_t inst, mat;
+    float3 wn;     // normalised world shading normal (not face-forwarded)
+    bool front;
+};
+
+// get_interpolated_normal (shader.wgsl:530-545), the world transform
+// (:573-576) and the ray query's front_face: counter-clockwise as seen from
+// the ray in object space.
+SRT_DEV Surface surface_at(const DevScene& S, uint32_t prim, float u, float v, float3 dir_world) {
+    Surface sf;
+    uint32_t ii = __ldg(&S.tri_inst[prim]);
+    const InstDev& in = S.inst[ii];
+    uint4 mi = __ldg(&S.mesh_infos[in.mesh_id]);
+    uint32_t io = mi.y + (prim - in.tri_offset) * 3u;
+    uint32_t i0 = __ldg(&S.indices[io]) + mi.x, i1 = __ldg(&S.indices[io + 1]) + mi.x,
+             i2 = __ldg(&S.indices[io + 2]) + mi.x;
+    float4 p0 = __ldg(&S.vtx[2 * i0]), n0 = __ldg(&S.vtx[2 * i0 + 1]);
+    float4 p1 = __ldg(&S.vtx[2 * i1]), n1 = __ldg(&S.vtx[2 * i1 + 1]);
+    float4 p2 = __ldg(&S.vtx[2 * i2]), n2 = __ldg(&S.vtx[2 * i2 + 1]);
+    float w = 1.0f - u - v;
+    float3 ln = normalize(xyz(n0) * w + xyz(n1) * u + xyz(n2) * v);
+    float4 r0 = in.w2o0, r1 = in.w2o1, r2 = in.w2o2;
+    // local_normal * mat3x3(w2o columns) = transpose(W2O) * n
+    float3 wn = f3(ln.x * r0.x + ln.y * r1.x + ln.z * r2.x, ln.x * r0.y + ln.y * r1.y + ln.z * r2.y,
+                   ln.x * r0.z + ln.y * r1.z + ln.z * r2.z);
+    sf.wn = normalize(wn);
+    float3 dobj = f3(dot(xyz(r0), dir_world), dot(xyz(r1), dir_world), dot(xyz(r2), dir_world));
+    float3 gn = cross(xyz(p1) - xyz(p0), xyz(p2) - xyz(p0));
+    sf.front = dot(dobj, gn) < 0.0f;
+    sf.inst = ii;
+    sf.mat = in.mat_id;
+    return sf;
+}
+
+}  // namespace srt

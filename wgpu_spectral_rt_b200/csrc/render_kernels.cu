@@ -1,0 +1,674 @@
+// render_kernels.cu — per-frame kernels of the spectral path tracer.
+//
+// One frame = one sample per pixel (src/renderer/mod.rs:168-207):
+//   photon pass   photon_emit.wgsl:154-331 (one thread per emitted photon,
+//                 inline BVH8 traversal, block-ordered compaction so the
+//                 stored photons keep emission order) and the grid
+//                 (build_grid.wgsl:25-73) as cell keys + radix sort + ranges
+//   camera paths  shader.wgsl:708-823 as a wavefront: raygen, then per
+//                 bounce trace_closest -> shade -> trace_shadow over SoA
+//                 queues compacted with warp ballots; finalize converts the
+//                 hero tuple to sRGB, accumulates and tonemaps.
+#include "radix_sort.cuh"
+#include "render_kernels.h"
+
+namespace srt {
+
+namespace {
+
+constexpr uint32_t FLAG_DIFFUSE = 0x1u;  // has_hit_diffuse (shader.wgsl:554)
+constexpr uint32_t FLAG_CAUSTIC = 0x2u;  // is_caustic_path (shader.wgsl:555)
+
+SRT_DEV uint32_t warp_push(bool pred, uint32_t* counter) {
+    uint32_t mask = __ballot_sync(0xFFFFFFFFu, pred);
+    int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (mask) {
+        int leader = __ffs(mask) - 1;
+        if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    }
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+SRT_DEV void warp_add_u64(unsigned long long* dst, uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, (unsigned long long)v);
+}
+
+// gather_photons: shader.wgsl:297-342 over a sorted range; the walk goes
+// from the highest photon index down (the LIFO order of the reference's
+// linked list for in-order insertion), at most `cap` entries.
+SRT_DEV float4 gather(const GatherArgs& g, uint32_t frame, float3 hit_pos, float3 normal, float4 wl) {
+    float3 j = grid_jitter(frame, g.cell);
+    float r = g.r0 * powf((float)(frame + 1u), g.rexp);
+    float r2 = r * r;
+    uint32_t h = grid_hash(hit_pos, j, g.cell, g.hash_bits);
+    uint2 rg = __ldg(&g.ranges[h]);
+    float4 total = splat4(0.f);
+    uint32_t stop = rg.y - min(rg.y - rg.x, g.cap);
+    for (uint32_t i = rg.y; i > stop; --i) {
+        float4 pa = __ldg(&g.photons[2 * (i - 1)]);
+        float4 pb = __ldg(&g.photons[2 * (i - 1) + 1]);
+        float3 dd = hit_pos - xyz(pa);
+        float d2 = dot(dd, dd);
+        if (d2 < r2 && dot(normal, xyz(pb)) > 0.0f) {
+            float sw = 1.0f - (sqrtf(d2) / r);
+            float4 spw = f4(fmaxf(1.0f - fabsf(wl.x - pa.w) / g.spectral_radius, 0.f),
+                            fmaxf(1.0f - fabsf(wl.y - pa.w) / g.spectral_radius, 0.f),
+                            fmaxf(1.0f - fabsf(wl.z - pa.w) / g.spectral_radius, 0.f),
+                            fmaxf(1.0f - fabsf(wl.w - pa.w) / g.spectral_radius, 0.f));
+            total = total + spw * (pb.w * sw);
+        }
+    }
+    float density = (3.0f / (PI * r2)) * (1.0f / g.spectral_radius) * g.inv_norm_count;
+    return total * density;
+}
+
+// ------------------------------------------------------------------ photon pass
+template <bool COUNT>
+__global__ void __launch_bounds__(PHOTON_BLOCK) k_photon_trace(FrameArgs a) {
+    extern __shared__ uint2 stack_smem[];
+    __shared__ uint32_t warp_cnt[PHOTON_BLOCK / 32];
+    const DevScene& S = a.scene;
+    uint32_t e = blockIdx.x * PHOTON_BLOCK + threadIdx.x;
+    uint32_t frame = a.cam->frame_count;
+    bool stored = false;
+    float4 out0 = splat4(0.f), out1 = splat4(0.f);
+    uint32_t n_rays = 0;
+    TravCounters tc{&a.stats->nodes_visited, &a.stats->tris_tested};
+    if (e < a.photons_per_frame && S.n_lights > 0u) {
+        uint32_t s = pcg_hash(e + frame * 927163u);
+        uint32_t nl = S.n_lights;
+        uint32_t li = min(__float2uint_rz(rng_next(s) * (float)nl), nl - 1u);
+        float4 L0 = S.lights[4 * li], L1 = S.lights[4 * li + 1], L2 = S.lights[4 * li + 2],
+               LP = S.lights[4 * li + 3];
+        float3 v0 = xyz(L0), v1 = xyz(L1), v2 = xyz(L2);
+        float3 c = cross(v1 - v0, v2 - v0);
+        float3 normal = normalize(c);
+        float area = length(c) * 0.5f;
+        float r1 = rng_next(s);
+        float r2 = rng_next(s);
+        float sr1 = sqrtf(r1);
+        float u = 1.0f - sr1, v = r2 * sr1, w = 1.0f - u - v;
+        float3 emit_pos = v0 * u + v1 * v + v2 * w;
+        float3 emit_dir = normalize(normal + random_unit_vector(s));
+        float cmin = cauchy_cdf(LAMBDA_MIN), cmax = cauchy_cdf(LAMBDA_MAX), crange = cmax - cmin;
+        float lambda = clampf(555.0f + 40.0f * tanf(PI * ((cmin + rng_next(s) * crange) - 0.5f)), LAMBDA_MIN,
+                              LAMBDA_MAX);
+        float dw = (lambda - 555.0f) / 40.0f;
+        float pdf = (1.0f / (crange * PI * 40.0f)) / (1.0f + dw * dw);
+        float energy = (blackbody(lambda, LP.y) / pdf) * area * PI * LP.z;
+        float3 pos = emit_pos + emit_dir * 0.001f;
+        float3 dir = emit_dir;
+        bool caustic = false;
+        for (uint32_t depth = 0; depth < a.photon_max_bounces; ++depth) {
+            Ray ray{pos, dir, 0.0001f, 100.0f};
+            float t, hu, hv;
+            uint32_t prim;
+            ++n_rays;
+            if (!traverse<false, COUNT>(S, ray, stack_smem + threadIdx.x, PHOTON_BLOCK, t, prim, hu, hv, a.err, tc))
+                break;
+            Surface sf = surface_at(S, prim, hu, hv, dir);
+            float4 extra = S.materials[2 * sf.mat + 1];
+            float3 ffn = sf.front ? sf.wn : -sf.wn;
+            uint32_t type = (uint32_t)extra.x;
+            float3 hp = pos + dir * t;
+            if (type == 0u) {
+                if (caustic) {
+                    stored = true;
+                    out0 = f4(hp.x, hp.y, hp.z, lambda);
+                    out1 = f4(-dir.x, -dir.y, -dir.z, energy);
+                }
+                break;
+            } else if (type == 1u) {
+                dir = reflect(normalize(dir), ffn);
+                pos = hp + ffn * 0.001f;
+            } else if (type == 2u) {
+                float lum = lambda / 1000.0f;
+                float ir = extra.z + (extra.w / (lum * lum));
+                float ratio = sf.front ? 1.0f / ir : ir;
+                float3 ud = normalize(dir);
+                float ct = fminf(dot(-ud, ffn), 1.0f);
+                float st = sqrtf(1.0f - ct * ct);
+                if (ratio * st > 1.0f || schlick(ct, ratio) > rng_next(s)) {
+                    dir = reflect(ud, ffn);
+                } else {
+                    caustic = true;
+                    dir = refract(ud, ffn, ratio);
+                }
+                pos = hp + (dot(dir, ffn) > 0.0f ? ffn : -ffn) * 0.001f;
+            } else if (type == 4u) {
+                float3 ud = normalize(dir);
+                float ct = fminf(dot(-ud, ffn), 1.0f);
+                // select(n1 / n3, n3 / n1, is_front_face) with n1 = 1
+                float ratio = sf.front ? extra.w / 1.0f : 1.0f / extra.w;
+                float stt = ratio * ratio * (1.0f - ct * ct);
+                if (stt > 1.0f) {
+                    dir = reflect(ud, ffn);
+                } else {
+                    bool tir;
+                    float F = thin_film1(ct, 1.0f, extra.z, extra.w, fmaxf(extra.y, 50.0f), lambda, tir);
+                    dir = rng_next(s) < F ? reflect(ud, ffn) : refract(ud, ffn, ratio);
+                }
+                caustic = true;  // the position is not advanced (photon_emit.wgsl:291-326)
+            } else if (type == 5u) {
+                float3 ud = normalize(dir);
+                float ct = fminf(dot(-ud, ffn), 1.0f);
+                bool tir;
+                float F = thin_film1(ct, 1.0f, extra.z, extra.w, fmaxf(extra.y, 50.0f), lambda, tir);
+                if (rng_next(s) < F) {
+                    dir = reflect(ud, ffn);
+                    pos = hp + ffn * 0.001f;
+                    caustic = true;
+                } else {
+                    break;
+                }
+            } else {
+                break;
+            }
+        }
+    }
+    warp_add_u64(&a.stats->closest_rays, n_rays);
+    // block-ordered compaction: rank = stored photons of lower ids in the block
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, stored);
+    if (lane == 0) warp_cnt[warp] = __popc(m);
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < PHOTON_BLOCK / 32; ++w) {
+        if (w < warp) before += warp_cnt[w];
+        total += warp_cnt[w];
+    }
+    if (stored) {
+        uint32_t slot = blockIdx.x * PHOTON_BLOCK + before + __popc(m & ((1u << lane) - 1u));
+        a.ph.staging[2 * slot] = out0;
+        a.ph.staging[2 * slot + 1] = out1;
+    }
+    if (threadIdx.x == 0) a.ph.block_counts[blockIdx.x] = total;
+}
+
+// staging -> emission-ordered photon array (offsets already scanned)
+__global__ void k_photon_compact(FrameArgs a) {
+    uint32_t b = blockIdx.x;
+    uint32_t off = a.ph.block_counts[b];
+    uint32_t next = (b + 1 < a.ph.n_blocks) ? a.ph.block_counts[b + 1] : a.counters->photons_stored;
+    uint32_t cnt = next - off;
+    if (threadIdx.x < cnt) {
+        uint32_t src = b * PHOTON_BLOCK + threadIdx.x;
+        a.ph.photons[2 * (off + threadIdx.x)] = a.ph.staging[2 * src];
+        a.ph.photons[2 * (off + threadIdx.x) + 1] = a.ph.staging[2 * src + 1];
+    }
+    if (b == 0 && threadIdx.x == 0) atomicAdd(&a.stats->photons_stored, (unsigned long long)a.counters->photons_stored);
+}
+
+__global__ void k_grid_keys(const float4* __restrict__ photons, const uint32_t* n_dev, uint32_t n_host,
+                            const uint32_t* frame_dev, uint32_t frame_host, float cell, uint32_t hash_bits,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    uint32_t n = n_dev ? *n_dev : n_host;
+    uint32_t frame = frame_dev ? *frame_dev : frame_host;
+    float3 j = grid_jitter(frame, cell);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 p0 = photons[2 * i], p1 = photons[2 * i + 1];
+        keys[i] = p1.w == 0.0f ? (1u << hash_bits) : grid_hash(xyz(p0), j, cell, hash_bits);
+        vals[i] = i;
+    }
+}
+
+__global__ void k_grid_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                              const uint32_t* n_dev, uint32_t n_host, uint32_t hash_bits,
+                              const float4* __restrict__ photons, float4* __restrict__ sorted, uint2* __restrict__ ranges) {
+    uint32_t n = n_dev ? *n_dev : n_host;
+    uint32_t sentinel = 1u << hash_bits;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t h = keys[i];
+        uint32_t v = vals[i];
+        sorted[2 * i] = photons[2 * v];
+        sorted[2 * i + 1] = photons[2 * v + 1];
+        if (h >= sentinel) continue;
+        if (i == 0 || keys[i - 1] != h) ranges[h].x = i;
+        if (i + 1 == n || keys[i + 1] != h) ranges[h].y = i + 1;
+    }
+}
+
+// ------------------------------------------------------------------ camera paths
+__global__ void k_raygen(FrameArgs a) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t n = a.width * a.height;
+    if (p >= n) return;
+    const srt_camera_uniform& cam = *a.cam;
+    uint32_t x = p % a.width, y = p / a.width;
+    uint32_t s = pcg_hash(x + y * a.width + cam.frame_count * 927163u);
+    float3 o, d;
+    camera_ray(cam, x, y, a.width, a.height, s, o, d);
+    float4 wl = sample_hero(s);
+    a.pb.ray_o[p] = f4(o.x, o.y, o.z, 0.0001f);
+    a.pb.ray_d[p] = f4(d.x, d.y, d.z, 100.0f);
+    a.pb.thr[p] = splat4(1.0f);
+    a.pb.wl[p] = wl;
+    a.pb.rad[p] = splat4(0.0f);
+    a.pb.misc[p] = make_uint4(s, 0u, p, 0u);
+    a.pb.queue[0][p] = p;
+    if (p == 0) a.counters->paths[0] = n;
+}
+
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace(DevScene S, const uint32_t* __restrict__ queue,
+                                                       const uint32_t* __restrict__ count, const float4* __restrict__ ro,
+                                                       const float4* __restrict__ rd, float4* __restrict__ hit,
+                                                       const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
+                                                       float4* __restrict__ rad, uint32_t* err, DevStats* stats) {
+    extern __shared__ uint2 stack_smem[];
+    uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    uint32_t n = *count;
+    if (q >= n) return;
+    uint32_t id = queue ? queue[q] : q;
+    float4 o = ro[ANY ? q : id], d = rd[ANY ? q : id];
+    Ray ray{xyz(o), xyz(d), o.w, d.w};
+    float t = 0.f, u = 0.f, v = 0.f;
+    uint32_t prim;
+    TravCounters tc{&stats->nodes_visited, &stats->tris_tested};
+    bool h = traverse<ANY, COUNT>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    if (ANY) {
+        // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
+        if (!h) {
+            uint32_t pid = sh_id[q];
+            rad[pid] = rad[pid] + sh_c[q];
+        }
+    } else {
+        hit[id] = h ? f4(t, __uint_as_float(prim), u, v) : f4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+    }
+}
+
+struct LightSample {
+    float3 dir;
+    float dist, pdf;
+    float4 radiance;
+};
+
+// sample_random_light: shader.wgsl:477-528
+SRT_DEV LightSample sample_light(const DevScene& S, float3 hp, float4 wl, uint32_t& s) {
+    LightSample ls;
+    ls.pdf = 0.f;
+    uint32_t nl = S.n_lights;
+    if (nl == 0u) return ls;
+    uint32_t li = min(__float2uint_rz(rng_next(s) * (float)nl), nl - 1u);
+    float4 L0 = S.lights[4 * li], L1 = S.lights[4 * li + 1], L2 = S.lights[4 * li + 2], LP = S.lights[4 * li + 3];
+    float r1 = rng_next(s);
+    float r2 = rng_next(s);
+    float sr1 = sqrtf(r1);
+    float u = 1.0f - sr1, v = r2 * sr1, w = 1.0f - u - v;
+    float3 v0 = xyz(L0), v1 = xyz(L1), v2 = xyz(L2);
+    float3 p = v0 * u + v1 * v + v2 * w;
+    float3 c = cross(v1 - v0, v2 - v0);
+    float3 normal = normalize(c);
+    float area = length(c) * 0.5f;
+    float3 to = p - hp;
+    float d2 = dot(to, to);
+    float dist = sqrtf(d2);
+    float3 l = to / dist;
+    float cl = fmaxf(dot(normal, -l), 0.0f);
+    if (cl <= 0.0001f) return ls;
+    ls.dir = l;
+    ls.dist = dist;
+    ls.pdf = d2 / (area * (float)nl * cl);
+    ls.radiance = blackbody4(wl, LP.y) * LP.z;
+    return ls;
+}
+
+// One iteration of ray_color's bounce loop after the closest-hit query
+// (shader.wgsl:568-700).
+__global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bounce) {
+    uint32_t n = a.counters->paths[bounce];
+    if (blockIdx.x * blockDim.x >= n) return;
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevScene& S = a.scene;
+    bool valid = q < n;
+    bool alive = false, shadow = false;
+    uint32_t id = valid ? a.pb.queue[bounce & 1][q] : 0u;
+    float3 sh_o = f3(0.f, 0.f, 0.f), sh_d = f3(0.f, 0.f, 0.f);
+    float sh_tmax = 0.f;
+    float4 sh_c = splat4(0.f);
+    if (valid) {
+        float4 h = a.pb.hit[id];
+        uint32_t prim = __float_as_uint(h.y);
+        if (prim != MISS) {
+            float4 o4 = a.pb.ray_o[id], d4 = a.pb.ray_d[id];
+            float3 o = xyz(o4), d = xyz(d4);
+            float4 thr = a.pb.thr[id], wl = a.pb.wl[id], rad = a.pb.rad[id];
+            uint4 misc = a.pb.misc[id];
+            uint32_t s = misc.x, flags = misc.y;
+            Surface sf = surface_at(S, prim, h.z, h.w, d);
+            float4 color = S.materials[2 * sf.mat], extra = S.materials[2 * sf.mat + 1];
+            float3 ffn = sf.front ? sf.wn : -sf.wn;
+            uint32_t type = (uint32_t)extra.x;
+            if (type == 3u) {
+                if (!(flags & FLAG_CAUSTIC) && (sf.front || extra.y > 0.0f)) {
+                    float4 em = blackbody4(wl, color.x) * color.y;
+                    a.pb.rad[id] = rad + em * thr;
+                }
+            } else {
+                if (type == 0u) flags = (flags | FLAG_DIFFUSE) & ~FLAG_CAUSTIC;
+                else if (type == 2u && (flags & FLAG_DIFFUSE)) flags |= FLAG_CAUSTIC;
+                if (type == 0u) {
+                    float4 spec = rgb_to_spectrum4(xyz(color), wl);
+                    float3 hp = o + d * h.x;
+                    if (a.gather.enabled) {
+                        float4 gl = gather(a.gather, a.cam->frame_count, hp, ffn, wl);
+                        rad = rad + thr * (spec / PI) * gl;
+                    }
+                    LightSample ls = sample_light(S, hp, wl, s);
+                    if (ls.pdf > 0.0f) {
+                        float ct = fmaxf(dot(ffn, ls.dir), 0.0f);
+                        float bpdf = ct / PI;
+                        float mis = ls.pdf / (ls.pdf + bpdf);
+                        sh_c = thr * (spec / PI) * ls.radiance * ct * (mis / ls.pdf);
+                        sh_o = hp;
+                        sh_d = ls.dir;
+                        sh_tmax = ls.dist - 0.001f;
+                        shadow = true;
+                    }
+                    a.pb.rad[id] = rad;
+                }
+                Scatter sc = sample_bsdf(d, ffn, color, extra, sf.front, wl, thr, s);
+                if (!sc.absorbed) {
+                    thr = thr * sc.att;
+                    o = o + d * h.x;
+                    alive = true;
+                    if (bounce > 3u) {
+                        float p = max4(thr);
+                        if (rng_next(s) > p) alive = false;
+                        else thr = thr / p;
+                    }
+                    if (bounce + 1u >= a.max_depth) alive = false;
+                    if (alive) {
+                        a.pb.thr[id] = thr;
+                        a.pb.ray_o[id] = f4(o.x, o.y, o.z, 0.0001f);
+                        a.pb.ray_d[id] = f4(sc.dir.x, sc.dir.y, sc.dir.z, 100.0f);
+                        a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
+                    }
+                }
+            }
+        }
+    }
+    uint32_t slot = warp_push(alive, &a.counters->paths[bounce + 1]);
+    if (alive) a.pb.queue[(bounce + 1) & 1][slot] = id;
+    uint32_t sslot = warp_push(shadow, &a.counters->shadow[bounce]);
+    if (shadow) {
+        a.pb.sh_o[sslot] = f4(sh_o.x, sh_o.y, sh_o.z, 0.001f);
+        a.pb.sh_d[sslot] = f4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+        a.pb.sh_c[sslot] = sh_c;
+        a.pb.sh_id[sslot] = id;
+    }
+}
+
+// shader.wgsl:774-822: hero tuple -> XYZ / sum pdf -> linear sRGB ->
+// accumulate (reset at frame 0) -> mean -> Reinhard on luma -> RGBA8.
+__global__ void k_finalize(FrameArgs a) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.width * a.height) return;
+    float4 L = a.pb.rad[p], wl = a.pb.wl[p];
+    float3 c = f3(0.f, 0.f, 0.f);
+    c = c + sample_cie_xyz(wl.x) * L.x;
+    c = c + sample_cie_xyz(wl.y) * L.y;
+    c = c + sample_cie_xyz(wl.z) * L.z;
+    c = c + sample_cie_xyz(wl.w) * L.w;
+    c = c * (1.0f / hero_pdf_sum(wl));
+    float3 rgb = xyz_to_srgb(c);
+    uint32_t frame = a.cam->frame_count;
+    float4 acc = frame > 0u ? a.accum[p] : splat4(0.f);
+    acc = acc + f4(rgb.x, rgb.y, rgb.z, 1.0f);
+    a.accum[p] = acc;
+    if (a.accum64) {
+        double4 d = frame > 0u ? a.accum64[p] : make_double4(0, 0, 0, 0);
+        a.accum64[p] = make_double4(d.x + rgb.x, d.y + rgb.y, d.z + rgb.z, d.w + 1.0);
+    }
+    float3 fc = f3(fmaxf(acc.x / acc.w * 1.0f, 0.f), fmaxf(acc.y / acc.w * 1.0f, 0.f), fmaxf(acc.z / acc.w * 1.0f, 0.f));
+    float luma = fc.x * 0.2126f + fc.y * 0.7152f + fc.z * 0.0722f;
+    float mapped = luma / (luma + 1.0f);
+    if (luma > 0.00001f) fc = fc * (mapped / luma);
+    a.ldr[p] = make_uchar4((unsigned char)__float2uint_rn(clampf(fc.x, 0.f, 1.f) * 255.0f),
+                           (unsigned char)__float2uint_rn(clampf(fc.y, 0.f, 1.f) * 255.0f),
+                           (unsigned char)__float2uint_rn(clampf(fc.z, 0.f, 1.f) * 255.0f), 255);
+}
+
+__global__ void k_frame_stats(FrameArgs a) {
+    if (threadIdx.x != 0) return;
+    unsigned long long c = 0, s = 0;
+    for (uint32_t i = 0; i < a.max_depth; ++i) {
+        c += a.counters->paths[i];
+        s += a.counters->shadow[i];
+    }
+    a.stats->closest_rays += c;
+    a.stats->shadow_rays += s;
+    a.stats->paths += a.counters->paths[0];
+}
+
+// ------------------------------------------------------------------ batch / test kernels
+__global__ void k_gather_queries(GatherArgs g, uint32_t frame, const float* __restrict__ q, uint32_t n,
+                                 float4* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* a = q + 10 * i;
+    out[i] = gather(g, frame, f3(a[0], a[1], a[2]), f3(a[3], a[4], a[5]), f4(a[6], a[7], a[8], a[9]));
+}
+
+template <bool ANY>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const float4* __restrict__ rays, uint32_t n,
+                                                             float4* __restrict__ hits, uint32_t* err) {
+    extern __shared__ uint2 stack_smem[];
+    uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    if (i >= n) return;
+    float4 o = rays[2 * i], d = rays[2 * i + 1];
+    Ray ray{xyz(o), xyz(d), o.w, d.w};
+    float t = 0.f, u = 0.f, v = 0.f;
+    uint32_t prim;
+    TravCounters tc{nullptr, nullptr};
+    bool h = traverse<ANY, false>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    if (ANY) hits[i] = f4(h ? t : 0.f, __uint_as_float(h ? 0u : MISS), 0.f, 0.f);
+    else hits[i] = h ? f4(t, __uint_as_float(prim), u, v) : f4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+}
+
+__global__ void k_test_math(int op, uint32_t n, const void* __restrict__ in, void* __restrict__ out,
+                            const void* __restrict__ aux) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* fi = (const float*)in;
+    const uint32_t* ui = (const uint32_t*)in;
+    float* fo = (float*)out;
+    uint32_t* uo = (uint32_t*)out;
+    switch (op) {
+        case 0:
+            uo[i] = pcg_hash(ui[i]);
+            break;
+        case 1: {
+            float3 c = sample_cie_xyz(fi[i]);
+            fo[3 * i] = c.x;
+            fo[3 * i + 1] = c.y;
+            fo[3 * i + 2] = c.z;
+        } break;
+        case 2:
+            fo[i] = blackbody(fi[2 * i], fi[2 * i + 1]);
+            break;
+        case 3: {
+            const float* p = fi + 7 * i;
+            float4 r = rgb_to_spectrum4(f3(p[0], p[1], p[2]), f4(p[3], p[4], p[5], p[6]));
+            reinterpret_cast<float4*>(fo)[i] = r;
+        } break;
+        case 4: {
+            const float* p = fi + 9 * i;
+            reinterpret_cast<float4*>(fo)[i] = thin_film4(p[0], p[1], p[2], p[3], p[4], f4(p[5], p[6], p[7], p[8]));
+        } break;
+        case 5: {
+            uint32_t s = ui[i];
+            float4 w = sample_hero(s);
+            float* o = fo + 5 * i;
+            o[0] = w.x;
+            o[1] = w.y;
+            o[2] = w.z;
+            o[3] = w.w;
+            o[4] = hero_pdf_sum(w);
+        } break;
+        case 6: {
+            const float* p = fi + 24 * i;
+            uint32_t s = __float_as_uint(p[23]);
+            Scatter sc = sample_bsdf(f3(p[0], p[1], p[2]), f3(p[3], p[4], p[5]), f4(p[6], p[7], p[8], p[9]),
+                                     f4(p[10], p[11], p[12], p[13]), p[14] != 0.0f, f4(p[15], p[16], p[17], p[18]),
+                                     f4(p[19], p[20], p[21], p[22]), s);
+            float* o = fo + 10 * i;
+            o[0] = sc.dir.x;
+            o[1] = sc.dir.y;
+            o[2] = sc.dir.z;
+            o[3] = sc.att.x;
+            o[4] = sc.att.y;
+            o[5] = sc.att.z;
+            o[6] = sc.att.w;
+            o[7] = sc.absorbed ? 1.0f : 0.0f;
+            o[8] = __uint_as_float(s);
+            o[9] = 0.f;
+        } break;
+        case 7: {
+            const float* p = fi + 5 * i;
+            float3 j = grid_jitter(__float_as_uint(p[3]), p[4]);
+            uo[i] = grid_hash(f3(p[0], p[1], p[2]), j, p[4], 22);
+        } break;
+        case 8: {
+            const uint32_t* p = ui + 5 * i;
+            uint32_t s = p[4];
+            float3 o, d;
+            camera_ray(*(const srt_camera_uniform*)aux, p[0], p[1], p[2], p[3], s, o, d);
+            float* r = fo + 7 * i;
+            r[0] = o.x;
+            r[1] = o.y;
+            r[2] = o.z;
+            r[3] = d.x;
+            r[4] = d.y;
+            r[5] = d.z;
+            r[6] = __uint_as_float(s);
+        } break;
+        default:
+            break;
+    }
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
+    int launches = 0;
+    size_t smem = sizeof(uint2) * TRAV_STACK * PHOTON_BLOCK;
+    if (a.count_visits)
+        k_photon_trace<true><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+    else
+        k_photon_trace<false><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+    ++launches;
+    // exclusive scan of the block counts in place; total -> photons_stored
+    k_rs_rowscan<<<1, 1024, 0, st>>>(a.ph.block_counts, a.ph.n_blocks, &a.counters->photons_stored);
+    k_photon_compact<<<a.ph.n_blocks, PHOTON_BLOCK, 0, st>>>(a);
+    launches += 2;
+    uint32_t grid = 148 * 8;
+    k_grid_keys<<<grid, 256, 0, st>>>(a.ph.photons, &a.counters->photons_stored, 0,
+                                      &a.cam->frame_count, 0, a.gather.cell, a.gather.hash_bits, a.ph.keys, a.ph.vals);
+    ++launches;
+    launches += sort_pairs(a.ph.keys, a.ph.vals, a.ph.keys2, a.ph.vals2, a.ph.capacity, &a.counters->photons_stored, 0,
+                           (int)a.gather.hash_bits + 1, a.ph.sort_scratch, st, &a.ph.sorted_keys, &a.ph.sorted_vals);
+    cudaMemsetAsync(a.ph.ranges, 0, sizeof(uint2) << a.gather.hash_bits, st);
+    k_grid_ranges<<<grid, 256, 0, st>>>(a.ph.sorted_keys, a.ph.sorted_vals, &a.counters->photons_stored, 0,
+                                        a.gather.hash_bits, a.ph.photons, a.ph.sorted, a.ph.ranges);
+    ++launches;
+    return launches;
+}
+
+int launch_grid_build(const float4* photons, uint32_t n, uint32_t frame, float cell, uint32_t hash_bits,
+                      PhotonBuffers& ph, cudaStream_t st) {
+    int launches = 0;
+    uint32_t grid = 148 * 8;
+    k_grid_keys<<<grid, 256, 0, st>>>(photons, nullptr, n, nullptr, frame, cell, hash_bits, ph.keys, ph.vals);
+    ++launches;
+    launches += sort_pairs(ph.keys, ph.vals, ph.keys2, ph.vals2, n, nullptr, 0, (int)hash_bits + 1, ph.sort_scratch, st,
+                           &ph.sorted_keys, &ph.sorted_vals);
+    cudaMemsetAsync(ph.ranges, 0, sizeof(uint2) << hash_bits, st);
+    k_grid_ranges<<<grid, 256, 0, st>>>(ph.sorted_keys, ph.sorted_vals, nullptr, n, hash_bits, photons, ph.sorted,
+                                        ph.ranges);
+    ++launches;
+    return launches;
+}
+
+int launch_raygen(const FrameArgs& a, cudaStream_t st) {
+    k_raygen<<<blocks_for((uint64_t)a.width * a.height, 256), 256, 0, st>>>(a);
+    return 1;
+}
+
+int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage) {
+    int launches = 0;
+    uint32_t n = a.width * a.height;
+    uint32_t grid = blocks_for(n, TRACE_BLOCK);
+    size_t smem = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
+    if (stage == 0 || stage == 1) {
+        if (a.count_visits)
+            k_trace<false, true><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
+                                                                  &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
+                                                                  a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
+        else
+            k_trace<false, false><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
+                                                                   &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
+                                                                   a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
+        ++launches;
+    }
+    if (stage == 0 || stage == 2) {
+        k_shade<<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
+        ++launches;
+    }
+    if (stage == 0 || stage == 3) {
+        if (a.count_visits)
+            k_trace<true, true><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce], a.pb.sh_o,
+                                                                 a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad,
+                                                                 a.err, a.stats);
+        else
+            k_trace<true, false><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
+                                                                  a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
+                                                                  a.pb.rad, a.err, a.stats);
+        ++launches;
+    }
+    return launches;
+}
+
+int launch_finalize(const FrameArgs& a, cudaStream_t st) {
+    k_finalize<<<blocks_for((uint64_t)a.width * a.height, 256), 256, 0, st>>>(a);
+    return 1;
+}
+
+int launch_frame_stats(const FrameArgs& a, cudaStream_t st) {
+    k_frame_stats<<<1, 32, 0, st>>>(a);
+    return 1;
+}
+
+int launch_gather_queries(const GatherArgs& g, uint32_t frame, const float* queries, uint32_t n_q, float4* out,
+                          cudaStream_t st) {
+    if (n_q == 0) return 0;
+    k_gather_queries<<<blocks_for(n_q, 128), 128, 0, st>>>(g, frame, queries, n_q, out);
+    return 1;
+}
+
+int launch_trace_batch(const DevScene& s, const float4* rays, uint32_t n, float4* hits, int any_hit, uint32_t* err,
+                       cudaStream_t st) {
+    if (n == 0) return 0;
+    size_t smem = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
+    if (any_hit)
+        k_trace_batch<true><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
+    else
+        k_trace_batch<false><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
+    return 1;
+}
+
+int launch_test_math(int op, uint32_t n, const void* in, void* out, const void* aux, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_test_math<<<blocks_for(n, 128), 128, 0, st>>>(op, n, in, out, aux);
+    return 1;
+}
+
+}  // namespace srt

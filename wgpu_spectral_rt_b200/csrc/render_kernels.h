@@ -1,0 +1,101 @@
+// render_kernels.h — launch interface of the per-frame kernels
+// (render_kernels.cu).  Host code fills these argument blocks; every
+// launcher returns the number of kernels it launched.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace srt {
+
+constexpr int MAX_BOUNCES = 31;     // max_depth limit (queue counters per bounce)
+constexpr int PHOTON_BLOCK = 128;   // emitter ids per photon-trace block
+constexpr int TRACE_BLOCK = 128;
+
+// Device counters of one frame (zeroed at frame start).
+struct FrameCounters {
+    uint32_t paths[MAX_BOUNCES + 1];    // active paths entering bounce i
+    uint32_t shadow[MAX_BOUNCES + 1];   // shadow rays emitted at bounce i
+    uint32_t photons_stored;
+    uint32_t pad[3];
+};
+
+// Device statistics accumulated over frames (64-bit).
+struct DevStats {
+    unsigned long long closest_rays;
+    unsigned long long shadow_rays;
+    unsigned long long photons_stored;
+    unsigned long long nodes_visited;
+    unsigned long long tris_tested;
+    unsigned long long paths;
+    unsigned long long pad[2];
+};
+
+struct PathBuffers {
+    float4 *ray_o, *ray_d, *hit, *thr, *wl, *rad;
+    uint4* misc;  // rng, flags, pixel, pad
+    uint32_t* queue[2];
+    float4 *sh_o, *sh_d, *sh_c;
+    uint32_t* sh_id;
+};
+
+struct PhotonBuffers {
+    float4* staging;        // 2 per slot: PHOTON_BLOCK slots per block
+    uint32_t* block_counts; // per block; scanned in place into offsets
+    float4* photons;        // emission order, 2 per photon
+    float4* sorted;         // (hash, index) order, 2 per photon
+    uint32_t *keys, *vals, *keys2, *vals2;
+    uint32_t* sort_scratch;
+    uint2* ranges;          // 2^hash_bits (start, end)
+    uint32_t capacity;      // = photons per frame
+    uint32_t n_blocks;
+    // after a sort: which buffers hold the sorted keys / values
+    uint32_t *sorted_keys, *sorted_vals;
+};
+
+struct GatherArgs {
+    const float4* photons;  // sorted
+    const uint2* ranges;
+    uint32_t hash_bits;
+    uint32_t cap;
+    float cell, r0, rexp, spectral_radius, inv_norm_count;
+    int enabled;
+};
+
+struct FrameArgs {
+    DevScene scene;
+    const srt_camera_uniform* cam;  // device
+    uint32_t width, height;
+    uint32_t max_depth;
+    uint32_t photons_per_frame;
+    uint32_t photon_max_bounces;
+    FrameCounters* counters;
+    DevStats* stats;
+    uint32_t* err;
+    PathBuffers pb;
+    PhotonBuffers ph;
+    GatherArgs gather;
+    float4* accum;
+    double4* accum64;  // optional
+    uchar4* ldr;
+    int count_visits;
+    int block_size;
+};
+
+// Photon pass: trace, compaction, grid keys, radix sort, ranges.
+int launch_photon_pass(FrameArgs& a, cudaStream_t st);
+// Camera paths: raygen, then per bounce trace / shade / shadow; finalize.
+int launch_raygen(const FrameArgs& a, cudaStream_t st);
+int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage /* 0 all, 1 trace, 2 shade, 3 shadow */);
+int launch_finalize(const FrameArgs& a, cudaStream_t st);
+int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
+
+// Grid over a photon array already on the device (n on host).
+int launch_grid_build(const float4* photons, uint32_t n, uint32_t frame, float cell, uint32_t hash_bits,
+                      PhotonBuffers& ph, cudaStream_t st);
+int launch_gather_queries(const GatherArgs& g, uint32_t frame, const float* queries, uint32_t n_q, float4* out,
+                          cudaStream_t st);
+int launch_trace_batch(const DevScene& s, const float4* rays, uint32_t n, float4* hits, int any_hit, uint32_t* err,
+                       cudaStream_t st);
+int launch_test_math(int op, uint32_t n, const void* in, void* out, const void* aux, cudaStream_t st);
+
+}  // namespace srt
