@@ -1,0 +1,396 @@
+"""Benchmark of the spectral path-tracing hot path on B200.
+
+Workload (default): the plain method at scale — a level-8 displaced
+icosphere (1,310,720 triangles) plus 64 thin-film-coated GGX spheres
+(4,032 triangles each) in a lit room, 1920x1080, max depth 12, 4M photons
+per frame (2^22), 4 hero wavelengths, FP32 transport.  One step = one frame
+= one sample per pixel (photon emit -> grid -> wavefront camera paths ->
+accumulate + tonemap), so the default 64 steps are the 64-spp image.
+
+Metric: Mpaths/s (camera paths per second, whole job).  Mphotons/s and
+Mrays/s are reported beside it.
+
+  value       device time (CUDA events on the library's stream) of K frames
+              with every input resident in HBM
+  e2e         the same frames through the public C ABI with host buffers:
+              the camera uniform is copied from host memory and the RGBA8
+              image is read back to host memory every step
+  roofline    the closest-hit traversal kernel: algorithmic bytes per
+              launch (32 B ray + 16 B hit per ray, 80 B per BVH8 node
+              visited, 48 B per triangle tested; visit counts from a
+              counting build over the same frames) / its mean CUDA-event
+              duration, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C++ restatement of the reference shader
+              math, OpenMP over all host threads) on a bounded sample of the
+              same frame: a row subset and the matching share of photons
+
+Multi-GPU: the path does not shard across GPUs (one frame is one GPU's
+work); --gpus N under torchrun runs N replicas, each rendering its own
+sample stream (frame offset = rank * steps), value = all ranks' paths / the
+max over ranks of the timed region ("scaling": "weak").
+
+--impl reference times the reference's CPU implementation of the path — the
+oracle port (the reference itself is Rust + WGSL on a Vulkan ray-query
+device and cannot run here) — with all host threads, on the same workload
+and metric; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    # name: (preset, width, height, max_depth, photons per frame)
+    "config2": ("PRESET_CONFIG2", 1920, 1080, 12, 1 << 22),
+    "config1": ("PRESET_CONFIG1", 256, 256, 8, 1 << 18),
+}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_from_profile(name: str):
+    """DRAM bytes per launch of the traversal kernel from a committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{name}.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_launch"), d.get("note")
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_scene(srt, ctx, preset_name: str, seed: int = 0):
+    b = srt.SceneBuilder()
+    cam = b.add_preset(getattr(srt, preset_name), seed)
+    scene = b.build(ctx)
+    return b, scene, cam
+
+
+def cpu_baseline(srt, b, cam, w, h, params, seconds_target=15.0, threads=0):
+    """The CPU oracle on a bounded sample of one frame (row subset + the same share of photons)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import binding as orc  # the checker, used here as the timed CPU baseline
+
+    t0 = time.perf_counter()
+    o = orc.OracleScene(b.arrays())
+    build_s = time.perf_counter() - t0
+    pos, yaw, pitch = cam
+    u = srt.camera_uniform(pos, yaw, pitch, w / h, 0)
+    # calibrate on a tiny sample, then size the sample to ~seconds_target
+    stride = 64
+    frac = 1.0 / stride
+
+    def run(stride):
+        p = srt.Params.from_buffer_copy(params)
+        p.photon_norm_count = float(params.photons_per_frame)
+        p.photons_per_frame = max(1, int(params.photons_per_frame // stride))
+        t = time.perf_counter()
+        _, _, _, st = o.render_frame(u, w, h, p, row_stride=stride, row_phase=0, want_ldr=False, threads=threads)
+        return time.perf_counter() - t, st
+
+    dt, st = run(stride)
+    while dt < seconds_target / 4 and stride > 1:
+        stride = max(1, stride // 4)
+        dt, st = run(stride)
+    frac = 1.0 / stride
+    paths = int(st[0])
+    value = paths / dt / 1e6
+    o.close()
+    return {
+        "value": round(value, 4), "unit": "Mpaths/s", "cores": orc.max_threads() if threads <= 0 else threads,
+        "kind": "port",
+        "sample": (f"1/{stride} of the rows ({paths} paths) and 1/{stride} of the photons "
+                   f"({int(params.photons_per_frame // stride)}) of one {w}x{h} frame; {dt:.1f} s; "
+                   f"oracle scene build {build_s:.1f} s not timed"),
+        "rays_closest": int(st[1]), "rays_shadow": int(st[2]), "seconds": round(dt, 3), "fraction": frac,
+    }
+
+
+def run_reference(args, cfg, rank, world):
+    """--impl reference: the CPU port of the reference path, all host threads, rank 0 only."""
+    if rank != 0:
+        return 0
+    import wgpu_spectral_rt_b200 as srt
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import binding as orc
+
+    preset, w, h, depth, photons = cfg
+    b = srt.SceneBuilder()
+    cam = b.add_preset(getattr(srt, preset), 0)
+    o = orc.OracleScene(b.arrays())
+    params = srt.default_params(max_depth=depth, photons_per_frame=photons)
+    pos, yaw, pitch = cam
+    # each step: 1/stride of the rows and of the photons of frame k; stride sized so a step is ~1-2 s
+    stride = args.ref_stride
+    total_paths, t_total = 0, 0.0
+    for k in range(args.warmup + args.steps):
+        u = srt.camera_uniform(pos, yaw, pitch, w / h, k)
+        p = srt.Params.from_buffer_copy(params)
+        p.photon_norm_count = float(photons)
+        p.photons_per_frame = max(1, photons // stride)
+        t = time.perf_counter()
+        _, _, _, st = o.render_frame(u, w, h, p, row_stride=stride, row_phase=k % stride, want_ldr=False)
+        dt = time.perf_counter() - t
+        if k >= args.warmup:
+            total_paths += int(st[0])
+            t_total += dt
+    value = total_paths / t_total / 1e6
+    cores = orc.max_threads()
+    line = {
+        "metric": "Mpaths/s", "value": round(value, 4), "unit": "Mpaths/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t_total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene)",
+        "impl": "reference",
+        "config": {"workload": f"{args.config}: {w}x{h}, depth {depth}, {photons} photons/frame, 1 spp per step",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port",
+                         "sample": f"per step 1/{stride} of the rows and of the photons of one frame"},
+        "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    o.close()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="config2", choices=sorted(CONFIGS))
+    ap.add_argument("--width", type=int, default=0)
+    ap.add_argument("--height", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-stride", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-roofline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    preset, w, h, depth, photons = CONFIGS[args.config]
+    if args.width:
+        w = args.width
+    if args.height:
+        h = args.height
+    cfg = (preset, w, h, depth, photons)
+    if args.impl == "reference":
+        return run_reference(args, cfg, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import wgpu_spectral_rt_b200 as srt
+
+    stream = torch.cuda.Stream(device=local_rank)
+    ctx = srt.Context(local_rank, stream.cuda_stream)
+    b, scene, cam = build_scene(srt, ctx, preset)
+    info = scene.info()
+    pos, yaw, pitch = cam
+    params = srt.default_params(max_depth=depth, photons_per_frame=photons)
+    r = srt.Renderer(ctx, scene, w, h, params)
+    f0 = rank * (args.steps + args.warmup)
+
+    def cam_u(k):
+        return srt.camera_uniform(pos, yaw, pitch, w / h, f0 + k)
+
+    for k in range(args.warmup):
+        r.render(cam_u(k))
+    ctx.synchronize()
+    r.reset_stats()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        start.record(stream)
+        for k in range(args.steps):
+            r.render(cam_u(args.warmup + k))
+        end.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    st = r.stats()
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    paths_all = w * h * args.steps * world
+    value = paths_all / (ms_max * 1e-3) / 1e6
+    photons_all = photons * args.steps * world
+    rays_all = (st["rays_closest"] + st["rays_shadow"] + st["rays_photon"]) * world
+
+    # ---- end to end through the C ABI with host buffers (camera in, RGBA8 out)
+    import numpy as np
+
+    ldr = np.zeros((h, w, 4), np.uint8)
+    e2e_steps = 0 if args.no_e2e else max(8, args.steps // 4)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        r.render(cam_u(args.warmup + args.steps + k))
+        ldr[:] = r.read_ldr()
+    t1 = time.perf_counter()
+    te = torch.tensor([t1 - t0], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = w * h * e2e_steps * world / float(te.item()) / 1e6 if e2e_steps else None
+
+    # ---- roofline of the closest-hit traversal kernel: timing pass + counting pass
+    roof = None
+    if rank == 0 and not args.no_roofline:
+        rt = srt.Renderer(ctx, scene, w, h, srt.default_params(max_depth=depth, photons_per_frame=photons,
+                                                               flags=srt.FLAG_STAGE_TIMING))
+        rc = srt.Renderer(ctx, scene, w, h, srt.default_params(max_depth=depth, photons_per_frame=photons,
+                                                               flags=srt.FLAG_COUNT_VISITS))
+        nf = 4
+        for k in range(nf):
+            rt.render(cam_u(k))
+            rc.render(cam_u(k))
+        s1, s2 = rt.stats(), rc.stats()
+        launches = s1["launches_trace_closest"]
+        ms_launch = s1["ms_trace_closest"] / launches
+        rays = s2["rays_closest"]
+        alg_bytes = rays * (32 + 16) + s2["nodes_visited"][0] * 80 + s2["tris_tested"][0] * 48
+        bytes_launch = alg_bytes / launches
+        achieved = bytes_launch / (ms_launch * 1e-3) / 1e9
+        peak, peak_kind = _peaks()
+        traffic, tnote = _traffic_from_profile(f"trace_closest_{args.config}")
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "k_trace<closest> (trace_kernels.cu)",
+                "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                "bytes_per_launch": round(bytes_launch), "ms_per_launch": round(ms_launch, 4),
+                "nodes_per_ray": round(s2["nodes_visited"][0] / max(1, rays), 2),
+                "tris_per_ray": round(s2["tris_tested"][0] / max(1, rays), 2),
+                "stage_ms_per_frame": {k: round(s1[k] / nf, 3) for k in
+                                       ("ms_photon_pass", "ms_raygen", "ms_trace_closest", "ms_shade",
+                                        "ms_trace_shadow", "ms_finalize")}}
+        if traffic is not None:
+            roof["traffic_note"] = tnote
+        rt.close()
+        rc.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(srt, b, cam, w, h, params, seconds_target=args.cpu_seconds)
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": "Mpaths/s", "value": round(value, 3), "unit": "Mpaths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (procedural scene, seeded)",
+            "config": {"workload": (f"{args.config}: {info['triangles']} triangles, {w}x{h}, depth {depth}, "
+                                    f"{photons} photons/frame, 1 spp per step"),
+                       "l2": "inputs larger than L2 (per-frame working set > 1 GB: path state, photons, BVH)",
+                       "parallelism": f"replicas x{world}", "bvh_nodes": info["nodes"], "bvh_depth": info["depth"]},
+            "mphotons_per_s": round(photons_all / (ms_max * 1e-3) / 1e6, 2),
+            "mrays_per_s": round(rays_all / (ms_max * 1e-3) / 1e6, 2),
+            "rays_per_path": round((st["rays_closest"] + st["rays_shadow"]) / max(1, st["paths"]), 3),
+            "photons_stored_per_frame": round(st["photons_stored"] / max(1, st["frames"])),
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": 272,
+                    "d2h_bytes_per_step": w * h * 4, "steps": e2e_steps} if e2e_steps else None,
+            "gpu_launches": int(st["kernel_launches"]),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    scene.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -156,14 +156,14 @@ typedef struct srt_params {
 typedef struct srt_stats {
     uint64_t frames;
     uint64_t paths;             /* camera paths started */
-    uint64_t rays_closest;      /* closest-hit rays traced (camera + photon) */
-    uint64_t rays_shadow;       /* any-hit rays traced */
+    uint64_t rays_closest;      /* camera-path closest-hit rays */
+    uint64_t rays_shadow;       /* any-hit (shadow) rays */
+    uint64_t rays_photon;       /* photon-pass closest-hit rays */
     uint64_t photons_emitted;
     uint64_t photons_stored;
-    uint64_t nodes_visited;     /* SRT_FLAG_COUNT_VISITS only */
-    uint64_t tris_tested;       /* SRT_FLAG_COUNT_VISITS only */
-    double ms_photon_trace;     /* SRT_FLAG_STAGE_TIMING only: summed stage times */
-    double ms_photon_grid;
+    uint64_t nodes_visited[3];  /* SRT_FLAG_COUNT_VISITS only: camera closest, shadow, photon */
+    uint64_t tris_tested[3];    /* SRT_FLAG_COUNT_VISITS only: camera closest, shadow, photon */
+    double ms_photon_pass;      /* SRT_FLAG_STAGE_TIMING only: summed stage times */
     double ms_trace_closest;
     double ms_shade;
     double ms_trace_shadow;

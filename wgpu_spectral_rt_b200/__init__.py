@@ -76,9 +76,9 @@ class Params(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("frames", C.c_uint64), ("paths", C.c_uint64), ("rays_closest", C.c_uint64),
-                ("rays_shadow", C.c_uint64), ("photons_emitted", C.c_uint64), ("photons_stored", C.c_uint64),
-                ("nodes_visited", C.c_uint64), ("tris_tested", C.c_uint64), ("ms_photon_trace", C.c_double),
-                ("ms_photon_grid", C.c_double), ("ms_trace_closest", C.c_double), ("ms_shade", C.c_double),
+                ("rays_shadow", C.c_uint64), ("rays_photon", C.c_uint64), ("photons_emitted", C.c_uint64),
+                ("photons_stored", C.c_uint64), ("nodes_visited", C.c_uint64 * 3), ("tris_tested", C.c_uint64 * 3),
+                ("ms_photon_pass", C.c_double), ("ms_trace_closest", C.c_double), ("ms_shade", C.c_double),
                 ("ms_trace_shadow", C.c_double), ("ms_finalize", C.c_double), ("ms_raygen", C.c_double),
                 ("launches_trace_closest", C.c_uint64), ("kernel_launches", C.c_uint64)]
 
@@ -428,7 +428,8 @@ class Renderer:
     def stats(self) -> dict:
         s = Stats()
         _check(lib().srt_renderer_get_stats(self.h, C.byref(s)), self.ctx.h)
-        return {f: getattr(s, f) for f, _ in Stats._fields_}
+        return {f: (list(getattr(s, f)) if f in ("nodes_visited", "tris_tested") else getattr(s, f))
+                for f, _ in Stats._fields_}
 
     def reset_stats(self):
         _check(lib().srt_renderer_reset_stats(self.h), self.ctx.h)

@@ -27,6 +27,10 @@ LIB = PKG / "libsrt_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                      "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
+# Per-file extra flags.  The shading kernels round every multiply and add
+# separately (no FMA contraction), as the WGSL reference and the CPU oracle
+# do; the traversal keeps contraction for its slab tests.
+FILE_FLAGS = {"render_kernels.cu": ["-fmad=false"], "trace_kernels.cu": ["-fmad=true"]}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
              f"-I{INCLUDE}", f"-I{CSRC}", "-I/usr/local/cuda/include"]
 
@@ -61,7 +65,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     for src in sorted(CSRC.glob("*.cu")):
         obj = BUILD / (src.stem + ".o")
         if force or _stale(obj, src, deps):
-            jobs.append([_nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+            jobs.append([_nvcc(), *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)])
     for src in sorted(CSRC.glob("*.cpp")):
         obj = BUILD / (src.stem + ".o")
         if force or _stale(obj, src, deps):

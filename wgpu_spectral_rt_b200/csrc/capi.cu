@@ -736,12 +736,14 @@ extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
     out->paths = d.paths;
     out->rays_closest = d.closest_rays;
     out->rays_shadow = d.shadow_rays;
+    out->rays_photon = d.photon_rays;
     out->photons_emitted = r->photons_emitted;
     out->photons_stored = d.photons_stored;
-    out->nodes_visited = d.nodes_visited;
-    out->tris_tested = d.tris_tested;
-    out->ms_photon_trace = r->ms[0];
-    out->ms_photon_grid = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        out->nodes_visited[k] = d.nodes_visited[k];
+        out->tris_tested[k] = d.tris_tested[k];
+    }
+    out->ms_photon_pass = r->ms[0];
     out->ms_trace_closest = r->ms[2];
     out->ms_shade = r->ms[3];
     out->ms_trace_shadow = r->ms[4];

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(PHOTON_BLOCK) k_photon_trace(FrameArgs a) {
     bool stored = false;
     float4 out0 = splat4(0.f), out1 = splat4(0.f);
     uint32_t n_rays = 0;
-    TravCounters tc{&a.stats->nodes_visited, &a.stats->tris_tested};
+    TravCounters tc{&a.stats->nodes_visited[TRAV_PHOTON], &a.stats->tris_tested[TRAV_PHOTON]};
     if (e < a.photons_per_frame && S.n_lights > 0u) {
         uint32_t s = pcg_hash(e + frame * 927163u);
         uint32_t nl = S.n_lights;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(PHOTON_BLOCK) k_photon_trace(FrameArgs a) {
             }
         }
     }
-    warp_add_u64(&a.stats->closest_rays, n_rays);
+    warp_add_u64(&a.stats->photon_rays, n_rays);
     // block-ordered compaction: rank = stored photons of lower ids in the block
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t m = __ballot_sync(0xFFFFFFFFu, stored);
@@ -252,34 +252,6 @@ __global__ void k_raygen(FrameArgs a) {
     a.pb.misc[p] = make_uint4(s, 0u, p, 0u);
     a.pb.queue[0][p] = p;
     if (p == 0) a.counters->paths[0] = n;
-}
-
-template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_trace(DevScene S, const uint32_t* __restrict__ queue,
-                                                       const uint32_t* __restrict__ count, const float4* __restrict__ ro,
-                                                       const float4* __restrict__ rd, float4* __restrict__ hit,
-                                                       const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
-                                                       float4* __restrict__ rad, uint32_t* err, DevStats* stats) {
-    extern __shared__ uint2 stack_smem[];
-    uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
-    uint32_t n = *count;
-    if (q >= n) return;
-    uint32_t id = queue ? queue[q] : q;
-    float4 o = ro[ANY ? q : id], d = rd[ANY ? q : id];
-    Ray ray{xyz(o), xyz(d), o.w, d.w};
-    float t = 0.f, u = 0.f, v = 0.f;
-    uint32_t prim;
-    TravCounters tc{&stats->nodes_visited, &stats->tris_tested};
-    bool h = traverse<ANY, COUNT>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
-    if (ANY) {
-        // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
-        if (!h) {
-            uint32_t pid = sh_id[q];
-            rad[pid] = rad[pid] + sh_c[q];
-        }
-    } else {
-        hit[id] = h ? f4(t, __uint_as_float(prim), u, v) : f4(0.f, __uint_as_float(MISS), 0.f, 0.f);
-    }
 }
 
 struct LightSample {
@@ -455,22 +427,6 @@ __global__ void k_gather_queries(GatherArgs g, uint32_t frame, const float* __re
     out[i] = gather(g, frame, f3(a[0], a[1], a[2]), f3(a[3], a[4], a[5]), f4(a[6], a[7], a[8], a[9]));
 }
 
-template <bool ANY>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const float4* __restrict__ rays, uint32_t n,
-                                                             float4* __restrict__ hits, uint32_t* err) {
-    extern __shared__ uint2 stack_smem[];
-    uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
-    if (i >= n) return;
-    float4 o = rays[2 * i], d = rays[2 * i + 1];
-    Ray ray{xyz(o), xyz(d), o.w, d.w};
-    float t = 0.f, u = 0.f, v = 0.f;
-    uint32_t prim;
-    TravCounters tc{nullptr, nullptr};
-    bool h = traverse<ANY, false>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
-    if (ANY) hits[i] = f4(h ? t : 0.f, __uint_as_float(h ? 0u : MISS), 0.f, 0.f);
-    else hits[i] = h ? f4(t, __uint_as_float(prim), u, v) : f4(0.f, __uint_as_float(MISS), 0.f, 0.f);
-}
-
 __global__ void k_test_math(int op, uint32_t n, const void* __restrict__ in, void* __restrict__ out,
                             const void* __restrict__ aux) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -605,35 +561,13 @@ int launch_raygen(const FrameArgs& a, cudaStream_t st) {
 
 int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage) {
     int launches = 0;
-    uint32_t n = a.width * a.height;
-    uint32_t grid = blocks_for(n, TRACE_BLOCK);
-    size_t smem = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
-    if (stage == 0 || stage == 1) {
-        if (a.count_visits)
-            k_trace<false, true><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
-                                                                  &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
-                                                                  a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
-        else
-            k_trace<false, false><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
-                                                                   &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
-                                                                   a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
-        ++launches;
-    }
+    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
+    if (stage == 0 || stage == 1) launches += launch_trace_closest(a, bounce, st);
     if (stage == 0 || stage == 2) {
         k_shade<<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         ++launches;
     }
-    if (stage == 0 || stage == 3) {
-        if (a.count_visits)
-            k_trace<true, true><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce], a.pb.sh_o,
-                                                                 a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad,
-                                                                 a.err, a.stats);
-        else
-            k_trace<true, false><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
-                                                                  a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
-                                                                  a.pb.rad, a.err, a.stats);
-        ++launches;
-    }
+    if (stage == 0 || stage == 3) launches += launch_trace_shadow(a, bounce, st);
     return launches;
 }
 
@@ -651,17 +585,6 @@ int launch_gather_queries(const GatherArgs& g, uint32_t frame, const float* quer
                           cudaStream_t st) {
     if (n_q == 0) return 0;
     k_gather_queries<<<blocks_for(n_q, 128), 128, 0, st>>>(g, frame, queries, n_q, out);
-    return 1;
-}
-
-int launch_trace_batch(const DevScene& s, const float4* rays, uint32_t n, float4* hits, int any_hit, uint32_t* err,
-                       cudaStream_t st) {
-    if (n == 0) return 0;
-    size_t smem = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
-    if (any_hit)
-        k_trace_batch<true><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
-    else
-        k_trace_batch<false><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
     return 1;
 }
 

@@ -21,14 +21,16 @@ struct FrameCounters {
 
 // Device statistics accumulated over frames (64-bit).
 struct DevStats {
-    unsigned long long closest_rays;
+    unsigned long long closest_rays;   // camera-path closest-hit rays
     unsigned long long shadow_rays;
+    unsigned long long photon_rays;    // photon-pass closest-hit rays
     unsigned long long photons_stored;
-    unsigned long long nodes_visited;
-    unsigned long long tris_tested;
     unsigned long long paths;
-    unsigned long long pad[2];
+    unsigned long long nodes_visited[3];  // by ray kind: TRAV_CLOSEST, TRAV_SHADOW, TRAV_PHOTON
+    unsigned long long tris_tested[3];
 };
+
+constexpr int TRAV_CLOSEST = 0, TRAV_SHADOW = 1, TRAV_PHOTON = 2;
 
 struct PathBuffers {
     float4 *ray_o, *ray_d, *hit, *thr, *wl, *rad;
@@ -86,6 +88,8 @@ int launch_photon_pass(FrameArgs& a, cudaStream_t st);
 // Camera paths: raygen, then per bounce trace / shade / shadow; finalize.
 int launch_raygen(const FrameArgs& a, cudaStream_t st);
 int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage /* 0 all, 1 trace, 2 shade, 3 shadow */);
+int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st);  // trace_kernels.cu
+int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);   // trace_kernels.cu
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
 

@@ -1,0 +1,100 @@
+// trace_kernels.cu — closest-hit and any-hit wavefront kernels over the
+// compressed BVH8 (the ray queries of shader.wgsl:561-566 and :654-659).
+//
+// Kept in their own translation unit: the traversal is compiled with
+// multiply-add contraction (fast slab tests), while the shading kernels are
+// compiled without it so that they round like the CPU oracle.
+#include "render_kernels.h"
+
+namespace srt {
+
+namespace {
+
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace(DevScene S, const uint32_t* __restrict__ queue,
+                                                       const uint32_t* __restrict__ count, const float4* __restrict__ ro,
+                                                       const float4* __restrict__ rd, float4* __restrict__ hit,
+                                                       const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
+                                                       float4* __restrict__ rad, uint32_t* err, DevStats* stats) {
+    extern __shared__ uint2 stack_smem[];
+    uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    uint32_t n = *count;
+    if (q >= n) return;
+    uint32_t id = queue ? queue[q] : q;
+    float4 o = ro[ANY ? q : id], d = rd[ANY ? q : id];
+    Ray ray{xyz(o), xyz(d), o.w, d.w};
+    float t = 0.f, u = 0.f, v = 0.f;
+    uint32_t prim;
+    TravCounters tc{&stats->nodes_visited[ANY ? TRAV_SHADOW : TRAV_CLOSEST],
+                    &stats->tris_tested[ANY ? TRAV_SHADOW : TRAV_CLOSEST]};
+    bool h = traverse<ANY, COUNT>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    if (ANY) {
+        // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
+        if (!h) {
+            uint32_t pid = sh_id[q];
+            float4 c = sh_c[q], r = rad[pid];
+            rad[pid] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z), __fadd_rn(r.w, c.w));
+        }
+    } else {
+        hit[id] = h ? make_float4(t, __uint_as_float(prim), u, v) : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+    }
+}
+
+template <bool ANY>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const float4* __restrict__ rays, uint32_t n,
+                                                             float4* __restrict__ hits, uint32_t* err) {
+    extern __shared__ uint2 stack_smem[];
+    uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    if (i >= n) return;
+    float4 o = rays[2 * i], d = rays[2 * i + 1];
+    Ray ray{xyz(o), xyz(d), o.w, d.w};
+    float t = 0.f, u = 0.f, v = 0.f;
+    uint32_t prim;
+    TravCounters tc{nullptr, nullptr};
+    bool h = traverse<ANY, false>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    if (ANY) hits[i] = make_float4(h ? t : 0.f, __uint_as_float(h ? 0u : MISS), 0.f, 0.f);
+    else hits[i] = h ? make_float4(t, __uint_as_float(prim), u, v) : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
+constexpr size_t STACK_SMEM = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
+
+}  // namespace
+
+int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
+    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
+    if (a.count_visits)
+        k_trace<false, true><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, a.pb.queue[bounce & 1],
+                                                                    &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
+                                                                    a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
+    else
+        k_trace<false, false><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, a.pb.queue[bounce & 1],
+                                                                     &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
+                                                                     a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
+    return 1;
+}
+
+int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
+    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
+    if (a.count_visits)
+        k_trace<true, true><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
+                                                                   a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
+                                                                   a.pb.rad, a.err, a.stats);
+    else
+        k_trace<true, false><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
+                                                                    a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
+                                                                    a.pb.rad, a.err, a.stats);
+    return 1;
+}
+
+int launch_trace_batch(const DevScene& s, const float4* rays, uint32_t n, float4* hits, int any_hit, uint32_t* err,
+                       cudaStream_t st) {
+    if (n == 0) return 0;
+    if (any_hit)
+        k_trace_batch<true><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, STACK_SMEM, st>>>(s, rays, n, hits, err);
+    else
+        k_trace_batch<false><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, STACK_SMEM, st>>>(s, rays, n, hits, err);
+    return 1;
+}
+
+}  // namespace srt
