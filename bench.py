@@ -65,12 +65,13 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic_from_profile(name: str):
-    """DRAM bytes per launch of the traversal kernel from a committed ncu summary, if any."""
+def _traffic_from_profile(name: str, rays_per_launch: float):
+    """DRAM bytes per launch of the traversal kernel: the per-ray DRAM traffic of a
+    committed ncu capture scaled to this run's rays per launch (None without one)."""
     p = ROOT / "profiles" / f"{name}.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get("dram_bytes_per_launch"), d.get("note")
+        return round(d["dram_bytes_per_ray"] * rays_per_launch), d.get("note")
     return None, None
 
 
@@ -341,7 +342,7 @@ def main(argv=None):
         bytes_launch = alg_bytes / launches
         achieved = bytes_launch / (ms_launch * 1e-3) / 1e9
         peak, peak_kind = _peaks()
-        traffic, tnote = _traffic_from_profile(f"trace_closest_{args.config}")
+        traffic, tnote = _traffic_from_profile(f"trace_closest_{args.config}", rays / launches)
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": "k_trace<closest> (trace_kernels.cu)",
