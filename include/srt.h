@@ -37,7 +37,8 @@ typedef enum srt_status {
     SRT_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
     SRT_ERR_DEVICE_ASSERT = 5, /* a device-side check recorded an error */
     SRT_ERR_NO_DEVICE = 6,
-    SRT_ERR_UNSUPPORTED = 7
+    SRT_ERR_UNSUPPORTED = 7,
+    SRT_ERR_CAPACITY = 8       /* the request exceeds a fixed capacity of the library */
 } srt_status;
 
 /* ------------------------------------------------------------------------ */
@@ -318,6 +319,33 @@ srt_status srt_trace_rays(srt_scene* s, const srt_ray* rays, uint32_t n, srt_hit
  * Any output may be NULL. */
 srt_status srt_photon_grid_build(srt_ctx* ctx, const srt_photon* photons, uint32_t n, uint32_t frame_count,
                                  float cell_size, uint32_t hash_bits, uint64_t* keys_out, uint32_t* ranges_out);
+
+/* Photon hash grid that allocates nothing.  This entry point has no
+ * counterpart in the reference.
+ *
+ * Who it is for: callers that cannot call cudaMalloc, e.g. an engine or
+ * framework whose own pool allocator already owns the GPU's memory (an
+ * allocation behind its back can fail or fragment the pool), or a real-time
+ * frame loop that forbids allocation once it is running.
+ *
+ * It computes the same keys_out and ranges_out as srt_photon_grid_build, but
+ * every pointer is DEVICE memory owned by the caller (photons: n records;
+ * keys_out: n entries; ranges_out: 2 * 2^hash_bits entries; either output
+ * may be NULL) and the work is enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream) of the current device.  No context is needed.
+ * Temporary storage comes from one fixed __device__ array in the library
+ * (16.5 MiB, held by every GPU that loads the library until exit); n above
+ * SRT_GRID_NOALLOC_MAX_PHOTONS returns SRT_ERR_CAPACITY.
+ *
+ * The first call on a device looks up that array's device address (once per
+ * device, with the device current); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Asynchronous: synchronise `stream`
+ * before reading the outputs. */
+#define SRT_GRID_NOALLOC_MAX_PHOTONS (1u << 20)
+srt_status srt_photon_grid_build_noalloc(void* stream, const srt_photon* photons, uint32_t n, uint32_t frame_count,
+                                         float cell_size, uint32_t hash_bits, uint64_t* keys_out,
+                                         uint32_t* ranges_out);
 
 /* Density estimate at query points (gather_photons, shader.wgsl:297-342)
  * against a photon set: builds the grid then gathers.  query = n_q records

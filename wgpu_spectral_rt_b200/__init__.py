@@ -108,7 +108,7 @@ PRESET_CONFIG2 = 3
 PRESET_CAUSTIC_SLAB = 4
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
-          7: "UNSUPPORTED"}
+          7: "UNSUPPORTED", 8: "CAPACITY"}
 
 # Every exported entry point with (restype, argtypes).
 _P = C.c_void_p
@@ -159,6 +159,7 @@ SIGNATURES = {
     "srt_trace_rays": (_I, [_P, _P, _U32, _P, _I]),
     "srt_photon_grid_build": (_I, [_P, _P, _U32, _U32, _F, _U32, _P, _P]),
     "srt_photon_gather": (_I, [_P, _P, _U32, _P, _U32, _U32, C.POINTER(Params), _P]),
+    "srt_photon_grid_build_noalloc": (_I, [_P, _P, _U32, _U32, _F, _U32, _P, _P]),
     "srt_test_device_math": (_I, [_P, _I, _U32, _P, _P, _P]),
 }
 
