@@ -23,7 +23,8 @@ from pathlib import Path
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libsrt_b200.so"
+# SRT_LIB_PATH selects another build of the same library (e.g. a variant build)
+LIB_PATH = Path(os.environ["SRT_LIB_PATH"]) if os.environ.get("SRT_LIB_PATH") else _PKG / "libsrt_b200.so"
 
 # --------------------------------------------------------------------------- records
 

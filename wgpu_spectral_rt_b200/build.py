@@ -58,16 +58,23 @@ def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
     return src.stat().st_mtime > t or any(d.stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, out: Path | None = None, build_dir: Path | None = None,
+          defines: list[str] | None = None) -> Path:
+    """Compiles what changed and links the library.  `out`, `build_dir` and
+    `defines` (-D macros for every CUDA file) produce a variant build beside
+    the default one (used to compare kernel configurations)."""
+    lib = Path(out) if out else LIB
+    bdir = Path(build_dir) if build_dir else BUILD
+    dflags = [f"-D{d}" for d in (defines or [])]
+    bdir.mkdir(parents=True, exist_ok=True)
     deps = _headers()
     jobs = []
     for src in sorted(CSRC.glob("*.cu")):
-        obj = BUILD / (src.stem + ".o")
+        obj = bdir / (src.stem + ".o")
         if force or _stale(obj, src, deps):
-            jobs.append([_nvcc(), *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)])
+            jobs.append([_nvcc(), *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), *dflags, "-c", str(src), "-o", str(obj)])
     for src in sorted(CSRC.glob("*.cpp")):
-        obj = BUILD / (src.stem + ".o")
+        obj = bdir / (src.stem + ".o")
         if force or _stale(obj, src, deps):
             jobs.append([_cxx(), *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
 
@@ -82,20 +89,23 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
     with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
         list(ex.map(run, jobs))
-    objs = sorted(BUILD.glob("*.o"))
-    if jobs or force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    objs = sorted(bdir.glob("*.o"))
+    if jobs or force or not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        tmp = lib.with_suffix(".so.tmp")
         run([_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("-v", "--verbose", action="store_true")
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--out", type=Path, default=None, help="library path (default: the package's libsrt_b200.so)")
+    ap.add_argument("--build-dir", type=Path, default=None)
+    ap.add_argument("-D", dest="defines", action="append", default=[], help="macro for every CUDA source")
     a = ap.parse_args(argv)
-    print(build(a.verbose, a.force))
+    print(build(a.verbose, a.force, a.out, a.build_dir, a.defines))
     return 0
 
 

@@ -379,6 +379,7 @@ extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt
     d.tris = s->bvh.tris;
     d.n_nodes = s->bvh.n_nodes;
     d.n_tris = (uint32_t)total;
+    d.depth = s->bvh.depth;
     *out = s.release();
     return SRT_OK;
 }

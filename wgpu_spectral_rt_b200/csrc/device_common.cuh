@@ -20,7 +20,8 @@ constexpr float LAMBDA_MIN = 380.0f;  // shader.wgsl:81-83
 constexpr float LAMBDA_MAX = 780.0f;
 constexpr float LAMBDA_RANGE = LAMBDA_MAX - LAMBDA_MIN;
 constexpr uint32_t MISS = 0xFFFFFFFFu;
-constexpr int TRAV_STACK = 32;  // BVH8 traversal stack entries per thread
+constexpr int TRAV_STACK = 32;        // BVH8 traversal stack entries per thread (deepest supported tree)
+constexpr int TRAV_STACK_SMALL = 16;  // stack for trees of at most 16 levels (less shared memory, more warps)
 
 // Device error word bits (read back by the host after synchronising).
 constexpr uint32_t ERR_STACK_OVERFLOW = 0x1u;
@@ -68,6 +69,7 @@ struct DevScene {
     const TriSlot* tris;
     uint32_t n_nodes;
     uint32_t n_tris;
+    uint32_t depth;  // 8-wide levels: a traversal stack needs at least this many entries
 };
 
 // ------------------------------------------------------------------ vector helpers
@@ -448,6 +450,12 @@ SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3
 }
 
 SRT_DEV uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xFFu; }
+// Byte k of w as a float, without the integer-to-float conversion unit: one
+// byte permute builds the bit pattern 0x4B0000bb (= 2^23 + b exactly) and one
+// subtraction removes 2^23.
+SRT_DEV float qbyte(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
+}
 
 struct TravCounters {
     unsigned long long* nodes;
@@ -460,8 +468,9 @@ struct TravCounters {
 // imask (bits 0..7); triangle hits go straight to the triangle loop.
 // ANY: return at the first hit in [tmin, tmax].  Closest: lexicographic
 // minimum of (t, flattened triangle id), independent of traversal order.
-// `stack` is this thread's slice of shared memory, stride `stride` entries.
-template <bool ANY, bool COUNT>
+// `stack` is this thread's slice of shared memory, stride `stride` entries,
+// STACK entries deep (at least the tree depth: one entry per level).
+template <bool ANY, bool COUNT, int STACK = TRAV_STACK>
 SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, float& t_out, uint32_t& prim_out,
                       float& u_out, float& v_out, uint32_t* err, TravCounters cnt) {
     prim_out = MISS;
@@ -526,7 +535,7 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
         uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
         uint32_t idx = g.x + __popc(g.y & ((1u << slot) - 1u) & 0xFFu);
         if (g.y & 0xFF000000u) {
-            if (sp >= TRAV_STACK) {
+            if (sp >= STACK) {
                 atomicOr(err, ERR_STACK_OVERFLOW);
                 break;
             }
@@ -559,14 +568,14 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
         uint32_t hits = 0u;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            int k = i & 3;
+            const uint32_t k = (uint32_t)(i & 3);
             uint32_t m = byte_of(i < 4 ? meta0 : meta1, k);
-            float tnx = (float)byte_of(i < 4 ? nx0 : nx1, k) * ax + bx;
-            float tny = (float)byte_of(i < 4 ? ny0 : ny1, k) * ay + by;
-            float tnz = (float)byte_of(i < 4 ? nz0 : nz1, k) * az + bz;
-            float tfx = (float)byte_of(i < 4 ? fx0 : fx1, k) * ax + bx;
-            float tfy = (float)byte_of(i < 4 ? fy0 : fy1, k) * ay + by;
-            float tfz = (float)byte_of(i < 4 ? fz0 : fz1, k) * az + bz;
+            float tnx = qbyte(i < 4 ? nx0 : nx1, k) * ax + bx;
+            float tny = qbyte(i < 4 ? ny0 : ny1, k) * ay + by;
+            float tnz = qbyte(i < 4 ? nz0 : nz1, k) * az + bz;
+            float tfx = qbyte(i < 4 ? fx0 : fx1, k) * ax + bx;
+            float tfy = qbyte(i < 4 ? fy0 : fy1, k) * ay + by;
+            float tfz = qbyte(i < 4 ? fz0 : fz1, k) * az + bz;
             float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
             float tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest)) * robust;
             if (m != 0u && tn <= tf) {

@@ -67,8 +67,11 @@ SRT_DEV float4 gather(const GatherArgs& g, uint32_t frame, float3 hit_pos, float
 }
 
 // ------------------------------------------------------------------ photon pass
-template <bool COUNT>
-__global__ void __launch_bounds__(PHOTON_BLOCK) k_photon_trace(FrameArgs a) {
+#ifndef SRT_PHOTON_MIN_BLOCKS
+#define SRT_PHOTON_MIN_BLOCKS 1
+#endif
+template <bool COUNT, int STACK>
+__global__ void __launch_bounds__(PHOTON_BLOCK, SRT_PHOTON_MIN_BLOCKS) k_photon_trace(FrameArgs a) {
     extern __shared__ uint2 stack_smem[];
     __shared__ uint32_t warp_cnt[PHOTON_BLOCK / 32];
     const DevScene& S = a.scene;
@@ -108,7 +111,8 @@ __global__ void __launch_bounds__(PHOTON_BLOCK) k_photon_trace(FrameArgs a) {
             float t, hu, hv;
             uint32_t prim;
             ++n_rays;
-            if (!traverse<false, COUNT>(S, ray, stack_smem + threadIdx.x, PHOTON_BLOCK, t, prim, hu, hv, a.err, tc))
+            if (!traverse<false, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, PHOTON_BLOCK, t, prim, hu, hv, a.err,
+                                               tc))
                 break;
             Surface sf = surface_at(S, prim, hu, hv, dir);
             float4 extra = S.materials[2 * sf.mat + 1];
@@ -516,11 +520,15 @@ inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 
 // ------------------------------------------------------------------ launchers
 int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
     int launches = 0;
-    size_t smem = sizeof(uint2) * TRAV_STACK * PHOTON_BLOCK;
-    if (a.count_visits)
-        k_photon_trace<true><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
-    else
-        k_photon_trace<false><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+    bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
+    size_t smem = sizeof(uint2) * (small ? TRAV_STACK_SMALL : TRAV_STACK) * PHOTON_BLOCK;
+    if (a.count_visits) {
+        if (small) k_photon_trace<true, TRAV_STACK_SMALL><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+        else k_photon_trace<true, TRAV_STACK><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+    } else {
+        if (small) k_photon_trace<false, TRAV_STACK_SMALL><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+        else k_photon_trace<false, TRAV_STACK><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
+    }
     ++launches;
     // exclusive scan of the block counts in place; total -> photons_stored
     k_rs_rowscan<<<1, 1024, 0, st>>>(a.ph.block_counts, a.ph.n_blocks, &a.counters->photons_stored);

@@ -4,18 +4,28 @@
 // Kept in their own translation unit: the traversal is compiled with
 // multiply-add contraction (fast slab tests), while the shading kernels are
 // compiled without it so that they round like the CPU oracle.
+//
+// The shared-memory stack is sized to the tree: STACK = 16 entries for trees
+// of at most 16 levels (config 2 builds 10), 32 otherwise.
 #include "render_kernels.h"
+
+// 8 resident blocks of 128 threads per SM caps the kernels at 64 registers:
+// the unbounded build takes ~110 and halves the warps in flight (measured:
+// 8.7 ms vs 6.1 ms of closest-hit traversal per config-2 frame).
+#ifndef SRT_TRACE_MIN_BLOCKS
+#define SRT_TRACE_MIN_BLOCKS 8
+#endif
 
 namespace srt {
 
 namespace {
 
-template <bool ANY, bool COUNT>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_trace(DevScene S, const uint32_t* __restrict__ queue,
-                                                       const uint32_t* __restrict__ count, const float4* __restrict__ ro,
-                                                       const float4* __restrict__ rd, float4* __restrict__ hit,
-                                                       const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
-                                                       float4* __restrict__ rad, uint32_t* err, DevStats* stats) {
+template <bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+    k_trace(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
+            const float4* __restrict__ ro, const float4* __restrict__ rd, float4* __restrict__ hit,
+            const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c, float4* __restrict__ rad,
+            uint32_t* err, DevStats* stats) {
     extern __shared__ uint2 stack_smem[];
     uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t n = *count;
@@ -27,7 +37,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(DevScene S, const uint32_
     uint32_t prim;
     TravCounters tc{&stats->nodes_visited[ANY ? TRAV_SHADOW : TRAV_CLOSEST],
                     &stats->tris_tested[ANY ? TRAV_SHADOW : TRAV_CLOSEST]};
-    bool h = traverse<ANY, COUNT>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    bool h = traverse<ANY, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
     if (ANY) {
         // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
         if (!h) {
@@ -57,43 +67,54 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const f
 }
 
 inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
-constexpr size_t STACK_SMEM = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
+
+template <bool ANY, bool COUNT, int STACK>
+void launch_k_trace(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
+    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
+    size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
+    if (ANY)
+        k_trace<true, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
+                                                                     a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id,
+                                                                     a.pb.sh_c, a.pb.rad, a.err, a.stats);
+    else
+        k_trace<false, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
+                                                                      &a.counters->paths[bounce], a.pb.ray_o,
+                                                                      a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr,
+                                                                      a.err, a.stats);
+}
+
+template <bool ANY>
+void launch_trace_kind(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
+    bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
+    if (a.count_visits) {
+        if (small) launch_k_trace<ANY, true, TRAV_STACK_SMALL>(a, bounce, st);
+        else launch_k_trace<ANY, true, TRAV_STACK>(a, bounce, st);
+    } else {
+        if (small) launch_k_trace<ANY, false, TRAV_STACK_SMALL>(a, bounce, st);
+        else launch_k_trace<ANY, false, TRAV_STACK>(a, bounce, st);
+    }
+}
 
 }  // namespace
 
 int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
-    if (a.count_visits)
-        k_trace<false, true><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, a.pb.queue[bounce & 1],
-                                                                    &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
-                                                                    a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
-    else
-        k_trace<false, false><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, a.pb.queue[bounce & 1],
-                                                                     &a.counters->paths[bounce], a.pb.ray_o, a.pb.ray_d,
-                                                                     a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats);
+    launch_trace_kind<false>(a, bounce, st);
     return 1;
 }
 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
-    if (a.count_visits)
-        k_trace<true, true><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
-                                                                   a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
-                                                                   a.pb.rad, a.err, a.stats);
-    else
-        k_trace<true, false><<<grid, TRACE_BLOCK, STACK_SMEM, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
-                                                                    a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c,
-                                                                    a.pb.rad, a.err, a.stats);
+    launch_trace_kind<true>(a, bounce, st);
     return 1;
 }
 
 int launch_trace_batch(const DevScene& s, const float4* rays, uint32_t n, float4* hits, int any_hit, uint32_t* err,
                        cudaStream_t st) {
     if (n == 0) return 0;
+    size_t smem = sizeof(uint2) * TRAV_STACK * TRACE_BLOCK;
     if (any_hit)
-        k_trace_batch<true><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, STACK_SMEM, st>>>(s, rays, n, hits, err);
+        k_trace_batch<true><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
     else
-        k_trace_batch<false><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, STACK_SMEM, st>>>(s, rays, n, hits, err);
+        k_trace_batch<false><<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(s, rays, n, hits, err);
     return 1;
 }
 
