@@ -446,7 +446,8 @@ struct srt_renderer {
         cudaFree(stats);
         cudaFree(err);
         void* bufs[] = {pb.ray_o, pb.ray_d, pb.hit, pb.thr, pb.wl, pb.rad, pb.misc, pb.queue[0], pb.queue[1],
-                        pb.sh_o, pb.sh_d, pb.sh_c, pb.sh_id, ph.staging, ph.block_counts, ph.photons, ph.sorted,
+                        pb.sh_o, pb.sh_d, pb.sh_c, pb.sh_id, ph.ray_o, ph.ray_d, ph.state, ph.hit, ph.flags,
+                        ph.queue[0], ph.queue[1], ph.staging, ph.block_counts, ph.photons, ph.sorted,
                         ph.keys, ph.vals, ph.keys2, ph.vals2, ph.sort_scratch, ph.ranges, accum, accum64, ldr};
         for (void* b : bufs) cudaFree(b);
     }
@@ -461,8 +462,8 @@ struct srt_renderer {
         };
         cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
         mark();  // 0
-        if (p.photons_per_frame > 0) {
-            // the trace kernel is the first launch of the photon pass
+        if (p.photons_per_frame > 0 && scene->n_lights > 0) {
+            // without lights the reference emits nothing (photon_emit.wgsl:161-162); the grid stays empty
             FrameArgs& a = args;
             n += launch_photon_pass(a, st);
         }
@@ -509,8 +510,9 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     if (p.max_depth == 0 || p.max_depth > (uint32_t)MAX_BOUNCES) return fail(c, SRT_ERR_INVALID_ARG, "max_depth must be 1..31");
     if (p.hash_bits < 4 || p.hash_bits > 26) return fail(c, SRT_ERR_INVALID_ARG, "hash_bits must be 4..26");
     if (p.photons_per_frame > (1u << 26)) return fail(c, SRT_ERR_INVALID_ARG, "photons_per_frame above 2^26");
-    if (!(p.cell_size > 0.f) || !(p.gather_radius0 > 0.f) || !(p.spectral_radius > 0.f) || p.photon_max_bounces > 64)
-        return fail(c, SRT_ERR_INVALID_ARG, "invalid photon parameters");
+    if (!(p.cell_size > 0.f) || !(p.gather_radius0 > 0.f) || !(p.spectral_radius > 0.f) ||
+        p.photon_max_bounces > (uint32_t)MAX_PHOTON_BOUNCES)
+        return fail(c, SRT_ERR_INVALID_ARG, "invalid photon parameters (photon_max_bounces must be <= 16)");
     if ((uint64_t)w * h > (1ull << 28)) return fail(c, SRT_ERR_INVALID_ARG, "viewport too large");
     cudaSetDevice(c->device);
     std::unique_ptr<srt_renderer> r(new (std::nothrow) srt_renderer());
@@ -556,7 +558,16 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     ph.capacity = cap;
     ph.n_blocks = (cap + PHOTON_BLOCK - 1) / PHOTON_BLOCK;
     if (cap > 0) {
-        CUDA_TRY(c, dev_alloc(&ph.staging, 2ull * ph.n_blocks * PHOTON_BLOCK));
+        size_t slots = (size_t)ph.n_blocks * PHOTON_BLOCK;
+        CUDA_TRY(c, dev_alloc(&ph.ray_o, slots));
+        CUDA_TRY(c, dev_alloc(&ph.ray_d, slots));
+        CUDA_TRY(c, dev_alloc(&ph.state, slots));
+        CUDA_TRY(c, dev_alloc(&ph.hit, slots));
+        CUDA_TRY(c, dev_alloc(&ph.flags, slots));
+        CUDA_TRY(c, cudaMemset(ph.flags, 0, slots));
+        CUDA_TRY(c, dev_alloc(&ph.queue[0], slots));
+        CUDA_TRY(c, dev_alloc(&ph.queue[1], slots));
+        CUDA_TRY(c, dev_alloc(&ph.staging, 2ull * slots));
         CUDA_TRY(c, dev_alloc(&ph.block_counts, ph.n_blocks));
         CUDA_TRY(c, dev_alloc(&ph.photons, 2ull * cap));
         CUDA_TRY(c, dev_alloc(&ph.sorted, 2ull * cap));

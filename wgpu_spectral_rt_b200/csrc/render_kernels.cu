@@ -1,10 +1,10 @@
 // render_kernels.cu — per-frame kernels of the spectral path tracer.
 //
 // One frame = one sample per pixel (src/renderer/mod.rs:168-207):
-//   photon pass   photon_emit.wgsl:154-331 (one thread per emitted photon,
-//                 inline BVH8 traversal, block-ordered compaction so the
-//                 stored photons keep emission order) and the grid
-//                 (build_grid.wgsl:25-73) as cell keys + radix sort + ranges
+//   photon pass   photon_emit.wgsl:154-331 as a wavefront (emit, direction
+//                 sort, per bounce trace + shade, emitter-ordered compaction
+//                 of the stored photons) and the grid (build_grid.wgsl:25-73)
+//                 as cell keys + radix sort + ranges
 //   camera paths  shader.wgsl:708-823 as a wavefront: raygen, then per
 //                 bounce trace_closest -> shade -> trace_shadow over SoA
 //                 queues compacted with warp ballots; finalize converts the
@@ -29,12 +29,6 @@ SRT_DEV uint32_t warp_push(bool pred, uint32_t* counter) {
         base = __shfl_sync(0xFFFFFFFFu, base, leader);
     }
     return base + __popc(mask & ((1u << lane) - 1u));
-}
-
-SRT_DEV void warp_add_u64(unsigned long long* dst, uint32_t v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, (unsigned long long)v);
 }
 
 // gather_photons: shader.wgsl:297-342 over a sorted range; the walk goes
@@ -67,82 +61,120 @@ SRT_DEV float4 gather(const GatherArgs& g, uint32_t frame, float3 hit_pos, float
 }
 
 // ------------------------------------------------------------------ photon pass
-#ifndef SRT_PHOTON_MIN_BLOCKS
-#define SRT_PHOTON_MIN_BLOCKS 1
-#endif
-template <bool COUNT, int STACK>
-__global__ void __launch_bounds__(PHOTON_BLOCK, SRT_PHOTON_MIN_BLOCKS) k_photon_trace(FrameArgs a) {
-    extern __shared__ uint2 stack_smem[];
-    __shared__ uint32_t warp_cnt[PHOTON_BLOCK / 32];
+// The photon pass of photon_emit.wgsl:154-331 as a wavefront: emit every
+// photon path (one thread per emitter id), sort the emitted rays by an
+// octahedral direction key so that a warp traces rays of similar direction,
+// then per bounce: the shared closest-hit kernel over the live queue and a
+// shading kernel for the photon's material logic.  A stored photon lands in
+// its emitter's slot and is flagged; an emitter-ordered compaction afterwards
+// reproduces the order a sequential run of the reference's atomicAdd gives.
+
+// Octahedral 12+12-bit direction code, Morton-interleaved (24 bits).
+SRT_DEV uint32_t dir_key(float3 d) {
+    float s = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+    float px = d.x / s, py = d.y / s;
+    if (d.z < 0.0f) {
+        float qx = (1.0f - fabsf(py)) * (px >= 0.0f ? 1.0f : -1.0f);
+        float qy = (1.0f - fabsf(px)) * (py >= 0.0f ? 1.0f : -1.0f);
+        px = qx;
+        py = qy;
+    }
+    uint32_t ux = (uint32_t)fminf(fmaxf((px * 0.5f + 0.5f) * 4096.0f, 0.0f), 4095.0f);
+    uint32_t uy = (uint32_t)fminf(fmaxf((py * 0.5f + 0.5f) * 4096.0f, 0.0f), 4095.0f);
+    uint32_t k = 0;
+#pragma unroll
+    for (int b = 0; b < 12; ++b) k |= (((ux >> b) & 1u) << (2 * b)) | (((uy >> b) & 1u) << (2 * b + 1));
+    return k;
+}
+
+constexpr uint32_t PH_CAUSTIC = 0x1u;
+
+// Emission: photon_emit.wgsl:159-214.
+__global__ void k_photon_emit(FrameArgs a) {
+    uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.photons_per_frame) return;
     const DevScene& S = a.scene;
-    uint32_t e = blockIdx.x * PHOTON_BLOCK + threadIdx.x;
     uint32_t frame = a.cam->frame_count;
-    bool stored = false;
-    float4 out0 = splat4(0.f), out1 = splat4(0.f);
-    uint32_t n_rays = 0;
-    TravCounters tc{&a.stats->nodes_visited[TRAV_PHOTON], &a.stats->tris_tested[TRAV_PHOTON]};
-    if (e < a.photons_per_frame && S.n_lights > 0u) {
-        uint32_t s = pcg_hash(e + frame * 927163u);
-        uint32_t nl = S.n_lights;
-        uint32_t li = min(__float2uint_rz(rng_next(s) * (float)nl), nl - 1u);
-        float4 L0 = S.lights[4 * li], L1 = S.lights[4 * li + 1], L2 = S.lights[4 * li + 2],
-               LP = S.lights[4 * li + 3];
-        float3 v0 = xyz(L0), v1 = xyz(L1), v2 = xyz(L2);
-        float3 c = cross(v1 - v0, v2 - v0);
-        float3 normal = normalize(c);
-        float area = length(c) * 0.5f;
-        float r1 = rng_next(s);
-        float r2 = rng_next(s);
-        float sr1 = sqrtf(r1);
-        float u = 1.0f - sr1, v = r2 * sr1, w = 1.0f - u - v;
-        float3 emit_pos = v0 * u + v1 * v + v2 * w;
-        float3 emit_dir = normalize(normal + random_unit_vector(s));
-        float cmin = cauchy_cdf(LAMBDA_MIN), cmax = cauchy_cdf(LAMBDA_MAX), crange = cmax - cmin;
-        float lambda = clampf(555.0f + 40.0f * tanf(PI * ((cmin + rng_next(s) * crange) - 0.5f)), LAMBDA_MIN,
-                              LAMBDA_MAX);
-        float dw = (lambda - 555.0f) / 40.0f;
-        float pdf = (1.0f / (crange * PI * 40.0f)) / (1.0f + dw * dw);
-        float energy = (blackbody(lambda, LP.y) / pdf) * area * PI * LP.z;
-        float3 pos = emit_pos + emit_dir * 0.001f;
-        float3 dir = emit_dir;
-        bool caustic = false;
-        for (uint32_t depth = 0; depth < a.photon_max_bounces; ++depth) {
-            Ray ray{pos, dir, 0.0001f, 100.0f};
-            float t, hu, hv;
-            uint32_t prim;
-            ++n_rays;
-            if (!traverse<false, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, PHOTON_BLOCK, t, prim, hu, hv, a.err,
-                                               tc))
-                break;
-            Surface sf = surface_at(S, prim, hu, hv, dir);
+    uint32_t s = pcg_hash(e + frame * 927163u);
+    uint32_t nl = S.n_lights;  // > 0: the pass is skipped without lights
+    uint32_t li = min(__float2uint_rz(rng_next(s) * (float)nl), nl - 1u);
+    float4 L0 = S.lights[4 * li], L1 = S.lights[4 * li + 1], L2 = S.lights[4 * li + 2], LP = S.lights[4 * li + 3];
+    float3 v0 = xyz(L0), v1 = xyz(L1), v2 = xyz(L2);
+    float3 c = cross(v1 - v0, v2 - v0);
+    float3 normal = normalize(c);
+    float area = length(c) * 0.5f;
+    float r1 = rng_next(s);
+    float r2 = rng_next(s);
+    float sr1 = sqrtf(r1);
+    float u = 1.0f - sr1, v = r2 * sr1, w = 1.0f - u - v;
+    float3 emit_pos = v0 * u + v1 * v + v2 * w;
+    float3 emit_dir = normalize(normal + random_unit_vector(s));
+    float cmin = cauchy_cdf(LAMBDA_MIN), cmax = cauchy_cdf(LAMBDA_MAX), crange = cmax - cmin;
+    float lambda =
+        clampf(555.0f + 40.0f * tanf(PI * ((cmin + rng_next(s) * crange) - 0.5f)), LAMBDA_MIN, LAMBDA_MAX);
+    float dw = (lambda - 555.0f) / 40.0f;
+    float pdf = (1.0f / (crange * PI * 40.0f)) / (1.0f + dw * dw);
+    float energy = (blackbody(lambda, LP.y) / pdf) * area * PI * LP.z;
+    float3 pos = emit_pos + emit_dir * 0.001f;
+    a.ph.ray_o[e] = f4(pos.x, pos.y, pos.z, 0.0001f);
+    a.ph.ray_d[e] = f4(emit_dir.x, emit_dir.y, emit_dir.z, 100.0f);
+    a.ph.state[e] = f4(lambda, energy, __uint_as_float(s), __uint_as_float(0u));
+    a.ph.flags[e] = 0u;
+    a.ph.keys[e] = dir_key(emit_dir);
+    a.ph.vals[e] = e;
+    if (e == 0) a.counters->photon_paths[0] = a.photons_per_frame;
+}
+
+// One bounce of the photon loop after its closest-hit query
+// (photon_emit.wgsl:227-330).  Material type 5 (no reference counterpart)
+// reflects with the probability of the film's Airy reflectance, else absorbs.
+__global__ void __launch_bounds__(TRACE_BLOCK) k_photon_shade(FrameArgs a, uint32_t bounce) {
+    uint32_t n = a.counters->photon_paths[bounce];
+    if (blockIdx.x * blockDim.x >= n) return;
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevScene& S = a.scene;
+    const uint32_t* qin = bounce == 0 ? a.ph.sorted_vals : a.ph.queue[bounce & 1];
+    bool alive = false;
+    uint32_t e = q < n ? qin[q] : 0u;
+    if (q < n) {
+        float4 h = a.ph.hit[e];
+        uint32_t prim = __float_as_uint(h.y);
+        if (prim != MISS) {
+            float4 o4 = a.ph.ray_o[e], d4 = a.ph.ray_d[e], st = a.ph.state[e];
+            float3 pos = xyz(o4), dir = xyz(d4);
+            float lambda = st.x, energy = st.y;
+            uint32_t s = __float_as_uint(st.z), fl = __float_as_uint(st.w);
+            Surface sf = surface_at(S, prim, h.z, h.w, dir);
             float4 extra = S.materials[2 * sf.mat + 1];
             float3 ffn = sf.front ? sf.wn : -sf.wn;
             uint32_t type = (uint32_t)extra.x;
-            float3 hp = pos + dir * t;
+            float3 hp = pos + dir * h.x;
+            bool caustic = (fl & PH_CAUSTIC) != 0u;
             if (type == 0u) {
                 if (caustic) {
-                    stored = true;
-                    out0 = f4(hp.x, hp.y, hp.z, lambda);
-                    out1 = f4(-dir.x, -dir.y, -dir.z, energy);
+                    a.ph.staging[2 * e] = f4(hp.x, hp.y, hp.z, lambda);
+                    a.ph.staging[2 * e + 1] = f4(-dir.x, -dir.y, -dir.z, energy);
+                    a.ph.flags[e] = 1u;
                 }
-                break;
             } else if (type == 1u) {
                 dir = reflect(normalize(dir), ffn);
                 pos = hp + ffn * 0.001f;
+                alive = true;
             } else if (type == 2u) {
                 float lum = lambda / 1000.0f;
                 float ir = extra.z + (extra.w / (lum * lum));
                 float ratio = sf.front ? 1.0f / ir : ir;
                 float3 ud = normalize(dir);
                 float ct = fminf(dot(-ud, ffn), 1.0f);
-                float st = sqrtf(1.0f - ct * ct);
-                if (ratio * st > 1.0f || schlick(ct, ratio) > rng_next(s)) {
+                float stn = sqrtf(1.0f - ct * ct);
+                if (ratio * stn > 1.0f || schlick(ct, ratio) > rng_next(s)) {
                     dir = reflect(ud, ffn);
                 } else {
                     caustic = true;
                     dir = refract(ud, ffn, ratio);
                 }
                 pos = hp + (dot(dir, ffn) > 0.0f ? ffn : -ffn) * 0.001f;
+                alive = true;
             } else if (type == 4u) {
                 float3 ud = normalize(dir);
                 float ct = fminf(dot(-ud, ffn), 1.0f);
@@ -157,6 +189,7 @@ __global__ void __launch_bounds__(PHOTON_BLOCK, SRT_PHOTON_MIN_BLOCKS) k_photon_
                     dir = rng_next(s) < F ? reflect(ud, ffn) : refract(ud, ffn, ratio);
                 }
                 caustic = true;  // the position is not advanced (photon_emit.wgsl:291-326)
+                alive = true;
             } else if (type == 5u) {
                 float3 ud = normalize(dir);
                 float ct = fminf(dot(-ud, ffn), 1.0f);
@@ -166,46 +199,54 @@ __global__ void __launch_bounds__(PHOTON_BLOCK, SRT_PHOTON_MIN_BLOCKS) k_photon_
                     dir = reflect(ud, ffn);
                     pos = hp + ffn * 0.001f;
                     caustic = true;
-                } else {
-                    break;
+                    alive = true;
                 }
-            } else {
-                break;
+            }
+            if (bounce + 1u >= a.photon_max_bounces) alive = false;
+            if (alive) {
+                a.ph.ray_o[e] = f4(pos.x, pos.y, pos.z, 0.0001f);
+                a.ph.ray_d[e] = f4(dir.x, dir.y, dir.z, 100.0f);
+                a.ph.state[e] = f4(lambda, energy, __uint_as_float(s), __uint_as_float(caustic ? PH_CAUSTIC : 0u));
             }
         }
     }
-    warp_add_u64(&a.stats->photon_rays, n_rays);
-    // block-ordered compaction: rank = stored photons of lower ids in the block
+    uint32_t slot = warp_push(alive, &a.counters->photon_paths[bounce + 1]);
+    if (alive) a.ph.queue[(bounce + 1) & 1][slot] = e;
+}
+
+// Emitter-ordered compaction of the stored photons: per-block counts, an
+// exclusive scan of the counts (k_rs_rowscan), then the scatter.
+__global__ void __launch_bounds__(PHOTON_BLOCK) k_deposit_count(FrameArgs a) {
+    __shared__ uint32_t warp_cnt[PHOTON_BLOCK / 32];
+    uint32_t e = blockIdx.x * PHOTON_BLOCK + threadIdx.x;
+    bool stored = e < a.photons_per_frame && a.ph.flags[e] != 0u;
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, stored);
+    if ((threadIdx.x & 31) == 0) warp_cnt[threadIdx.x >> 5] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < PHOTON_BLOCK / 32; ++w) t += warp_cnt[w];
+        a.ph.block_counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(PHOTON_BLOCK) k_deposit_scatter(FrameArgs a) {
+    __shared__ uint32_t warp_cnt[PHOTON_BLOCK / 32];
+    uint32_t e = blockIdx.x * PHOTON_BLOCK + threadIdx.x;
+    bool stored = e < a.photons_per_frame && a.ph.flags[e] != 0u;
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t m = __ballot_sync(0xFFFFFFFFu, stored);
     if (lane == 0) warp_cnt[warp] = __popc(m);
     __syncthreads();
-    uint32_t before = 0, total = 0;
-#pragma unroll
-    for (int w = 0; w < PHOTON_BLOCK / 32; ++w) {
-        if (w < warp) before += warp_cnt[w];
-        total += warp_cnt[w];
-    }
+    uint32_t before = a.ph.block_counts[blockIdx.x];
+    for (int w = 0; w < warp; ++w) before += warp_cnt[w];
     if (stored) {
-        uint32_t slot = blockIdx.x * PHOTON_BLOCK + before + __popc(m & ((1u << lane) - 1u));
-        a.ph.staging[2 * slot] = out0;
-        a.ph.staging[2 * slot + 1] = out1;
+        uint32_t dst = before + __popc(m & ((1u << lane) - 1u));
+        a.ph.photons[2 * dst] = a.ph.staging[2 * e];
+        a.ph.photons[2 * dst + 1] = a.ph.staging[2 * e + 1];
     }
-    if (threadIdx.x == 0) a.ph.block_counts[blockIdx.x] = total;
-}
-
-// staging -> emission-ordered photon array (offsets already scanned)
-__global__ void k_photon_compact(FrameArgs a) {
-    uint32_t b = blockIdx.x;
-    uint32_t off = a.ph.block_counts[b];
-    uint32_t next = (b + 1 < a.ph.n_blocks) ? a.ph.block_counts[b + 1] : a.counters->photons_stored;
-    uint32_t cnt = next - off;
-    if (threadIdx.x < cnt) {
-        uint32_t src = b * PHOTON_BLOCK + threadIdx.x;
-        a.ph.photons[2 * (off + threadIdx.x)] = a.ph.staging[2 * src];
-        a.ph.photons[2 * (off + threadIdx.x) + 1] = a.ph.staging[2 * src + 1];
-    }
-    if (b == 0 && threadIdx.x == 0) atomicAdd(&a.stats->photons_stored, (unsigned long long)a.counters->photons_stored);
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(&a.stats->photons_stored, (unsigned long long)a.counters->photons_stored);
 }
 
 __global__ void k_grid_keys(const float4* __restrict__ photons, const uint32_t* n_dev, uint32_t n_host,
@@ -420,6 +461,10 @@ __global__ void k_frame_stats(FrameArgs a) {
     a.stats->closest_rays += c;
     a.stats->shadow_rays += s;
     a.stats->paths += a.counters->paths[0];
+    unsigned long long pr = 0;
+    if (a.photons_per_frame > 0u)
+        for (uint32_t i = 0; i < a.photon_max_bounces; ++i) pr += a.counters->photon_paths[i];
+    a.stats->photon_rays += pr;
 }
 
 // ------------------------------------------------------------------ batch / test kernels
@@ -520,20 +565,26 @@ inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 
 // ------------------------------------------------------------------ launchers
 int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
     int launches = 0;
-    bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
-    size_t smem = sizeof(uint2) * (small ? TRAV_STACK_SMALL : TRAV_STACK) * PHOTON_BLOCK;
-    if (a.count_visits) {
-        if (small) k_photon_trace<true, TRAV_STACK_SMALL><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
-        else k_photon_trace<true, TRAV_STACK><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
-    } else {
-        if (small) k_photon_trace<false, TRAV_STACK_SMALL><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
-        else k_photon_trace<false, TRAV_STACK><<<a.ph.n_blocks, PHOTON_BLOCK, smem, st>>>(a);
-    }
+    const uint32_t n = a.photons_per_frame;
+    // emit, then order the emitted rays by direction for coherent traversal
+    k_photon_emit<<<blocks_for(n, 256), 256, 0, st>>>(a);
     ++launches;
-    // exclusive scan of the block counts in place; total -> photons_stored
+    uint32_t *dir_keys, *order;
+    launches += sort_pairs(a.ph.keys, a.ph.vals, a.ph.keys2, a.ph.vals2, n, nullptr, 0, 24, a.ph.sort_scratch, st,
+                           &dir_keys, &order);
+    a.ph.sorted_vals = order;  // bounce-0 queue (read by k_photon_shade at bounce 0)
+    for (uint32_t b = 0; b < a.photon_max_bounces; ++b) {
+        launches += launch_trace_queue(a.scene, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b], n,
+                                       a.ph.ray_o, a.ph.ray_d, a.ph.hit, TRAV_PHOTON, a.count_visits, a.err, a.stats,
+                                       st);
+        k_photon_shade<<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, 0, st>>>(a, b);
+        ++launches;
+    }
+    // stored photons in emitter order
+    k_deposit_count<<<a.ph.n_blocks, PHOTON_BLOCK, 0, st>>>(a);
     k_rs_rowscan<<<1, 1024, 0, st>>>(a.ph.block_counts, a.ph.n_blocks, &a.counters->photons_stored);
-    k_photon_compact<<<a.ph.n_blocks, PHOTON_BLOCK, 0, st>>>(a);
-    launches += 2;
+    k_deposit_scatter<<<a.ph.n_blocks, PHOTON_BLOCK, 0, st>>>(a);
+    launches += 3;
     uint32_t grid = 148 * 8;
     k_grid_keys<<<grid, 256, 0, st>>>(a.ph.photons, &a.counters->photons_stored, 0,
                                       &a.cam->frame_count, 0, a.gather.cell, a.gather.hash_bits, a.ph.keys, a.ph.vals);

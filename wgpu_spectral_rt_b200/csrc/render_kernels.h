@@ -8,6 +8,7 @@
 namespace srt {
 
 constexpr int MAX_BOUNCES = 31;     // max_depth limit (queue counters per bounce)
+constexpr int MAX_PHOTON_BOUNCES = 16;  // photon_max_bounces limit (the reference uses 5)
 constexpr int PHOTON_BLOCK = 128;   // emitter ids per photon-trace block
 constexpr int TRACE_BLOCK = 128;
 
@@ -15,8 +16,9 @@ constexpr int TRACE_BLOCK = 128;
 struct FrameCounters {
     uint32_t paths[MAX_BOUNCES + 1];    // active paths entering bounce i
     uint32_t shadow[MAX_BOUNCES + 1];   // shadow rays emitted at bounce i
+    uint32_t photon_paths[MAX_PHOTON_BOUNCES + 1];  // live photon paths entering bounce i
     uint32_t photons_stored;
-    uint32_t pad[3];
+    uint32_t pad[2];
 };
 
 // Device statistics accumulated over frames (64-bit).
@@ -41,8 +43,13 @@ struct PathBuffers {
 };
 
 struct PhotonBuffers {
-    float4* staging;        // 2 per slot: PHOTON_BLOCK slots per block
-    uint32_t* block_counts; // per block; scanned in place into offsets
+    float4 *ray_o, *ray_d;  // per emitter: ray origin + tmin, direction + tmax
+    float4* state;          // per emitter: wavelength, energy, rng (bits), flags (bits)
+    float4* hit;            // per emitter: closest hit (t, triangle, u, v)
+    uint8_t* flags;         // per emitter: 1 if a photon was stored
+    uint32_t* queue[2];     // live emitter ids after bounce 0
+    float4* staging;        // per emitter: the stored photon, 2 float4
+    uint32_t* block_counts; // per block of PHOTON_BLOCK emitters; scanned in place into offsets
     float4* photons;        // emission order, 2 per photon
     float4* sorted;         // (hash, index) order, 2 per photon
     uint32_t *keys, *vals, *keys2, *vals2;
@@ -90,6 +97,11 @@ int launch_raygen(const FrameArgs& a, cudaStream_t st);
 int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage /* 0 all, 1 trace, 2 shade, 3 shadow */);
 int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st);  // trace_kernels.cu
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);   // trace_kernels.cu
+// Closest hit for the rays named by queue[0 .. *count) (queue NULL: 0 .. *count),
+// max_n bounding *count; traversal statistics go to slot `kind` (TRAV_*).
+int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n,
+                       const float4* ro, const float4* rd, float4* hit, int kind, int count_visits, uint32_t* err,
+                       DevStats* stats, cudaStream_t st);  // trace_kernels.cu
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
 

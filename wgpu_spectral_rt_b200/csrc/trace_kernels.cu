@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     k_trace(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
             const float4* __restrict__ ro, const float4* __restrict__ rd, float4* __restrict__ hit,
             const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c, float4* __restrict__ rad,
-            uint32_t* err, DevStats* stats) {
+            uint32_t* err, DevStats* stats, int kind) {
     extern __shared__ uint2 stack_smem[];
     uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t n = *count;
@@ -35,8 +35,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     Ray ray{xyz(o), xyz(d), o.w, d.w};
     float t = 0.f, u = 0.f, v = 0.f;
     uint32_t prim;
-    TravCounters tc{&stats->nodes_visited[ANY ? TRAV_SHADOW : TRAV_CLOSEST],
-                    &stats->tris_tested[ANY ? TRAV_SHADOW : TRAV_CLOSEST]};
+    TravCounters tc{&stats->nodes_visited[kind], &stats->tris_tested[kind]};
     bool h = traverse<ANY, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
     if (ANY) {
         // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
@@ -75,12 +74,19 @@ void launch_k_trace(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     if (ANY)
         k_trace<true, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
                                                                      a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id,
-                                                                     a.pb.sh_c, a.pb.rad, a.err, a.stats);
+                                                                     a.pb.sh_c, a.pb.rad, a.err, a.stats, TRAV_SHADOW);
     else
         k_trace<false, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
                                                                       &a.counters->paths[bounce], a.pb.ray_o,
                                                                       a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr,
-                                                                      a.err, a.stats);
+                                                                      a.err, a.stats, TRAV_CLOSEST);
+}
+
+template <bool COUNT, int STACK>
+void launch_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n, const float4* ro,
+                  const float4* rd, float4* hit, int kind, uint32_t* err, DevStats* stats, cudaStream_t st) {
+    k_trace<false, COUNT, STACK><<<blocks_for(max_n, TRACE_BLOCK), TRACE_BLOCK, sizeof(uint2) * STACK * TRACE_BLOCK,
+                                   st>>>(s, queue, count, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind);
 }
 
 template <bool ANY>
@@ -104,6 +110,21 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     launch_trace_kind<true>(a, bounce, st);
+    return 1;
+}
+
+int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n,
+                       const float4* ro, const float4* rd, float4* hit, int kind, int count_visits, uint32_t* err,
+                       DevStats* stats, cudaStream_t st) {
+    if (max_n == 0) return 0;
+    bool small = s.depth <= (uint32_t)TRAV_STACK_SMALL;
+    if (count_visits) {
+        if (small) launch_queue<true, TRAV_STACK_SMALL>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
+        else launch_queue<true, TRAV_STACK>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
+    } else {
+        if (small) launch_queue<false, TRAV_STACK_SMALL>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
+        else launch_queue<false, TRAV_STACK>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
+    }
     return 1;
 }
 
