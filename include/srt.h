@@ -152,6 +152,8 @@ typedef struct srt_params {
 #define SRT_FLAG_NO_GRAPH     0x2u  /* launch kernels directly instead of a CUDA graph */
 #define SRT_FLAG_STAGE_TIMING 0x4u  /* record per-stage CUDA events (srt_renderer_get_stats) */
 #define SRT_FLAG_COUNT_VISITS 0x8u  /* traversal counts visited nodes and tested triangles */
+#define SRT_FLAG_RAY_SORT     0x10u /* sort secondary camera rays by direction and origin before
+                                       tracing (pays off only when the BVH does not fit in L2) */
 
 /* Per-renderer statistics of the frames rendered since the last reset. */
 typedef struct srt_stats {

@@ -101,6 +101,7 @@ FLAG_FP64_ACCUM = 0x1
 FLAG_NO_GRAPH = 0x2
 FLAG_STAGE_TIMING = 0x4
 FLAG_COUNT_VISITS = 0x8
+FLAG_RAY_SORT = 0x10
 
 PRESET_CORNELL_BOX = 0
 PRESET_CUSTOM_PRISM = 1

@@ -301,7 +301,10 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         slot_of[bc] = bsl;
         child_in[bsl] = bc;
     }
-    // quantisation frame
+    // quantisation frame: 250 quanta span the node; the origin sits two
+    // quanta below it, and every child plane is padded outward by one
+    // quantum, which covers the half-quantum error of the traversal's
+    // biased-byte evaluation (see traverse<> in device_common.cuh)
     uint32_t ebyte[3];
     float scale[3];
     float nlov[3] = {nlo.x, nlo.y, nlo.z}, nhiv[3] = {nhi.x, nhi.y, nhi.z};
@@ -309,13 +312,20 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         double ext = (double)nhiv[a] - (double)nlov[a];
         int ex = -126;
         if (ext > 0.0) {
-            ex = (int)ceil(log2(ext / 255.0));
-            if (ldexp(255.0, ex) < ext) ++ex;
-            ex = max(ex, -126);
-            ex = min(ex, 127);
+            ex = (int)ceil(log2(ext / 250.0));
+            if (ldexp(250.0, ex) < ext) ++ex;
         }
+        // a quantum of at least 4 float ulps of the node's coordinates, so the
+        // shifted origin below stays exact to a quarter quantum
+        double mag = fmax(fabs((double)nlov[a]), fabs((double)nhiv[a]));
+        ex = max(ex, (int)ceil(log2(fmax(mag, 1e-30) * 4.0 / 8388608.0)));
+        ex = max(ex, -126);
+        ex = min(ex, 127);
         ebyte[a] = (uint32_t)(ex + 127);
         scale[a] = __uint_as_float(ebyte[a] << 23);
+        double lo_exact = (double)nlov[a];
+        nlov[a] = (float)(lo_exact - 2.0 * (double)scale[a]);
+        while ((double)nlov[a] > lo_exact - 2.0 * (double)scale[a]) nlov[a] = nextafterf(nlov[a], -3.4e38f);
     }
     uint32_t meta[2] = {0u, 0u}, qlo[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}}, qhi[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}};
     uint32_t imask = 0u, int_rank = 0u, tri_off = 0u;
@@ -325,12 +335,15 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         float lo3[3] = {clo[c].x, clo[c].y, clo[c].z}, hi3[3] = {chi[c].x, chi[c].y, chi[c].z};
         for (int a = 0; a < 3; ++a) {
             double sc = (double)scale[a];
-            int ql = (int)floor(((double)lo3[a] - (double)nlov[a]) / sc);
-            int qh = (int)ceil(((double)hi3[a] - (double)nlov[a]) / sc);
+            // one quantum of padding on each side
+            int ql = (int)floor(((double)lo3[a] - (double)nlov[a]) / sc) - 1;
+            int qh = (int)ceil(((double)hi3[a] - (double)nlov[a]) / sc) + 1;
             ql = min(max(ql, 0), 255);
             qh = min(max(qh, 0), 255);
-            while (ql > 0 && nlov[a] + (float)ql * scale[a] > lo3[a]) --ql;
-            while (qh < 255 && nlov[a] + (float)qh * scale[a] < hi3[a]) ++qh;
+            while (ql > 0 && (double)nlov[a] + ql * sc > (double)lo3[a] - sc) --ql;
+            while (qh < 255 && (double)nlov[a] + qh * sc < (double)hi3[a] + sc) ++qh;
+            if ((double)nlov[a] + ql * sc > (double)lo3[a] - sc || (double)nlov[a] + qh * sc < (double)hi3[a] + sc)
+                atomicOr(err, ERR_BAD_INDEX);  // the frame cannot hold the padded child: reject the tree
             qlo[a][s >> 2] |= (uint32_t)ql << (8 * (s & 3));
             qhi[a][s >> 2] |= (uint32_t)qh << (8 * (s & 3));
         }
@@ -349,7 +362,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         meta[s >> 2] |= m << (8 * (s & 3));
     }
     Node8 nd;
-    nd.a = make_uint4(__float_as_uint(nlo.x), __float_as_uint(nlo.y), __float_as_uint(nlo.z),
+    nd.a = make_uint4(__float_as_uint(nlov[0]), __float_as_uint(nlov[1]), __float_as_uint(nlov[2]),
                       ebyte[0] | (ebyte[1] << 8) | (ebyte[2] << 16) | (imask << 24));
     nd.b = make_uint4(child_base, tri_base, meta[0], meta[1]);
     nd.c = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);

@@ -380,6 +380,37 @@ extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt
     d.n_nodes = s->bvh.n_nodes;
     d.n_tris = (uint32_t)total;
     d.depth = s->bvh.depth;
+    {
+        // world bounds: each instance's object-space vertex box, transformed
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (uint32_t i = 0; i < a->n_instances; ++i) {
+            const srt_instance& in = a->instances[i];
+            uint32_t m = in.mesh_id;
+            uint32_t vb = a->mesh_infos[m].vertex_offset;
+            uint32_t ve = m + 1 < a->n_meshes ? a->mesh_infos[m + 1].vertex_offset : a->n_vertices;
+            double olo[3] = {1e300, 1e300, 1e300}, ohi[3] = {-1e300, -1e300, -1e300};
+            for (uint32_t v = vb; v < ve; ++v)
+                for (int k = 0; k < 3; ++k) {
+                    olo[k] = std::min(olo[k], (double)a->vertices[v].pos[k]);
+                    ohi[k] = std::max(ohi[k], (double)a->vertices[v].pos[k]);
+                }
+            if (olo[0] > ohi[0]) continue;
+            const float* M = in.transform;
+            for (int c8 = 0; c8 < 8; ++c8) {
+                double p[3] = {(c8 & 1) ? ohi[0] : olo[0], (c8 & 2) ? ohi[1] : olo[1], (c8 & 4) ? ohi[2] : olo[2]};
+                for (int r = 0; r < 3; ++r) {
+                    double w = M[r] * p[0] + M[4 + r] * p[1] + M[8 + r] * p[2] + M[12 + r];
+                    lo[r] = std::min(lo[r], w);
+                    hi[r] = std::max(hi[r], w);
+                }
+            }
+        }
+        if (lo[0] > hi[0]) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0.0;
+        float inv[3];
+        for (int k = 0; k < 3; ++k) inv[k] = (float)(1.0 / std::max(hi[k] - lo[k], 1e-6));
+        d.bmin = make_float4((float)lo[0], (float)lo[1], (float)lo[2], 0.f);
+        d.binv = make_float4(inv[0], inv[1], inv[2], 0.f);
+    }
     *out = s.release();
     return SRT_OK;
 }
@@ -446,7 +477,8 @@ struct srt_renderer {
         cudaFree(stats);
         cudaFree(err);
         void* bufs[] = {pb.ray_o, pb.ray_d, pb.hit, pb.thr, pb.wl, pb.rad, pb.misc, pb.queue[0], pb.queue[1],
-                        pb.sh_o, pb.sh_d, pb.sh_c, pb.sh_id, ph.ray_o, ph.ray_d, ph.state, ph.hit, ph.flags,
+                        pb.sh_o, pb.sh_d, pb.sh_c, pb.sh_id, pb.sort_keys, pb.sort_keys_alt, pb.sort_vals_alt,
+                        pb.sort_scratch, ph.ray_o, ph.ray_d, ph.state, ph.hit, ph.flags,
                         ph.queue[0], ph.queue[1], ph.staging, ph.block_counts, ph.photons, ph.sorted,
                         ph.keys, ph.vals, ph.keys2, ph.vals2, ph.sort_scratch, ph.ranges, accum, accum64, ldr};
         for (void* b : bufs) cudaFree(b);
@@ -545,6 +577,12 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     CUDA_TRY(c, dev_alloc(&pb.sh_d, np));
     CUDA_TRY(c, dev_alloc(&pb.sh_c, np));
     CUDA_TRY(c, dev_alloc(&pb.sh_id, np));
+    if (p.flags & SRT_FLAG_RAY_SORT) {
+        CUDA_TRY(c, dev_alloc(&pb.sort_keys, np));
+        CUDA_TRY(c, dev_alloc(&pb.sort_keys_alt, np));
+        CUDA_TRY(c, dev_alloc(&pb.sort_vals_alt, np));
+        CUDA_TRY(c, dev_alloc(&pb.sort_scratch, radix_scratch_words((uint32_t)np)));
+    }
     CUDA_TRY(c, dev_alloc(&r->accum, np));
     CUDA_TRY(c, cudaMemset(r->accum, 0, np * sizeof(float4)));
     if (p.flags & SRT_FLAG_FP64_ACCUM) {
@@ -607,6 +645,8 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     a.ldr = r->ldr;
     a.count_visits = (p.flags & SRT_FLAG_COUNT_VISITS) ? 1 : 0;
     a.block_size = (int)p.block_size;
+    a.ray_sort = (p.flags & SRT_FLAG_RAY_SORT) ? 1 : 0;
+    a.sm_count = c->sm_count;
     size_t n_events = 4 + 3 * (size_t)p.max_depth;
     r->ev.resize(n_events);
     for (auto& e : r->ev) CUDA_TRY(c, cudaEventCreate(&e));

@@ -70,6 +70,8 @@ struct DevScene {
     uint32_t n_nodes;
     uint32_t n_tris;
     uint32_t depth;  // 8-wide levels: a traversal stack needs at least this many entries
+    float4 bmin;     // world bounds of the scene (xyz), for ray sort keys
+    float4 binv;     // 1 / extent of the bounds (xyz)
 };
 
 // ------------------------------------------------------------------ vector helpers
@@ -450,12 +452,13 @@ SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3
 }
 
 SRT_DEV uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xFFu; }
-// Byte k of w as a float, without the integer-to-float conversion unit: one
-// byte permute builds the bit pattern 0x4B0000bb (= 2^23 + b exactly) and one
-// subtraction removes 2^23.
-SRT_DEV float qbyte(uint32_t w, uint32_t k) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
-}
+// Byte k of w plus 2^23 as a float, without the integer-to-float conversion
+// unit: one byte permute builds the bit pattern 0x4B0000bb (= 2^23 + b
+// exactly).  The slab test folds the 2^23 bias into its addend,
+// t = fma(2^23 + q, a, b - 2^23 a), whose rounding moves a plane by at most
+// half a quantum; the builder pads every child box by one quantum.
+SRT_DEV float qbyte(uint32_t w, uint32_t k) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | k)); }
+SRT_DEV float unbias(float a, float b) { return fmaf(-8388608.0f, a, b); }
 
 struct TravCounters {
     unsigned long long* nodes;
@@ -554,7 +557,8 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
               sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
         uint32_t imask = w0.w >> 24;
         float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;
-        float bx = (px - ray.o.x) * idir.x, by = (py - ray.o.y) * idir.y, bz = (pz - ray.o.z) * idir.z;
+        float bx = unbias(ax, (px - ray.o.x) * idir.x), by = unbias(ay, (py - ray.o.y) * idir.y),
+              bz = unbias(az, (pz - ray.o.z) * idir.z);
         // near/far quantised planes per axis by ray octant
         uint32_t lx0 = w2.x, lx1 = w2.y, ly0 = w2.z, ly1 = w2.w, lz0 = w3.x, lz1 = w3.y;
         uint32_t hx0 = w3.z, hx1 = w3.w, hy0 = w4.x, hy1 = w4.y, hz0 = w4.z, hz1 = w4.w;
@@ -570,12 +574,12 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
         for (int i = 0; i < 8; ++i) {
             const uint32_t k = (uint32_t)(i & 3);
             uint32_t m = byte_of(i < 4 ? meta0 : meta1, k);
-            float tnx = qbyte(i < 4 ? nx0 : nx1, k) * ax + bx;
-            float tny = qbyte(i < 4 ? ny0 : ny1, k) * ay + by;
-            float tnz = qbyte(i < 4 ? nz0 : nz1, k) * az + bz;
-            float tfx = qbyte(i < 4 ? fx0 : fx1, k) * ax + bx;
-            float tfy = qbyte(i < 4 ? fy0 : fy1, k) * ay + by;
-            float tfz = qbyte(i < 4 ? fz0 : fz1, k) * az + bz;
+            float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, k), ax, bx);
+            float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, k), ay, by);
+            float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, k), az, bz);
+            float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, k), ax, bx);
+            float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, k), ay, by);
+            float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, k), az, bz);
             float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
             float tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest)) * robust;
             if (m != 0u && tn <= tf) {
@@ -600,6 +604,152 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
     u_out = bu;
     v_out = bv;
     return true;
+}
+
+// ------------------------------------------------------------------ resumable traversal
+// The same traversal as traverse<>, split into an init and a step so that a
+// persistent warp can hand a finished lane a new ray between steps.  One
+// step = the pending triangle tests of the last node + one node visit.
+struct TravState {
+    float3 o, idir;
+    float tmin, tbest;
+    float sx, sy, sz;
+    uint32_t axes;  // kx | ky << 2 | kz << 4 | oct << 8
+    uint2 g, tg;
+    int sp;
+    uint32_t best;
+    float bu, bv;
+};
+
+SRT_DEV float comp_i(float3 v, uint32_t k) { return k == 0u ? v.x : (k == 1u ? v.y : v.z); }
+
+// Returns false when the ray cannot hit anything (finished at once).
+SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, float tmin, float tmax) {
+    T.best = MISS;
+    T.tbest = tmax;
+    T.tmin = tmin;
+    T.sp = 0;
+    T.tg = make_uint2(0u, 0u);
+    T.g = make_uint2(0u, 0u);
+    T.bu = T.bv = 0.f;
+    T.o = o;
+    if (S.n_nodes == 0u || !(d.x != 0.0f || d.y != 0.0f || d.z != 0.0f) || !(tmin <= tmax)) return false;
+    RayShear sh = make_shear(d);
+    T.sx = sh.sx;
+    T.sy = sh.sy;
+    T.sz = sh.sz;
+    const float eps = 1e-12f;
+    T.idir = f3(1.0f / (fabsf(d.x) > eps ? d.x : copysignf(eps, d.x)),
+                1.0f / (fabsf(d.y) > eps ? d.y : copysignf(eps, d.y)),
+                1.0f / (fabsf(d.z) > eps ? d.z : copysignf(eps, d.z)));
+    uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    T.axes = (uint32_t)sh.kx | ((uint32_t)sh.ky << 2) | ((uint32_t)sh.kz << 4) | (oct << 8);
+    T.g = make_uint2(0u, (1u << (24 + (0u ^ (oct ^ 7u)))) | 1u);
+    return true;
+}
+
+// Returns true when the ray is finished (for ANY: T.best != MISS on a hit).
+template <bool ANY, int STACK>
+SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
+                       uint32_t& n_tris) {
+    const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
+    while (T.tg.y != 0u) {
+        int b = __ffs(T.tg.y) - 1;
+        T.tg.y &= T.tg.y - 1u;
+        const TriSlot* ts = S.tris + T.tg.x + (uint32_t)b;
+        float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
+        ++n_tris;
+        // watertight test (Woop, Benthin, Wald 2013), as intersect_tri
+        float3 A = xyz(a0) - T.o, B = xyz(a1) - T.o, C = xyz(a2) - T.o;
+        float Az = comp_i(A, kz), Bz = comp_i(B, kz), Cz = comp_i(C, kz);
+        float Ax = comp_i(A, kx) - T.sx * Az, Ay = comp_i(A, ky) - T.sy * Az;
+        float Bx = comp_i(B, kx) - T.sx * Bz, By = comp_i(B, ky) - T.sy * Bz;
+        float Cx = comp_i(C, kx) - T.sx * Cz, Cy = comp_i(C, ky) - T.sy * Cz;
+        float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+        if (U == 0.0f || V == 0.0f || W == 0.0f) {
+            U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+            V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+            W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+        }
+        if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) continue;
+        float det = U + V + W;
+        if (det == 0.0f) continue;
+        float inv = 1.0f / det;
+        float t = (U * (T.sz * Az) + V * (T.sz * Bz) + W * (T.sz * Cz)) * inv;
+        if (!(t >= T.tmin && t <= T.tbest)) continue;
+        uint32_t id = __float_as_uint(a0.w);
+        if (ANY) {
+            T.best = id;
+            T.tbest = t;
+            return true;
+        }
+        if (t < T.tbest || id < T.best) {  // (t, id) lexicographic; t <= tbest holds here
+            T.tbest = t;
+            T.best = id;
+            T.bu = V * inv;
+            T.bv = W * inv;
+        }
+    }
+    if ((T.g.y & 0xFF000000u) == 0u) {
+        if (T.sp == 0) return true;
+        --T.sp;
+        T.g = stack[T.sp * stride];
+    }
+    int bit = 31 - __clz(T.g.y & 0xFF000000u);
+    T.g.y &= ~(1u << bit);
+    uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
+    uint32_t idx = T.g.x + __popc(T.g.y & ((1u << slot) - 1u) & 0xFFu);
+    if (T.g.y & 0xFF000000u) {
+        if (T.sp >= STACK) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+            return true;
+        }
+        stack[T.sp * stride] = T.g;
+        ++T.sp;
+    }
+    if (idx >= S.n_nodes) {
+        atomicOr(err, ERR_BAD_INDEX);
+        return true;
+    }
+    const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
+    uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    ++n_nodes;
+    float sxs = __uint_as_float((w0.w & 0xFFu) << 23), sys = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
+          szs = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    uint32_t imask = w0.w >> 24;
+    float ax = sxs * T.idir.x, ay = sys * T.idir.y, az = szs * T.idir.z;
+    float bx = unbias(ax, (__uint_as_float(w0.x) - T.o.x) * T.idir.x),
+          by = unbias(ay, (__uint_as_float(w0.y) - T.o.y) * T.idir.y),
+          bz = unbias(az, (__uint_as_float(w0.z) - T.o.z) * T.idir.z);
+    uint32_t nx0 = (oct & 1u) ? w3.z : w2.x, nx1 = (oct & 1u) ? w3.w : w2.y;
+    uint32_t fx0 = (oct & 1u) ? w2.x : w3.z, fx1 = (oct & 1u) ? w2.y : w3.w;
+    uint32_t ny0 = (oct & 2u) ? w4.x : w2.z, ny1 = (oct & 2u) ? w4.y : w2.w;
+    uint32_t fy0 = (oct & 2u) ? w2.z : w4.x, fy1 = (oct & 2u) ? w2.w : w4.y;
+    uint32_t nz0 = (oct & 4u) ? w4.z : w3.x, nz1 = (oct & 4u) ? w4.w : w3.y;
+    uint32_t fz0 = (oct & 4u) ? w3.x : w4.z, fz1 = (oct & 4u) ? w3.y : w4.w;
+    const float robust = 1.0000004f;
+    uint32_t hits = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t k = (uint32_t)(i & 3);
+        uint32_t m = byte_of(i < 4 ? w1.z : w1.w, k);
+        float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, k), ax, bx);
+        float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, k), ay, by);
+        float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, k), az, bz);
+        float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, k), ax, bx);
+        float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, k), ay, by);
+        float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, k), az, bz);
+        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, T.tmin));
+        float tf = fminf(fminf(tfx, tfy), fminf(tfz, T.tbest)) * robust;
+        if (m != 0u && tn <= tf) {
+            uint32_t c = m >> 5;
+            if (c == 7u) hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
+            else hits |= ((1u << c) - 1u) << (m & 31u);
+        }
+    }
+    T.g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
+    T.tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+    return false;
 }
 
 // ------------------------------------------------------------------ surface data at a hit

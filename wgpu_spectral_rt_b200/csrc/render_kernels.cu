@@ -87,6 +87,21 @@ SRT_DEV uint32_t dir_key(float3 d) {
     return k;
 }
 
+// Sort key of a secondary camera ray: direction first (octahedral 7+7 bits,
+// Morton order), then origin (6 bits per axis of the scene bounds, Morton).
+SRT_DEV uint32_t ray_sort_key(float3 o, float3 d, float4 bmin, float4 binv) {
+    uint32_t dk = dir_key(d) >> 10;  // top 7 bits of each octahedral coordinate
+    uint32_t q[3];
+    q[0] = (uint32_t)fminf(fmaxf((o.x - bmin.x) * binv.x * 64.0f, 0.0f), 63.0f);
+    q[1] = (uint32_t)fminf(fmaxf((o.y - bmin.y) * binv.y * 64.0f, 0.0f), 63.0f);
+    q[2] = (uint32_t)fminf(fmaxf((o.z - bmin.z) * binv.z * 64.0f, 0.0f), 63.0f);
+    uint32_t ok = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b)
+        ok |= (((q[0] >> b) & 1u) << (3 * b)) | (((q[1] >> b) & 1u) << (3 * b + 1)) | (((q[2] >> b) & 1u) << (3 * b + 2));
+    return (dk << 18) | ok;
+}
+
 constexpr uint32_t PH_CAUSTIC = 0x1u;
 
 // Emission: photon_emit.wgsl:159-214.
@@ -346,6 +361,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
     bool alive = false, shadow = false;
     uint32_t id = valid ? a.pb.queue[bounce & 1][q] : 0u;
     float3 sh_o = f3(0.f, 0.f, 0.f), sh_d = f3(0.f, 0.f, 0.f);
+    uint32_t key = 0u;
     float sh_tmax = 0.f;
     float4 sh_c = splat4(0.f);
     if (valid) {
@@ -405,13 +421,17 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
                         a.pb.ray_o[id] = f4(o.x, o.y, o.z, 0.0001f);
                         a.pb.ray_d[id] = f4(sc.dir.x, sc.dir.y, sc.dir.z, 100.0f);
                         a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
+                        if (a.ray_sort) key = ray_sort_key(o, sc.dir, S.bmin, S.binv);
                     }
                 }
             }
         }
     }
     uint32_t slot = warp_push(alive, &a.counters->paths[bounce + 1]);
-    if (alive) a.pb.queue[(bounce + 1) & 1][slot] = id;
+    if (alive) {
+        a.pb.queue[(bounce + 1) & 1][slot] = id;
+        if (a.ray_sort) a.pb.sort_keys[slot] = key;
+    }
     uint32_t sslot = warp_push(shadow, &a.counters->shadow[bounce]);
     if (shadow) {
         a.pb.sh_o[sslot] = f4(sh_o.x, sh_o.y, sh_o.z, 0.001f);
@@ -574,9 +594,9 @@ int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
                            &dir_keys, &order);
     a.ph.sorted_vals = order;  // bounce-0 queue (read by k_photon_shade at bounce 0)
     for (uint32_t b = 0; b < a.photon_max_bounces; ++b) {
-        launches += launch_trace_queue(a.scene, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b], n,
-                                       a.ph.ray_o, a.ph.ray_d, a.ph.hit, TRAV_PHOTON, a.count_visits, a.err, a.stats,
-                                       st);
+        launches += launch_trace_queue(a.scene, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b],
+                                       &a.counters->fetch[TRAV_PHOTON][b], n, a.ph.ray_o, a.ph.ray_d, a.ph.hit,
+                                       TRAV_PHOTON, a.count_visits, a.err, a.stats, a.sm_count, st);
         k_photon_shade<<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, 0, st>>>(a, b);
         ++launches;
     }
@@ -625,6 +645,13 @@ int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stag
     if (stage == 0 || stage == 2) {
         k_shade<<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         ++launches;
+        if (a.ray_sort && bounce + 1 < a.max_depth) {
+            // 4 passes: the sorted queue lands back in the queue buffer
+            uint32_t *sk, *sv;
+            launches += sort_pairs(a.pb.sort_keys, a.pb.queue[(bounce + 1) & 1], a.pb.sort_keys_alt,
+                                   a.pb.sort_vals_alt, a.width * a.height, &a.counters->paths[bounce + 1], 0, 32,
+                                   a.pb.sort_scratch, st, &sk, &sv);
+        }
     }
     if (stage == 0 || stage == 3) launches += launch_trace_shadow(a, bounce, st);
     return launches;

@@ -17,6 +17,7 @@ struct FrameCounters {
     uint32_t paths[MAX_BOUNCES + 1];    // active paths entering bounce i
     uint32_t shadow[MAX_BOUNCES + 1];   // shadow rays emitted at bounce i
     uint32_t photon_paths[MAX_PHOTON_BOUNCES + 1];  // live photon paths entering bounce i
+    uint32_t fetch[3][MAX_BOUNCES + 1];  // persistent traversal: next queue position, by TRAV_* kind and bounce
     uint32_t photons_stored;
     uint32_t pad[2];
 };
@@ -40,6 +41,8 @@ struct PathBuffers {
     uint32_t* queue[2];
     float4 *sh_o, *sh_d, *sh_c;
     uint32_t* sh_id;
+    // ray reordering of the live queue between bounces
+    uint32_t *sort_keys, *sort_keys_alt, *sort_vals_alt, *sort_scratch;
 };
 
 struct PhotonBuffers {
@@ -88,6 +91,8 @@ struct FrameArgs {
     uchar4* ldr;
     int count_visits;
     int block_size;
+    int ray_sort;  // sort the live queue by (direction, origin) before each bounce >= 1
+    int sm_count;  // persistent traversal grid = sm_count * blocks per SM
 };
 
 // Photon pass: trace, compaction, grid keys, radix sort, ranges.
@@ -99,9 +104,10 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st); 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);   // trace_kernels.cu
 // Closest hit for the rays named by queue[0 .. *count) (queue NULL: 0 .. *count),
 // max_n bounding *count; traversal statistics go to slot `kind` (TRAV_*).
-int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n,
-                       const float4* ro, const float4* rd, float4* hit, int kind, int count_visits, uint32_t* err,
-                       DevStats* stats, cudaStream_t st);  // trace_kernels.cu
+// `fetch` is a zeroed counter the persistent warps draw queue positions from.
+int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t* fetch,
+                       uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
+                       uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st);  // trace_kernels.cu
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
 

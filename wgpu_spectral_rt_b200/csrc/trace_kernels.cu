@@ -5,8 +5,14 @@
 // multiply-add contraction (fast slab tests), while the shading kernels are
 // compiled without it so that they round like the CPU oracle.
 //
+// Persistent warps with dynamic ray fetch (Aila and Laine, HPG 2009): the
+// grid holds one wave of resident blocks; each warp draws queue positions
+// from a counter, and once REFILL lanes have finished their rays the warp
+// hands those lanes new rays, so divergent ray lengths do not idle lanes.
 // The shared-memory stack is sized to the tree: STACK = 16 entries for trees
 // of at most 16 levels (config 2 builds 10), 32 otherwise.
+#include <algorithm>
+
 #include "render_kernels.h"
 
 // 8 resident blocks of 128 threads per SM caps the kernels at 64 registers:
@@ -15,11 +21,19 @@
 #ifndef SRT_TRACE_MIN_BLOCKS
 #define SRT_TRACE_MIN_BLOCKS 8
 #endif
+// idle lanes that trigger a refill of the warp
+#ifndef SRT_TRACE_REFILL
+#define SRT_TRACE_REFILL 12
+#endif
+#ifndef SRT_TRACE_PERSISTENT
+#define SRT_TRACE_PERSISTENT 1
+#endif
 
 namespace srt {
 
 namespace {
 
+// One ray per thread, one launch over the whole queue.
 template <bool ANY, bool COUNT, int STACK>
 __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     k_trace(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
@@ -49,6 +63,74 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     }
 }
 
+// Persistent form: same inputs and outputs, queue positions from *fetch.
+template <bool ANY, bool COUNT, int STACK>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+    k_trace_pt(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
+               uint32_t* __restrict__ fetch, const float4* __restrict__ ro, const float4* __restrict__ rd,
+               float4* __restrict__ hit, const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
+               float4* __restrict__ rad, uint32_t* err, DevStats* stats, int kind) {
+    extern __shared__ uint2 stack_smem[];
+    uint2* stack = stack_smem + threadIdx.x;
+    const uint32_t n = *count;
+    if (n == 0u) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    TravState T;
+    bool active = false, exhausted = false;
+    uint32_t q = 0, id = 0, n_nodes = 0, n_tris = 0;
+    while (true) {
+        uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
+        if (!exhausted && __popc(idle) >= SRT_TRACE_REFILL) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base + (uint32_t)__popc(idle) >= n) exhausted = true;
+            if (!active) {
+                uint32_t my = base + __popc(idle & lt);
+                if (my < n) {
+                    q = my;
+                    id = queue ? queue[q] : q;
+                    float4 o = ro[ANY ? q : id], d = rd[ANY ? q : id];
+                    active = trav_init(T, S, xyz(o), xyz(d), o.w, d.w);
+                    if (!active) {  // degenerate ray: finished without a hit
+                        if (ANY) {
+                            uint32_t pid = sh_id[q];
+                            float4 c = sh_c[q], r = rad[pid];
+                            rad[pid] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z),
+                                                   __fadd_rn(r.w, c.w));
+                        } else {
+                            hit[id] = make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+                        }
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active && trav_step<ANY, STACK>(S, T, stack, TRACE_BLOCK, err, n_nodes, n_tris)) {
+            active = false;
+            if (ANY) {
+                if (T.best == MISS) {
+                    uint32_t pid = sh_id[q];
+                    float4 c = sh_c[q], r = rad[pid];
+                    rad[pid] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z),
+                                           __fadd_rn(r.w, c.w));
+                }
+            } else {
+                hit[id] = T.best != MISS ? make_float4(T.tbest, __uint_as_float(T.best), T.bu, T.bv)
+                                         : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+            }
+        }
+    }
+    if (COUNT) {
+        atomicAdd(&stats->nodes_visited[kind], (unsigned long long)n_nodes);
+        atomicAdd(&stats->tris_tested[kind], (unsigned long long)n_tris);
+    }
+}
+
 template <bool ANY>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const float4* __restrict__ rays, uint32_t n,
                                                              float4* __restrict__ hits, uint32_t* err) {
@@ -67,64 +149,81 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const f
 
 inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
 
-template <bool ANY, bool COUNT, int STACK>
-void launch_k_trace(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
-    size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
-    if (ANY)
-        k_trace<true, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, nullptr, &a.counters->shadow[bounce],
-                                                                     a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id,
-                                                                     a.pb.sh_c, a.pb.rad, a.err, a.stats, TRAV_SHADOW);
-    else
-        k_trace<false, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a.scene, a.pb.queue[bounce & 1],
-                                                                      &a.counters->paths[bounce], a.pb.ray_o,
-                                                                      a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr,
-                                                                      a.err, a.stats, TRAV_CLOSEST);
-}
+struct TraceLaunch {
+    DevScene s;
+    const uint32_t* queue;
+    const uint32_t* count;
+    uint32_t* fetch;
+    uint32_t max_n;
+    const float4 *ro, *rd;
+    float4* hit;
+    const uint32_t* sh_id;
+    const float4* sh_c;
+    float4* rad;
+    uint32_t* err;
+    DevStats* stats;
+    int kind;
+    int sm_count;
+};
 
-template <bool COUNT, int STACK>
-void launch_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n, const float4* ro,
-                  const float4* rd, float4* hit, int kind, uint32_t* err, DevStats* stats, cudaStream_t st) {
-    k_trace<false, COUNT, STACK><<<blocks_for(max_n, TRACE_BLOCK), TRACE_BLOCK, sizeof(uint2) * STACK * TRACE_BLOCK,
-                                   st>>>(s, queue, count, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind);
+template <bool ANY, bool COUNT, int STACK>
+void launch_one(const TraceLaunch& L, cudaStream_t st) {
+    size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
+    if (SRT_TRACE_PERSISTENT && L.fetch) {
+        uint32_t grid = (uint32_t)(L.sm_count > 0 ? L.sm_count : 148) * SRT_TRACE_MIN_BLOCKS;
+        grid = std::min(grid, std::max(1u, blocks_for(L.max_n, TRACE_BLOCK)));
+        k_trace_pt<ANY, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(L.s, L.queue, L.count, L.fetch, L.ro, L.rd,
+                                                                      L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats,
+                                                                      L.kind);
+    } else {
+        k_trace<ANY, COUNT, STACK><<<blocks_for(L.max_n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(
+            L.s, L.queue, L.count, L.ro, L.rd, L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats, L.kind);
+    }
 }
 
 template <bool ANY>
-void launch_trace_kind(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
-    if (a.count_visits) {
-        if (small) launch_k_trace<ANY, true, TRAV_STACK_SMALL>(a, bounce, st);
-        else launch_k_trace<ANY, true, TRAV_STACK>(a, bounce, st);
+void launch_kind(const TraceLaunch& L, int count_visits, cudaStream_t st) {
+    bool small = L.s.depth <= (uint32_t)TRAV_STACK_SMALL;
+    if (count_visits) {
+        if (small) launch_one<ANY, true, TRAV_STACK_SMALL>(L, st);
+        else launch_one<ANY, true, TRAV_STACK>(L, st);
     } else {
-        if (small) launch_k_trace<ANY, false, TRAV_STACK_SMALL>(a, bounce, st);
-        else launch_k_trace<ANY, false, TRAV_STACK>(a, bounce, st);
+        if (small) launch_one<ANY, false, TRAV_STACK_SMALL>(L, st);
+        else launch_one<ANY, false, TRAV_STACK>(L, st);
     }
 }
 
 }  // namespace
 
 int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    launch_trace_kind<false>(a, bounce, st);
+    // primary rays (bounce 0) are pixel-ordered and coherent: one ray per
+    // thread; later bounces are incoherent: persistent warps with refill
+    TraceLaunch L{a.scene, a.pb.queue[bounce & 1], &a.counters->paths[bounce],
+                  bounce == 0 ? nullptr : &a.counters->fetch[TRAV_CLOSEST][bounce],
+                  a.width * a.height, a.pb.ray_o, a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats,
+                  TRAV_CLOSEST, a.sm_count};
+    launch_kind<false>(L, a.count_visits, st);
     return 1;
 }
 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    launch_trace_kind<true>(a, bounce, st);
+    // one ray per thread: the shadow queue is in pixel order and coherent, and
+    // refilling lanes from a shared counter scatters it (measured +28 %)
+    TraceLaunch L{a.scene, nullptr, &a.counters->shadow[bounce], nullptr, a.width * a.height, a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad, a.err, a.stats,
+                  TRAV_SHADOW, a.sm_count};
+    launch_kind<true>(L, a.count_visits, st);
     return 1;
 }
 
-int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t max_n,
-                       const float4* ro, const float4* rd, float4* hit, int kind, int count_visits, uint32_t* err,
-                       DevStats* stats, cudaStream_t st) {
+int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t* fetch,
+                       uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
+                       uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st) {
     if (max_n == 0) return 0;
-    bool small = s.depth <= (uint32_t)TRAV_STACK_SMALL;
-    if (count_visits) {
-        if (small) launch_queue<true, TRAV_STACK_SMALL>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
-        else launch_queue<true, TRAV_STACK>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
-    } else {
-        if (small) launch_queue<false, TRAV_STACK_SMALL>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
-        else launch_queue<false, TRAV_STACK>(s, queue, count, max_n, ro, rd, hit, kind, err, stats, st);
-    }
+    // photon rays arrive direction-sorted: one ray per thread keeps that order
+    // (persistent refill measured slower, 3.35 vs 3.15 ms per photon pass)
+    (void)fetch;
+    TraceLaunch L{s, queue, count, nullptr, max_n, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind, sm_count};
+    launch_kind<false>(L, count_visits, st);
     return 1;
 }
 
