@@ -129,6 +129,27 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_frame_offset(rank: int, steps: int, warmup: int) -> int:
+    """First frame index of a replica: each rank renders its own sample stream."""
+    return rank * (steps + warmup)
+
+
+def replica_reduce(local_ms: float, local_paths: int, dist=None, device="cpu"):
+    """(max over ranks of the timed region in ms, paths summed over ranks).
+
+    Replicas never exchange path data; the only collectives are this timing
+    reduction and the barriers around the timed region."""
+    if dist is None:
+        return local_ms, local_paths
+    import torch
+
+    t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    p = torch.tensor([local_paths], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(p, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(p.item())
+
+
 def build_scene(srt, ctx, preset_name: str, seed: int = 0):
     b = srt.SceneBuilder()
     cam = b.add_preset(getattr(srt, preset_name), seed)
@@ -272,7 +293,7 @@ def main(argv=None):
     pos, yaw, pitch = cam
     params = srt.default_params(max_depth=depth, photons_per_frame=photons)
     r = srt.Renderer(ctx, scene, w, h, params)
-    f0 = rank * (args.steps + args.warmup)
+    f0 = rank_frame_offset(rank, args.steps, args.warmup)
 
     def cam_u(k):
         return srt.camera_uniform(pos, yaw, pitch, w / h, f0 + k)
@@ -296,11 +317,7 @@ def main(argv=None):
         dist.barrier()
     ms = start.elapsed_time(end)
     st = r.stats()
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    paths_all = w * h * args.steps * world
+    ms_max, paths_all = replica_reduce(ms, w * h * args.steps, dist, f"cuda:{local_rank}")
     value = paths_all / (ms_max * 1e-3) / 1e6
     photons_all = photons * args.steps * world
     rays_all = (st["rays_closest"] + st["rays_shadow"] + st["rays_photon"]) * world

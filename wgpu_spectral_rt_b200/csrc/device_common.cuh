@@ -610,6 +610,10 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
 // The same traversal as traverse<>, split into an init and a step so that a
 // persistent warp can hand a finished lane a new ray between steps.  One
 // step = the pending triangle tests of the last node + one node visit.
+#ifndef SRT_TRAV_ONE_TRI_PER_STEP
+#define SRT_TRAV_ONE_TRI_PER_STEP 0
+#endif
+
 struct TravState {
     float3 o, idir;
     float tmin, tbest;
@@ -653,7 +657,14 @@ template <bool ANY, int STACK>
 SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
                        uint32_t& n_tris) {
     const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
+#if SRT_TRAV_ONE_TRI_PER_STEP
+    // one item per step: a triangle if one is pending, else a node, so a lane
+    // with a long triangle list does not hold up the lanes visiting nodes
+    const bool tri_step = T.tg.y != 0u;
+    for (int once = 0; once < 1 && T.tg.y != 0u; ++once) {
+#else
     while (T.tg.y != 0u) {
+#endif
         int b = __ffs(T.tg.y) - 1;
         T.tg.y &= T.tg.y - 1u;
         const TriSlot* ts = S.tris + T.tg.x + (uint32_t)b;
@@ -690,6 +701,9 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
             T.bv = W * inv;
         }
     }
+#if SRT_TRAV_ONE_TRI_PER_STEP
+    if (tri_step) return false;
+#endif
     if ((T.g.y & 0xFF000000u) == 0u) {
         if (T.sp == 0) return true;
         --T.sp;

@@ -28,6 +28,10 @@
 #ifndef SRT_TRACE_PERSISTENT
 #define SRT_TRACE_PERSISTENT 1
 #endif
+// first bounce whose shadow rays use persistent warps (0: none)
+#ifndef SRT_SHADOW_PERSISTENT_FROM
+#define SRT_SHADOW_PERSISTENT_FROM 0
+#endif
 
 namespace srt {
 
@@ -209,7 +213,11 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     // one ray per thread: the shadow queue is in pixel order and coherent, and
     // refilling lanes from a shared counter scatters it (measured +28 %)
-    TraceLaunch L{a.scene, nullptr, &a.counters->shadow[bounce], nullptr, a.width * a.height, a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad, a.err, a.stats,
+    TraceLaunch L{a.scene, nullptr, &a.counters->shadow[bounce],
+                  (SRT_SHADOW_PERSISTENT_FROM > 0 && bounce >= (uint32_t)SRT_SHADOW_PERSISTENT_FROM)
+                      ? &a.counters->fetch[TRAV_SHADOW][bounce]
+                      : nullptr,
+                  a.width * a.height, a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad, a.err, a.stats,
                   TRAV_SHADOW, a.sm_count};
     launch_kind<true>(L, a.count_visits, st);
     return 1;
