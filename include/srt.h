@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SRT_ABI_VERSION 1u
+#define SRT_ABI_VERSION 2u
 
 /* Status codes.  Replaces unwrap()/panic! and wgpu::SurfaceError
  * (src/app.rs:70-77, src/wgpu_ctx.rs:36-42). */
@@ -154,6 +154,10 @@ typedef struct srt_params {
 #define SRT_FLAG_COUNT_VISITS 0x8u  /* traversal counts visited nodes and tested triangles */
 #define SRT_FLAG_RAY_SORT     0x10u /* sort secondary camera rays by direction and origin before
                                        tracing (pays off only when the BVH does not fit in L2) */
+#define SRT_FLAG_GUIDING      0x20u /* neural path guiding of Lambert continuations (no reference
+                                       counterpart): a learned vMF mixture, one-sample MIS with the
+                                       cosine lobe, trained after every frame; not with RAY_SORT */
+#define SRT_FLAG_GUIDE_FROZEN 0x40u /* with SRT_FLAG_GUIDING: sample the guide, do not train it */
 
 /* Per-renderer statistics of the frames rendered since the last reset. */
 typedef struct srt_stats {
@@ -174,6 +178,7 @@ typedef struct srt_stats {
     double ms_raygen;
     uint64_t launches_trace_closest;
     uint64_t kernel_launches;   /* kernels launched by the library in these frames */
+    double ms_guide_train;      /* SRT_FLAG_STAGE_TIMING + SRT_FLAG_GUIDING: training step times */
 } srt_stats;
 
 typedef struct srt_ctx srt_ctx;
@@ -371,6 +376,35 @@ srt_status srt_photon_gather(srt_ctx* ctx, const srt_photon* photons, uint32_t n
  *    -> out f32[7] origin[3] dir[3] rng out (bits)
  * in/out strides are the per-op sizes above; n records. */
 srt_status srt_test_device_math(srt_ctx* ctx, int op, uint32_t n, const void* in, void* out, const void* aux);
+
+/* ------------------------------------------------------------------------ */
+/* Neural path guiding (no reference counterpart; SRT_FLAG_GUIDING).          */
+/* Network: 10 inputs (position in the scene bounds, shading normal,          */
+/* outgoing direction, wavelength) -> sin/cos encoding of 6 octaves (128)     */
+/* -> 4 x 64 ReLU -> 48 outputs: 8 vMF lobes (direction 3, log kappa,          */
+/* logit) and the selection logit.  Weights: one float vector of              */
+/* srt_guide_param_count() values, W_l [out][in] row-major then b_l, l=0..4.  */
+/* ------------------------------------------------------------------------ */
+uint32_t srt_guide_param_count(void);
+/* Deterministic initial weights (He-uniform, output layer scaled by 0.1). */
+srt_status srt_guide_default_weights(uint64_t seed, float* out, uint32_t n);
+/* Checkpoint / restore of a guiding renderer's FP32 weights (restore resets Adam). */
+srt_status srt_renderer_guide_get_weights(srt_renderer* r, float* out, uint32_t n);
+srt_status srt_renderer_guide_set_weights(srt_renderer* r, const float* w, uint32_t n);
+srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_steps, uint32_t* record_threshold);
+srt_status srt_renderer_guide_set_learning_rate(srt_renderer* r, float lr);
+/* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
+ * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),
+ * sampled direction).  train: loss gradients summed over n samples
+ * (weights as given) and, when params_out/m_out/v_out are non-NULL, one Adam
+ * step (gradients divided by n; step adam_step + 1). */
+srt_status srt_guide_test_forward(srt_ctx* ctx, const float* params, const float* x, uint32_t n, float* out);
+srt_status srt_guide_test_mixture(srt_ctx* ctx, const float* raw, const float* omega, const float* u, uint32_t n,
+                                  float* out);
+srt_status srt_guide_test_train(srt_ctx* ctx, const float* params, const float* adam_m, const float* adam_v,
+                                uint32_t adam_step, float lr, const float* x, const float* omega,
+                                const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
+                                float* params_out, float* m_out, float* v_out);
 
 #ifdef __cplusplus
 }

@@ -81,7 +81,8 @@ class Stats(C.Structure):
                 ("photons_stored", C.c_uint64), ("nodes_visited", C.c_uint64 * 3), ("tris_tested", C.c_uint64 * 3),
                 ("ms_photon_pass", C.c_double), ("ms_trace_closest", C.c_double), ("ms_shade", C.c_double),
                 ("ms_trace_shadow", C.c_double), ("ms_finalize", C.c_double), ("ms_raygen", C.c_double),
-                ("launches_trace_closest", C.c_uint64), ("kernel_launches", C.c_uint64)]
+                ("launches_trace_closest", C.c_uint64), ("kernel_launches", C.c_uint64),
+                ("ms_guide_train", C.c_double)]
 
 
 class SceneArrays(C.Structure):
@@ -102,6 +103,8 @@ FLAG_NO_GRAPH = 0x2
 FLAG_STAGE_TIMING = 0x4
 FLAG_COUNT_VISITS = 0x8
 FLAG_RAY_SORT = 0x10
+FLAG_GUIDING = 0x20
+FLAG_GUIDE_FROZEN = 0x40
 
 PRESET_CORNELL_BOX = 0
 PRESET_CUSTOM_PRISM = 1
@@ -163,6 +166,15 @@ SIGNATURES = {
     "srt_photon_gather": (_I, [_P, _P, _U32, _P, _U32, _U32, C.POINTER(Params), _P]),
     "srt_photon_grid_build_noalloc": (_I, [_P, _P, _U32, _U32, _F, _U32, _P, _P]),
     "srt_test_device_math": (_I, [_P, _I, _U32, _P, _P, _P]),
+    "srt_guide_param_count": (_U32, []),
+    "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
+    "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
+    "srt_renderer_guide_set_weights": (_I, [_P, _P, _U32]),
+    "srt_renderer_guide_info": (_I, [_P, C.POINTER(_U32), C.POINTER(_U32)]),
+    "srt_renderer_guide_set_learning_rate": (_I, [_P, _F]),
+    "srt_guide_test_forward": (_I, [_P, _P, _P, _U32, _P]),
+    "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
+    "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -444,6 +456,24 @@ class Renderer:
         _check(lib().srt_renderer_read_photons(self.h, ptr(out), n.value, C.byref(n)), self.ctx.h)
         return out
 
+    # neural path guiding (FLAG_GUIDING)
+    def guide_weights(self) -> np.ndarray:
+        out = np.zeros(guide_param_count(), np.float32)
+        _check(lib().srt_renderer_guide_get_weights(self.h, ptr(out), len(out)), self.ctx.h)
+        return out
+
+    def set_guide_weights(self, w: np.ndarray) -> None:
+        a = np.ascontiguousarray(w, np.float32)
+        _check(lib().srt_renderer_guide_set_weights(self.h, ptr(a), len(a)), self.ctx.h)
+
+    def guide_info(self) -> dict:
+        steps, thr = C.c_uint32(), C.c_uint32()
+        _check(lib().srt_renderer_guide_info(self.h, C.byref(steps), C.byref(thr)), self.ctx.h)
+        return {"adam_steps": steps.value, "record_threshold": thr.value}
+
+    def set_guide_learning_rate(self, lr: float) -> None:
+        _check(lib().srt_renderer_guide_set_learning_rate(self.h, lr), self.ctx.h)
+
     def close(self):
         if self.h:
             lib().srt_renderer_destroy(self.h)
@@ -495,3 +525,56 @@ def device_math(ctx: Context, op: int, inp: np.ndarray, aux: CameraUniform | Non
     out = np.zeros(n * osz // 4, np.uint32 if op in (0, 7) else np.float32)
     _check(lib().srt_test_device_math(ctx.h, op, n, ptr(a), ptr(out), C.byref(aux) if aux is not None else None), ctx.h)
     return out.reshape(n, osz // 4)
+
+
+# --------------------------------------------------------------------------- path guiding
+
+
+def guide_param_count() -> int:
+    return int(lib().srt_guide_param_count())
+
+
+def guide_default_weights(seed: int = 1) -> np.ndarray:
+    out = np.zeros(guide_param_count(), np.float32)
+    _check(lib().srt_guide_default_weights(seed, ptr(out), len(out)))
+    return out
+
+
+def guide_forward(ctx: Context, params: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """Raw network outputs [n, 48] for inputs x [n, 10] (srt_guide_test_forward)."""
+    w = np.ascontiguousarray(params, np.float32)
+    a = np.ascontiguousarray(x, np.float32).reshape(-1, 10)
+    out = np.zeros((len(a), 48), np.float32)
+    _check(lib().srt_guide_test_forward(ctx.h, ptr(w), ptr(a), len(a), ptr(out)), ctx.h)
+    return out
+
+
+def guide_mixture(ctx: Context, raw: np.ndarray, omega: np.ndarray, u: np.ndarray) -> np.ndarray:
+    """[n, 4]: mixture pdf at omega and a direction sampled with u (srt_guide_test_mixture)."""
+    r = np.ascontiguousarray(raw, np.float32).reshape(-1, 48)
+    o = np.ascontiguousarray(omega, np.float32).reshape(-1, 3)
+    uu = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+    out = np.zeros((len(r), 4), np.float32)
+    _check(lib().srt_guide_test_mixture(ctx.h, ptr(r), ptr(o), ptr(uu), len(r), ptr(out)), ctx.h)
+    return out
+
+
+def guide_train_step(ctx: Context, params, x, omega, pdf_bsdf, weight, adam_m=None, adam_v=None, adam_step=0,
+                     lr=1e-3, adam=True):
+    """Loss gradients (summed over the samples) and, with adam, the parameters
+    and Adam moments after one step (srt_guide_test_train)."""
+    n = len(x)
+    w = np.ascontiguousarray(params, np.float32)
+    m = None if adam_m is None else np.ascontiguousarray(adam_m, np.float32)
+    v = None if adam_v is None else np.ascontiguousarray(adam_v, np.float32)
+    xs = np.ascontiguousarray(x, np.float32).reshape(-1, 10)
+    om = np.ascontiguousarray(omega, np.float32).reshape(-1, 3)
+    pb = np.ascontiguousarray(pdf_bsdf, np.float32).reshape(-1)
+    wt = np.ascontiguousarray(weight, np.float32).reshape(-1)
+    grad = np.zeros_like(w)
+    outs = [np.zeros_like(w) for _ in range(3)] if adam else [None, None, None]
+    _check(lib().srt_guide_test_train(ctx.h, ptr(w), ptr(m) if m is not None else None,
+                                      ptr(v) if v is not None else None, adam_step, lr, ptr(xs), ptr(om), ptr(pb),
+                                      ptr(wt), n, ptr(grad), *(ptr(o) if o is not None else None for o in outs)),
+           ctx.h)
+    return (grad, *outs) if adam else grad

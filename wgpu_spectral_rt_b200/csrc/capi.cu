@@ -462,8 +462,9 @@ struct srt_renderer {
     int launches_per_frame = 0;
     uint32_t frame_count = 0;
     uint64_t frames = 0, launches = 0, photons_emitted = 0, trace_launches = 0;
-    double ms[7] = {0, 0, 0, 0, 0, 0, 0};  // photon trace, grid, closest, shade, shadow, finalize, raygen
+    double ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // photon, -, closest, shade, shadow, finalize, raygen, guide training
     std::vector<cudaEvent_t> ev;
+    GuideArgs guide{};  // SRT_FLAG_GUIDING only
 
     ~srt_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -482,6 +483,7 @@ struct srt_renderer {
                         ph.queue[0], ph.queue[1], ph.staging, ph.block_counts, ph.photons, ph.sorted,
                         ph.keys, ph.vals, ph.keys2, ph.vals2, ph.sort_scratch, ph.ranges, accum, accum64, ldr};
         for (void* b : bufs) cudaFree(b);
+        guide_free(guide);
     }
 
     // Enqueues one frame (after the camera upload).  stage timing: events
@@ -512,6 +514,8 @@ struct srt_renderer {
         }
         n += launch_finalize(args, st);
         n += launch_frame_stats(args, st);
+        mark();
+        if (args.guiding) n += launch_guide_train(args, st);
         mark();
         return n;
     }
@@ -546,6 +550,8 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
         p.photon_max_bounces > (uint32_t)MAX_PHOTON_BOUNCES)
         return fail(c, SRT_ERR_INVALID_ARG, "invalid photon parameters (photon_max_bounces must be <= 16)");
     if ((uint64_t)w * h > (1ull << 28)) return fail(c, SRT_ERR_INVALID_ARG, "viewport too large");
+    if ((p.flags & SRT_FLAG_GUIDING) && (p.flags & SRT_FLAG_RAY_SORT))
+        return fail(c, SRT_ERR_INVALID_ARG, "SRT_FLAG_GUIDING and SRT_FLAG_RAY_SORT cannot be combined");
     cudaSetDevice(c->device);
     std::unique_ptr<srt_renderer> r(new (std::nothrow) srt_renderer());
     if (!r) return SRT_ERR_OOM;
@@ -647,7 +653,17 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     a.block_size = (int)p.block_size;
     a.ray_sort = (p.flags & SRT_FLAG_RAY_SORT) ? 1 : 0;
     a.sm_count = c->sm_count;
-    size_t n_events = 4 + 3 * (size_t)p.max_depth;
+    if (p.flags & SRT_FLAG_GUIDING) {
+        CUDA_TRY(c, guide_configure());
+        CUDA_TRY(c, guide_alloc(r->guide, np));
+        std::vector<float> w(G_NPARAMS);
+        guide_default_params(1, w.data());
+        CUDA_TRY(c, guide_upload(r->guide, w.data(), nullptr, nullptr, 0));
+        r->guide.train = (p.flags & SRT_FLAG_GUIDE_FROZEN) ? 0 : 1;
+        a.guiding = 1;
+        a.guide = r->guide;
+    }
+    size_t n_events = 5 + 3 * (size_t)p.max_depth;
     r->ev.resize(n_events);
     for (auto& e : r->ev) CUDA_TRY(c, cudaEventCreate(&e));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
@@ -693,7 +709,7 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
         r->launches += (uint64_t)n;
         CUDA_TRY(c, cudaGetLastError());
         if (timed) {
-            CUDA_TRY(c, cudaEventSynchronize(r->ev[3 + 3 * r->p.max_depth]));
+            CUDA_TRY(c, cudaEventSynchronize(r->ev.back()));
             float t;
             auto el = [&](size_t a, size_t b) {
                 cudaEventElapsedTime(&t, r->ev[a], r->ev[b]);
@@ -708,6 +724,7 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
                 r->ms[4] += el(base + 2, base + 3);
             }
             r->ms[5] += el(2 + 3 * r->p.max_depth, 3 + 3 * r->p.max_depth);
+            r->ms[7] += el(3 + 3 * r->p.max_depth, 4 + 3 * r->p.max_depth);
         }
     }
     r->trace_launches += r->p.max_depth;
@@ -801,6 +818,7 @@ extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
     out->ms_trace_shadow = r->ms[4];
     out->ms_finalize = r->ms[5];
     out->ms_raygen = r->ms[6];
+    out->ms_guide_train = r->ms[7];
     out->launches_trace_closest = r->trace_launches;
     out->kernel_launches = r->launches;
     return check_device_error(c, r->err);
@@ -962,5 +980,164 @@ extern "C" srt_status srt_test_device_math(srt_ctx* c, int op, uint32_t n, const
     cudaFree(dout);
     cudaFree(daux);
     if (e != cudaSuccess) return cuda_fail(c, e, "test_device_math");
+    return SRT_OK;
+}
+
+// ------------------------------------------------------------------ path guiding
+extern "C" uint32_t srt_guide_param_count(void) { return (uint32_t)G_NPARAMS; }
+
+extern "C" srt_status srt_guide_default_weights(uint64_t seed, float* out, uint32_t n) {
+    if (!out || n != (uint32_t)G_NPARAMS) return SRT_ERR_INVALID_ARG;
+    guide_default_params(seed, out);
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_get_weights(srt_renderer* r, float* out, uint32_t n) {
+    if (!r || !out || n != (uint32_t)G_NPARAMS) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemcpyAsync(out, r->guide.net.master, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_set_weights(srt_renderer* r, const float* w, uint32_t n) {
+    if (!r || !w || n != (uint32_t)G_NPARAMS) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, guide_upload(r->guide, w, nullptr, nullptr, 0));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_steps, uint32_t* threshold) {
+    if (!r) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    GuideCounters gc;
+    CUDA_TRY(c, cudaMemcpyAsync(&gc, r->guide.gc, sizeof gc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (adam_steps) *adam_steps = gc.adam_step;
+    if (threshold) *threshold = gc.threshold;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_set_learning_rate(srt_renderer* r, float lr) {
+    if (!r || !(lr >= 0.0f) || !(lr < 1.0f)) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->guide.lr = lr;
+    r->args.guide = r->guide;
+    if (r->graph) {  // the learning rate is a kernel argument of the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return SRT_OK;
+}
+
+namespace {
+struct GuideScratch {
+    GuideArgs g{};
+    float* x = nullptr;
+    float* y = nullptr;
+    float* z = nullptr;
+    ~GuideScratch() {
+        guide_free(g);
+        cudaFree(x);
+        cudaFree(y);
+        cudaFree(z);
+    }
+};
+}  // namespace
+
+extern "C" srt_status srt_guide_test_forward(srt_ctx* c, const float* params, const float* x, uint32_t n, float* out) {
+    if (!c || !params || (n && (!x || !out))) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (n == 0) return SRT_OK;
+    GuideScratch s;
+    CUDA_TRY(c, guide_configure());
+    CUDA_TRY(c, guide_alloc(s.g, 0));
+    CUDA_TRY(c, guide_upload(s.g, params, nullptr, nullptr, 0));
+    CUDA_TRY(c, dev_alloc(&s.x, (size_t)n * G_IN));
+    CUDA_TRY(c, dev_alloc(&s.y, (size_t)n * G_OUT));
+    CUDA_TRY(c, cudaMemcpyAsync(s.x, x, (size_t)n * G_IN * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_guide_test_forward(s.g.net, s.x, n, s.y, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(out, s.y, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_guide_test_mixture(srt_ctx* c, const float* raw, const float* omega, const float* u,
+                                             uint32_t n, float* out) {
+    if (!c || (n && (!raw || !omega || !u || !out))) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (n == 0) return SRT_OK;
+    GuideScratch s;
+    CUDA_TRY(c, dev_alloc(&s.x, (size_t)n * (G_OUT + 6)));
+    CUDA_TRY(c, dev_alloc(&s.y, (size_t)n * 4));
+    float* d_raw = s.x;
+    float* d_om = s.x + (size_t)n * G_OUT;
+    float* d_u = d_om + (size_t)n * 3;
+    CUDA_TRY(c, cudaMemcpyAsync(d_raw, raw, (size_t)n * G_OUT * 4, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(d_om, omega, (size_t)n * 12, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(d_u, u, (size_t)n * 12, cudaMemcpyHostToDevice, c->stream));
+    launch_guide_test_mixture(d_raw, d_om, d_u, n, s.y, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(out, s.y, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, const float* adam_m, const float* adam_v,
+                                           uint32_t adam_step, float lr, const float* x, const float* omega,
+                                           const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
+                                           float* params_out, float* m_out, float* v_out) {
+    if (!c || !params || !x || !omega || !pdf_bsdf || !weight || !grad_out || n == 0 || n > G_REC_CAP)
+        return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    GuideScratch s;
+    CUDA_TRY(c, guide_configure());
+    CUDA_TRY(c, guide_alloc(s.g, 0));
+    CUDA_TRY(c, guide_upload(s.g, params, adam_m, adam_v, adam_step));
+    s.g.lr = lr;
+    std::vector<float4> x0(n), x1(n), x2(n), w(n), b(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* xi = x + (size_t)i * G_IN;
+        x0[i] = make_float4(xi[0], xi[1], xi[2], xi[3]);
+        x1[i] = make_float4(xi[4], xi[5], xi[6], xi[7]);
+        x2[i] = make_float4(xi[8], xi[9], 0.f, 0.f);
+        w[i] = make_float4(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2], 1.0f);
+        b[i] = make_float4(pdf_bsdf[i], 0.f, 0.f, 0.f);
+    }
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.x0, x0.data(), n * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.x1, x1.data(), n * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.x2, x2.data(), n * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.w, w.data(), n * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.b, b.data(), n * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(s.g.rec.weight, weight, n * 4, cudaMemcpyHostToDevice));
+    // weights are used as given: their mean is set to 1 by weight_sum = n
+    GuideCounters gc{};
+    gc.records = n;
+    gc.weight_sum = (float)n;
+    gc.adam_step = adam_step;
+    CUDA_TRY(c, cudaMemcpy(s.g.gc, &gc, sizeof gc, cudaMemcpyHostToDevice));
+    launch_guide_test_train(s.g, 0, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(grad_out, s.g.net.grad, G_NPARAMS * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (params_out || m_out || v_out) {
+        launch_guide_test_train(s.g, 1, c->stream);
+        CUDA_TRY(c, cudaGetLastError());
+        if (params_out)
+            CUDA_TRY(c, cudaMemcpyAsync(params_out, s.g.net.master, G_NPARAMS * 4, cudaMemcpyDeviceToHost, c->stream));
+        if (m_out) CUDA_TRY(c, cudaMemcpyAsync(m_out, s.g.net.adam_m, G_NPARAMS * 4, cudaMemcpyDeviceToHost, c->stream));
+        if (v_out) CUDA_TRY(c, cudaMemcpyAsync(v_out, s.g.net.adam_v, G_NPARAMS * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SRT_OK;
 }

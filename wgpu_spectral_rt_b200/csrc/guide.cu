@@ -1,0 +1,950 @@
+// guide.cu — neural path guiding kernels (BF16 tensor cores, FP32 accumulate).
+//
+// The guide replaces the cosine sampling of Lambert vertices
+// (shader.wgsl:461-467) by a one-sample mixture of the learned vMF mixture q
+// and the cosine lobe: with probability sel sample q, else the BSDF; the
+// weight is f cos / (sel q + (1 - sel) cos / pi), so the estimator stays
+// unbiased and converges to the same image as the plain method (the NEE
+// weight of shader.wgsl:666 keeps its cos / pi term).
+//
+// Matrix products use mma.sync.m16n8k16 (bf16 x bf16 -> fp32).  A warp owns
+// 16 samples; the accumulator fragments of two adjacent 8-column tiles form
+// the A fragment of the next layer's 16-wide k step, so hidden activations
+// stay in registers between layers.  Training: a forward/backward pass that
+// writes every layer's activations and deltas (bf16), a split-K weight
+// gradient product over the samples, and Adam on FP32 master weights.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <vector>
+
+#include "guide.cuh"
+#include "render_kernels.h"
+
+namespace srt {
+
+namespace {
+
+constexpr int GW = 4;  // warps per block in the inference / fwd-bwd kernels
+
+SRT_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+SRT_DEV void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+SRT_DEV void ldsm4(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+SRT_DEV void ldsm4t(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+SRT_DEV uint32_t pack2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+SRT_DEV float2 unpack2(uint32_t u) {
+    __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162*>(&u);
+    return __bfloat1622float2(v);
+}
+
+// A fragment (16 x 16 at column k0) of a row-major bf16 matrix in shared memory.
+SRT_DEV void load_a(uint32_t (&a)[4], const __nv_bfloat16* m, int stride, int k0) {
+    int t = threadIdx.x & 31;
+    const __nv_bfloat16* p = m + ((t & 7) + 8 * ((t >> 3) & 1)) * stride + k0 + 8 * (t >> 4);
+    ldsm4(a, p);
+}
+// B fragments of two 8-column tiles (n0, n0 + 8) at k0 from W [n][k] row-major.
+SRT_DEV void load_b2(uint32_t (&b)[4], const __nv_bfloat16* W, int stride, int n0, int k0) {
+    int t = threadIdx.x & 31;
+    const __nv_bfloat16* p = W + (n0 + (t & 7) + 8 * (t >> 4)) * stride + k0 + 8 * ((t >> 3) & 1);
+    ldsm4(b, p);
+}
+
+// One dense layer for the warp's 16 samples: c = a W^T + bias.
+template <int K, int N>
+SRT_DEV void layer(const uint32_t (&a)[K / 16][4], const __nv_bfloat16* W, const float* bias, float (&c)[N / 8][4]) {
+    int t = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < N / 8; ++j) {
+        float b0 = bias[8 * j + 2 * (t & 3)], b1 = bias[8 * j + 2 * (t & 3) + 1];
+        c[j][0] = b0;
+        c[j][1] = b1;
+        c[j][2] = b0;
+        c[j][3] = b1;
+    }
+#pragma unroll
+    for (int s = 0; s < K / 16; ++s) {
+#pragma unroll
+        for (int j = 0; j < N / 8; j += 2) {
+            uint32_t b[4];
+            load_b2(b, W, g_pad(K), 8 * j, 16 * s);
+            mma16816(c[j], a[s], b[0], b[1]);
+            mma16816(c[j + 1], a[s], b[2], b[3]);
+        }
+    }
+}
+
+// Accumulators -> next A fragments (ReLU, bf16).
+template <int N>
+SRT_DEV void relu_to_a(const float (&c)[N / 8][4], uint32_t (&a)[N / 16][4]) {
+#pragma unroll
+    for (int s = 0; s < N / 16; ++s) {
+        a[s][0] = pack2(fmaxf(c[2 * s][0], 0.f), fmaxf(c[2 * s][1], 0.f));
+        a[s][1] = pack2(fmaxf(c[2 * s][2], 0.f), fmaxf(c[2 * s][3], 0.f));
+        a[s][2] = pack2(fmaxf(c[2 * s + 1][0], 0.f), fmaxf(c[2 * s + 1][1], 0.f));
+        a[s][3] = pack2(fmaxf(c[2 * s + 1][2], 0.f), fmaxf(c[2 * s + 1][3], 0.f));
+    }
+}
+
+// Frequency encoding of 5 of the 10 inputs (half h) of one sample into its
+// bf16 row: feature 12 d + 2 k = sin(2^k pi x_d), + 1 = cos; 120..127 = 0.
+// Octaves k >= 1 come from the double-angle identities with every rounding
+// pinned (sin' = (2 s) c, cos' = fma(c, c, -(s s))), so a CPU restatement
+// reproduces them bit for bit from the same octave-0 values.
+SRT_DEV void encode_half(const float* x, int h, __nv_bfloat16* row) {
+#pragma unroll
+    for (int dd = 0; dd < 5; ++dd) {
+        int d = 5 * h + dd;
+        float s, c;
+        sincospif(x[d], &s, &c);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            row[12 * d + 2 * k] = __float2bfloat16_rn(s);
+            row[12 * d + 2 * k + 1] = __float2bfloat16_rn(c);
+            float s2 = __fmul_rn(__fmul_rn(2.0f, s), c);
+            float c2 = __fmaf_rn(c, c, -__fmul_rn(s, s));
+            s = s2;
+            c = c2;
+        }
+    }
+    if (h == 1)
+        for (int f = 120; f < 128; ++f) row[f] = __float2bfloat16_rn(0.0f);
+}
+
+// Raw outputs of one sample -> mixture parameters.
+struct Mix {
+    float3 mu[G_LOBES];
+    float kappa[G_LOBES];
+    float pi[G_LOBES];
+    float sel, sel_sig;
+    float norm[G_LOBES];
+    float lk[G_LOBES];
+};
+SRT_DEV void mixture(const float* r, Mix& m) {
+    float mx = -3.4e38f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) mx = fmaxf(mx, r[5 * j + 4]);
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) {
+        float3 v = f3(r[5 * j], r[5 * j + 1], r[5 * j + 2]);
+        float n = fmaxf(length(v), 1e-12f);
+        m.norm[j] = n;
+        m.mu[j] = v / n;
+        m.lk[j] = r[5 * j + 3];
+        m.kappa[j] = expf(clampf(r[5 * j + 3], G_KAPPA_LO, G_KAPPA_HI));
+        m.pi[j] = expf(r[5 * j + 4] - mx);
+        sum += m.pi[j];
+    }
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) m.pi[j] /= sum;
+    m.sel_sig = 1.0f / (1.0f + expf(-r[40]));
+    m.sel = G_SEL_LO + G_SEL_SPAN * m.sel_sig;
+}
+SRT_DEV float vmf(float3 mu, float k, float3 w) {
+    return k / (2.0f * PI * (-expm1f(-2.0f * k))) * expf(k * (dot(mu, w) - 1.0f));
+}
+SRT_DEV float mix_pdf(const Mix& m, float3 w) {
+    float q = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) q += m.pi[j] * vmf(m.mu[j], m.kappa[j], w);
+    return q;
+}
+// Sample a vMF lobe (Wenzel Jakob's stable form of Wood's method).
+SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
+    float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
+    w = clampf(w, -1.0f, 1.0f);
+    float r = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    float sp, cp;
+    sincospif(2.0f * u2, &sp, &cp);
+    float3 t = fabsf(mu.x) > 0.9f ? f3(0.f, 1.f, 0.f) : f3(1.f, 0.f, 0.f);
+    float3 b1 = normalize(cross(mu, t));
+    float3 b2 = cross(mu, b1);
+    return normalize(mu * w + b1 * (r * cp) + b2 * (r * sp));
+}
+
+// Loads all layer weights (bf16, padded rows) and biases into shared memory.
+SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb, bool transposed, __nv_bfloat16* swt) {
+    int off = 0;
+    for (int l = 0; l < G_LAYERS; ++l) {
+        int K = g_in(l), N = g_out(l);
+        for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
+            int n = i / K, k = i - n * K;
+            sw[off + n * g_pad(K) + k] = net.wbf[g_woff(l) + i];
+        }
+        off += N * g_pad(K);
+    }
+    int bo = 0;
+    for (int l = 0; l < G_LAYERS; ++l) {
+        for (int i = threadIdx.x; i < g_out(l); i += blockDim.x) sb[bo + i] = net.master[g_boff(l) + i];
+        bo += g_out(l);
+    }
+    if (transposed) {  // W^T [in][out] of layers 1..4 for the backward pass
+        int o2 = 0;
+        for (int l = 1; l < G_LAYERS; ++l) {
+            int K = g_in(l), N = g_out(l);
+            for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
+                int k = i / N, n = i - k * N;  // wtbf is [in][out]
+                swt[o2 + k * g_pad(N) + n] = net.wtbf[g_woff(l) + i];
+            }
+            o2 += K * g_pad(N);
+        }
+    }
+}
+constexpr int SW_ELEMS = G_HID * g_pad(G_ENC) + 3 * G_HID * g_pad(G_HID) + G_OUT * g_pad(G_HID);
+constexpr int SWT_ELEMS = 3 * G_HID * g_pad(G_HID) + G_HID * g_pad(G_OUT);
+constexpr int SB_ELEMS = 4 * G_HID + G_OUT;
+SRT_DEV const __nv_bfloat16* wl(const __nv_bfloat16* sw, int l) {
+    int off = 0;
+    for (int i = 0; i < l; ++i) off += g_out(i) * g_pad(g_in(i));
+    return sw + off;
+}
+SRT_DEV const __nv_bfloat16* wtl(const __nv_bfloat16* swt, int l) {  // l = 1..4
+    int off = 0;
+    for (int i = 1; i < l; ++i) off += g_in(i) * g_pad(g_out(i));
+    return swt + off;
+}
+SRT_DEV const float* bl(const float* sb, int l) { return sb + l * G_HID; }
+
+// Forward pass of the warp's 16 encoded samples (smem rows `in`) -> raw
+// outputs in smem `out` [16][52].  With `act`, post-ReLU activations are also
+// stored to smem (act[l] [16][72]).
+SRT_DEV void forward16(const __nv_bfloat16* sw, const float* sb, const __nv_bfloat16* in, float* out,
+                       __nv_bfloat16* act) {
+    int t = threadIdx.x & 31;
+    int g = t >> 2, cq = t & 3;
+    float c[8][4];
+    {
+        uint32_t a0[8][4];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) load_a(a0[s], in, g_pad(G_ENC), 16 * s);
+        layer<G_ENC, G_HID>(a0, wl(sw, 0), bl(sb, 0), c);
+    }
+    uint32_t a[4][4];
+#pragma unroll
+    for (int l = 1; l < 4; ++l) {
+        relu_to_a<G_HID>(c, a);
+        if (act) {
+            __nv_bfloat16* m = act + (l - 1) * 16 * g_pad(G_HID);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                *reinterpret_cast<uint32_t*>(m + g * g_pad(G_HID) + 16 * s + 2 * cq) = a[s][0];
+                *reinterpret_cast<uint32_t*>(m + (g + 8) * g_pad(G_HID) + 16 * s + 2 * cq) = a[s][1];
+                *reinterpret_cast<uint32_t*>(m + g * g_pad(G_HID) + 16 * s + 8 + 2 * cq) = a[s][2];
+                *reinterpret_cast<uint32_t*>(m + (g + 8) * g_pad(G_HID) + 16 * s + 8 + 2 * cq) = a[s][3];
+            }
+        }
+        layer<G_HID, G_HID>(a, wl(sw, l), bl(sb, l), c);
+    }
+    relu_to_a<G_HID>(c, a);
+    if (act) {
+        __nv_bfloat16* m = act + 3 * 16 * g_pad(G_HID);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            *reinterpret_cast<uint32_t*>(m + g * g_pad(G_HID) + 16 * s + 2 * cq) = a[s][0];
+            *reinterpret_cast<uint32_t*>(m + (g + 8) * g_pad(G_HID) + 16 * s + 2 * cq) = a[s][1];
+            *reinterpret_cast<uint32_t*>(m + g * g_pad(G_HID) + 16 * s + 8 + 2 * cq) = a[s][2];
+            *reinterpret_cast<uint32_t*>(m + (g + 8) * g_pad(G_HID) + 16 * s + 8 + 2 * cq) = a[s][3];
+        }
+    }
+    float o[6][4];
+    layer<G_HID, G_OUT>(a, wl(sw, 4), bl(sb, 4), o);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        out[g * 52 + 8 * j + 2 * cq] = o[j][0];
+        out[g * 52 + 8 * j + 2 * cq + 1] = o[j][1];
+        out[(g + 8) * 52 + 8 * j + 2 * cq] = o[j][2];
+        out[(g + 8) * 52 + 8 * j + 2 * cq + 1] = o[j][3];
+    }
+}
+
+// Network inputs of a vertex, each mapped to [0, 1].
+SRT_DEV void vertex_inputs(float3 p, float3 n, float3 wo, float lambda, float4 bmin, float4 binv, float* x) {
+    x[0] = (p.x - bmin.x) * binv.x;
+    x[1] = (p.y - bmin.y) * binv.y;
+    x[2] = (p.z - bmin.z) * binv.z;
+    x[3] = n.x * 0.5f + 0.5f;
+    x[4] = n.y * 0.5f + 0.5f;
+    x[5] = n.z * 0.5f + 0.5f;
+    x[6] = wo.x * 0.5f + 0.5f;
+    x[7] = wo.y * 0.5f + 0.5f;
+    x[8] = wo.z * 0.5f + 0.5f;
+    x[9] = (lambda - LAMBDA_MIN) / LAMBDA_RANGE;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- inference
+// The continuation of every Lambert vertex of this bounce (the tail of
+// shader.wgsl:677-700 for material 0): mixture sampling, throughput,
+// Russian roulette, next queue; plus the recording of training samples.
+__global__ void __launch_bounds__(GW * 32) k_guide_infer(FrameArgs a, uint32_t bounce) {
+    const GuideArgs& G = a.guide;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
+    unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4));
+    float* out = reinterpret_cast<float*>(in + 16 * g_pad(G_ENC));
+    const uint32_t n = G.gc->verts[bounce];
+    if (blockIdx.x * GW * 16 >= n) return;
+    load_weights(G.net, sw, sb, false, nullptr);
+    __syncthreads();
+    const DevScene& S = a.scene;
+    const uint32_t frame = a.cam->frame_count;
+    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+        // encode: two lanes per sample
+        {
+            uint32_t v = base + (lane & 15);
+            float x[G_IN];
+            if (v < n) {
+                float4 p = G.gv.p[v], nn = G.gv.n[v], wo = G.gv.wo[v];
+                vertex_inputs(xyz(p), xyz(nn), xyz(wo), p.w, S.bmin, S.binv, x);
+            } else {
+                for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
+            }
+            encode_half(x, lane >> 4, in + (lane & 15) * g_pad(G_ENC));
+        }
+        __syncwarp();
+        forward16(sw, sb, in, out, nullptr);
+        __syncwarp();
+        bool alive = false;
+        uint32_t id = 0;
+        if (lane < 16 && base + lane < n) {
+            uint32_t v = base + lane;
+            id = G.gv.id[v];
+            float4 p = G.gv.p[v], nn = G.gv.n[v], wo4 = G.gv.wo[v], spec = G.gv.spec[v];
+            float3 hp = xyz(p), ffn = xyz(nn);
+            Mix m;
+            mixture(out + lane * 52, m);
+            uint4 misc = a.pb.misc[id];
+            uint32_t s = misc.x;
+            float4 thr = a.pb.thr[id];
+            float3 dir;
+            if (rng_next(s) < m.sel) {
+                float u = rng_next(s), acc = 0.f;
+                int j = G_LOBES - 1;
+                for (int i = 0; i < G_LOBES; ++i) {
+                    acc += m.pi[i];
+                    if (u < acc) {
+                        j = i;
+                        break;
+                    }
+                }
+                float u1 = rng_next(s), u2 = rng_next(s);
+                dir = vmf_sample(m.mu[j], m.kappa[j], u1, u2);
+            } else {
+                float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
+                if (length(d) < 0.001f) d = ffn;
+                dir = normalize(d);
+            }
+            float cosv = dot(ffn, dir);
+            uint32_t rec = 0u;  // record index + 1 (0: none)
+            if (cosv > 0.0f) {
+                float pb = cosv / PI;
+                float q = mix_pdf(m, dir);
+                float pdf = m.sel * q + (1.0f - m.sel) * pb;
+                float4 att = spec * (pb / pdf);  // (spec / pi) cos / pdf
+                thr = thr * att;
+                // training sample (a hashed subset of the vertices)
+                if (G.train) {
+                    atomicAdd(&G.gc->candidates, 1u);
+                    uint32_t h = pcg_hash(id ^ (bounce << 24) ^ (frame * 0x9E3779B9u)) & 0xFFFFu;
+                    if (h < G.gc->threshold) {
+                        uint32_t r = atomicAdd(&G.gc->records, 1u);
+                        if (r < G_REC_CAP) {
+                            float x[G_IN];
+                            vertex_inputs(hp, ffn, xyz(wo4), p.w, S.bmin, S.binv, x);
+                            G.rec.x0[r] = f4(x[0], x[1], x[2], x[3]);
+                            G.rec.x1[r] = f4(x[4], x[5], x[6], x[7]);
+                            G.rec.x2[r] = f4(x[8], x[9], 0.f, 0.f);
+                            G.rec.w[r] = f4(dir.x, dir.y, dir.z, pdf);
+                            float fcos = (spec.x + spec.y + spec.z + spec.w) * 0.25f * pb;
+                            G.rec.b[r] = f4(pb, fcos, 0.f, 0.f);
+                            G.rec.thr[r] = thr;
+                            G.rec.rad[r] = splat4(__int_as_float(0x7FC00000));  // NaN: not reached yet
+                            G.rec.pid[r] = id;
+                            rec = r + 1u;
+                        }
+                    }
+                }
+                alive = true;
+                if (bounce > 3u) {
+                    float pr = max4(thr);
+                    if (rng_next(s) > pr) alive = false;
+                    else thr = thr / pr;
+                }
+                if (bounce + 1u >= a.max_depth) alive = false;
+            }
+            if (alive) {
+                a.pb.thr[id] = thr;
+                a.pb.ray_o[id] = f4(hp.x, hp.y, hp.z, 0.0001f);
+                a.pb.ray_d[id] = f4(dir.x, dir.y, dir.z, 100.0f);
+            }
+            a.pb.misc[id] = make_uint4(s, misc.y, misc.z, rec);
+        }
+        // push the survivors into the next bounce's queue
+        uint32_t mask = __ballot_sync(0xFFFFFFFFu, alive);
+        uint32_t slot_base = 0;
+        if (mask) {
+            int leader = __ffs(mask) - 1;
+            if (lane == leader) slot_base = atomicAdd(&a.counters->paths[bounce + 1], (uint32_t)__popc(mask));
+            slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, leader);
+        }
+        if (alive) a.pb.queue[(bounce + 1) & 1][slot_base + __popc(mask & ((1u << lane) - 1u))] = id;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- training
+// Per record: the radiance that arrived along the sampled direction and the
+// training weight F / p = L f cos / p.  Records whose path ended before its
+// next vertex carry no later radiance (L = 0).
+__global__ void k_guide_targets(FrameArgs a) {
+    const GuideArgs& G = a.guide;
+    uint32_t n = min(G.gc->records, G_REC_CAP);
+    float local = 0.f;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        float4 fin = a.pb.rad[G.rec.pid[r]];
+        float4 nx = G.rec.rad[r];
+        if (nx.x != nx.x) nx = fin;
+        float4 t = G.rec.thr[r];
+        float L = 0.f;
+        L += t.x > 0.f ? (fin.x - nx.x) / t.x : 0.f;
+        L += t.y > 0.f ? (fin.y - nx.y) / t.y : 0.f;
+        L += t.z > 0.f ? (fin.z - nx.z) / t.z : 0.f;
+        L += t.w > 0.f ? (fin.w - nx.w) / t.w : 0.f;
+        L = fmaxf(L * 0.25f, 0.f);
+        float4 w = G.rec.w[r], b = G.rec.b[r];
+        float wt = L * b.y / fmaxf(w.w, 1e-20f);
+        if (!(wt < 3.4e38f)) wt = 0.f;
+        G.rec.weight[r] = wt;
+        local += wt;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xFFFFFFFFu, local, o);
+    if ((threadIdx.x & 31) == 0 && local != 0.f) atomicAdd(&G.gc->weight_sum, local);
+}
+
+// Forward + backward of 16 records per warp: stores the encoded inputs,
+// post-ReLU activations and per-layer deltas (bf16) for the weight-gradient
+// product.  Loss per sample (weight w normalised by the batch mean):
+//   -w log q(omega) for the lobes, -w log(sel q + (1 - sel) p_bsdf) for sel.
+__global__ void __launch_bounds__(GW * 32) k_guide_fwdbwd(GuideArgs G) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* swt = sw + SW_ELEMS;
+    float* sb = reinterpret_cast<float*>(swt + SWT_ELEMS);
+    unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per_warp = 16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2;
+    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * per_warp);
+    __nv_bfloat16* act = in + 16 * g_pad(G_ENC);
+    float* out = reinterpret_cast<float*>(act + 4 * 16 * g_pad(G_HID));
+    __nv_bfloat16* d4 = reinterpret_cast<__nv_bfloat16*>(out + 16 * 52);
+    const uint32_t n = min(G.gc->records, G_REC_CAP);
+    if (blockIdx.x * GW * 16 >= n) return;
+    load_weights(G.net, sw, sb, true, swt);
+    __syncthreads();
+    const float inv_mean = G.gc->weight_sum > 0.f ? (float)n / G.gc->weight_sum : 0.f;
+    const int g = lane >> 2, cq = lane & 3;
+    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+        {
+            uint32_t r = base + (lane & 15);
+            float x[G_IN];
+            if (r < n) {
+                float4 x0 = G.rec.x0[r], x1 = G.rec.x1[r], x2 = G.rec.x2[r];
+                x[0] = x0.x; x[1] = x0.y; x[2] = x0.z; x[3] = x0.w;
+                x[4] = x1.x; x[5] = x1.y; x[6] = x1.z; x[7] = x1.w;
+                x[8] = x2.x; x[9] = x2.y;
+            } else {
+                for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
+            }
+            encode_half(x, lane >> 4, in + (lane & 15) * g_pad(G_ENC));
+        }
+        __syncwarp();
+        forward16(sw, sb, in, out, act);
+        __syncwarp();
+        // output gradient, one lane per sample
+        if (lane < 16) {
+            uint32_t r = base + lane;
+            float gr[G_OUT];
+            for (int i = 0; i < G_OUT; ++i) gr[i] = 0.f;
+            if (r < n) {
+                const float* raw = out + lane * 52;
+                Mix m;
+                mixture(raw, m);
+                float4 w4 = G.rec.w[r], b4 = G.rec.b[r];
+                float3 om = xyz(w4);
+                float wt = G.rec.weight[r] * inv_mean;
+                float vm[G_LOBES], q = 0.f;
+                for (int j = 0; j < G_LOBES; ++j) {
+                    vm[j] = vmf(m.mu[j], m.kappa[j], om);
+                    q += m.pi[j] * vm[j];
+                }
+                q = fmaxf(q, 1e-30f);
+                for (int j = 0; j < G_LOBES; ++j) {
+                    float gam = m.pi[j] * vm[j] / q;
+                    gr[5 * j + 4] = wt * (m.pi[j] - gam);
+                    float k = m.kappa[j];
+                    float mw = dot(m.mu[j], om);
+                    float dl = 1.0f / k - 2.0f / expm1f(2.0f * k) + mw - 1.0f;
+                    bool inside = m.lk[j] > G_KAPPA_LO && m.lk[j] < G_KAPPA_HI;
+                    gr[5 * j + 3] = inside ? -wt * gam * dl * k : 0.f;
+                    float3 gd = (om - m.mu[j] * mw) * (-wt * gam * k / m.norm[j]);
+                    gr[5 * j] = gd.x;
+                    gr[5 * j + 1] = gd.y;
+                    gr[5 * j + 2] = gd.z;
+                }
+                float pb = b4.x;
+                float pmix = fmaxf(m.sel * q + (1.0f - m.sel) * pb, 1e-30f);
+                gr[40] = -wt * (q - pb) / pmix * G_SEL_SPAN * m.sel_sig * (1.0f - m.sel_sig);
+            }
+            for (int i = 0; i < G_OUT; i += 2)
+                *reinterpret_cast<uint32_t*>(d4 + lane * g_pad(G_OUT) + i) = pack2(gr[i], gr[i + 1]);
+        }
+        __syncwarp();
+        // store inputs, activations and the output delta for the weight gradients
+        for (int e = lane; e < 16 * (G_ACT_STRIDE / 8); e += 32) {
+            int row = e / (G_ACT_STRIDE / 8), ch = e % (G_ACT_STRIDE / 8);
+            uint32_t r = base + row;
+            if (r >= n) continue;
+            const __nv_bfloat16* src = ch < 16 ? in + row * g_pad(G_ENC) + 8 * ch
+                                               : act + ((ch - 16) / 8) * 16 * g_pad(G_HID) + row * g_pad(G_HID) +
+                                                     8 * ((ch - 16) % 8);
+            *reinterpret_cast<uint4*>(G.rec.act + (size_t)r * G_ACT_STRIDE + 8 * ch) =
+                *reinterpret_cast<const uint4*>(src);
+        }
+        for (int e = lane; e < 16 * (G_OUT / 8); e += 32) {
+            int row = e / (G_OUT / 8), ch = e % (G_OUT / 8);
+            uint32_t r = base + row;
+            if (r >= n) continue;
+            *reinterpret_cast<uint4*>(G.rec.delta + (size_t)r * G_DELTA_STRIDE + g_delta_off(4) + 8 * ch) =
+                *reinterpret_cast<const uint4*>(d4 + row * g_pad(G_OUT) + 8 * ch);
+        }
+        // backward: delta_l = (delta_{l+1} W_{l+1}) * relu'(a_l), l = 3..0
+        uint32_t da[4][4];  // A fragments of the current delta (K up to 64)
+#pragma unroll
+        for (int s = 0; s < 3; ++s) load_a(da[s], d4, g_pad(G_OUT), 16 * s);
+#pragma unroll
+        for (int l = 3; l >= 0; --l) {
+            const int K = l == 3 ? G_OUT : G_HID;
+            float c[8][4];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+            const __nv_bfloat16* WT = wtl(swt, l + 1);  // [in = 64][out = K]
+#pragma unroll
+            for (int s = 0; s < K / 16; ++s) {
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) {
+                    uint32_t b[4];
+                    load_b2(b, WT, g_pad(K), 8 * j, 16 * s);
+                    mma16816(c[j], da[s], b[0], b[1]);
+                    mma16816(c[j + 1], da[s], b[2], b[3]);
+                }
+            }
+            // relu' mask from the stored activation a_l
+            const __nv_bfloat16* am = act + l * 16 * g_pad(G_HID);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float2 lo = unpack2(*reinterpret_cast<const uint32_t*>(am + g * g_pad(G_HID) + 8 * j + 2 * cq));
+                float2 hi = unpack2(*reinterpret_cast<const uint32_t*>(am + (g + 8) * g_pad(G_HID) + 8 * j + 2 * cq));
+                c[j][0] = lo.x > 0.f ? c[j][0] : 0.f;
+                c[j][1] = lo.y > 0.f ? c[j][1] : 0.f;
+                c[j][2] = hi.x > 0.f ? c[j][2] : 0.f;
+                c[j][3] = hi.y > 0.f ? c[j][3] : 0.f;
+            }
+            // to A fragments (no ReLU: already masked) and to global memory
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                da[s][0] = pack2(c[2 * s][0], c[2 * s][1]);
+                da[s][1] = pack2(c[2 * s][2], c[2 * s][3]);
+                da[s][2] = pack2(c[2 * s + 1][0], c[2 * s + 1][1]);
+                da[s][3] = pack2(c[2 * s + 1][2], c[2 * s + 1][3]);
+            }
+            uint32_t r0 = base + g, r1 = base + g + 8;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                __nv_bfloat16* d0 = G.rec.delta + g_delta_off(l) + 16 * s + 2 * cq;
+                if (r0 < n) {
+                    *reinterpret_cast<uint32_t*>(d0 + (size_t)r0 * G_DELTA_STRIDE) = da[s][0];
+                    *reinterpret_cast<uint32_t*>(d0 + (size_t)r0 * G_DELTA_STRIDE + 8) = da[s][2];
+                }
+                if (r1 < n) {
+                    *reinterpret_cast<uint32_t*>(d0 + (size_t)r1 * G_DELTA_STRIDE) = da[s][1];
+                    *reinterpret_cast<uint32_t*>(d0 + (size_t)r1 * G_DELTA_STRIDE + 8) = da[s][3];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Weight gradients dW_l = sum_s delta_l[s]^T a_{l-1}[s] (and bias sums),
+// split over the samples; job (blockIdx.y): 0, 1 = layer 0 input halves,
+// 2..5 = layers 1..4.  8 warps: warp w owns output rows 16 (w & 3) .. + 15
+// and input columns 32 (w >> 2) .. + 31 of the 64 x 64 block.
+constexpr int WGRAD_BLOCKS = 64;  // sample splits per job
+__global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) {
+    __shared__ __align__(16) __nv_bfloat16 sd[32 * g_pad(G_HID)];
+    __shared__ __align__(16) __nv_bfloat16 sa[32 * g_pad(G_HID)];
+    const uint32_t n = min(G.gc->records, G_REC_CAP);
+    const int job = blockIdx.y;
+    const int l = job <= 1 ? 0 : job - 1;
+    const int in0 = job == 1 ? 64 : 0;
+    const int nout = g_out(l), nin = g_in(l);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = warp & 3, nh = warp >> 2;
+    const bool active_rows = 16 * mt < nout;
+    float c[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+    float bsum = 0.f;
+    const uint32_t chunk = 32;
+    uint32_t per = (((n + gridDim.x - 1) / gridDim.x) + chunk - 1) / chunk * chunk;
+    uint32_t s0 = blockIdx.x * per, s1 = min(n, s0 + per);
+    for (uint32_t s = s0; s < s1; s += chunk) {
+        // stage 32 samples: deltas (out columns) and activations (input columns)
+        {
+            int row = threadIdx.x >> 3, ch = threadIdx.x & 7;
+            uint32_t r = s + row;
+            uint4 dv = make_uint4(0, 0, 0, 0), av = make_uint4(0, 0, 0, 0);
+            if (r < s1) {
+                if (8 * ch < nout)
+                    dv = *reinterpret_cast<const uint4*>(G.rec.delta + (size_t)r * G_DELTA_STRIDE + g_delta_off(l) + 8 * ch);
+                av = *reinterpret_cast<const uint4*>(G.rec.act + (size_t)r * G_ACT_STRIDE + g_act_off(l - 1) + in0 + 8 * ch);
+            }
+            *reinterpret_cast<uint4*>(sd + row * g_pad(G_HID) + 8 * ch) = dv;
+            *reinterpret_cast<uint4*>(sa + row * g_pad(G_HID) + 8 * ch) = av;
+        }
+        __syncthreads();
+        if (job != 1 && threadIdx.x < nout) {
+            for (int row = 0; row < 32; ++row) bsum += __bfloat162float(sd[row * g_pad(G_HID) + threadIdx.x]);
+        }
+        if (active_rows) {
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                uint32_t af[4];
+                {
+                    // A = delta^T: rows = outputs 16 mt.., k = samples 16 ks..
+                    const __nv_bfloat16* p =
+                        sd + (16 * ks + (lane & 7) + 8 * (lane >> 4)) * g_pad(G_HID) + 16 * mt + 8 * ((lane >> 3) & 1);
+                    ldsm4t(af, p);
+                }
+#pragma unroll
+                for (int jp = 0; jp < 2; ++jp) {
+                    uint32_t bf[4];
+                    // B = activations: k = samples 16 ks.., n = inputs 32 nh + 16 jp ..
+                    const __nv_bfloat16* p = sa + (16 * ks + (lane & 7) + 8 * ((lane >> 3) & 1)) * g_pad(G_HID) +
+                                             32 * nh + 16 * jp + 8 * (lane >> 4);
+                    ldsm4t(bf, p);
+                    mma16816(c[2 * jp], af, bf[0], bf[1]);
+                    mma16816(c[2 * jp + 1], af, bf[2], bf[3]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (s0 >= s1) return;
+    if (active_rows) {
+        const int g = lane >> 2, cq = lane & 3;
+        float* gw = G.net.grad + g_woff(l);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int col = in0 + 32 * nh + 8 * j + 2 * cq;
+            int r0 = 16 * mt + g, r1 = r0 + 8;
+            atomicAdd(gw + r0 * nin + col, c[j][0]);
+            atomicAdd(gw + r0 * nin + col + 1, c[j][1]);
+            atomicAdd(gw + r1 * nin + col, c[j][2]);
+            atomicAdd(gw + r1 * nin + col + 1, c[j][3]);
+        }
+    }
+    if (job != 1 && threadIdx.x < nout && bsum != 0.f) atomicAdd(G.net.grad + g_boff(l) + threadIdx.x, bsum);
+}
+
+// Adam on the FP32 master weights (gradients are sums over the batch and
+// are divided by its size), then the bf16 copies; clears the gradients.
+__global__ void k_guide_adam(GuideArgs G) {
+    const uint32_t n = min(G.gc->records, G_REC_CAP);
+    if (n == 0) return;
+    const float inv = 1.0f / (float)n;
+    const float t = (float)(G.gc->adam_step + 1u);
+    const float b1t = 1.0f - powf(0.9f, t), b2t = 1.0f - powf(0.999f, t);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G_NPARAMS; i += gridDim.x * blockDim.x) {
+        float gr = G.net.grad[i] * inv;
+        G.net.grad[i] = 0.f;
+        float m = 0.9f * G.net.adam_m[i] + 0.1f * gr;
+        float v = 0.999f * G.net.adam_v[i] + 0.001f * gr * gr;
+        G.net.adam_m[i] = m;
+        G.net.adam_v[i] = v;
+        float w = G.net.master[i] - G.lr * (m / b1t) / (sqrtf(v / b2t) + 1e-8f);
+        G.net.master[i] = w;
+        int l = 0;
+        while (l < 4 && i >= g_woff(l + 1)) ++l;
+        int k = i - g_woff(l);
+        if (k < g_in(l) * g_out(l)) {
+            __nv_bfloat16 h = __float2bfloat16_rn(w);
+            G.net.wbf[i] = h;
+            int o = k / g_in(l), in = k - o * g_in(l);
+            G.net.wtbf[g_woff(l) + in * g_out(l) + o] = h;
+        }
+    }
+}
+
+// Next frame's recording threshold (of 65536) so that about 90 % of the
+// record capacity fills; counts the Adam step; clears the per-frame counters.
+__global__ void k_guide_frame_end(GuideArgs G, int trained) {
+    GuideCounters* gc = G.gc;
+    if (threadIdx.x < 32) gc->verts[threadIdx.x] = 0u;
+    if (threadIdx.x != 0) return;
+    uint32_t c = gc->candidates;
+    if (c > 0) {
+        double t = 65536.0 * 0.9 * (double)G_REC_CAP / (double)c;
+        gc->threshold = (uint32_t)fmin(65536.0, fmax(1.0, t));
+    }
+    if (trained && gc->records > 0u) gc->adam_step += 1u;
+    gc->records = 0u;
+    gc->candidates = 0u;
+    gc->weight_sum = 0.f;
+}
+
+// ---------------------------------------------------------------- test kernels
+// Forward pass of n samples (inputs [n][10]) -> raw outputs [n][48].
+__global__ void __launch_bounds__(GW * 32) k_guide_test_forward(GuideNet net, const float* __restrict__ x, uint32_t n,
+                                                                float* __restrict__ y) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
+    unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4));
+    float* out = reinterpret_cast<float*>(in + 16 * g_pad(G_ENC));
+    load_weights(net, sw, sb, false, nullptr);
+    __syncthreads();
+    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+        uint32_t r = base + (lane & 15);
+        float xi[G_IN];
+        for (int i = 0; i < G_IN; ++i) xi[i] = r < n ? x[(size_t)r * G_IN + i] : 0.f;
+        encode_half(xi, lane >> 4, in + (lane & 15) * g_pad(G_ENC));
+        __syncwarp();
+        forward16(sw, sb, in, out, nullptr);
+        __syncwarp();
+        if (lane < 16 && base + lane < n)
+            for (int i = 0; i < G_OUT; ++i) y[(size_t)(base + lane) * G_OUT + i] = out[lane * 52 + i];
+        __syncwarp();
+    }
+}
+
+// Mixture pdf and samples from raw outputs: out[i] = (pdf(omega_i), sample xyz)
+__global__ void k_guide_test_mixture(const float* __restrict__ raw, const float* __restrict__ omega,
+                                     const float* __restrict__ u, uint32_t n, float* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Mix m;
+    mixture(raw + (size_t)i * G_OUT, m);
+    float3 w = f3(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2]);
+    float pdf = mix_pdf(m, w);
+    float uu = u[3 * i], acc = 0.f;
+    int j = G_LOBES - 1;
+    for (int k = 0; k < G_LOBES; ++k) {
+        acc += m.pi[k];
+        if (uu < acc) {
+            j = k;
+            break;
+        }
+    }
+    float3 s = vmf_sample(m.mu[j], m.kappa[j], u[3 * i + 1], u[3 * i + 2]);
+    out[4 * i] = pdf;
+    out[4 * i + 1] = s.x;
+    out[4 * i + 2] = s.y;
+    out[4 * i + 3] = s.z;
+}
+
+// ---------------------------------------------------------------- launchers
+size_t guide_infer_smem() {
+    return SW_ELEMS * 2 + SB_ELEMS * 4 + GW * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4);
+}
+size_t guide_train_smem() {
+    return (SW_ELEMS + SWT_ELEMS) * 2 + SB_ELEMS * 4 +
+           GW * (16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2);
+}
+
+cudaError_t guide_configure() {
+    cudaError_t e = cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_infer_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_test_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)guide_infer_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_fwdbwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_train_smem());
+    return e;
+}
+
+int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
+    uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * 2;
+    k_guide_infer<<<grid, GW * 32, guide_infer_smem(), st>>>(a, bounce);
+    return 1;
+}
+
+namespace {
+int launch_train_steps(const GuideArgs& g, int sm, int adam, cudaStream_t st) {
+    k_guide_fwdbwd<<<sm, GW * 32, guide_train_smem(), st>>>(g);
+    dim3 wg(WGRAD_BLOCKS, 6);
+    k_guide_wgrad<<<wg, 256, 0, st>>>(g);
+    if (!adam) return 2;
+    k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g);
+    return 3;
+}
+}  // namespace
+
+int launch_guide_train(const FrameArgs& a, cudaStream_t st) {
+    const GuideArgs& g = a.guide;
+    int sm = a.sm_count > 0 ? a.sm_count : 148;
+    int n = 0;
+    if (g.train) {
+        k_guide_targets<<<sm * 4, 256, 0, st>>>(a);
+        n = 1 + launch_train_steps(g, sm, 1, st);
+    }
+    k_guide_frame_end<<<1, 32, 0, st>>>(g, g.train);
+    return n + 1;
+}
+
+int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st) {
+    if (phase == 0) return launch_train_steps(g, 148, 0, st);
+    k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g);
+    return 1;
+}
+
+// ---------------------------------------------------------------- host side
+namespace {
+template <class T>
+cudaError_t galloc(T** p, size_t n) {
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+// splitmix64: the deterministic stream of the default initialisation
+uint64_t splitmix(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+}  // namespace
+
+void guide_default_params(uint64_t seed, float* out) {
+    uint64_t x = seed;
+    for (int l = 0; l < G_LAYERS; ++l) {
+        // He-uniform; the output layer starts 10x smaller so the first
+        // mixtures are broad and nearly uniform
+        float a = sqrtf(6.0f / (float)g_in(l)) * (l == 4 ? 0.1f : 1.0f);
+        for (int i = 0; i < g_in(l) * g_out(l); ++i) {
+            double u = (double)(splitmix(x) >> 11) * (1.0 / 9007199254740992.0);
+            out[g_woff(l) + i] = (float)((2.0 * u - 1.0) * a);
+        }
+        for (int i = 0; i < g_out(l); ++i) out[g_boff(l) + i] = 0.0f;
+    }
+    for (int j = 0; j < G_LOBES; ++j) out[g_boff(4) + 5 * j + 3] = 1.0f;  // kappa ~ e
+    out[g_boff(4) + 40] = -1.0f;  // selection ~ 0.05 + 0.85 sigmoid(-1) = 0.28
+}
+
+cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
+    g = GuideArgs{};
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
+    chk(galloc(&g.net.master, G_NPARAMS));
+    chk(galloc(&g.net.wbf, G_NPARAMS));
+    chk(galloc(&g.net.wtbf, G_NPARAMS));
+    chk(galloc(&g.net.adam_m, G_NPARAMS));
+    chk(galloc(&g.net.adam_v, G_NPARAMS));
+    chk(galloc(&g.net.grad, G_NPARAMS));
+    if (n_verts > 0) {
+        chk(galloc(&g.gv.p, n_verts));
+        chk(galloc(&g.gv.n, n_verts));
+        chk(galloc(&g.gv.wo, n_verts));
+        chk(galloc(&g.gv.spec, n_verts));
+        chk(galloc(&g.gv.id, n_verts));
+    }
+    chk(galloc(&g.rec.x0, G_REC_CAP));
+    chk(galloc(&g.rec.x1, G_REC_CAP));
+    chk(galloc(&g.rec.x2, G_REC_CAP));
+    chk(galloc(&g.rec.w, G_REC_CAP));
+    chk(galloc(&g.rec.b, G_REC_CAP));
+    chk(galloc(&g.rec.thr, G_REC_CAP));
+    chk(galloc(&g.rec.rad, G_REC_CAP));
+    chk(galloc(&g.rec.pid, G_REC_CAP));
+    chk(galloc(&g.rec.weight, G_REC_CAP));
+    chk(galloc(&g.rec.act, (size_t)G_REC_CAP * G_ACT_STRIDE));
+    chk(galloc(&g.rec.delta, (size_t)G_REC_CAP * G_DELTA_STRIDE));
+    chk(galloc(&g.gc, 1));
+    if (e == cudaSuccess) {
+        GuideCounters gc{};
+        gc.threshold = 65536u;
+        e = cudaMemcpy(g.gc, &gc, sizeof(gc), cudaMemcpyHostToDevice);
+    }
+    g.lr = 1e-3f;
+    g.train = 1;
+    return e;
+}
+
+void guide_free(GuideArgs& g) {
+    void* bufs[] = {g.net.master, g.net.wbf, g.net.wtbf, g.net.adam_m, g.net.adam_v, g.net.grad,
+                    g.gv.p, g.gv.n, g.gv.wo, g.gv.spec, g.gv.id, g.rec.x0, g.rec.x1, g.rec.x2, g.rec.w, g.rec.b,
+                    g.rec.thr, g.rec.rad, g.rec.pid, g.rec.weight, g.rec.act, g.rec.delta, g.gc};
+    for (void* b : bufs) cudaFree(b);
+    g = GuideArgs{};
+}
+
+cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m, const float* adam_v,
+                         uint32_t adam_step) {
+    std::vector<__nv_bfloat16> wbf(G_NPARAMS, __float2bfloat16_rn(0.0f)), wtbf(G_NPARAMS, __float2bfloat16_rn(0.0f));
+    for (int l = 0; l < G_LAYERS; ++l)
+        for (int o = 0; o < g_out(l); ++o)
+            for (int i = 0; i < g_in(l); ++i) {
+                __nv_bfloat16 h = __float2bfloat16_rn(params[g_woff(l) + o * g_in(l) + i]);
+                wbf[g_woff(l) + o * g_in(l) + i] = h;
+                wtbf[g_woff(l) + i * g_out(l) + o] = h;
+            }
+    std::vector<float> zero(G_NPARAMS, 0.0f);
+    cudaError_t e = cudaMemcpy(g.net.master, params, G_NPARAMS * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(g.net.wbf, wbf.data(), G_NPARAMS * 2, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(g.net.wtbf, wtbf.data(), G_NPARAMS * 2, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(g.net.adam_m, adam_m ? adam_m : zero.data(), G_NPARAMS * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(g.net.adam_v, adam_v ? adam_v : zero.data(), G_NPARAMS * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(g.net.grad, zero.data(), G_NPARAMS * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&g.gc->adam_step, &adam_step, 4, cudaMemcpyHostToDevice);
+    return e;
+}
+
+int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, cudaStream_t st) {
+    k_guide_test_forward<<<64, GW * 32, guide_infer_smem(), st>>>(net, x, n, y);
+    return 1;
+}
+int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,
+                              cudaStream_t st) {
+    k_guide_test_mixture<<<(n + 127) / 128, 128, 0, st>>>(raw, omega, u, n, out);
+    return 1;
+}
+
+}  // namespace srt

@@ -352,6 +352,8 @@ SRT_DEV LightSample sample_light(const DevScene& S, float3 hp, float4 wl, uint32
 
 // One iteration of ray_color's bounce loop after the closest-hit query
 // (shader.wgsl:568-700).
+// GUIDE: Lambert continuations are left to k_guide_infer (guide.cu).
+template <bool GUIDE>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bounce) {
     uint32_t n = a.counters->paths[bounce];
     if (blockIdx.x * blockDim.x >= n) return;
@@ -364,6 +366,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
     uint32_t key = 0u;
     float sh_tmax = 0.f;
     float4 sh_c = splat4(0.f);
+    bool guided = false;  // continuation deferred to the guide
+    float4 g_p = splat4(0.f), g_n = splat4(0.f), g_wo = splat4(0.f), g_spec = splat4(0.f);
     if (valid) {
         float4 h = a.pb.hit[id];
         uint32_t prim = __float_as_uint(h.y);
@@ -373,6 +377,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
             float4 thr = a.pb.thr[id], wl = a.pb.wl[id], rad = a.pb.rad[id];
             uint4 misc = a.pb.misc[id];
             uint32_t s = misc.x, flags = misc.y;
+            // a training record of the previous vertex: radiance before this vertex
+            if (GUIDE && misc.w != 0u) a.guide.rec.rad[misc.w - 1u] = rad;
             Surface sf = surface_at(S, prim, h.z, h.w, d);
             float4 color = S.materials[2 * sf.mat], extra = S.materials[2 * sf.mat + 1];
             float3 ffn = sf.front ? sf.wn : -sf.wn;
@@ -404,8 +410,18 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
                         shadow = true;
                     }
                     a.pb.rad[id] = rad;
+                    if (GUIDE && bounce + 1u < a.max_depth) {
+                        guided = true;
+                        g_p = f4(hp.x, hp.y, hp.z, wl.x);
+                        g_n = f4(ffn.x, ffn.y, ffn.z, 0.f);
+                        g_wo = f4(-d.x, -d.y, -d.z, 0.f);
+                        g_spec = spec;
+                        a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
+                    }
                 }
-                Scatter sc = sample_bsdf(d, ffn, color, extra, sf.front, wl, thr, s);
+                Scatter sc;
+                sc.absorbed = true;
+                if (!guided) sc = sample_bsdf(d, ffn, color, extra, sf.front, wl, thr, s);
                 if (!sc.absorbed) {
                     thr = thr * sc.att;
                     o = o + d * h.x;
@@ -438,6 +454,16 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bou
         a.pb.sh_d[sslot] = f4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
         a.pb.sh_c[sslot] = sh_c;
         a.pb.sh_id[sslot] = id;
+    }
+    if (GUIDE) {
+        uint32_t gslot = warp_push(guided, &a.guide.gc->verts[bounce]);
+        if (guided) {
+            a.guide.gv.p[gslot] = g_p;
+            a.guide.gv.n[gslot] = g_n;
+            a.guide.gv.wo[gslot] = g_wo;
+            a.guide.gv.spec[gslot] = g_spec;
+            a.guide.gv.id[gslot] = id;
+        }
     }
 }
 
@@ -643,8 +669,10 @@ int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stag
     uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
     if (stage == 0 || stage == 1) launches += launch_trace_closest(a, bounce, st);
     if (stage == 0 || stage == 2) {
-        k_shade<<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
+        if (a.guiding) k_shade<true><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
+        else k_shade<false><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         ++launches;
+        if (a.guiding && bounce + 1 < a.max_depth) launches += launch_guide_infer(a, bounce, st);
         if (a.ray_sort && bounce + 1 < a.max_depth) {
             // 4 passes: the sorted queue lands back in the queue buffer
             uint32_t *sk, *sv;

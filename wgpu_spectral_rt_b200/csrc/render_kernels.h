@@ -4,6 +4,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "guide.cuh"
 
 namespace srt {
 
@@ -93,6 +94,8 @@ struct FrameArgs {
     int block_size;
     int ray_sort;  // sort the live queue by (direction, origin) before each bounce >= 1
     int sm_count;  // persistent traversal grid = sm_count * blocks per SM
+    int guiding;   // Lambert continuations sampled by the guide (k_guide_infer)
+    GuideArgs guide;
 };
 
 // Photon pass: trace, compaction, grid keys, radix sort, ranges.
