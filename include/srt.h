@@ -258,7 +258,9 @@ typedef enum srt_preset {
     SRT_PRESET_CUSTOM_PRISM = 1,  /* custom.rs:6-116 */
     SRT_PRESET_CONFIG1 = 2,       /* Cornell walls + 2-tri light + dispersive UV sphere */
     SRT_PRESET_CONFIG2 = 3,       /* displaced level-8 icosphere + 64 coated GGX spheres */
-    SRT_PRESET_CAUSTIC_SLAB = 4   /* dispersive slab under a slit light + floor + config-1 mesh */
+    SRT_PRESET_CAUSTIC_SLAB = 4,  /* dispersive slab under a slit light + floor + config-1 mesh */
+    SRT_PRESET_INDIRECT_ROOM = 5  /* Cornell walls lit only by the ceiling spot above an
+                                     upward-facing light hidden under a panel (guiding study) */
 } srt_preset;
 srt_status srt_scene_builder_add_preset(srt_scene_builder* b, int preset, uint32_t seed, float camera_out[5]);
 
@@ -392,7 +394,9 @@ srt_status srt_guide_default_weights(uint64_t seed, float* out, uint32_t n);
 srt_status srt_renderer_guide_get_weights(srt_renderer* r, float* out, uint32_t n);
 srt_status srt_renderer_guide_set_weights(srt_renderer* r, const float* w, uint32_t n);
 srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_steps, uint32_t* record_threshold);
-srt_status srt_renderer_guide_set_learning_rate(srt_renderer* r, float lr);
+/* Adam learning rate (default 1e-3; < 0 keeps it) and training samples
+ * recorded per frame (default 65536, at most 262144; 0 keeps it). */
+srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batch);
 /* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
  * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),
  * sampled direction).  train: loss gradients summed over n samples

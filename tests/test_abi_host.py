@@ -97,7 +97,7 @@ def test_light_expansion_matches_builder(srt):
     assert list(L.v0) == [-0.5 + 1, 2, 0.5 + 3, 1.0] and list(L.params) == [0, 6500, 1, 0]
 
 
-@pytest.mark.parametrize("preset,tris", [(0, 10 + 2 + 12 + 5120), (2, 10 + 2 + 4032)])
+@pytest.mark.parametrize("preset,tris", [(0, 10 + 2 + 12 + 5120), (2, 10 + 2 + 4032), (5, 10 + 2 + 2 * 12)])
 def test_presets(srt, preset, tris):
     b = srt.SceneBuilder()
     pos, yaw, pitch = b.add_preset(preset)

@@ -111,6 +111,7 @@ PRESET_CUSTOM_PRISM = 1
 PRESET_CONFIG1 = 2
 PRESET_CONFIG2 = 3
 PRESET_CAUSTIC_SLAB = 4
+PRESET_INDIRECT_ROOM = 5
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
@@ -171,7 +172,7 @@ SIGNATURES = {
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
     "srt_renderer_guide_set_weights": (_I, [_P, _P, _U32]),
     "srt_renderer_guide_info": (_I, [_P, C.POINTER(_U32), C.POINTER(_U32)]),
-    "srt_renderer_guide_set_learning_rate": (_I, [_P, _F]),
+    "srt_renderer_guide_configure": (_I, [_P, _F, _U32]),
     "srt_guide_test_forward": (_I, [_P, _P, _P, _U32, _P]),
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
@@ -471,8 +472,9 @@ class Renderer:
         _check(lib().srt_renderer_guide_info(self.h, C.byref(steps), C.byref(thr)), self.ctx.h)
         return {"adam_steps": steps.value, "record_threshold": thr.value}
 
-    def set_guide_learning_rate(self, lr: float) -> None:
-        _check(lib().srt_renderer_guide_set_learning_rate(self.h, lr), self.ctx.h)
+    def configure_guide(self, lr: float | None = None, batch: int | None = None) -> None:
+        """Adam learning rate and training samples recorded per frame."""
+        _check(lib().srt_renderer_guide_configure(self.h, -1.0 if lr is None else lr, batch or 0), self.ctx.h)
 
     def close(self):
         if self.h:

@@ -1025,15 +1025,16 @@ extern "C" srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_st
     return SRT_OK;
 }
 
-extern "C" srt_status srt_renderer_guide_set_learning_rate(srt_renderer* r, float lr) {
-    if (!r || !(lr >= 0.0f) || !(lr < 1.0f)) return SRT_ERR_INVALID_ARG;
+extern "C" srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batch) {
+    if (!r || !(lr < 1.0f) || batch > G_REC_CAP) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    r->guide.lr = lr;
+    if (lr >= 0.0f) r->guide.lr = lr;
+    if (batch > 0) r->guide.batch = batch;
     r->args.guide = r->guide;
-    if (r->graph) {  // the learning rate is a kernel argument of the captured frame
+    if (r->graph) {  // both are kernel arguments of the captured frame
         cudaGraphExecDestroy(r->graph);
         r->graph = nullptr;
     }
@@ -1106,6 +1107,7 @@ extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, cons
     CUDA_TRY(c, guide_alloc(s.g, 0));
     CUDA_TRY(c, guide_upload(s.g, params, adam_m, adam_v, adam_step));
     s.g.lr = lr;
+    s.g.batch = n;
     std::vector<float4> x0(n), x1(n), x2(n), w(n), b(n);
     for (uint32_t i = 0; i < n; ++i) {
         const float* xi = x + (size_t)i * G_IN;

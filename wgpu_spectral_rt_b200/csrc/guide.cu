@@ -25,7 +25,13 @@ namespace srt {
 
 namespace {
 
-constexpr int GW = 4;  // warps per block in the inference / fwd-bwd kernels
+constexpr int GWI = 8;  // warps per block of the inference kernels (2 blocks per SM)
+constexpr int GWT = 4;  // warps per block of the training forward/backward kernel
+// Per-warp staging of the inference kernels: the encoded rows (16 x 136
+// bf16); the raw outputs (16 x 52 fp32) reuse the same bytes once the
+// first layer has taken its A fragments.
+constexpr int IN_BYTES = 16 * g_pad(G_ENC) * 2;
+static_assert(16 * 52 * 4 <= IN_BYTES, "outputs alias the encoded rows");
 
 SRT_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -162,12 +168,6 @@ SRT_DEV void mixture(const float* r, Mix& m) {
 SRT_DEV float vmf(float3 mu, float k, float3 w) {
     return k / (2.0f * PI * (-expm1f(-2.0f * k))) * expf(k * (dot(mu, w) - 1.0f));
 }
-SRT_DEV float mix_pdf(const Mix& m, float3 w) {
-    float q = 0.f;
-#pragma unroll
-    for (int j = 0; j < G_LOBES; ++j) q += m.pi[j] * vmf(m.mu[j], m.kappa[j], w);
-    return q;
-}
 // Sample a vMF lobe (Wenzel Jakob's stable form of Wood's method).
 SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
     float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
@@ -181,16 +181,89 @@ SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
     return normalize(mu * w + b1 * (r * cp) + b2 * (r * sp));
 }
 
+// Copies a rows x cols bf16 matrix (rows contiguous in global memory) into
+// shared memory rows padded to g_pad(cols), 16 bytes per load.
+// The copies are asynchronous (cp.async, all in flight at once); the caller
+// waits with cp_async_wait_all() and then synchronises the block.
+SRT_DEV void copy_rows(__nv_bfloat16* dst, const __nv_bfloat16* src, int rows, int cols) {
+    const int cpr = cols / 8;  // 16-byte chunks per row
+    for (int i = threadIdx.x; i < rows * cpr; i += blockDim.x) {
+        int r = i / cpr, c = i - r * cpr;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst + r * g_pad(cols) + 8 * c)),
+                     "l"(src + 8 * i));
+    }
+}
+SRT_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The mixture of one sample held by a lane pair (lanes l and l ^ 16): this
+// lane owns lobes 4 half .. 4 half + 3.  Every function here is called by
+// all 32 lanes of the warp (it shuffles).
+struct HalfMix {
+    float3 mu[4];
+    float kappa[4];
+    float pi[4];  // normalised over all 8 lobes
+    float cdf0;   // total weight of lobes 0..3
+    float sel;
+};
+SRT_DEV void half_mixture(const float* r, int half, HalfMix& m) {
+    float mx = -3.4e38f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mx = fmaxf(mx, r[5 * (4 * half + i) + 4]);
+    mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, 16));
+    float sum = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int j = 4 * half + i;
+        float3 v = f3(r[5 * j], r[5 * j + 1], r[5 * j + 2]);
+        m.mu[i] = v / fmaxf(length(v), 1e-12f);
+        m.kappa[i] = expf(clampf(r[5 * j + 3], G_KAPPA_LO, G_KAPPA_HI));
+        m.pi[i] = expf(r[5 * j + 4] - mx);
+        sum += m.pi[i];
+    }
+    const float other = __shfl_xor_sync(0xFFFFFFFFu, sum, 16);
+    const float inv = 1.0f / (sum + other);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) m.pi[i] *= inv;
+    m.cdf0 = (half == 0 ? sum : other) * inv;
+    m.sel = G_SEL_LO + G_SEL_SPAN / (1.0f + expf(-r[40]));
+}
+// Direction drawn from the mixture with (u0: lobe, u1, u2: vMF); the lobe's
+// owner samples it and both lanes receive it.
+SRT_DEV float3 half_sample(const HalfMix& m, int half, float u0, float u1, float u2) {
+    const bool first = u0 < m.cdf0;  // the lobe lies in lanes-0 half
+    const bool mine = (half == 0) == first;
+    float acc = half == 0 ? 0.f : m.cdf0;
+    float3 mu = m.mu[3];
+    float k = m.kappa[3];  // rounding fallback: the half's last lobe
+    bool found = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        acc += m.pi[i];
+        if (!found && u0 < acc) {
+            found = true;
+            mu = m.mu[i];
+            k = m.kappa[i];
+        }
+    }
+    float3 d = mine ? vmf_sample(mu, k, u1, u2) : f3(0.f, 0.f, 0.f);
+    const int owner = (threadIdx.x & 15) | (first ? 0 : 16);
+    return f3(__shfl_sync(0xFFFFFFFFu, d.x, owner), __shfl_sync(0xFFFFFFFFu, d.y, owner),
+              __shfl_sync(0xFFFFFFFFu, d.z, owner));
+}
+SRT_DEV float half_pdf(const HalfMix& m, float3 w) {
+    float q = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q += m.pi[i] * vmf(m.mu[i], m.kappa[i], w);
+    return q + __shfl_xor_sync(0xFFFFFFFFu, q, 16);
+}
+
 // Loads all layer weights (bf16, padded rows) and biases into shared memory.
+// Every weight block starts on a 16-byte boundary (g_woff(l) is a multiple of 8).
 SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb, bool transposed, __nv_bfloat16* swt) {
     int off = 0;
     for (int l = 0; l < G_LAYERS; ++l) {
-        int K = g_in(l), N = g_out(l);
-        for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
-            int n = i / K, k = i - n * K;
-            sw[off + n * g_pad(K) + k] = net.wbf[g_woff(l) + i];
-        }
-        off += N * g_pad(K);
+        copy_rows(sw + off, net.wbf + g_woff(l), g_out(l), g_in(l));
+        off += g_out(l) * g_pad(g_in(l));
     }
     int bo = 0;
     for (int l = 0; l < G_LAYERS; ++l) {
@@ -200,14 +273,11 @@ SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb, boo
     if (transposed) {  // W^T [in][out] of layers 1..4 for the backward pass
         int o2 = 0;
         for (int l = 1; l < G_LAYERS; ++l) {
-            int K = g_in(l), N = g_out(l);
-            for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
-                int k = i / N, n = i - k * N;  // wtbf is [in][out]
-                swt[o2 + k * g_pad(N) + n] = net.wtbf[g_woff(l) + i];
-            }
-            o2 += K * g_pad(N);
+            copy_rows(swt + o2, net.wtbf + g_woff(l), g_in(l), g_out(l));
+            o2 += g_in(l) * g_pad(g_out(l));
         }
     }
+    cp_async_wait_all();
 }
 constexpr int SW_ELEMS = G_HID * g_pad(G_ENC) + 3 * G_HID * g_pad(G_HID) + G_OUT * g_pad(G_HID);
 constexpr int SWT_ELEMS = 3 * G_HID * g_pad(G_HID) + G_HID * g_pad(G_OUT);
@@ -296,22 +366,22 @@ SRT_DEV void vertex_inputs(float3 p, float3 n, float3 wo, float lambda, float4 b
 // The continuation of every Lambert vertex of this bounce (the tail of
 // shader.wgsl:677-700 for material 0): mixture sampling, throughput,
 // Russian roulette, next queue; plus the recording of training samples.
-__global__ void __launch_bounds__(GW * 32) k_guide_infer(FrameArgs a, uint32_t bounce) {
+__global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32_t bounce) {
     const GuideArgs& G = a.guide;
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
     unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4));
-    float* out = reinterpret_cast<float*>(in + 16 * g_pad(G_ENC));
+    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * IN_BYTES);
+    float* out = reinterpret_cast<float*>(in);
     const uint32_t n = G.gc->verts[bounce];
-    if (blockIdx.x * GW * 16 >= n) return;
+    if (blockIdx.x * GWI * 16 >= n) return;
     load_weights(G.net, sw, sb, false, nullptr);
     __syncthreads();
     const DevScene& S = a.scene;
     const uint32_t frame = a.cam->frame_count;
-    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+    for (uint32_t base = (blockIdx.x * GWI + warp) * 16; base < n; base += gridDim.x * GWI * 16) {
         // encode: two lanes per sample
         {
             uint32_t v = base + (lane & 15);
@@ -327,41 +397,49 @@ __global__ void __launch_bounds__(GW * 32) k_guide_infer(FrameArgs a, uint32_t b
         __syncwarp();
         forward16(sw, sb, in, out, nullptr);
         __syncwarp();
-        bool alive = false;
-        uint32_t id = 0;
-        if (lane < 16 && base + lane < n) {
-            uint32_t v = base + lane;
+        // mixture sampling: lanes l and l + 16 share sample l & 15, four lobes each
+        const int sl = lane & 15, half = lane >> 4;
+        const uint32_t v = base + sl;
+        const bool valid = v < n;
+        HalfMix m;
+        half_mixture(out + sl * 52, half, m);
+        uint32_t id = 0, s = 0;
+        float4 p = splat4(0.f), nn = splat4(0.f), wo4 = splat4(0.f), spec = splat4(0.f), thr = splat4(0.f);
+        uint4 misc = make_uint4(0, 0, 0, 0);
+        if (valid) {
             id = G.gv.id[v];
-            float4 p = G.gv.p[v], nn = G.gv.n[v], wo4 = G.gv.wo[v], spec = G.gv.spec[v];
-            float3 hp = xyz(p), ffn = xyz(nn);
-            Mix m;
-            mixture(out + lane * 52, m);
-            uint4 misc = a.pb.misc[id];
-            uint32_t s = misc.x;
-            float4 thr = a.pb.thr[id];
-            float3 dir;
-            if (rng_next(s) < m.sel) {
-                float u = rng_next(s), acc = 0.f;
-                int j = G_LOBES - 1;
-                for (int i = 0; i < G_LOBES; ++i) {
-                    acc += m.pi[i];
-                    if (u < acc) {
-                        j = i;
-                        break;
-                    }
-                }
-                float u1 = rng_next(s), u2 = rng_next(s);
-                dir = vmf_sample(m.mu[j], m.kappa[j], u1, u2);
-            } else {
-                float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
-                if (length(d) < 0.001f) d = ffn;
-                dir = normalize(d);
-            }
+            p = G.gv.p[v];
+            nn = G.gv.n[v];
+            misc = a.pb.misc[id];
+            s = misc.x;
+        }
+        const float3 ffn = xyz(nn);
+        // both lanes of a pair replay the same random stream
+        const bool use_guide = valid && rng_next(s) < m.sel;
+        float u0 = 0.f, u1 = 0.f, u2 = 0.f;
+        float3 dir = ffn;
+        if (use_guide) {
+            u0 = rng_next(s);
+            u1 = rng_next(s);
+            u2 = rng_next(s);
+        } else if (valid) {
+            float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
+            if (length(d) < 0.001f) d = ffn;
+            dir = normalize(d);
+        }
+        const float3 gdir = half_sample(m, half, u0, u1, u2);
+        if (use_guide) dir = gdir;
+        const float q = half_pdf(m, dir);
+        bool alive = false;
+        if (valid && half == 0) {
+            wo4 = G.gv.wo[v];
+            spec = G.gv.spec[v];
+            thr = a.pb.thr[id];
+            const float3 hp = xyz(p);
             float cosv = dot(ffn, dir);
             uint32_t rec = 0u;  // record index + 1 (0: none)
             if (cosv > 0.0f) {
                 float pb = cosv / PI;
-                float q = mix_pdf(m, dir);
                 float pdf = m.sel * q + (1.0f - m.sel) * pb;
                 float4 att = spec * (pb / pdf);  // (spec / pi) cos / pdf
                 thr = thr * att;
@@ -371,7 +449,7 @@ __global__ void __launch_bounds__(GW * 32) k_guide_infer(FrameArgs a, uint32_t b
                     uint32_t h = pcg_hash(id ^ (bounce << 24) ^ (frame * 0x9E3779B9u)) & 0xFFFFu;
                     if (h < G.gc->threshold) {
                         uint32_t r = atomicAdd(&G.gc->records, 1u);
-                        if (r < G_REC_CAP) {
+                        if (r < G.batch) {
                             float x[G_IN];
                             vertex_inputs(hp, ffn, xyz(wo4), p.w, S.bmin, S.binv, x);
                             G.rec.x0[r] = f4(x[0], x[1], x[2], x[3]);
@@ -421,7 +499,7 @@ __global__ void __launch_bounds__(GW * 32) k_guide_infer(FrameArgs a, uint32_t b
 // next vertex carry no later radiance (L = 0).
 __global__ void k_guide_targets(FrameArgs a) {
     const GuideArgs& G = a.guide;
-    uint32_t n = min(G.gc->records, G_REC_CAP);
+    uint32_t n = min(G.gc->records, G.batch);
     float local = 0.f;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         float4 fin = a.pb.rad[G.rec.pid[r]];
@@ -449,7 +527,7 @@ __global__ void k_guide_targets(FrameArgs a) {
 // post-ReLU activations and per-layer deltas (bf16) for the weight-gradient
 // product.  Loss per sample (weight w normalised by the batch mean):
 //   -w log q(omega) for the lobes, -w log(sel q + (1 - sel) p_bsdf) for sel.
-__global__ void __launch_bounds__(GW * 32) k_guide_fwdbwd(GuideArgs G) {
+__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     __nv_bfloat16* swt = sw + SW_ELEMS;
@@ -461,13 +539,13 @@ __global__ void __launch_bounds__(GW * 32) k_guide_fwdbwd(GuideArgs G) {
     __nv_bfloat16* act = in + 16 * g_pad(G_ENC);
     float* out = reinterpret_cast<float*>(act + 4 * 16 * g_pad(G_HID));
     __nv_bfloat16* d4 = reinterpret_cast<__nv_bfloat16*>(out + 16 * 52);
-    const uint32_t n = min(G.gc->records, G_REC_CAP);
-    if (blockIdx.x * GW * 16 >= n) return;
+    const uint32_t n = min(G.gc->records, G.batch);
+    if (blockIdx.x * GWT * 16 >= n) return;
     load_weights(G.net, sw, sb, true, swt);
     __syncthreads();
     const float inv_mean = G.gc->weight_sum > 0.f ? (float)n / G.gc->weight_sum : 0.f;
     const int g = lane >> 2, cq = lane & 3;
-    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+    for (uint32_t base = (blockIdx.x * GWT + warp) * 16; base < n; base += gridDim.x * GWT * 16) {
         {
             uint32_t r = base + (lane & 15);
             float x[G_IN];
@@ -607,7 +685,7 @@ constexpr int WGRAD_BLOCKS = 64;  // sample splits per job
 __global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) {
     __shared__ __align__(16) __nv_bfloat16 sd[32 * g_pad(G_HID)];
     __shared__ __align__(16) __nv_bfloat16 sa[32 * g_pad(G_HID)];
-    const uint32_t n = min(G.gc->records, G_REC_CAP);
+    const uint32_t n = min(G.gc->records, G.batch);
     const int job = blockIdx.y;
     const int l = job <= 1 ? 0 : job - 1;
     const int in0 = job == 1 ? 64 : 0;
@@ -684,7 +762,7 @@ __global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) {
 // Adam on the FP32 master weights (gradients are sums over the batch and
 // are divided by its size), then the bf16 copies; clears the gradients.
 __global__ void k_guide_adam(GuideArgs G) {
-    const uint32_t n = min(G.gc->records, G_REC_CAP);
+    const uint32_t n = min(G.gc->records, G.batch);
     if (n == 0) return;
     const float inv = 1.0f / (float)n;
     const float t = (float)(G.gc->adam_step + 1u);
@@ -711,14 +789,14 @@ __global__ void k_guide_adam(GuideArgs G) {
 }
 
 // Next frame's recording threshold (of 65536) so that about 90 % of the
-// record capacity fills; counts the Adam step; clears the per-frame counters.
+// training batch fills; counts the Adam step; clears the per-frame counters.
 __global__ void k_guide_frame_end(GuideArgs G, int trained) {
     GuideCounters* gc = G.gc;
     if (threadIdx.x < 32) gc->verts[threadIdx.x] = 0u;
     if (threadIdx.x != 0) return;
     uint32_t c = gc->candidates;
     if (c > 0) {
-        double t = 65536.0 * 0.9 * (double)G_REC_CAP / (double)c;
+        double t = 65536.0 * 0.9 * (double)G.batch / (double)c;
         gc->threshold = (uint32_t)fmin(65536.0, fmax(1.0, t));
     }
     if (trained && gc->records > 0u) gc->adam_step += 1u;
@@ -729,18 +807,18 @@ __global__ void k_guide_frame_end(GuideArgs G, int trained) {
 
 // ---------------------------------------------------------------- test kernels
 // Forward pass of n samples (inputs [n][10]) -> raw outputs [n][48].
-__global__ void __launch_bounds__(GW * 32) k_guide_test_forward(GuideNet net, const float* __restrict__ x, uint32_t n,
-                                                                float* __restrict__ y) {
+__global__ void __launch_bounds__(GWI * 32, 2) k_guide_test_forward(GuideNet net, const float* __restrict__ x,
+                                                                    uint32_t n, float* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
     unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4));
-    float* out = reinterpret_cast<float*>(in + 16 * g_pad(G_ENC));
+    __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * IN_BYTES);
+    float* out = reinterpret_cast<float*>(in);
     load_weights(net, sw, sb, false, nullptr);
     __syncthreads();
-    for (uint32_t base = (blockIdx.x * GW + warp) * 16; base < n; base += gridDim.x * GW * 16) {
+    for (uint32_t base = (blockIdx.x * GWI + warp) * 16; base < n; base += gridDim.x * GWI * 16) {
         uint32_t r = base + (lane & 15);
         float xi[G_IN];
         for (int i = 0; i < G_IN; ++i) xi[i] = r < n ? x[(size_t)r * G_IN + i] : 0.f;
@@ -754,38 +832,36 @@ __global__ void __launch_bounds__(GW * 32) k_guide_test_forward(GuideNet net, co
     }
 }
 
-// Mixture pdf and samples from raw outputs: out[i] = (pdf(omega_i), sample xyz)
+// Mixture pdf and samples from raw outputs: out[i] = (pdf(omega_i), sample
+// xyz), evaluated by lane pairs exactly as in k_guide_infer.
 __global__ void k_guide_test_mixture(const float* __restrict__ raw, const float* __restrict__ omega,
                                      const float* __restrict__ u, uint32_t n, float* __restrict__ out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Mix m;
-    mixture(raw + (size_t)i * G_OUT, m);
-    float3 w = f3(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2]);
-    float pdf = mix_pdf(m, w);
-    float uu = u[3 * i], acc = 0.f;
-    int j = G_LOBES - 1;
-    for (int k = 0; k < G_LOBES; ++k) {
-        acc += m.pi[k];
-        if (uu < acc) {
-            j = k;
-            break;
-        }
+    const int lane = threadIdx.x & 31, half = lane >> 4;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32 * 16 + (lane & 15);
+    const bool valid = i < n;
+    float r[G_OUT];
+    for (int k = 0; k < G_OUT; ++k) r[k] = valid ? raw[(size_t)i * G_OUT + k] : 0.f;
+    HalfMix m;
+    half_mixture(r, half, m);
+    float3 w = valid ? f3(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2]) : f3(0.f, 0.f, 1.f);
+    const float pdf = half_pdf(m, w);
+    const float3 d = valid ? half_sample(m, half, u[3 * i], u[3 * i + 1], u[3 * i + 2])
+                           : half_sample(m, half, 0.f, 0.5f, 0.5f);
+    if (valid && half == 0) {
+        out[4 * i] = pdf;
+        out[4 * i + 1] = d.x;
+        out[4 * i + 2] = d.y;
+        out[4 * i + 3] = d.z;
     }
-    float3 s = vmf_sample(m.mu[j], m.kappa[j], u[3 * i + 1], u[3 * i + 2]);
-    out[4 * i] = pdf;
-    out[4 * i + 1] = s.x;
-    out[4 * i + 2] = s.y;
-    out[4 * i + 3] = s.z;
 }
 
 // ---------------------------------------------------------------- launchers
 size_t guide_infer_smem() {
-    return SW_ELEMS * 2 + SB_ELEMS * 4 + GW * (16 * g_pad(G_ENC) * 2 + 16 * 52 * 4);
+    return SW_ELEMS * 2 + SB_ELEMS * 4 + GWI * IN_BYTES;
 }
 size_t guide_train_smem() {
     return (SW_ELEMS + SWT_ELEMS) * 2 + SB_ELEMS * 4 +
-           GW * (16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2);
+           GWT * (16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2);
 }
 
 cudaError_t guide_configure() {
@@ -800,13 +876,13 @@ cudaError_t guide_configure() {
 
 int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * 2;
-    k_guide_infer<<<grid, GW * 32, guide_infer_smem(), st>>>(a, bounce);
+    k_guide_infer<<<grid, GWI * 32, guide_infer_smem(), st>>>(a, bounce);
     return 1;
 }
 
 namespace {
 int launch_train_steps(const GuideArgs& g, int sm, int adam, cudaStream_t st) {
-    k_guide_fwdbwd<<<sm, GW * 32, guide_train_smem(), st>>>(g);
+    k_guide_fwdbwd<<<sm, GWT * 32, guide_train_smem(), st>>>(g);
     dim3 wg(WGRAD_BLOCKS, 6);
     k_guide_wgrad<<<wg, 256, 0, st>>>(g);
     if (!adam) return 2;
@@ -902,6 +978,7 @@ cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
     }
     g.lr = 1e-3f;
     g.train = 1;
+    g.batch = G_BATCH_DEFAULT;
     return e;
 }
 
@@ -938,12 +1015,12 @@ cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m,
 }
 
 int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, cudaStream_t st) {
-    k_guide_test_forward<<<64, GW * 32, guide_infer_smem(), st>>>(net, x, n, y);
+    k_guide_test_forward<<<64, GWI * 32, guide_infer_smem(), st>>>(net, x, n, y);
     return 1;
 }
 int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,
                               cudaStream_t st) {
-    k_guide_test_mixture<<<(n + 127) / 128, 128, 0, st>>>(raw, omega, u, n, out);
+    k_guide_test_mixture<<<(n + 63) / 64, 128, 0, st>>>(raw, omega, u, n, out);  // 16 samples per warp
     return 1;
 }
 

@@ -75,6 +75,7 @@ struct GuideRecords {
     __nv_bfloat16* delta;  // G_REC_CAP x (4 x 64 + 48)
 };
 constexpr uint32_t G_REC_CAP = 1u << 18;
+constexpr uint32_t G_BATCH_DEFAULT = 1u << 16;  // training samples per frame
 constexpr int G_ACT_STRIDE = G_ENC + 4 * G_HID;    // 384
 constexpr int G_DELTA_STRIDE = 4 * G_HID + G_OUT;  // 304
 __host__ __device__ constexpr int g_act_off(int l) { return l < 0 ? 0 : G_ENC + l * G_HID; }  // input of layer l+1
@@ -98,7 +99,11 @@ struct GuideArgs {
     GuideCounters* gc;
     int train;               // run a training step after each frame
     float lr;
+    uint32_t batch;          // training samples recorded per frame (<= G_REC_CAP)
 };
+static_assert(G_NPARAMS % 8 == 0 && g_woff(1) % 8 == 0 && g_woff(2) % 8 == 0 && g_woff(3) % 8 == 0 &&
+                  g_woff(4) % 8 == 0,
+              "bf16 weight blocks start on 16-byte boundaries");
 
 // Launchers (guide.cu); each returns the number of kernels it launched.
 struct FrameArgs;

@@ -521,6 +521,27 @@ bool preset_fill(srt_scene_builder* b, int preset, uint32_t seed, float cam[5]) 
             b->add_instance(sphere, stone, mat4_mul(mat4_translation(0.5f, -0.65f, -0.3f), mat4_scale(0.7f, 0.7f, 0.7f)));
             return true;
         }
+        case SRT_PRESET_INDIRECT_ROOM: {
+            // Cornell walls; a 0.3 x 0.3 light 0.05 below the ceiling, facing
+            // it, hidden from the room by a 0.5 x 0.5 panel just below it.
+            // Every room point is lit through the small bright ceiling spot
+            // alone (its light samples face away), the case where guided
+            // sampling of the diffuse continuation pays off.
+            uint32_t light = b->add_material(mat(6500, 8, 0, 1, 3, 0, 0, 0));
+            uint32_t red = b->add_material(mat(0.65f, 0.05f, 0.05f, 1, 0, 0, 0, 0));
+            uint32_t green = b->add_material(mat(0.12f, 0.45f, 0.15f, 1, 0, 0, 0, 0));
+            uint32_t white = b->add_material(mat(0.73f, 0.73f, 0.73f, 1, 0, 0, 0, 0));
+            uint32_t plane = add_geom(b, geom_plane);
+            uint32_t cube = add_geom(b, geom_cube);
+            cornell_walls(b, plane, white, red, green);
+            float lp[4] = {0.0f, 6500.0f, 8.0f, 0.0f};
+            b->add_light_instance(plane, light, mat4_mul(mat4_translation(0, 0.95f, 0), mat4_scale(0.3f, 0.3f, 0.3f)), lp);
+            b->add_instance(cube, white, mat4_mul(mat4_translation(0, 0.93f, 0), mat4_scale(0.5f, 0.02f, 0.5f)));
+            b->add_instance(cube, white,
+                            mat4_mul(mat4_mul(mat4_translation(-0.35f, -0.6f, -0.3f), mat4_rotation_y(0.4f)),
+                                     mat4_scale(0.5f, 0.8f, 0.5f)));
+            return true;
+        }
         default:
             return false;
     }
