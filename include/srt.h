@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SRT_ABI_VERSION 2u
+#define SRT_ABI_VERSION 3u
 
 /* Status codes.  Replaces unwrap()/panic! and wgpu::SurfaceError
  * (src/app.rs:70-77, src/wgpu_ctx.rs:36-42). */
@@ -146,6 +146,8 @@ typedef struct srt_params {
     float photon_norm_count;     /* count in the density estimate; 0 = photons_per_frame
                                     (the reference divides by MAX_PHOTON: shader.wgsl:339) */
     uint32_t block_size;         /* trace/shade block size; 0 = autotuned default */
+    uint32_t seed;               /* added to the per-frame random seeds of camera paths and
+                                    photons; 0 = the reference's sample streams */
 } srt_params;
 
 #define SRT_FLAG_FP64_ACCUM   0x1u  /* keep an FP64 accumulation buffer beside the FP32 one */
@@ -409,6 +411,28 @@ srt_status srt_guide_test_train(srt_ctx* ctx, const float* params, const float* 
                                 uint32_t adam_step, float lr, const float* x, const float* omega,
                                 const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
                                 float* params_out, float* m_out, float* v_out);
+
+/* ------------------------------------------------------------------------ */
+/* Headless presentation: the reference's raster steps as CUDA kernels.       */
+/* ------------------------------------------------------------------------ */
+/* Letterbox blit (shaders/blit.wgsl:7-34, renderer/blit_pass.rs:114-154):
+ * the RGBA8 image src (sw x sh) drawn as an aspect-fit quad into an RGBA8
+ * window (ww x wh, row 0 at the top) cleared to blue, nearest-texel
+ * sampling; srgb_target encodes with the sRGB OETF as an *Srgb swapchain
+ * format would.  Host buffers, tightly packed. */
+srt_status srt_blit_letterbox(srt_ctx* ctx, const uint8_t* src, uint32_t sw, uint32_t sh, uint32_t ww,
+                              uint32_t wh, int srgb_target, uint8_t* out);
+/* The same for the renderer's current RGBA8 image. */
+srt_status srt_renderer_blit(srt_renderer* r, uint32_t ww, uint32_t wh, int srgb_target, uint8_t* out);
+/* Photon point splat (shaders/debug_photons.wgsl:24-47, renderer/
+ * debug_photons_pass.rs:74-139): photons with non-zero energy projected with
+ * cam's view and proj matrices, one pixel each, colour (1, 0.6, 0.1) x 0.3
+ * added (saturating) to rgba (w x h, in/out), alpha set to 0.3. */
+srt_status srt_photon_splat(srt_ctx* ctx, const srt_photon* photons, uint32_t n, const srt_camera_uniform* cam,
+                            uint32_t w, uint32_t h, uint8_t* rgba);
+/* The same for the photons the renderer stored in its last frame. */
+srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
+                                      uint8_t* rgba);
 
 #ifdef __cplusplus
 }

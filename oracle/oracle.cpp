@@ -835,9 +835,10 @@ struct Emitted {
 // photon_emit main: photon_emit.wgsl:154-331.  Material type 5 (no
 // reference counterpart) reflects specularly with the probability of the
 // film's Airy reflectance at the photon wavelength, else absorbs.
-Emitted emit_photon(const orc_scene* s, uint32_t id, uint32_t frame, uint32_t max_bounces, Counters* cnt) {
+Emitted emit_photon(const orc_scene* s, uint32_t id, uint32_t frame, uint32_t max_bounces, Counters* cnt,
+                    uint32_t seed = 0) {
     Emitted out{};
-    Rng rng{pcg_hash(id + frame * 927163u)};
+    Rng rng{pcg_hash(id + frame * 927163u + seed)};
     uint32_t nl = (uint32_t)s->lights.size();
     if (nl == 0u) return out;
     uint32_t li = std::min((uint32_t)(rng.next() * (float)nl), nl - 1u);
@@ -1228,7 +1229,7 @@ void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : ph_rays)
         for (int64_t i = 0; i < (int64_t)np; ++i) {
             Counters local;
-            em[i] = emit_photon(s, (uint32_t)i, frame, params->photon_max_bounces, &local);
+            em[i] = emit_photon(s, (uint32_t)i, frame, params->photon_max_bounces, &local, params->seed);
             ph_rays += local.closest;
         }
         cnt.closest += ph_rays;
@@ -1249,7 +1250,7 @@ void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_
     for (int64_t idx = 0; idx < total; ++idx) {
         uint32_t x = (uint32_t)(idx % w), y = (uint32_t)(idx / w);
         if (y % row_stride != row_phase) continue;
-        Rng rng{pcg_hash(x + y * w + frame * 927163u)};
+        Rng rng{pcg_hash(x + y * w + frame * 927163u + params->seed)};
         f3 o, d;
         camera_ray(cam, x, y, w, h, rng, &o, &d);
         Hero hero = sample_hero(rng);

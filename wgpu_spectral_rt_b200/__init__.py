@@ -72,7 +72,8 @@ class Params(C.Structure):
     _fields_ = [("max_depth", C.c_uint32), ("photons_per_frame", C.c_uint32), ("hash_bits", C.c_uint32),
                 ("photon_max_bounces", C.c_uint32), ("gather_cap", C.c_uint32), ("flags", C.c_uint32),
                 ("cell_size", C.c_float), ("gather_radius0", C.c_float), ("radius_exponent", C.c_float),
-                ("spectral_radius", C.c_float), ("photon_norm_count", C.c_float), ("block_size", C.c_uint32)]
+                ("spectral_radius", C.c_float), ("photon_norm_count", C.c_float), ("block_size", C.c_uint32),
+                ("seed", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -95,7 +96,7 @@ class SceneArrays(C.Structure):
 
 
 for _t, _n in ((Vertex, 32), (Material, 32), (Light, 64), (MeshInfo, 16), (Instance, 80), (CameraUniform, 272),
-               (Photon, 32), (Ray, 32), (Hit, 16), (Params, 48)):
+               (Photon, 32), (Ray, 32), (Hit, 16), (Params, 52)):
     assert C.sizeof(_t) == _n, (_t, C.sizeof(_t))
 
 FLAG_FP64_ACCUM = 0x1
@@ -167,6 +168,10 @@ SIGNATURES = {
     "srt_photon_gather": (_I, [_P, _P, _U32, _P, _U32, _U32, C.POINTER(Params), _P]),
     "srt_photon_grid_build_noalloc": (_I, [_P, _P, _U32, _U32, _F, _U32, _P, _P]),
     "srt_test_device_math": (_I, [_P, _I, _U32, _P, _P, _P]),
+    "srt_blit_letterbox": (_I, [_P, _P, _U32, _U32, _U32, _U32, _I, _P]),
+    "srt_renderer_blit": (_I, [_P, _U32, _U32, _I, _P]),
+    "srt_photon_splat": (_I, [_P, _P, _U32, _P, _U32, _U32, _P]),
+    "srt_renderer_splat_photons": (_I, [_P, _P, _U32, _U32, _P]),
     "srt_guide_param_count": (_U32, []),
     "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
@@ -457,6 +462,19 @@ class Renderer:
         _check(lib().srt_renderer_read_photons(self.h, ptr(out), n.value, C.byref(n)), self.ctx.h)
         return out
 
+    def blit(self, window_width: int, window_height: int, srgb_target: bool = False) -> np.ndarray:
+        """Headless letterbox blit of the current image into a window-sized RGBA8 array (row 0 on top)."""
+        out = np.zeros((window_height, window_width, 4), np.uint8)
+        _check(lib().srt_renderer_blit(self.h, window_width, window_height, int(srgb_target), ptr(out)), self.ctx.h)
+        return out
+
+    def splat_photons(self, camera: CameraUniform, rgba: np.ndarray) -> np.ndarray:
+        """Photon point splat of the last frame's stored photons over rgba [h, w, 4] (returns a copy)."""
+        a = np.ascontiguousarray(rgba, np.uint8).copy()
+        h, w = a.shape[:2]
+        _check(lib().srt_renderer_splat_photons(self.h, C.byref(camera), w, h, ptr(a)), self.ctx.h)
+        return a
+
     # neural path guiding (FLAG_GUIDING)
     def guide_weights(self) -> np.ndarray:
         out = np.zeros(guide_param_count(), np.float32)
@@ -580,3 +598,26 @@ def guide_train_step(ctx: Context, params, x, omega, pdf_bsdf, weight, adam_m=No
                                       ptr(wt), n, ptr(grad), *(ptr(o) if o is not None else None for o in outs)),
            ctx.h)
     return (grad, *outs) if adam else grad
+
+
+# --------------------------------------------------------------------------- headless presentation
+
+
+def blit_letterbox(ctx: Context, src: np.ndarray, window_width: int, window_height: int,
+                   srgb_target: bool = False) -> np.ndarray:
+    """BlitPass (blit.wgsl, blit_pass.rs:114-154) headless: src RGBA8 [sh, sw, 4] -> window RGBA8."""
+    a = np.ascontiguousarray(src, np.uint8)
+    sh, sw = a.shape[:2]
+    out = np.zeros((window_height, window_width, 4), np.uint8)
+    _check(lib().srt_blit_letterbox(ctx.h, ptr(a), sw, sh, window_width, window_height, int(srgb_target), ptr(out)),
+           ctx.h)
+    return out
+
+
+def photon_splat(ctx: Context, photons: np.ndarray, camera: CameraUniform, rgba: np.ndarray) -> np.ndarray:
+    """DebugPhotonsPass (debug_photons.wgsl) headless: photons float32 [n, 8] over rgba [h, w, 4]."""
+    p = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+    a = np.ascontiguousarray(rgba, np.uint8).copy()
+    h, w = a.shape[:2]
+    _check(lib().srt_photon_splat(ctx.h, ptr(p), len(p), C.byref(camera), w, h, ptr(a)), ctx.h)
+    return a

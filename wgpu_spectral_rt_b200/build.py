@@ -30,7 +30,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-
 # Per-file extra flags.  The shading kernels round every multiply and add
 # separately (no FMA contraction), as the WGSL reference and the CPU oracle
 # do; the traversal keeps contraction for its slab tests.
-FILE_FLAGS = {"render_kernels.cu": ["-fmad=false"], "trace_kernels.cu": ["-fmad=true"]}
+FILE_FLAGS = {"render_kernels.cu": ["-fmad=false"], "trace_kernels.cu": ["-fmad=true"], "present.cu": ["-fmad=false"]}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
              f"-I{INCLUDE}", f"-I{CSRC}", "-I/usr/local/cuda/include"]
 

@@ -653,6 +653,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     a.block_size = (int)p.block_size;
     a.ray_sort = (p.flags & SRT_FLAG_RAY_SORT) ? 1 : 0;
     a.sm_count = c->sm_count;
+    a.seed = p.seed;
     if (p.flags & SRT_FLAG_GUIDING) {
         CUDA_TRY(c, guide_configure());
         CUDA_TRY(c, guide_alloc(r->guide, np));
@@ -1142,4 +1143,98 @@ extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, cons
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SRT_OK;
+}
+
+// ------------------------------------------------------------------ headless presentation
+namespace {
+struct DevBufs {
+    std::vector<void*> p;
+    ~DevBufs() {
+        for (void* b : p) cudaFree(b);
+    }
+    template <class T>
+    cudaError_t alloc(T** out, size_t n) {
+        cudaError_t e = cudaMalloc((void**)out, n * sizeof(T));
+        if (e == cudaSuccess) p.push_back(*out);
+        return e;
+    }
+};
+}  // namespace
+
+extern "C" srt_status srt_blit_letterbox(srt_ctx* c, const uint8_t* src, uint32_t sw, uint32_t sh, uint32_t ww,
+                                         uint32_t wh, int srgb_target, uint8_t* out) {
+    if (!c || !src || !out || sw == 0 || sh == 0 || ww == 0 || wh == 0) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    DevBufs b;
+    uchar4 *ds = nullptr, *dd = nullptr;
+    CUDA_TRY(c, b.alloc(&ds, (size_t)sw * sh));
+    CUDA_TRY(c, b.alloc(&dd, (size_t)ww * wh));
+    CUDA_TRY(c, cudaMemcpyAsync(ds, src, (size_t)sw * sh * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_blit_letterbox(ds, sw, sh, dd, ww, wh, srgb_target, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(out, dd, (size_t)ww * wh * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_blit(srt_renderer* r, uint32_t ww, uint32_t wh, int srgb_target, uint8_t* out) {
+    if (!r || !out || ww == 0 || wh == 0) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    DevBufs b;
+    uchar4* dd = nullptr;
+    CUDA_TRY(c, b.alloc(&dd, (size_t)ww * wh));
+    launch_blit_letterbox(r->ldr, r->w, r->h, dd, ww, wh, srgb_target, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(out, dd, (size_t)ww * wh * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_photon_splat(srt_ctx* c, const srt_photon* photons, uint32_t n,
+                                       const srt_camera_uniform* cam, uint32_t w, uint32_t h, uint8_t* rgba) {
+    if (!c || !cam || !rgba || (n && !photons) || w == 0 || h == 0) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    DevBufs b;
+    float4* dp = nullptr;
+    srt_camera_uniform* dc = nullptr;
+    uint32_t* counts = nullptr;
+    uchar4* img = nullptr;
+    CUDA_TRY(c, b.alloc(&dp, 2 * (size_t)(n ? n : 1)));
+    CUDA_TRY(c, b.alloc(&dc, 1));
+    CUDA_TRY(c, b.alloc(&counts, (size_t)w * h));
+    CUDA_TRY(c, b.alloc(&img, (size_t)w * h));
+    if (n) CUDA_TRY(c, cudaMemcpyAsync(dp, photons, (size_t)n * sizeof(srt_photon), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(dc, cam, sizeof *cam, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(img, rgba, (size_t)w * h * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_photon_splat(dp, n, dc, w, h, counts, img, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(rgba, img, (size_t)w * h * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_camera_uniform* cam, uint32_t w,
+                                                 uint32_t h, uint8_t* rgba) {
+    if (!r || !cam || !rgba || w == 0 || h == 0) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    FrameCounters fc;
+    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->counters, sizeof fc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    uint32_t n = r->p.photons_per_frame ? std::min(fc.photons_stored, r->p.photons_per_frame) : 0u;
+    DevBufs b;
+    srt_camera_uniform* dc = nullptr;
+    uint32_t* counts = nullptr;
+    uchar4* img = nullptr;
+    CUDA_TRY(c, b.alloc(&dc, 1));
+    CUDA_TRY(c, b.alloc(&counts, (size_t)w * h));
+    CUDA_TRY(c, b.alloc(&img, (size_t)w * h));
+    CUDA_TRY(c, cudaMemcpyAsync(dc, cam, sizeof *cam, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(img, rgba, (size_t)w * h * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_photon_splat(r->ph.photons, n, dc, w, h, counts, img, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(rgba, img, (size_t)w * h * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c, r->err);
 }

@@ -110,7 +110,7 @@ __global__ void k_photon_emit(FrameArgs a) {
     if (e >= a.photons_per_frame) return;
     const DevScene& S = a.scene;
     uint32_t frame = a.cam->frame_count;
-    uint32_t s = pcg_hash(e + frame * 927163u);
+    uint32_t s = pcg_hash(e + frame * 927163u + a.seed);
     uint32_t nl = S.n_lights;  // > 0: the pass is skipped without lights
     uint32_t li = min(__float2uint_rz(rng_next(s) * (float)nl), nl - 1u);
     float4 L0 = S.lights[4 * li], L1 = S.lights[4 * li + 1], L2 = S.lights[4 * li + 2], LP = S.lights[4 * li + 3];
@@ -300,7 +300,7 @@ __global__ void k_raygen(FrameArgs a) {
     if (p >= n) return;
     const srt_camera_uniform& cam = *a.cam;
     uint32_t x = p % a.width, y = p / a.width;
-    uint32_t s = pcg_hash(x + y * a.width + cam.frame_count * 927163u);
+    uint32_t s = pcg_hash(x + y * a.width + cam.frame_count * 927163u + a.seed);
     float3 o, d;
     camera_ray(cam, x, y, a.width, a.height, s, o, d);
     float4 wl = sample_hero(s);

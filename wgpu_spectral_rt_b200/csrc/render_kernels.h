@@ -94,6 +94,7 @@ struct FrameArgs {
     int block_size;
     int ray_sort;  // sort the live queue by (direction, origin) before each bounce >= 1
     int sm_count;  // persistent traversal grid = sm_count * blocks per SM
+    uint32_t seed; // added to the per-frame seeds of camera paths and photons (0: reference streams)
     int guiding;   // Lambert continuations sampled by the guide (k_guide_infer)
     GuideArgs guide;
 };
@@ -113,6 +114,15 @@ int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t*
                        uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st);  // trace_kernels.cu
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
+
+// Headless presentation (present.cu): letterbox blit of an RGBA8 image into a
+// window-sized RGBA8 target, and the photon point splat over an RGBA8 target
+// (counts: w*h scratch words).
+void letterbox_scale(uint32_t tw, uint32_t th, uint32_t ww, uint32_t wh, float* sx, float* sy);
+int launch_blit_letterbox(const uchar4* src, uint32_t sw, uint32_t sh, uchar4* dst, uint32_t ww, uint32_t wh,
+                          int srgb, cudaStream_t st);
+int launch_photon_splat(const float4* photons, uint32_t n, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
+                        uint32_t* counts, uchar4* img, cudaStream_t st);
 
 // Grid over a photon array already on the device (n on host).
 int launch_grid_build(const float4* photons, uint32_t n, uint32_t frame, float cell, uint32_t hash_bits,

@@ -1,17 +1,21 @@
-"""Equal-time and equal-sample comparison of guided and plain path tracing.
+"""Equal-time comparison of guided and plain path tracing against an FP64 reference.
 
-Both renderers run the same scene and camera without the photon pass (so the
-comparison is about the sampling of the diffuse continuation alone).  The
-reference image is plain path tracing accumulated in FP64 over `ref_spp`
-frames whose sample streams are disjoint from the compared runs (frame
-indices offset by 2^30).  The guided renderer learns online: its training
-steps run inside its time budget, and its image includes the frames
-rendered while the guide was still untrained.
+Both arms render the same scene, camera, depth and photon pass.  The
+reference image is the plain method accumulated in FP64 over `ref_spp`
+frames, on sample streams decorrelated from the two arms (a different
+`seed`; the progressive photon radius schedule is the arms' one).  The
+guided arm learns online: its training steps run inside its time, and its
+image includes the frames rendered while the guide was untrained.
 
-    python -m wgpu_spectral_rt_b200.guide_study --seconds 2 --ref-spp 65536
+Each arm renders for `seconds` of wall time (frames launched back to back,
+the stream synchronised at checkpoints; the image read-back for the error
+is outside the timed region).  Reported per arm: frames, ms per frame, and
+relMSE (mean over pixels and RGB of (x - ref)^2 / (ref^2 + 0.01)) at each
+checkpoint; and the time the guided arm needs to reach the plain arm's
+final relMSE, as a fraction of the plain arm's time.
 
-prints one JSON object: per arm the frames rendered, ms per frame and the
-relMSE, mean over pixels and RGB of (x - ref)^2 / (ref^2 + 0.01).
+    python -m wgpu_spectral_rt_b200.guide_study --preset 4 --width 1920 --height 1080 \\
+        --max-depth 16 --batch 262144 --seconds 20 --ref-spp 65536
 """
 from __future__ import annotations
 
@@ -23,7 +27,7 @@ import numpy as np
 
 import wgpu_spectral_rt_b200 as srt
 
-REF_FRAME_OFFSET = 1 << 30
+REF_SEED = 0x5EED0001
 
 
 def relmse(x: np.ndarray, ref: np.ndarray) -> float:
@@ -35,76 +39,100 @@ def _mean_rgb(r: srt.Renderer) -> np.ndarray:
     return a[..., :3] / a[..., 3:4]
 
 
-def _renderer(ctx, scene, w, h, flags, max_depth):
-    p = srt.default_params(photons_per_frame=0, flags=flags | srt.FLAG_FP64_ACCUM, max_depth=max_depth)
+def _renderer(ctx, scene, w, h, flags, max_depth, photons, seed=0):
+    p = srt.default_params(photons_per_frame=photons, flags=flags | srt.FLAG_FP64_ACCUM, max_depth=max_depth,
+                           seed=seed)
     return srt.Renderer(ctx, scene, w, h, p)
 
 
-def _run_for(ctx, r, ctl, aspect, seconds=None, frames=None, offset=0, chunk=8):
-    """Renders until `seconds` of wall time (synchronised every `chunk`
-    frames) or `frames` frames; returns (frames, seconds)."""
+def _render(ctx, r, ctl, aspect, first, count):
+    for f in range(first, first + count):
+        r.render(ctl.build_uniform(aspect, f))
     ctx.synchronize()
+
+
+def _arm(ctx, r, ctl, aspect, seconds, ref, n_checkpoints=8):
+    """Renders for `seconds`; returns (frames, seconds, [(t, frames, relmse)])."""
+    # frames per checkpoint from a short timed probe, then geometric checkpoints
     t0 = time.perf_counter()
-    f = 0
-    while True:
-        for _ in range(chunk):
-            r.render(ctl.build_uniform(aspect, offset + f))
-            f += 1
-            if frames is not None and f >= frames:
-                break
-        ctx.synchronize()
-        el = time.perf_counter() - t0
-        if (frames is not None and f >= frames) or (seconds is not None and el >= seconds):
-            return f, el
+    _render(ctx, r, ctl, aspect, 0, 4)
+    t_probe = time.perf_counter() - t0
+    ms = t_probe / 4
+    frames, elapsed = 4, t_probe
+    curve = []
+    targets = [seconds * (2.0 ** (k - n_checkpoints + 1)) for k in range(n_checkpoints)]
+    for tgt in targets:
+        n = max(1, int((tgt - elapsed) / ms))
+        if elapsed >= tgt:
+            n = 0
+        t0 = time.perf_counter()
+        if n:
+            _render(ctx, r, ctl, aspect, frames, n)
+        dt = time.perf_counter() - t0
+        frames += n
+        elapsed += dt
+        if n:
+            ms = dt / n
+        curve.append((round(elapsed, 4), frames, relmse(_mean_rgb(r), ref)))
+    return frames, elapsed, curve
 
 
-def study(preset=srt.PRESET_INDIRECT_ROOM, width=256, height=192, ref_spp=65536, seconds=2.0, max_depth=12,
-          equal_spp=None, lr=None, batch=None):
+def _time_to_reach(curve, target):
+    """Interpolated (log-log) time at which the error curve reaches `target`."""
+    prev = None
+    for t, _, e in curve:
+        if e <= target:
+            if prev is None:
+                return t
+            t0, e0 = prev
+            if e0 <= e or t0 <= 0:
+                return t
+            a = (np.log(target) - np.log(e0)) / (np.log(e) - np.log(e0))
+            return float(np.exp(np.log(t0) + a * (np.log(t) - np.log(t0))))
+        prev = (t, e)
+    return None
+
+
+def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16, photons=1 << 20, ref_spp=65536,
+          seconds=20.0, lr=None, batch=None):
     ctx = srt.Context(0)
     b = srt.SceneBuilder()
     cam = b.add_preset(preset)
     scene = b.build(ctx)
     ctl = srt.CameraController(*cam)
     aspect = width / height
-    out = {"scene_preset": preset, "width": width, "height": height, "max_depth": max_depth, "ref_spp": ref_spp,
-           "photons_per_frame": 0, "lr": lr, "batch": batch}
+    out = {"scene_preset": preset, "width": width, "height": height, "max_depth": max_depth,
+           "photons_per_frame": photons, "ref_spp": ref_spp, "lr": lr if lr is not None else 1e-3,
+           "batch": batch if batch else 65536, "seconds": seconds}
 
-    ref_r = _renderer(ctx, scene, width, height, 0, max_depth)
-    f, el = _run_for(ctx, ref_r, ctl, aspect, frames=ref_spp, offset=REF_FRAME_OFFSET, chunk=64)
+    t0 = time.perf_counter()
+    ref_r = _renderer(ctx, scene, width, height, 0, max_depth, photons, REF_SEED)
+    for f0 in range(0, ref_spp, 256):
+        _render(ctx, ref_r, ctl, aspect, f0, min(256, ref_spp - f0))
     ref = _mean_rgb(ref_r)
-    out["reference"] = {"frames": f, "seconds": round(el, 3)}
     ref_r.close()
+    out["reference"] = {"frames": ref_spp, "seconds": round(time.perf_counter() - t0, 2),
+                        "accumulation": "fp64", "seed": REF_SEED}
 
-    arms = {"plain": 0, "guided": srt.FLAG_GUIDING}
-    for name, flags in arms.items():
-        r = _renderer(ctx, scene, width, height, flags, max_depth)
+    for name, flags in (("plain", 0), ("guided", srt.FLAG_GUIDING)):
+        # warm-up (library load, graph capture) on a throwaway renderer
+        w = _renderer(ctx, scene, width, height, flags, max_depth, photons, 7)
+        _render(ctx, w, ctl, aspect, 0, 4)
+        w.close()
+        r = _renderer(ctx, scene, width, height, flags, max_depth, photons)
         if flags:
             r.configure_guide(lr, batch)
-        # warm-up (graph capture, first-launch costs) on a throwaway renderer state
-        _run_for(ctx, r, ctl, aspect, frames=8, offset=REF_FRAME_OFFSET // 2)
-        r.close()
-        r = _renderer(ctx, scene, width, height, flags, max_depth)
+        frames, el, curve = _arm(ctx, r, ctl, aspect, seconds, ref)
+        out[name] = {"frames": frames, "seconds": round(el, 3), "ms_per_frame": round(1e3 * el / frames, 4),
+                     "relmse": curve[-1][2], "curve": curve}
         if flags:
-            r.configure_guide(lr, batch)
-        f, el = _run_for(ctx, r, ctl, aspect, seconds=seconds)
-        img = _mean_rgb(r)
-        arm = {"frames": f, "seconds": round(el, 3), "ms_per_frame": round(1e3 * el / f, 4),
-               "relmse_equal_time": relmse(img, ref)}
-        if equal_spp:
-            r2 = _renderer(ctx, scene, width, height, flags, max_depth)
-            if flags:
-                r2.configure_guide(lr, batch)
-            _run_for(ctx, r2, ctl, aspect, frames=equal_spp)
-            arm["relmse_equal_spp"] = relmse(_mean_rgb(r2), ref)
-            r2.close()
-        out[name] = arm
+            out[name]["guide"] = r.guide_info()
         r.close()
-    out["equal_spp"] = equal_spp
-    out["relmse_ratio_plain_over_guided_equal_time"] = out["plain"]["relmse_equal_time"] / max(
-        out["guided"]["relmse_equal_time"], 1e-30)
-    if equal_spp:
-        out["relmse_ratio_plain_over_guided_equal_spp"] = out["plain"]["relmse_equal_spp"] / max(
-            out["guided"]["relmse_equal_spp"], 1e-30)
+    target = out["plain"]["relmse"]
+    t_g = _time_to_reach(out["guided"]["curve"], target)
+    out["guided_time_to_plain_relmse"] = t_g
+    out["time_fraction"] = (t_g / out["plain"]["seconds"]) if t_g is not None else None
+    out["relmse_ratio_plain_over_guided"] = target / max(out["guided"]["relmse"], 1e-30)
     scene.close()
     ctx.close()
     return out
@@ -112,18 +140,18 @@ def study(preset=srt.PRESET_INDIRECT_ROOM, width=256, height=192, ref_spp=65536,
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--preset", type=int, default=srt.PRESET_INDIRECT_ROOM)
-    ap.add_argument("--width", type=int, default=256)
-    ap.add_argument("--height", type=int, default=192)
+    ap.add_argument("--preset", type=int, default=srt.PRESET_CAUSTIC_SLAB)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--max-depth", type=int, default=16)
+    ap.add_argument("--photons", type=int, default=1 << 20)
     ap.add_argument("--ref-spp", type=int, default=65536)
-    ap.add_argument("--seconds", type=float, default=2.0)
-    ap.add_argument("--max-depth", type=int, default=12)
-    ap.add_argument("--equal-spp", type=int, default=0)
+    ap.add_argument("--seconds", type=float, default=20.0)
     ap.add_argument("--lr", type=float, default=None)
     ap.add_argument("--batch", type=int, default=None, help="training samples per frame")
     a = ap.parse_args()
-    print(json.dumps(study(a.preset, a.width, a.height, a.ref_spp, a.seconds, a.max_depth, a.equal_spp or None,
-                           a.lr, a.batch)))
+    print(json.dumps(study(a.preset, a.width, a.height, a.max_depth, a.photons, a.ref_spp, a.seconds, a.lr,
+                           a.batch)))
 
 
 if __name__ == "__main__":
