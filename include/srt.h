@@ -7,8 +7,9 @@
  * plain C types, pointers and sizes; no CUDA or torch type appears here.
  *
  * Ownership: the library owns every device allocation.  Host arrays passed in
- * are copied before the call returns.  Handles are destroyed in reverse order
- * of creation (renderer, scene, context).  A handle is not thread-safe; use
+ * are copied before the call returns.  Handles may be destroyed in any order:
+ * a context destroyed while scenes, renderers or batches created on it are
+ * alive is released with the last of them.  A handle is not thread-safe; use
  * one context per host thread.
  *
  * Errors: every call returns an srt_status.  No exception or abort crosses
@@ -261,8 +262,11 @@ typedef enum srt_preset {
     SRT_PRESET_CONFIG1 = 2,       /* Cornell walls + 2-tri light + dispersive UV sphere */
     SRT_PRESET_CONFIG2 = 3,       /* displaced level-8 icosphere + 64 coated GGX spheres */
     SRT_PRESET_CAUSTIC_SLAB = 4,  /* dispersive slab under a slit light + floor + config-1 mesh */
-    SRT_PRESET_INDIRECT_ROOM = 5  /* Cornell walls lit only by the ceiling spot above an
+    SRT_PRESET_INDIRECT_ROOM = 5, /* Cornell walls lit only by the ceiling spot above an
                                      upward-facing light hidden under a panel (guiding study) */
+    SRT_PRESET_BATCH_RANDOM = 6   /* seeded batch scene: a triangle budget log-uniform in
+                                     [1e4, 2e6] filled by a displaced icosphere and GGX,
+                                     thin-film and dielectric UV spheres in a Cornell room */
 } srt_preset;
 srt_status srt_scene_builder_add_preset(srt_scene_builder* b, int preset, uint32_t seed, float camera_out[5]);
 
@@ -433,6 +437,40 @@ srt_status srt_photon_splat(srt_ctx* ctx, const srt_photon* photons, uint32_t n,
 /* The same for the photons the renderer stored in its last frame. */
 srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
                                       uint8_t* rgba);
+
+/* ------------------------------------------------------------------------ */
+/* Batched rendering (no reference counterpart): many scenes and viewports   */
+/* of uneven size per iteration.  Per-scene photon passes, ray generation,   */
+/* shading and finalisation run as parallel branches of one CUDA graph; the  */
+/* closest-hit and shadow rays of all scenes are traced in one persistent    */
+/* launch per bounce over per-scene queues.                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct srt_batch srt_batch;
+typedef struct srt_batch_tuning {
+    uint32_t blocks_per_sm;  /* resident blocks per SM of the batched traversal (1..8) */
+    uint32_t chunk;          /* rays a warp draws from the shared queue at once (32..1024, x32) */
+    float ms_per_iteration;  /* autotune: time of one iteration with this choice */
+    uint32_t candidates;     /* autotune: configurations timed */
+} srt_batch_tuning;
+/* n <= 64 scenes; params: n entries (NULL: defaults); no STAGE_TIMING,
+ * COUNT_VISITS or RAY_SORT flag in a batch. */
+srt_status srt_batch_create(srt_ctx* ctx, uint32_t n, srt_scene* const* scenes, const uint32_t* widths,
+                            const uint32_t* heights, const srt_params* params, srt_batch** out);
+srt_status srt_batch_destroy(srt_batch* b);
+uint32_t srt_batch_size(const srt_batch* b);
+/* Borrowed handle of scene i's renderer: read its accumulation, image, stats
+ * and photons with the srt_renderer_* calls; it is not destroyed or rendered
+ * on its own. */
+srt_renderer* srt_batch_renderer(srt_batch* b, uint32_t i);
+/* One iteration (one sample per pixel) of every scene whose active[i] != 0
+ * (active NULL: all); cams: n camera uniforms. */
+srt_status srt_batch_render(srt_batch* b, const srt_camera_uniform* cams, const uint8_t* active);
+srt_status srt_batch_get_tuning(const srt_batch* b, srt_batch_tuning* out);
+srt_status srt_batch_set_tuning(srt_batch* b, const srt_batch_tuning* t);
+/* Times `iterations` iterations of every candidate (blocks per SM x chunk),
+ * keeps the fastest, then clears every scene's accumulation and statistics. */
+srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform* cams, uint32_t iterations,
+                              srt_batch_tuning* out);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,101 @@
+"""Batched rendering (srt_batch_*): scenes of uneven size in one CUDA graph per
+iteration, their rays traced in shared launches, give the same images as
+rendering each scene alone; inactive scenes are left untouched; the
+autotuner picks one of its candidates and clears the tuning frames."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _scenes(srt, ctx):
+    out = []
+    for preset in (srt.PRESET_CORNELL_BOX, srt.PRESET_CONFIG1, srt.PRESET_CAUSTIC_SLAB):
+        b = srt.SceneBuilder()
+        cam = b.add_preset(preset)
+        out.append((b.build(ctx), srt.CameraController(*cam)))
+    return out
+
+
+SIZES = [(64, 48), (96, 64), (80, 80)]
+
+
+def _params(srt):
+    return [srt.default_params(photons_per_frame=1 << 16, max_depth=8),
+            srt.default_params(photons_per_frame=1 << 15),
+            srt.default_params(photons_per_frame=1 << 16, max_depth=16, seed=7)]
+
+
+def _cams(ctls, frame):
+    return [c.build_uniform(w / h, frame) for c, (w, h) in zip(ctls, SIZES)]
+
+
+def test_batch_matches_single_scene_renders(srt, ctx):
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    params = _params(srt)
+    batch = srt.Batch(ctx, scenes, SIZES, params)
+    frames = 4
+    for f in range(frames):
+        batch.render(_cams(ctls, f))
+    ctx.synchronize()
+    for i, (scene, (w, h)) in enumerate(zip(scenes, SIZES)):
+        r = srt.Renderer(ctx, scene, w, h, params[i])
+        for f in range(frames):
+            r.render(ctls[i].build_uniform(w / h, f))
+        ref = r.read_accum()
+        got = batch.renderers[i].read_accum()
+        np.testing.assert_array_equal(got, ref)
+        np.testing.assert_array_equal(batch.renderers[i].read_ldr(), r.read_ldr())
+        st = batch.renderers[i].stats()
+        assert st["frames"] == frames and st["paths"] == frames * w * h
+        r.close()
+    # an inactive scene keeps its image
+    before = batch.renderers[1].read_accum()
+    batch.render(_cams(ctls, frames), active=[1, 0, 1])
+    ctx.synchronize()
+    np.testing.assert_array_equal(batch.renderers[1].read_accum(), before)
+    assert batch.renderers[0].stats()["frames"] == frames + 1
+    assert batch.renderers[1].stats()["frames"] == frames
+    batch.close()
+
+
+def test_batch_autotune(srt, ctx):
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    batch = srt.Batch(ctx, scenes, SIZES, _params(srt))
+    t = batch.autotune(_cams(ctls, 0), iterations=1)
+    assert t["candidates"] == 9
+    assert t["blocks_per_sm"] in (2, 4, 8) and t["chunk"] in (32, 64, 128)
+    assert t["ms_per_iteration"] > 0
+    assert batch.tuning()["chunk"] == t["chunk"]
+    for r in batch.renderers:
+        assert not np.any(r.read_accum())  # tuning frames cleared
+        assert r.stats()["frames"] == 0
+    batch.render(_cams(ctls, 0))
+    ctx.synchronize()
+    assert all(r.stats()["frames"] == 1 for r in batch.renderers)
+    with pytest.raises(srt.SrtError):
+        batch.renderers[0].render(_cams(ctls, 1)[0])
+    batch.close()
+
+
+def test_handles_destroyed_in_any_order(srt):
+    """The context outlives its scenes, renderers and batches whatever the
+    order of the destroy calls (garbage collectors pick their own order)."""
+    ctx = srt.Context(0)
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b.build(ctx)
+    r = srt.Renderer(ctx, scene, 32, 24, srt.default_params(photons_per_frame=1 << 12))
+    batch = srt.Batch(ctx, [scene], [(16, 16)], [srt.default_params(photons_per_frame=1 << 12)])
+    r.render(srt.CameraController(*cam).build_uniform(32 / 24, 0))
+    batch.render([srt.CameraController(*cam).build_uniform(1.0, 0)])
+    ctx.close()  # deferred: children alive
+    img = r.read_accum()
+    assert img.shape == (24, 32, 4) and np.all(np.isfinite(img))
+    scene.close()
+    batch.close()
+    r.close()

@@ -76,6 +76,11 @@ class Params(C.Structure):
                 ("seed", C.c_uint32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_uint32), ("chunk", C.c_uint32), ("ms_per_iteration", C.c_float),
+                ("candidates", C.c_uint32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("frames", C.c_uint64), ("paths", C.c_uint64), ("rays_closest", C.c_uint64),
                 ("rays_shadow", C.c_uint64), ("rays_photon", C.c_uint64), ("photons_emitted", C.c_uint64),
@@ -113,6 +118,7 @@ PRESET_CONFIG1 = 2
 PRESET_CONFIG2 = 3
 PRESET_CAUSTIC_SLAB = 4
 PRESET_INDIRECT_ROOM = 5
+PRESET_BATCH_RANDOM = 6
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
@@ -172,6 +178,14 @@ SIGNATURES = {
     "srt_renderer_blit": (_I, [_P, _U32, _U32, _I, _P]),
     "srt_photon_splat": (_I, [_P, _P, _U32, _P, _U32, _U32, _P]),
     "srt_renderer_splat_photons": (_I, [_P, _P, _U32, _U32, _P]),
+    "srt_batch_create": (_I, [_P, _U32, _P, _P, _P, _P, _P]),
+    "srt_batch_destroy": (_I, [_P]),
+    "srt_batch_size": (_U32, [_P]),
+    "srt_batch_renderer": (_P, [_P, _U32]),
+    "srt_batch_render": (_I, [_P, _P, _P]),
+    "srt_batch_get_tuning": (_I, [_P, _P]),
+    "srt_batch_set_tuning": (_I, [_P, _P]),
+    "srt_batch_autotune": (_I, [_P, _P, _U32, _P]),
     "srt_guide_param_count": (_U32, []),
     "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
@@ -621,3 +635,80 @@ def photon_splat(ctx: Context, photons: np.ndarray, camera: CameraUniform, rgba:
     h, w = a.shape[:2]
     _check(lib().srt_photon_splat(ctx.h, ptr(p), len(p), C.byref(camera), w, h, ptr(a)), ctx.h)
     return a
+
+
+# --------------------------------------------------------------------------- batched rendering
+
+
+class _BorrowedRenderer(Renderer):
+    """A scene's renderer inside a Batch (read-only use; owned by the batch)."""
+
+    def __init__(self, batch, i, handle, width, height, params):
+        self.ctx, self.scene = batch.ctx, batch.scenes[i]
+        self.target_width, self.target_height = int(width), int(height)
+        self.params = params
+        self.h = handle
+
+    def render(self, camera):
+        raise SrtError(1, "a batched scene renders through Batch.render")
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Many scenes and viewports per iteration (srt_batch_*): per-scene stages as
+    parallel CUDA-graph branches, all scenes' rays traced in shared launches."""
+
+    def __init__(self, ctx: Context, scenes, sizes, params=None):
+        self.ctx, self.scenes = ctx, list(scenes)
+        n = len(self.scenes)
+        self.sizes = [(int(w), int(h)) for w, h in sizes]
+        self.params = list(params) if params is not None else [default_params() for _ in range(n)]
+        hs = (C.c_void_p * n)(*[s.h.value if isinstance(s.h, C.c_void_p) else s.h for s in self.scenes])
+        ws = (C.c_uint32 * n)(*[w for w, _ in self.sizes])
+        hh = (C.c_uint32 * n)(*[h for _, h in self.sizes])
+        ps = (Params * n)(*self.params)
+        h = C.c_void_p()
+        _check(lib().srt_batch_create(ctx.h, n, hs, ws, hh, ps, C.byref(h)), ctx.h)
+        self.h = h
+        self.renderers = [_BorrowedRenderer(self, i, C.c_void_p(lib().srt_batch_renderer(self.h, i)), w, hgt,
+                                            self.params[i]) for i, (w, hgt) in enumerate(self.sizes)]
+
+    def __len__(self):
+        return len(self.scenes)
+
+    def render(self, cameras, active=None) -> None:
+        n = len(self.scenes)
+        cams = (CameraUniform * n)(*cameras)
+        act = None if active is None else (C.c_uint8 * n)(*[1 if a else 0 for a in active])
+        _check(lib().srt_batch_render(self.h, cams, act), self.ctx.h)
+
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        _check(lib().srt_batch_get_tuning(self.h, C.byref(t)), self.ctx.h)
+        return {f: getattr(t, f) for f, _ in BatchTuning._fields_}
+
+    def set_tuning(self, blocks_per_sm: int, chunk: int) -> None:
+        t = BatchTuning(blocks_per_sm, chunk, 0.0, 0)
+        _check(lib().srt_batch_set_tuning(self.h, C.byref(t)), self.ctx.h)
+
+    def autotune(self, cameras, iterations: int = 2) -> dict:
+        n = len(self.scenes)
+        cams = (CameraUniform * n)(*cameras)
+        t = BatchTuning()
+        _check(lib().srt_batch_autotune(self.h, cams, iterations, C.byref(t)), self.ctx.h)
+        return {f: getattr(t, f) for f, _ in BatchTuning._fields_}
+
+    def close(self):
+        if self.h:
+            for r in self.renderers:
+                r.h = None
+            lib().srt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -37,7 +37,26 @@ struct srt_ctx {
     int sm_count = 0;
     std::string err;
     uint32_t* d_err = nullptr;  // device error word for batch entry points
+    // Scenes, renderers and batches created on this context that are still
+    // alive; srt_ctx_destroy defers the release until the last one is gone,
+    // so handles may be destroyed in any order (e.g. by a garbage collector).
+    int children = 0;
+    bool closing = false;
 };
+
+namespace {
+void ctx_free(srt_ctx* c) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_err);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+void ctx_retain(srt_ctx* c) { ++c->children; }
+void ctx_release(srt_ctx* c) {
+    if (--c->children == 0 && c->closing) ctx_free(c);
+}
+}  // namespace
 
 namespace {
 
@@ -123,12 +142,14 @@ srt_status srt_ctx_create(int device, void* stream, srt_ctx** out) {
 }
 
 srt_status srt_ctx_destroy(srt_ctx* c) {
-    if (!c) return SRT_ERR_INVALID_ARG;
-    cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
-    cudaFree(c->d_err);
-    if (c->own_stream) cudaStreamDestroy(c->stream);
-    delete c;
+    if (!c || c->closing) return SRT_ERR_INVALID_ARG;
+    if (c->children > 0) {
+        c->closing = true;  // released with its last scene, renderer or batch
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        return SRT_OK;
+    }
+    ctx_free(c);
     return SRT_OK;
 }
 
@@ -411,6 +432,7 @@ extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt
         d.bmin = make_float4((float)lo[0], (float)lo[1], (float)lo[2], 0.f);
         d.binv = make_float4(inv[0], inv[1], inv[2], 0.f);
     }
+    ctx_retain(c);
     *out = s.release();
     return SRT_OK;
 }
@@ -424,9 +446,11 @@ extern "C" srt_status srt_scene_builder_build(srt_ctx* c, const srt_scene_builde
 
 extern "C" srt_status srt_scene_destroy(srt_scene* s) {
     if (!s) return SRT_ERR_INVALID_ARG;
-    cudaSetDevice(s->ctx->device);
-    cudaStreamSynchronize(s->ctx->stream);
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
     delete s;
+    ctx_release(c);
     return SRT_OK;
 }
 
@@ -519,6 +543,42 @@ struct srt_renderer {
         mark();
         return n;
     }
+
+    // The same frame in three parts for the batched renderer, which traces
+    // the rays of all its scenes in shared launches between them.
+    int record_begin(cudaStream_t st) {
+        int n = 0;
+        cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
+        if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
+        return n + launch_raygen(args, st);
+    }
+    int record_shade(uint32_t b, cudaStream_t st) { return b < p.max_depth ? launch_bounce(args, b, st, 2) : 0; }
+    int record_end(cudaStream_t st) {
+        int n = launch_finalize(args, st) + launch_frame_stats(args, st);
+        if (args.guiding) n += launch_guide_train(args, st);
+        return n;
+    }
+    MultiTraceItem trace_item(uint32_t b, bool shadow) const {
+        MultiTraceItem it{};
+        it.s = args.scene;
+        it.err = args.err;
+        if (shadow) {
+            it.count = &counters->shadow[b];
+            it.ro = pb.sh_o;
+            it.rd = pb.sh_d;
+            it.sh_id = pb.sh_id;
+            it.sh_c = pb.sh_c;
+            it.rad = pb.rad;
+        } else {
+            it.queue = pb.queue[b & 1];
+            it.count = &counters->paths[b];
+            it.ro = pb.ray_o;
+            it.rd = pb.ray_d;
+            it.hit = pb.hit;
+        }
+        return it;
+    }
+    bool batch_owned = false;
 };
 
 extern "C" srt_params srt_params_default(void) {
@@ -669,20 +729,23 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     for (auto& e : r->ev) CUDA_TRY(c, cudaEventCreate(&e));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
     if (env_fault("launch")) return fail(c, SRT_ERR_CUDA, "injected launch failure");
+    ctx_retain(c);
     *out = r.release();
     return SRT_OK;
 }
 
 extern "C" srt_status srt_renderer_destroy(srt_renderer* r) {
-    if (!r) return SRT_ERR_INVALID_ARG;
-    cudaSetDevice(r->ctx->device);
-    cudaStreamSynchronize(r->ctx->stream);
+    if (!r || r->batch_owned) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
     delete r;
+    ctx_release(c);
     return SRT_OK;
 }
 
 extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform* cam) {
-    if (!r || !cam) return SRT_ERR_INVALID_ARG;
+    if (!r || !cam || r->batch_owned) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     cudaSetDevice(c->device);
     cudaStream_t st = c->stream;
@@ -1237,4 +1300,267 @@ extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_came
     CUDA_TRY(c, cudaMemcpyAsync(rgba, img, (size_t)w * h * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_device_error(c, r->err);
+}
+
+// ------------------------------------------------------------------ batched renderer
+// Many scenes (each with its own viewport, parameters and accumulation) per
+// iteration: per-scene photon passes, ray generation, shading and
+// finalisation run as parallel branches of one CUDA graph; the closest-hit
+// and shadow rays of all scenes are traced in one launch per bounce
+// (k_trace_multi).  The graph is re-captured when the set of active scenes
+// or the tuning changes.
+struct srt_batch {
+    srt_ctx* ctx = nullptr;
+    std::vector<srt_renderer*> r;
+    srt_camera_uniform* cams_dev = nullptr;
+    srt_camera_uniform* cams_host = nullptr;  // pinned, 2 slots of n
+    cudaEvent_t up_ev[2] = {};
+    int up_i = 0;
+    MultiTraceItem* items_dev = nullptr;  // [2 kinds][MAX_BOUNCES][MAX_BATCH]
+    uint32_t* fetch_dev = nullptr;        // [2 kinds][MAX_BOUNCES]
+    std::vector<cudaStream_t> side;
+    cudaStream_t cap = nullptr;
+    cudaEvent_t fork_ev = nullptr;
+    std::vector<cudaEvent_t> join_ev;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint8_t> graph_active;
+    int graph_launches = 0;
+    srt_batch_tuning tune{8, 32, 0.0f, 0};
+    uint32_t max_depth = 0;
+    bool small_stack = true;
+
+    ~srt_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto s : side)
+            if (s) cudaStreamDestroy(s);
+        if (cap) cudaStreamDestroy(cap);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        for (auto e : join_ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : up_ev)
+            if (e) cudaEventDestroy(e);
+        cudaFree(cams_dev);
+        cudaFreeHost(cams_host);
+        cudaFree(items_dev);
+        cudaFree(fetch_dev);
+        for (srt_renderer* x : r) {
+            if (x) {
+                x->batch_owned = false;
+                delete x;
+                ctx_release(ctx);
+            }
+        }
+    }
+
+    srt_status capture(const std::vector<uint8_t>& active) {
+        srt_ctx* c = ctx;
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+        std::vector<int> act;
+        for (size_t i = 0; i < r.size(); ++i)
+            if (active[i]) act.push_back((int)i);
+        const int na = (int)act.size();
+        std::vector<MultiTraceItem> items((size_t)2 * MAX_BOUNCES * MAX_BATCH);
+        for (uint32_t b = 0; b < max_depth; ++b)
+            for (int k = 0; k < na; ++k) {
+                items[((size_t)0 * MAX_BOUNCES + b) * MAX_BATCH + k] = r[act[k]]->trace_item(b, false);
+                items[((size_t)1 * MAX_BOUNCES + b) * MAX_BATCH + k] = r[act[k]]->trace_item(b, true);
+            }
+        CUDA_TRY(c, cudaMemcpy(items_dev, items.data(), items.size() * sizeof(MultiTraceItem), cudaMemcpyHostToDevice));
+        cudaGraph_t g;
+        int n = 0;
+        CUDA_TRY(c, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        auto fork_join = [&](auto&& body) {
+            cudaEventRecord(fork_ev, cap);
+            for (int k = 0; k < na; ++k) {
+                cudaStreamWaitEvent(side[k], fork_ev, 0);
+                n += body(r[act[k]], side[k]);
+                cudaEventRecord(join_ev[k], side[k]);
+            }
+            for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
+        };
+        cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 2 * MAX_BOUNCES, cap);
+        fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_begin(s); });
+        for (uint32_t b = 0; b < max_depth; ++b) {
+            n += launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
+                                    (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
+            fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s); });
+            n += launch_trace_multi(items_dev + ((size_t)MAX_BOUNCES + b) * MAX_BATCH, na, 1, small_stack,
+                                    fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
+        }
+        fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_end(s); });
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        CUDA_TRY(c, e);
+        e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        CUDA_TRY(c, e);
+        graph_active = active;
+        graph_launches = n;
+        return SRT_OK;
+    }
+
+    srt_status render(const srt_camera_uniform* cams, const uint8_t* active_in) {
+        srt_ctx* c = ctx;
+        cudaSetDevice(c->device);
+        const size_t n = r.size();
+        std::vector<uint8_t> active(n, 1);
+        if (active_in)
+            for (size_t i = 0; i < n; ++i) active[i] = active_in[i] ? 1 : 0;
+        bool any = false;
+        for (uint8_t a : active) any = any || a;
+        if (!any) return SRT_OK;
+        if (!graph || active != graph_active) {
+            srt_status s = capture(active);
+            if (s != SRT_OK) return s;
+        }
+        int slot = up_i++ & 1;
+        CUDA_TRY(c, cudaEventSynchronize(up_ev[slot]));
+        std::memcpy(cams_host + slot * n, cams, n * sizeof(srt_camera_uniform));
+        CUDA_TRY(c, cudaMemcpyAsync(cams_dev, cams_host + slot * n, n * sizeof(srt_camera_uniform),
+                                    cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaEventRecord(up_ev[slot], c->stream));
+        CUDA_TRY(c, cudaGraphLaunch(graph, c->stream));
+        for (size_t i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            srt_renderer* x = r[i];
+            x->frames += 1;
+            x->photons_emitted += x->p.photons_per_frame;
+            x->frame_count += 1;
+        }
+        if (!r.empty()) r[0]->launches += (uint64_t)graph_launches;
+        return SRT_OK;
+    }
+};
+
+extern "C" srt_status srt_batch_create(srt_ctx* c, uint32_t n, srt_scene* const* scenes, const uint32_t* widths,
+                                       const uint32_t* heights, const srt_params* params, srt_batch** out) {
+    if (!c || !out || n == 0 || n > (uint32_t)MAX_BATCH || !scenes || !widths || !heights) return SRT_ERR_INVALID_ARG;
+    *out = nullptr;
+    cudaSetDevice(c->device);
+    std::unique_ptr<srt_batch> B(new (std::nothrow) srt_batch());
+    if (!B) return SRT_ERR_OOM;
+    B->ctx = c;
+    CUDA_TRY(c, dev_alloc(&B->cams_dev, n));
+    CUDA_TRY(c, cudaMallocHost((void**)&B->cams_host, 2 * n * sizeof(srt_camera_uniform)));
+    std::memset(B->cams_host, 0, 2 * n * sizeof(srt_camera_uniform));
+    CUDA_TRY(c, cudaMemset(B->cams_dev, 0, n * sizeof(srt_camera_uniform)));
+    for (auto& e : B->up_ev) CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CUDA_TRY(c, dev_alloc(&B->items_dev, (size_t)2 * MAX_BOUNCES * MAX_BATCH));
+    CUDA_TRY(c, dev_alloc(&B->fetch_dev, (size_t)2 * MAX_BOUNCES));
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&B->fork_ev, cudaEventDisableTiming));
+    B->side.assign(n, nullptr);
+    B->join_ev.assign(n, nullptr);
+    for (uint32_t i = 0; i < n; ++i) {
+        CUDA_TRY(c, cudaStreamCreateWithFlags(&B->side[i], cudaStreamNonBlocking));
+        CUDA_TRY(c, cudaEventCreateWithFlags(&B->join_ev[i], cudaEventDisableTiming));
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        srt_params p = params ? params[i] : srt_params_default();
+        if (p.flags & (SRT_FLAG_STAGE_TIMING | SRT_FLAG_COUNT_VISITS | SRT_FLAG_RAY_SORT))
+            return fail(c, SRT_ERR_INVALID_ARG, "batched scenes take no STAGE_TIMING, COUNT_VISITS or RAY_SORT flag");
+        srt_renderer* x = nullptr;
+        srt_status s = srt_renderer_create(c, scenes[i], widths[i], heights[i], &p, &x);
+        if (s != SRT_OK) return s;
+        x->batch_owned = true;
+        x->args.cam = B->cams_dev + i;
+        B->r.push_back(x);
+        B->max_depth = std::max(B->max_depth, p.max_depth);
+        if (scenes[i]->dev.depth > (uint32_t)TRAV_STACK_SMALL) B->small_stack = false;
+    }
+    ctx_retain(c);
+    *out = B.release();
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_batch_destroy(srt_batch* b) {
+    if (!b) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    delete b;
+    ctx_release(c);
+    return SRT_OK;
+}
+
+extern "C" uint32_t srt_batch_size(const srt_batch* b) { return b ? (uint32_t)b->r.size() : 0u; }
+
+extern "C" srt_renderer* srt_batch_renderer(srt_batch* b, uint32_t i) {
+    return (b && i < b->r.size()) ? b->r[i] : nullptr;
+}
+
+extern "C" srt_status srt_batch_render(srt_batch* b, const srt_camera_uniform* cams, const uint8_t* active) {
+    if (!b || !cams) return SRT_ERR_INVALID_ARG;
+    return b->render(cams, active);
+}
+
+extern "C" srt_status srt_batch_get_tuning(const srt_batch* b, srt_batch_tuning* out) {
+    if (!b || !out) return SRT_ERR_INVALID_ARG;
+    *out = b->tune;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_batch_set_tuning(srt_batch* b, const srt_batch_tuning* t) {
+    if (!b || !t || t->blocks_per_sm < 1 || t->blocks_per_sm > 8 || t->chunk < 32 || t->chunk > 1024 ||
+        t->chunk % 32 != 0)
+        return SRT_ERR_INVALID_ARG;
+    b->tune.blocks_per_sm = t->blocks_per_sm;
+    b->tune.chunk = t->chunk;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform* cams, uint32_t iterations,
+                                         srt_batch_tuning* out) {
+    if (!b || !cams || iterations == 0) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
+    static const uint32_t bps[] = {2, 4, 8};
+    static const uint32_t chunks[] = {32, 64, 128};
+    cudaEvent_t e0, e1;
+    CUDA_TRY(c, cudaEventCreate(&e0));
+    CUDA_TRY(c, cudaEventCreate(&e1));
+    srt_batch_tuning best{8, 32, 3.4e38f, 0};
+    srt_status st = SRT_OK;
+    for (uint32_t bp : bps)
+        for (uint32_t ch : chunks) {
+            srt_batch_tuning t{bp, ch, 0.0f, 0};
+            srt_batch_set_tuning(b, &t);
+            st = b->render(cams, nullptr);  // capture + warm-up
+            if (st != SRT_OK) break;
+            cudaEventRecord(e0, c->stream);
+            for (uint32_t i = 0; i < iterations && st == SRT_OK; ++i) st = b->render(cams, nullptr);
+            cudaEventRecord(e1, c->stream);
+            if (st != SRT_OK) break;
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= (float)iterations;
+            best.candidates += 1;
+            if (ms < best.ms_per_iteration) {
+                best.blocks_per_sm = bp;
+                best.chunk = ch;
+                best.ms_per_iteration = ms;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != SRT_OK) return st;
+    uint32_t n_cand = best.candidates;
+    srt_batch_set_tuning(b, &best);
+    b->tune.ms_per_iteration = best.ms_per_iteration;
+    b->tune.candidates = n_cand;
+    // the tuning frames are not part of any image
+    for (srt_renderer* x : b->r) {
+        srt_status s = srt_reset_accumulation(x);
+        if (s != SRT_OK) return s;
+        srt_renderer_reset_stats(x);
+    }
+    if (out) *out = b->tune;
+    return SRT_OK;
 }

@@ -542,6 +542,54 @@ bool preset_fill(srt_scene_builder* b, int preset, uint32_t seed, float cam[5]) 
                                      mat4_scale(0.5f, 0.8f, 0.5f)));
             return true;
         }
+        case SRT_PRESET_BATCH_RANDOM: {
+            uint32_t st = pcg(seed * 747796405u + 2891336453u);
+            auto rnd = [&]() {
+                st = pcg(st);
+                return (float)st / 4294967296.0f;
+            };
+            const double budget = std::exp(std::log(1e4) + rnd() * (std::log(2e6) - std::log(1e4)));
+            uint32_t light = b->add_material(mat(6500, 2, 0, 1, 3, 0, 0, 0));
+            uint32_t red = b->add_material(mat(0.65f, 0.05f, 0.05f, 1, 0, 0, 0, 0));
+            uint32_t green = b->add_material(mat(0.12f, 0.45f, 0.15f, 1, 0, 0, 0, 0));
+            uint32_t white = b->add_material(mat(0.73f, 0.73f, 0.73f, 1, 0, 0, 0, 0));
+            uint32_t stone = b->add_material(mat(0.3f + 0.5f * rnd(), 0.3f + 0.5f * rnd(), 0.3f + 0.5f * rnd(), 1, 0,
+                                                 0, 0, 0));
+            uint32_t plane = add_geom(b, geom_plane);
+            cornell_walls(b, plane, white, red, green);
+            float lp[4] = {0.0f, 6500.0f, 2.0f, 0.0f};
+            b->add_light_instance(
+                plane, light,
+                mat4_mul(mat4_mul(mat4_translation(0, 0.99f, 0), mat4_rotation_x(F_PI)), mat4_scale(0.6f, 0.6f, 0.6f)),
+                lp);
+            // the largest displaced icosphere within the budget (level 4..8)
+            uint32_t level = 4;
+            while (level < 8 && 20.0 * std::pow(4.0, (double)(level + 1)) <= budget) ++level;
+            std::vector<srt_vertex> v;
+            std::vector<uint32_t> i;
+            geom_icosphere(level, v, i);
+            geom_displace(v, i, 0.05f, seed);
+            uint32_t ico = b->add_mesh(v.data(), (uint32_t)v.size(), i.data(), (uint32_t)i.size());
+            b->add_instance(ico, stone, mat4_mul(mat4_translation(-0.3f, -0.45f, -0.2f), mat4_scale(0.9f, 0.9f, 0.9f)));
+            double used = 20.0 * std::pow(4.0, (double)level);
+            geom_uv_sphere(64, 32, v, i);
+            uint32_t ball = b->add_mesh(v.data(), (uint32_t)v.size(), i.data(), (uint32_t)i.size());
+            const double per_ball = (double)(i.size() / 3);
+            for (int k = 0; used + per_ball <= budget && k < 512; ++k, used += per_ball) {
+                float kind = rnd();
+                uint32_t m;
+                if (kind < 0.4f) m = b->add_material(mat(0.9f, 0.8f, 0.7f, 1, 1, 0.05f + 0.45f * rnd(), 0, 0));
+                else if (kind < 0.8f)
+                    m = b->add_material(mat(1, 1, 1, 0.05f + 0.45f * rnd(), 5, 200.0f + 600.0f * rnd(), 1.33f, 1.5f));
+                else m = b->add_material(mat(1, 1, 1, 1, 2, 0, 1.5f, 0.0042f));
+                float r = 0.05f + 0.1f * rnd();
+                b->add_instance(ball, m,
+                                mat4_mul(mat4_translation(-0.85f + 1.7f * rnd(), -1.0f + r + 1.2f * rnd(),
+                                                          -0.85f + 1.7f * rnd()),
+                                         mat4_scale(2 * r, 2 * r, 2 * r)));
+            }
+            return true;
+        }
         default:
             return false;
     }

@@ -124,6 +124,23 @@ int launch_blit_letterbox(const uchar4* src, uint32_t sw, uint32_t sh, uchar4* d
 int launch_photon_splat(const float4* photons, uint32_t n, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
                         uint32_t* counts, uchar4* img, cudaStream_t st);
 
+// Batched rendering: the rays of one kind and bounce of many scenes, traced
+// in one launch (trace_kernels.cu).  Visit counting is not available here.
+constexpr int MAX_BATCH = 64;
+struct MultiTraceItem {
+    DevScene s;
+    const uint32_t* queue;  // closest: path ids (NULL: identity)
+    const uint32_t* count;  // device ray count
+    const float4 *ro, *rd;
+    float4* hit;            // closest
+    const uint32_t* sh_id;  // shadow
+    const float4* sh_c;
+    float4* rad;
+    uint32_t* err;
+};
+int launch_trace_multi(const MultiTraceItem* items, int n_items, int any_hit, bool small_stack, uint32_t* fetch,
+                       int blocks_per_sm, uint32_t chunk, int sm_count, cudaStream_t st);
+
 // Grid over a photon array already on the device (n on host).
 int launch_grid_build(const float4* photons, uint32_t n, uint32_t frame, float cell, uint32_t hash_bits,
                       PhotonBuffers& ph, cudaStream_t st);

@@ -151,6 +151,62 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_batch(DevScene S, const f
     else hits[i] = h ? make_float4(t, __uint_as_float(prim), u, v) : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
 }
 
+// Rays of many scenes in one launch (the batched renderer): a virtual queue
+// concatenates every item's rays, each item padded to whole chunks, so a
+// warp's chunk never straddles two scenes; warps draw chunks from *fetch
+// and trace them lane per ray (persistent, no refill).
+template <bool ANY, int STACK>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+    k_trace_multi(const MultiTraceItem* __restrict__ items, int n_items, uint32_t* __restrict__ fetch,
+                  uint32_t chunk) {
+    extern __shared__ uint2 stack_smem[];
+    __shared__ uint32_t pre[MAX_BATCH + 1];
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < n_items; ++i) {
+            pre[i] = acc;
+            acc += (*items[i].count + chunk - 1u) / chunk * chunk;
+        }
+        pre[n_items] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = pre[n_items];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint2* stack = stack_smem + threadIdx.x;
+    while (true) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(fetch, chunk);
+        g = __shfl_sync(0xFFFFFFFFu, g, 0);
+        if (g >= total) break;
+        int s = 0;
+        while (s + 1 < n_items && pre[s + 1] <= g) ++s;
+        const MultiTraceItem& I = items[s];
+        const uint32_t n = *I.count;
+        for (uint32_t k = 0; k < chunk; k += 32u) {
+            const uint32_t q = g - pre[s] + k + lane;
+            if (q >= n) continue;
+            const uint32_t id = I.queue ? I.queue[q] : q;
+            float4 o = I.ro[ANY ? q : id], d = I.rd[ANY ? q : id];
+            Ray ray{xyz(o), xyz(d), o.w, d.w};
+            float t = 0.f, u = 0.f, v = 0.f;
+            uint32_t prim;
+            TravCounters tc{nullptr, nullptr};
+            bool h = traverse<ANY, false, STACK>(I.s, ray, stack, TRACE_BLOCK, t, prim, u, v, I.err, tc);
+            if (ANY) {
+                if (!h) {
+                    uint32_t pid = I.sh_id[q];
+                    float4 c = I.sh_c[q], r = I.rad[pid];
+                    I.rad[pid] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z),
+                                             __fadd_rn(r.w, c.w));
+                }
+            } else {
+                I.hit[id] = h ? make_float4(t, __uint_as_float(prim), u, v)
+                              : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+            }
+        }
+    }
+}
+
 inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
 
 struct TraceLaunch {
@@ -232,6 +288,22 @@ int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t*
     (void)fetch;
     TraceLaunch L{s, queue, count, nullptr, max_n, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind, sm_count};
     launch_kind<false>(L, count_visits, st);
+    return 1;
+}
+
+int launch_trace_multi(const MultiTraceItem* items, int n_items, int any_hit, bool small_stack, uint32_t* fetch,
+                       int blocks_per_sm, uint32_t chunk, int sm_count, cudaStream_t st) {
+    if (n_items <= 0) return 0;
+    uint32_t grid = (uint32_t)(sm_count > 0 ? sm_count : 148) * (uint32_t)std::max(1, blocks_per_sm);
+    const int stack = small_stack ? TRAV_STACK_SMALL : TRAV_STACK;
+    size_t smem = sizeof(uint2) * stack * TRACE_BLOCK;
+    if (any_hit) {
+        if (small_stack) k_trace_multi<true, TRAV_STACK_SMALL><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
+        else k_trace_multi<true, TRAV_STACK><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
+    } else {
+        if (small_stack) k_trace_multi<false, TRAV_STACK_SMALL><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
+        else k_trace_multi<false, TRAV_STACK><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
+    }
     return 1;
 }
 
