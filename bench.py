@@ -244,6 +244,83 @@ def run_reference(args, cfg, rank, world):
     return 0
 
 
+def batched_section(srt, ctx, stream, n_scenes=32, iters=3, seed=12345):
+    """C3: n seeded scenes (triangle budgets log-uniform in [1e4, 2e6], square
+    viewports of 256..1024, 1M..8M photons each), one iteration = 1 spp of
+    every scene; batched renderer after autotuning vs the same scenes rendered
+    one after another with single-scene renderers."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(seed)
+    scenes, ctls, sizes, params = [], [], [], []
+    for s in range(n_scenes):
+        b = srt.SceneBuilder()
+        cam = b.add_preset(srt.PRESET_BATCH_RANDOM, s)
+        scenes.append(b.build(ctx))
+        ctls.append(srt.CameraController(*cam))
+        r = int(rng.choice([256, 512, 768, 1024]))
+        sizes.append((r, r))
+        ph = int(round(float(np.exp(rng.uniform(np.log(1e6), np.log(8e6))))))
+        params.append(srt.default_params(photons_per_frame=ph, seed=s))
+    tris = [sc.info()["triangles"] for sc in scenes]
+    paths = sum(w * h for w, h in sizes)
+    photons = sum(p.photons_per_frame for p in params)
+
+    def cams(f):
+        return [c.build_uniform(w / h, f) for c, (w, h) in zip(ctls, sizes)]
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for f in range(k):
+            fn(f)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    singles = [srt.Renderer(ctx, sc, w, h, p) for sc, (w, h), p in zip(scenes, sizes, params)]
+
+    def seq(f):
+        cs = cams(f)
+        for i, r in enumerate(singles):
+            r.render(cs[i])
+
+    seq(0)
+    ms_seq = timed(lambda f: seq(f + 1), iters)
+    for r in singles:
+        r.close()
+    batch = srt.Batch(ctx, scenes, sizes, params)
+    tune = batch.autotune(cams(0), iterations=1)
+    batch.render(cams(0))
+    ms_batch = timed(lambda f: batch.render(cams(f + 1)), iters)
+    batch.close()
+    for sc in scenes:
+        sc.close()
+    return {"workload": (f"C3: {n_scenes} seeded scenes, {min(tris)}..{max(tris)} triangles, viewports "
+                         f"256^2..1024^2, {paths} paths and {photons} photons per iteration, depth 12"),
+            "iterations": iters, "ms_per_iteration": round(ms_batch, 3),
+            "mpaths_per_s": round(paths / ms_batch / 1e3, 2), "mphotons_per_s": round(photons / ms_batch / 1e3, 2),
+            "sequential_ms_per_iteration": round(ms_seq, 3), "speedup_vs_sequential": round(ms_seq / ms_batch, 3),
+            "tuning": tune}
+
+
+def guided_section(seconds=3.0, ref_spp=4096):
+    """C4 reduced to 480x270 (full-size study: wgpu_spectral_rt_b200.guide_study):
+    equal-time relMSE of guided vs plain against an FP64 reference."""
+    from wgpu_spectral_rt_b200 import guide_study
+
+    d = guide_study.study(preset=4, width=480, height=270, max_depth=16, photons=1 << 20, ref_spp=ref_spp,
+                          seconds=seconds, batch=1 << 18)
+    return {"workload": f"C4 at 480x270 (slab + slit light), depth 16, 2^20 photons, 2^18 training samples/frame; "
+                        f"reference {ref_spp} spp FP64, {seconds} s per arm",
+            "relmse_plain": round(d["plain"]["relmse"], 6), "relmse_guided": round(d["guided"]["relmse"], 6),
+            "relmse_ratio_plain_over_guided": round(d["relmse_ratio_plain_over_guided"], 3),
+            "time_fraction_to_plain_relmse": (round(d["time_fraction"], 3) if d["time_fraction"] else None),
+            "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"]}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -258,6 +335,8 @@ def main(argv=None):
     ap.add_argument("--ref-stride", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the C3 batched-renderer section")
+    ap.add_argument("--no-guided", action="store_true", help="skip the C4 guided-vs-plain section")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -375,6 +454,13 @@ def main(argv=None):
         rt.close()
         rc.close()
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_section(srt, ctx, stream)
+    guided = None
+    if rank == 0 and world == 1 and not args.no_guided:
+        guided = guided_section()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(srt, b, cam, w, h, params, seconds_target=args.cpu_seconds)
@@ -397,6 +483,8 @@ def main(argv=None):
                     "d2h_bytes_per_step": w * h * 4, "steps": e2e_steps} if e2e_steps else None,
             "gpu_launches": int(st["kernel_launches"]),
             "roofline": roof,
+            "batched": batched,
+            "guided": guided,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
