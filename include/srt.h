@@ -242,6 +242,21 @@ srt_status srt_scene_builder_build(srt_ctx* ctx, const srt_scene_builder* b, srt
  * n_lights may be 0 (no light sampling, no photons). */
 srt_status srt_scene_build(srt_ctx* ctx, const srt_scene_arrays* arrays, srt_scene** out);
 srt_status srt_scene_destroy(srt_scene* s);
+/* Moves instances (scene-side GPU ingestion for dynamic scenes; no reference
+ * counterpart): ids[k] gets the column-major object-to-world transform
+ * transforms[16 k .. 16 k + 15].  On the device: the moved instances'
+ * triangles are re-transformed, the light triangles of moved light
+ * instances (srt_scene_builder_add_light_instance) re-expanded, and the BVH8
+ * refitted (same topology; boxes recomputed bottom-up and re-quantised).
+ * Buffers are updated in place, so renderers (and their captured graphs)
+ * keep working; the scene bounds used to normalise guide inputs stay as
+ * built.  Waits for the context's stream before and after. */
+srt_status srt_scene_update_instances(srt_scene* scene, const uint32_t* ids, const float* transforms, uint32_t n);
+/* The scene's world-space light triangles as the device holds them (for a
+ * builder scene: expanded on the GPU); *count = number of lights. */
+srt_status srt_scene_read_lights(srt_scene* scene, srt_light* out, uint32_t capacity, uint32_t* count);
+/* Raw copies of the BVH8 nodes (80 B each) and leaf triangle slots (48 B). */
+srt_status srt_scene_read_bvh(srt_scene* scene, void* nodes, uint64_t node_bytes, void* tris, uint64_t tri_bytes);
 /* Flattened triangle count and BVH node count of a built scene. */
 srt_status srt_scene_info(const srt_scene* s, uint64_t* n_triangles, uint64_t* n_nodes, uint32_t* bvh_depth);
 

@@ -186,6 +186,9 @@ SIGNATURES = {
     "srt_batch_get_tuning": (_I, [_P, _P]),
     "srt_batch_set_tuning": (_I, [_P, _P]),
     "srt_batch_autotune": (_I, [_P, _P, _U32, _P]),
+    "srt_scene_update_instances": (_I, [_P, _P, _P, _U32]),
+    "srt_scene_read_lights": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
+    "srt_scene_read_bvh": (_I, [_P, _P, C.c_uint64, _P, C.c_uint64]),
     "srt_guide_param_count": (_U32, []),
     "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
@@ -381,6 +384,26 @@ class Scene:
         out = np.zeros(len(r), dtype=[("t", np.float32), ("prim", np.uint32), ("u", np.float32), ("v", np.float32)])
         _check(lib().srt_trace_rays(self.h, ptr(r), len(r), ptr(out), 1 if any_hit else 0), self.ctx.h)
         return out
+
+    def update_instances(self, ids, transforms) -> None:
+        """Moves instances: transforms [n, 16] column-major object-to-world (GPU re-transform + BVH refit)."""
+        i = np.ascontiguousarray(ids, np.uint32).reshape(-1)
+        t = np.ascontiguousarray(transforms, np.float32).reshape(-1, 16)
+        _check(lib().srt_scene_update_instances(self.h, ptr(i), ptr(t), len(i)), self.ctx.h)
+
+    def read_lights(self) -> np.ndarray:
+        n = C.c_uint32()
+        _check(lib().srt_scene_read_lights(self.h, None, 0, C.byref(n)), self.ctx.h)
+        out = np.zeros((n.value, 16), np.float32)
+        _check(lib().srt_scene_read_lights(self.h, ptr(out), n.value, C.byref(n)), self.ctx.h)
+        return out
+
+    def read_bvh(self):
+        info = self.info()
+        nodes = np.zeros((info["nodes"], 20), np.uint32)
+        tris = np.zeros((info["triangles"], 12), np.float32)
+        _check(lib().srt_scene_read_bvh(self.h, ptr(nodes), nodes.nbytes, ptr(tris), tris.nbytes), self.ctx.h)
+        return nodes, tris
 
     def close(self):
         if self.h:

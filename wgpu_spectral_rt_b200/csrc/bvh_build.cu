@@ -61,9 +61,7 @@ __global__ void k_flatten(const float4* __restrict__ vtx, const uint32_t* __rest
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             float4 p = vtx[2 * (indices[io + k] + mi.x)];
-            w[k] = f3(f.r0.x * p.x + f.r0.y * p.y + f.r0.z * p.z + f.r0.w,
-                      f.r1.x * p.x + f.r1.y * p.y + f.r1.z * p.z + f.r1.w,
-                      f.r2.x * p.x + f.r2.y * p.y + f.r2.z * p.z + f.r2.w);
+            w[k] = xform_point(f, p.x, p.y, p.z);
         }
         TriSlot s;
         s.v0 = make_float4(w[0].x, w[0].y, w[0].z, __uint_as_float(t));
@@ -216,6 +214,158 @@ __device__ __forceinline__ void ref_range(const Bvh2& b, uint32_t r, uint32_t& f
     }
 }
 
+// Quantisation frame and 8-bit child boxes of one node, children indexed by
+// slot (slots outside `used` empty): writes nd.a (origin, exponent bytes,
+// imask), nd.c, nd.d, nd.e.  250 quanta span the node; the origin sits two
+// quanta below it, and every child plane is padded outward by one quantum,
+// which covers the half-quantum error of the traversal's biased-byte
+// evaluation (see traverse<> in device_common.cuh).
+__device__ void quantize_node(float3 nlo, float3 nhi, const float3* slo, const float3* shi, uint32_t used,
+                              uint32_t imask, Node8& nd, uint32_t* err) {
+    uint32_t ebyte[3];
+    float scale[3];
+    float nlov[3] = {nlo.x, nlo.y, nlo.z}, nhiv[3] = {nhi.x, nhi.y, nhi.z};
+    for (int a = 0; a < 3; ++a) {
+        double ext = (double)nhiv[a] - (double)nlov[a];
+        int ex = -126;
+        if (ext > 0.0) {
+            ex = (int)ceil(log2(ext / 250.0));
+            if (ldexp(250.0, ex) < ext) ++ex;
+        }
+        // a quantum of at least 4 float ulps of the node's coordinates, so the
+        // shifted origin below stays exact to a quarter quantum
+        double mag = fmax(fabs((double)nlov[a]), fabs((double)nhiv[a]));
+        ex = max(ex, (int)ceil(log2(fmax(mag, 1e-30) * 4.0 / 8388608.0)));
+        ex = max(ex, -126);
+        ex = min(ex, 127);
+        ebyte[a] = (uint32_t)(ex + 127);
+        scale[a] = __uint_as_float(ebyte[a] << 23);
+        double lo_exact = (double)nlov[a];
+        nlov[a] = (float)(lo_exact - 2.0 * (double)scale[a]);
+        while ((double)nlov[a] > lo_exact - 2.0 * (double)scale[a]) nlov[a] = nextafterf(nlov[a], -3.4e38f);
+    }
+    uint32_t qlo[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}}, qhi[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}};
+    for (int s = 0; s < 8; ++s) {
+        if (!((used >> s) & 1u)) continue;
+        float lo3[3] = {slo[s].x, slo[s].y, slo[s].z}, hi3[3] = {shi[s].x, shi[s].y, shi[s].z};
+        for (int a = 0; a < 3; ++a) {
+            double sc = (double)scale[a];
+            // one quantum of padding on each side
+            int ql = (int)floor(((double)lo3[a] - (double)nlov[a]) / sc) - 1;
+            int qh = (int)ceil(((double)hi3[a] - (double)nlov[a]) / sc) + 1;
+            ql = min(max(ql, 0), 255);
+            qh = min(max(qh, 0), 255);
+            while (ql > 0 && (double)nlov[a] + ql * sc > (double)lo3[a] - sc) --ql;
+            while (qh < 255 && (double)nlov[a] + qh * sc < (double)hi3[a] + sc) ++qh;
+            if ((double)nlov[a] + ql * sc > (double)lo3[a] - sc || (double)nlov[a] + qh * sc < (double)hi3[a] + sc)
+                atomicOr(err, ERR_BAD_INDEX);  // the frame cannot hold the padded child: reject the tree
+            qlo[a][s >> 2] |= (uint32_t)ql << (8 * (s & 3));
+            qhi[a][s >> 2] |= (uint32_t)qh << (8 * (s & 3));
+        }
+    }
+    nd.a = make_uint4(__float_as_uint(nlov[0]), __float_as_uint(nlov[1]), __float_as_uint(nlov[2]),
+                      ebyte[0] | (ebyte[1] << 8) | (ebyte[2] << 16) | (imask << 24));
+    nd.c = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
+    nd.d = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
+    nd.e = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
+}
+
+// Refit of one level's nodes: child boxes from the deeper level's results
+// (aux) or from the leaf triangles, then the node's frame is re-quantised.
+__global__ void k_refit8(Node8* __restrict__ nodes, const TriSlot* __restrict__ tris, uint32_t begin, uint32_t end,
+                         float4* __restrict__ aux, uint32_t* __restrict__ err) {
+    uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    Node8 nd = nodes[i];
+    const uint32_t imask = nd.a.w >> 24, child_base = nd.b.x, tri_base = nd.b.y;
+    const uint32_t meta[2] = {nd.b.z, nd.b.w};
+    float3 slo[8], shi[8];
+    float3 nlo = f3(3.4e38f, 3.4e38f, 3.4e38f), nhi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+    uint32_t used = 0u;
+    for (int s = 0; s < 8; ++s) {
+        const uint32_t m = (meta[s >> 2] >> (8 * (s & 3))) & 0xFFu;
+        if (m == 0u) continue;
+        used |= 1u << s;
+        float3 lo, hi;
+        if ((imask >> s) & 1u) {
+            const uint32_t child = child_base + __popc(imask & ((1u << s) - 1u));
+            float4 a = aux[2 * child], b = aux[2 * child + 1];
+            lo = f3(a.x, a.y, a.z);
+            hi = f3(b.x, b.y, b.z);
+        } else {
+            lo = f3(3.4e38f, 3.4e38f, 3.4e38f);
+            hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+            const uint32_t cnt = m >> 5, off = m & 31u;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const TriSlot& t = tris[tri_base + off + k];
+                float3 v[3] = {f3(t.v0.x, t.v0.y, t.v0.z), f3(t.v1.x, t.v1.y, t.v1.z), f3(t.v2.x, t.v2.y, t.v2.z)};
+                for (int j = 0; j < 3; ++j) {
+                    lo = f3(fminf(lo.x, v[j].x), fminf(lo.y, v[j].y), fminf(lo.z, v[j].z));
+                    hi = f3(fmaxf(hi.x, v[j].x), fmaxf(hi.y, v[j].y), fmaxf(hi.z, v[j].z));
+                }
+            }
+        }
+        slo[s] = lo;
+        shi[s] = hi;
+        nlo = f3(fminf(nlo.x, lo.x), fminf(nlo.y, lo.y), fminf(nlo.z, lo.z));
+        nhi = f3(fmaxf(nhi.x, hi.x), fmaxf(nhi.y, hi.y), fmaxf(nhi.z, hi.z));
+    }
+    aux[2 * i] = make_float4(nlo.x, nlo.y, nlo.z, 0.f);
+    aux[2 * i + 1] = make_float4(nhi.x, nhi.y, nhi.z, 0.f);
+    quantize_node(nlo, nhi, slo, shi, used, imask, nd, err);
+    nodes[i] = nd;
+}
+
+__device__ __forceinline__ const InstFwd& fwd_of(const InstFwd* fwd, uint32_t i) { return fwd[i]; }
+
+// Leaf slots of moved instances, re-transformed from object space.
+__global__ void k_update_slots(TriSlot* __restrict__ tris, uint32_t n_tris, const uint32_t* __restrict__ tri_inst,
+                               const uint8_t* __restrict__ moved, const float4* __restrict__ vtx,
+                               const uint32_t* __restrict__ indices, const uint4* __restrict__ mesh_infos,
+                               const InstDev* __restrict__ inst, const InstFwd* __restrict__ fwd) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_tris) return;
+    TriSlot s = tris[k];
+    const uint32_t t = __float_as_uint(s.v0.w);
+    const uint32_t ii = tri_inst[t];
+    if (!moved[ii]) return;
+    const InstDev& in = inst[ii];
+    const InstFwd f = fwd[ii];
+    const uint4 mi = mesh_infos[in.mesh_id];
+    const uint32_t io = mi.y + (t - in.tri_offset) * 3u;
+    float3 w[3];
+    for (int j = 0; j < 3; ++j) {
+        float4 p = vtx[2 * (indices[io + j] + mi.x)];
+        w[j] = xform_point(f, p.x, p.y, p.z);
+    }
+    s.v0 = make_float4(w[0].x, w[0].y, w[0].z, s.v0.w);
+    s.v1 = make_float4(w[1].x, w[1].y, w[1].z, 0.f);
+    s.v2 = make_float4(w[2].x, w[2].y, w[2].z, 0.f);
+    tris[k] = s;
+}
+
+// One block per light instance: its triangles in world space
+// (builder.rs:101-129; w = 1, params copied).
+__global__ void k_expand_lights(const LightInst* __restrict__ li, const uint8_t* __restrict__ moved,
+                                const float4* __restrict__ vtx, const uint32_t* __restrict__ indices,
+                                const uint4* __restrict__ mesh_infos, const InstDev* __restrict__ inst,
+                                const InstFwd* __restrict__ fwd, float4* __restrict__ lights) {
+    const LightInst L = li[blockIdx.x];
+    if (moved && !moved[L.inst]) return;
+    const InstDev& in = inst[L.inst];
+    const InstFwd f = fwd[L.inst];
+    const uint4 mi = mesh_infos[in.mesh_id];
+    for (uint32_t k = threadIdx.x; k < L.count; k += blockDim.x) {
+        float4* o = lights + 4ull * (L.first + k);
+        for (int j = 0; j < 3; ++j) {
+            float4 p = vtx[2 * (indices[mi.y + 3u * k + j] + mi.x)];
+            float3 w = xform_point(f, p.x, p.y, p.z);
+            o[j] = make_float4(w.x, w.y, w.z, 1.0f);
+        }
+        o[3] = L.params;
+    }
+}
+
 // One thread per 8-wide node of this level: queue entries (bvh2 ref, node).
 __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in, uint2* __restrict__ qout,
                            uint32_t* __restrict__ n_out, Node8* __restrict__ nodes, uint32_t* __restrict__ node_alloc,
@@ -301,52 +451,15 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         slot_of[bc] = bsl;
         child_in[bsl] = bc;
     }
-    // quantisation frame: 250 quanta span the node; the origin sits two
-    // quanta below it, and every child plane is padded outward by one
-    // quantum, which covers the half-quantum error of the traversal's
-    // biased-byte evaluation (see traverse<> in device_common.cuh)
-    uint32_t ebyte[3];
-    float scale[3];
-    float nlov[3] = {nlo.x, nlo.y, nlo.z}, nhiv[3] = {nhi.x, nhi.y, nhi.z};
-    for (int a = 0; a < 3; ++a) {
-        double ext = (double)nhiv[a] - (double)nlov[a];
-        int ex = -126;
-        if (ext > 0.0) {
-            ex = (int)ceil(log2(ext / 250.0));
-            if (ldexp(250.0, ex) < ext) ++ex;
-        }
-        // a quantum of at least 4 float ulps of the node's coordinates, so the
-        // shifted origin below stays exact to a quarter quantum
-        double mag = fmax(fabs((double)nlov[a]), fabs((double)nhiv[a]));
-        ex = max(ex, (int)ceil(log2(fmax(mag, 1e-30) * 4.0 / 8388608.0)));
-        ex = max(ex, -126);
-        ex = min(ex, 127);
-        ebyte[a] = (uint32_t)(ex + 127);
-        scale[a] = __uint_as_float(ebyte[a] << 23);
-        double lo_exact = (double)nlov[a];
-        nlov[a] = (float)(lo_exact - 2.0 * (double)scale[a]);
-        while ((double)nlov[a] > lo_exact - 2.0 * (double)scale[a]) nlov[a] = nextafterf(nlov[a], -3.4e38f);
-    }
-    uint32_t meta[2] = {0u, 0u}, qlo[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}}, qhi[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}};
-    uint32_t imask = 0u, int_rank = 0u, tri_off = 0u;
+    uint32_t meta[2] = {0u, 0u};
+    uint32_t imask = 0u, int_rank = 0u, tri_off = 0u, used = 0u;
+    float3 slo[8], shi[8];
     for (int s = 0; s < 8; ++s) {
         int c = child_in[s];
         if (c < 0) continue;
-        float lo3[3] = {clo[c].x, clo[c].y, clo[c].z}, hi3[3] = {chi[c].x, chi[c].y, chi[c].z};
-        for (int a = 0; a < 3; ++a) {
-            double sc = (double)scale[a];
-            // one quantum of padding on each side
-            int ql = (int)floor(((double)lo3[a] - (double)nlov[a]) / sc) - 1;
-            int qh = (int)ceil(((double)hi3[a] - (double)nlov[a]) / sc) + 1;
-            ql = min(max(ql, 0), 255);
-            qh = min(max(qh, 0), 255);
-            while (ql > 0 && (double)nlov[a] + ql * sc > (double)lo3[a] - sc) --ql;
-            while (qh < 255 && (double)nlov[a] + qh * sc < (double)hi3[a] + sc) ++qh;
-            if ((double)nlov[a] + ql * sc > (double)lo3[a] - sc || (double)nlov[a] + qh * sc < (double)hi3[a] + sc)
-                atomicOr(err, ERR_BAD_INDEX);  // the frame cannot hold the padded child: reject the tree
-            qlo[a][s >> 2] |= (uint32_t)ql << (8 * (s & 3));
-            qhi[a][s >> 2] |= (uint32_t)qh << (8 * (s & 3));
-        }
+        used |= 1u << s;
+        slo[s] = clo[c];
+        shi[s] = chi[c];
         uint32_t m;
         if (ccount[c] <= 3u) {
             m = (ccount[c] << 5) | tri_off;
@@ -362,12 +475,8 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         meta[s >> 2] |= m << (8 * (s & 3));
     }
     Node8 nd;
-    nd.a = make_uint4(__float_as_uint(nlov[0]), __float_as_uint(nlov[1]), __float_as_uint(nlov[2]),
-                      ebyte[0] | (ebyte[1] << 8) | (ebyte[2] << 16) | (imask << 24));
+    quantize_node(nlo, nhi, slo, shi, used, imask, nd, err);
     nd.b = make_uint4(child_base, tri_base, meta[0], meta[1]);
-    nd.c = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
-    nd.d = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
-    nd.e = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
     nodes[q.y] = nd;
 }
 
@@ -451,6 +560,8 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
         CK(cudaMemcpyAsync(counters, init_counts, sizeof(init_counts), cudaMemcpyHostToDevice, st));
         uint32_t n_in = 1;
         uint32_t depth = 0;
+        out->level_start[0] = 0u;
+        out->level_start[1] = 1u;
         while (n_in > 0) {
             CK(cudaMemsetAsync(counters + 2, 0, 4, st));
             k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(b, qa, n_in, qb, counters + 2, out->nodes, counters,
@@ -458,8 +569,11 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
             ++out->kernel_launches;
             ++depth;
             CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(&n_in, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+            uint32_t hc3[3];
+            CK(cudaMemcpyAsync(hc3, counters, sizeof(hc3), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            n_in = hc3[2];
+            if (depth < 65) out->level_start[depth + 1] = hc3[0];  // nodes of the next level end here
             uint2* t = qa;
             qa = qb;
             qb = t;
@@ -510,6 +624,35 @@ done:
     }
 #undef CK
     return e;
+}
+
+int launch_update_slots(TriSlot* tris, uint32_t n_tris, const uint32_t* tri_inst, const uint8_t* moved,
+                        const float4* vtx, const uint32_t* indices, const uint4* mesh_infos, const InstDev* inst,
+                        const InstFwd* fwd, cudaStream_t st) {
+    if (n_tris == 0) return 0;
+    k_update_slots<<<(n_tris + 255) / 256, 256, 0, st>>>(tris, n_tris, tri_inst, moved, vtx, indices, mesh_infos, inst,
+                                                         fwd);
+    return 1;
+}
+
+int launch_expand_lights(const LightInst* li, uint32_t n_li, const uint8_t* moved, const float4* vtx,
+                         const uint32_t* indices, const uint4* mesh_infos, const InstDev* inst, const InstFwd* fwd,
+                         float4* lights, cudaStream_t st) {
+    if (n_li == 0) return 0;
+    k_expand_lights<<<n_li, 128, 0, st>>>(li, moved, vtx, indices, mesh_infos, inst, fwd, lights);
+    return 1;
+}
+
+int refit_bvh8(Node8* nodes, const TriSlot* tris, const BvhOutputs& lv, float4* aux, uint32_t* err,
+               cudaStream_t st) {
+    int n = 0;
+    for (int L = (int)lv.depth - 1; L >= 0; --L) {
+        uint32_t b = lv.level_start[L], e = lv.level_start[L + 1];
+        if (e <= b) continue;
+        k_refit8<<<(e - b + 127) / 128, 128, 0, st>>>(nodes, tris, b, e, aux, err);
+        ++n;
+    }
+    return n;
 }
 
 }  // namespace srt

@@ -12,6 +12,23 @@ struct InstFwd {
     float4 r0, r1, r2;
 };
 
+// Object -> world with every rounding pinned (((m0 x + m1 y) + m2 z) + m3),
+// the order of the host builder's light expansion, so the flattened
+// triangles, the refit and the light expansion agree bit for bit.
+__device__ __forceinline__ float3 xform_point(const InstFwd& f, float x, float y, float z) {
+    return make_float3(
+        __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.r0.x, x), __fmul_rn(f.r0.y, y)), __fmul_rn(f.r0.z, z)), f.r0.w),
+        __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.r1.x, x), __fmul_rn(f.r1.y, y)), __fmul_rn(f.r1.z, z)), f.r1.w),
+        __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.r2.x, x), __fmul_rn(f.r2.y, y)), __fmul_rn(f.r2.z, z)), f.r2.w));
+}
+
+// A light instance (add_light_instance): its triangles' world-space copies
+// are lights[first .. first + count).
+struct LightInst {
+    uint32_t inst, first, count, pad;
+    float4 params;
+};
+
 struct BvhInputs {
     const float4* vtx;        // device srt_vertex array (pos, normal)
     const uint32_t* indices;  // device global index buffer
@@ -29,10 +46,25 @@ struct BvhOutputs {
     uint32_t n_nodes;
     uint32_t depth;      // number of 8-wide levels
     int kernel_launches;
+    uint32_t level_start[66];  // nodes of level L: [level_start[L], level_start[L + 1]), L < depth
 };
 
 // Builds the tree on `st` (synchronising it); device memory in `out` is
 // owned by the caller afterwards (cudaFree).
 cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, std::string* msg);
+
+// Scene updates (moved instances), all on `st`:
+// re-transform the leaf slots of instances with moved[inst] != 0,
+int launch_update_slots(TriSlot* tris, uint32_t n_tris, const uint32_t* tri_inst, const uint8_t* moved,
+                        const float4* vtx, const uint32_t* indices, const uint4* mesh_infos, const InstDev* inst,
+                        const InstFwd* fwd, cudaStream_t st);
+// expand light instances (all, or those with moved[inst] != 0) into world-space lights,
+int launch_expand_lights(const LightInst* li, uint32_t n_li, const uint8_t* moved, const float4* vtx,
+                         const uint32_t* indices, const uint4* mesh_infos, const InstDev* inst, const InstFwd* fwd,
+                         float4* lights, cudaStream_t st);
+// recompute every node's boxes bottom-up (topology kept) and re-quantise;
+// aux: 2 float4 per node of scratch; err: device error word.
+int refit_bvh8(Node8* nodes, const TriSlot* tris, const BvhOutputs& levels, float4* aux, uint32_t* err,
+               cudaStream_t st);
 
 }  // namespace srt

@@ -289,7 +289,21 @@ struct srt_scene {
     DevScene dev{};
     uint64_t n_tris = 0;
     uint32_t n_lights = 0;
+    // instance updates: host copies of the instances, light instances (device),
+    // refit scratch
+    std::vector<srt_instance> h_inst;
+    std::vector<uint32_t> h_mesh_tris;
+    std::vector<InstDev> h_instdev;
+    LightInst* light_insts = nullptr;
+    uint32_t n_light_insts = 0;
+    uint8_t* moved = nullptr;
+    float4* refit_aux = nullptr;
+    uint32_t* refit_err = nullptr;
     ~srt_scene() {
+        cudaFree(light_insts);
+        cudaFree(moved);
+        cudaFree(refit_aux);
+        cudaFree(refit_err);
         cudaFree(vtx);
         cudaFree(idx);
         cudaFree(mesh_infos);
@@ -313,7 +327,42 @@ cudaError_t upload(T** dst, const void* src, size_t bytes, size_t alloc_bytes, c
 }
 }  // namespace
 
+namespace {
+// World-to-object rows (FP64 inverse of the 3x3 part) and object-to-world
+// rows of one instance; false when the transform is singular.
+bool instance_rows(const srt_instance& in, InstDev* d, InstFwd* f) {
+    const float* M = in.transform;
+    double r[9] = {M[0], M[4], M[8], M[1], M[5], M[9], M[2], M[6], M[10]};  // row-major 3x3
+    double det = r[0] * (r[4] * r[8] - r[5] * r[7]) - r[1] * (r[3] * r[8] - r[5] * r[6]) +
+                 r[2] * (r[3] * r[7] - r[4] * r[6]);
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+    for (int k = 12; k < 15; ++k)
+        if (!std::isfinite(M[k])) return false;
+    double iv[9] = {(r[4] * r[8] - r[5] * r[7]) / det, (r[2] * r[7] - r[1] * r[8]) / det,
+                    (r[1] * r[5] - r[2] * r[4]) / det, (r[5] * r[6] - r[3] * r[8]) / det,
+                    (r[0] * r[8] - r[2] * r[6]) / det, (r[2] * r[3] - r[0] * r[5]) / det,
+                    (r[3] * r[7] - r[4] * r[6]) / det, (r[1] * r[6] - r[0] * r[7]) / det,
+                    (r[0] * r[4] - r[1] * r[3]) / det};
+    d->w2o0 = make_float4((float)iv[0], (float)iv[1], (float)iv[2], 0.f);
+    d->w2o1 = make_float4((float)iv[3], (float)iv[4], (float)iv[5], 0.f);
+    d->w2o2 = make_float4((float)iv[6], (float)iv[7], (float)iv[8], 0.f);
+    f->r0 = make_float4(M[0], M[4], M[8], M[12]);
+    f->r1 = make_float4(M[1], M[5], M[9], M[13]);
+    f->r2 = make_float4(M[2], M[6], M[10], M[14]);
+    return true;
+}
+
+srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
+                            const std::vector<srt_light_instance_rec>* light_instances, srt_scene** out);
+}  // namespace
+
 extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt_scene** out) {
+    return scene_build_impl(c, a, nullptr, out);
+}
+
+namespace {
+srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
+                            const std::vector<srt_light_instance_rec>* light_instances, srt_scene** out) {
     if (!c || !a || !out) return SRT_ERR_INVALID_ARG;
     *out = nullptr;
     cudaSetDevice(c->device);
@@ -341,29 +390,13 @@ extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt
         const srt_instance& in = a->instances[i];
         if (in.mesh_id >= a->n_meshes || in.mat_id >= a->n_materials)
             return fail(c, SRT_ERR_INVALID_ARG, "instance mesh/material id out of range");
-        const float* M = in.transform;
-        double r[9] = {M[0], M[4], M[8], M[1], M[5], M[9], M[2], M[6], M[10]};  // row-major 3x3
-        double det = r[0] * (r[4] * r[8] - r[5] * r[7]) - r[1] * (r[3] * r[8] - r[5] * r[6]) +
-                     r[2] * (r[3] * r[7] - r[4] * r[6]);
-        if (!(std::fabs(det) > 0.0) || !std::isfinite(det))
-            return fail(c, SRT_ERR_INVALID_ARG, "instance transform is singular");
-        double iv[9] = {(r[4] * r[8] - r[5] * r[7]) / det, (r[2] * r[7] - r[1] * r[8]) / det,
-                        (r[1] * r[5] - r[2] * r[4]) / det, (r[5] * r[6] - r[3] * r[8]) / det,
-                        (r[0] * r[8] - r[2] * r[6]) / det, (r[2] * r[3] - r[0] * r[5]) / det,
-                        (r[3] * r[7] - r[4] * r[6]) / det, (r[1] * r[6] - r[0] * r[7]) / det,
-                        (r[0] * r[4] - r[1] * r[3]) / det};
         InstDev d{};
+        if (!instance_rows(in, &d, &fwd[i])) return fail(c, SRT_ERR_INVALID_ARG, "instance transform is singular");
         d.mesh_id = in.mesh_id;
         d.mat_id = in.mat_id;
         d.tri_offset = (uint32_t)total;
         d.tri_count = mesh_tris[in.mesh_id];
-        d.w2o0 = make_float4((float)iv[0], (float)iv[1], (float)iv[2], 0.f);
-        d.w2o1 = make_float4((float)iv[3], (float)iv[4], (float)iv[5], 0.f);
-        d.w2o2 = make_float4((float)iv[6], (float)iv[7], (float)iv[8], 0.f);
         inst[i] = d;
-        fwd[i].r0 = make_float4(M[0], M[4], M[8], M[12]);
-        fwd[i].r1 = make_float4(M[1], M[5], M[9], M[13]);
-        fwd[i].r2 = make_float4(M[2], M[6], M[10], M[14]);
         total += mesh_tris[in.mesh_id];
     }
     if (total >= 0x7FFFFFFFull) return fail(c, SRT_ERR_INVALID_ARG, "too many triangles");
@@ -432,16 +465,116 @@ extern "C" srt_status srt_scene_build(srt_ctx* c, const srt_scene_arrays* a, srt
         d.bmin = make_float4((float)lo[0], (float)lo[1], (float)lo[2], 0.f);
         d.binv = make_float4(inv[0], inv[1], inv[2], 0.f);
     }
+    s->h_inst.assign(a->instances, a->instances + a->n_instances);
+    s->h_mesh_tris = mesh_tris;
+    s->h_instdev = inst;
+    if (light_instances && !light_instances->empty()) {
+        // scene-side GPU ingestion: the light instances' triangles are
+        // expanded to world space on the device (builder.rs:101-129)
+        std::vector<LightInst> li;
+        for (const srt_light_instance_rec& r : *light_instances) {
+            if (r.instance >= a->n_instances || (uint64_t)r.first_light + r.count > a->n_lights ||
+                r.count != mesh_tris[a->instances[r.instance].mesh_id])
+                return fail(c, SRT_ERR_INVALID_ARG, "light instance record out of range");
+            LightInst L{r.instance, r.first_light, r.count, 0u,
+                        make_float4(r.params[0], r.params[1], r.params[2], r.params[3])};
+            li.push_back(L);
+        }
+        CUDA_TRY(c, upload(&s->light_insts, li.data(), sizeof(LightInst) * li.size(), sizeof(LightInst) * li.size(), st));
+        s->n_light_insts = (uint32_t)li.size();
+        launch_expand_lights(s->light_insts, s->n_light_insts, nullptr, s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd,
+                             s->lights, st);
+        CUDA_TRY(c, cudaGetLastError());
+        CUDA_TRY(c, cudaStreamSynchronize(st));
+    }
     ctx_retain(c);
     *out = s.release();
     return SRT_OK;
 }
+}  // namespace
 
 extern "C" srt_status srt_scene_builder_build(srt_ctx* c, const srt_scene_builder* b, srt_scene** out) {
     srt_scene_arrays a;
     srt_status st = srt_scene_builder_arrays(b, &a);
     if (st != SRT_OK) return st;
-    return srt_scene_build(c, &a, out);
+    return scene_build_impl(c, &a, &b->light_instances, out);
+}
+
+extern "C" srt_status srt_scene_update_instances(srt_scene* s, const uint32_t* ids, const float* transforms,
+                                                 uint32_t n) {
+    if (!s || (n && (!ids || !transforms))) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    const uint32_t ni = (uint32_t)s->h_inst.size();
+    if (n == 0 || ni == 0) return SRT_OK;
+    std::vector<InstDev> nd(n);
+    std::vector<InstFwd> nf(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        if (ids[k] >= ni) return fail(c, SRT_ERR_INVALID_ARG, "instance id out of range");
+        srt_instance in = s->h_inst[ids[k]];
+        std::memcpy(in.transform, transforms + 16ull * k, 64);
+        nd[k] = s->h_instdev[ids[k]];
+        if (!instance_rows(in, &nd[k], &nf[k])) return fail(c, SRT_ERR_INVALID_ARG, "instance transform is singular");
+    }
+    if (!s->moved) {
+        CUDA_TRY(c, dev_alloc(&s->moved, ni));
+        CUDA_TRY(c, dev_alloc(&s->refit_aux, 2ull * std::max(1u, s->bvh.n_nodes)));
+        CUDA_TRY(c, dev_alloc(&s->refit_err, 1));
+    }
+    std::vector<uint8_t> moved(ni, 0);
+    CUDA_TRY(c, cudaStreamSynchronize(st));  // frames in flight read the instances
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = ids[k];
+        moved[i] = 1;
+        std::memcpy(s->h_inst[i].transform, transforms + 16ull * k, 64);
+        s->h_instdev[i] = nd[k];
+        CUDA_TRY(c, cudaMemcpyAsync(s->inst + i, &nd[k], sizeof(InstDev), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(c, cudaMemcpyAsync(s->fwd + i, &nf[k], sizeof(InstFwd), cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(s->moved, moved.data(), ni, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaMemsetAsync(s->refit_err, 0, 4, st));
+    launch_update_slots(s->bvh.tris, (uint32_t)s->n_tris, s->bvh.tri_inst, s->moved, s->vtx, s->idx, s->mesh_infos,
+                        s->inst, s->fwd, st);
+    launch_expand_lights(s->light_insts, s->n_light_insts, s->moved, s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd,
+                         s->lights, st);
+    refit_bvh8(s->bvh.nodes, s->bvh.tris, s->bvh, s->refit_aux, s->refit_err, st);
+    CUDA_TRY(c, cudaGetLastError());
+    uint32_t herr = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&herr, s->refit_err, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+    if (herr) return fail(c, SRT_ERR_DEVICE_ASSERT, "BVH refit could not quantise a node");
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_scene_read_lights(srt_scene* s, srt_light* out, uint32_t capacity, uint32_t* count) {
+    if (!s || !count) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    *count = s->n_lights;
+    uint32_t m = std::min(capacity, s->n_lights);
+    if (out && m) {
+        CUDA_TRY(c, cudaMemcpyAsync(out, s->lights, 64ull * m, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_scene_read_bvh(srt_scene* s, void* nodes, uint64_t node_bytes, void* tris,
+                                         uint64_t tri_bytes) {
+    if (!s) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    if (nodes && node_bytes) {
+        if (node_bytes > 80ull * s->bvh.n_nodes) return SRT_ERR_INVALID_ARG;
+        CUDA_TRY(c, cudaMemcpyAsync(nodes, s->bvh.nodes, node_bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (tris && tri_bytes) {
+        if (tri_bytes > 48ull * s->n_tris) return SRT_ERR_INVALID_ARG;
+        CUDA_TRY(c, cudaMemcpyAsync(tris, s->bvh.tris, tri_bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
 }
 
 extern "C" srt_status srt_scene_destroy(srt_scene* s) {

@@ -96,6 +96,9 @@ void srt_scene_builder::add_instance(uint32_t mesh, uint32_t mat, const Mat4& t)
 void srt_scene_builder::add_light_instance(uint32_t mesh, uint32_t mat, const Mat4& t, const float params[4]) {
     // builder.rs:101-129: one world-space LightInfo per triangle
     add_instance(mesh, mat, t);
+    srt_light_instance_rec rec{(uint32_t)instances.size() - 1u, (uint32_t)lights.size(), mesh_tris[mesh], {}};
+    std::memcpy(rec.params, params, 16);
+    light_instances.push_back(rec);
     const srt_mesh_info& mi = mesh_infos[mesh];
     for (uint32_t k = 0; k < mesh_tris[mesh]; ++k) {
         srt_light L{};

@@ -20,7 +20,15 @@ Mat4 mat4_rotation_x(float a);
 Mat4 mat4_rotation_y(float a);
 Mat4 mat4_rotation_z(float a);
 
+// A light instance recorded by the builder: its triangles became
+// lights[first_light .. first_light + count).
+struct srt_light_instance_rec {
+    uint32_t instance, first_light, count;
+    float params[4];
+};
+
 struct srt_scene_builder {
+    std::vector<srt_light_instance_rec> light_instances;
     std::vector<srt_vertex> vertices;
     std::vector<uint32_t> indices;
     std::vector<srt_mesh_info> mesh_infos;
