@@ -205,6 +205,12 @@ srt_status srt_ctx_synchronize(srt_ctx* ctx);
 uint32_t srt_abi_version(void);
 /* Number of SMs of the context's device. */
 int srt_ctx_sm_count(const srt_ctx* ctx);
+/* BVH builder for the scenes built next on this context: binned SAH
+ * (default) or the Morton-ordered LBVH.  Both are collapsed into the same
+ * 8-wide compressed nodes; the choice changes speed, never results. */
+#define SRT_BVH_SAH  0
+#define SRT_BVH_LBVH 1
+srt_status srt_ctx_set_bvh_builder(srt_ctx* ctx, int builder);
 
 /* ------------------------------------------------------------------------ */
 /* Scene API: SceneBuilder (src/scene/builder.rs:47-267).                     */

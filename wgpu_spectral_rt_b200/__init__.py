@@ -120,6 +120,9 @@ PRESET_CAUSTIC_SLAB = 4
 PRESET_INDIRECT_ROOM = 5
 PRESET_BATCH_RANDOM = 6
 
+BVH_SAH = 0
+BVH_LBVH = 1
+
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
 
@@ -189,6 +192,7 @@ SIGNATURES = {
     "srt_scene_update_instances": (_I, [_P, _P, _P, _U32]),
     "srt_scene_read_lights": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
     "srt_scene_read_bvh": (_I, [_P, _P, C.c_uint64, _P, C.c_uint64]),
+    "srt_ctx_set_bvh_builder": (_I, [_P, _I]),
     "srt_guide_param_count": (_U32, []),
     "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
@@ -263,6 +267,10 @@ class Context:
     @property
     def sm_count(self) -> int:
         return lib().srt_ctx_sm_count(self.h)
+
+    def set_bvh_builder(self, builder: int) -> None:
+        """BVH_SAH (default) or BVH_LBVH for the scenes built next."""
+        _check(lib().srt_ctx_set_bvh_builder(self.h, builder), self.h)
 
     def synchronize(self):
         _check(lib().srt_ctx_synchronize(self.h), self.h)

@@ -14,6 +14,7 @@
 //      largest surface area until 8 children; subtrees of <= 3 triangles
 //      become leaves; children are placed in slots by ray octant; child
 //      boxes are quantised to 8 bits against the node's box.
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -191,6 +192,272 @@ __global__ void k_refit(const TriSlot* __restrict__ flat, const uint32_t* __rest
     }
 }
 
+// ---------------------------------------------------------------- binned SAH
+// Top-down, one level of the binary tree per round: every node still to be
+// split (a task: a contiguous range of the primitive permutation) bins its
+// primitives' centroids into SAH_BINS bins along its widest centroid axis,
+// picks the bin boundary of least surface-area cost N_L A_L + N_R A_R (a
+// median split by position when all centroids share one bin, and for every
+// node below SAH_MEDIAN_LEVEL levels, which bounds the depth), and
+// partitions its range.  The result is the same binary tree format as the
+// LBVH (internal nodes over contiguous ranges, single-primitive leaves), so
+// the bottom-up box pass and the 8-wide collapse are shared.
+constexpr int SAH_BINS = 16;
+constexpr int SAH_REC = 13;  // count, box lo/hi, centroid lo/hi (flipped floats)
+constexpr uint32_t SAH_MEDIAN = 0xFFFFFFFFu;
+constexpr uint32_t SAH_MEDIAN_LEVEL = 48;
+
+struct SahTask {
+    uint32_t node, first, count, axis;
+    float cmin, cscale;  // bin = (c - cmin) * cscale
+    uint32_t split, left_count;
+    uint32_t lcur, rcur;
+    uint32_t child_task[2];  // next-level task of each child, 0xFFFFFFFF for a leaf
+};
+
+__device__ __forceinline__ uint32_t sah_bin(const SahTask& t, float4 c) {
+    float v = t.axis == 0 ? c.x : (t.axis == 1 ? c.y : c.z);
+    float f = (v - t.cmin) * t.cscale;
+    int b = (int)f;
+    return (uint32_t)min(max(b, 0), SAH_BINS - 1);
+}
+
+__global__ void k_sah_init_bins(uint32_t* __restrict__ bins, uint32_t n_words) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_words) return;
+    uint32_t k = i % SAH_REC;
+    // lo fields start at +inf (min of flipped), hi fields at 0
+    bins[i] = (k == 0u) ? 0u : ((k >= 1 && k <= 3) || (k >= 7 && k <= 9)) ? 0xFFFFFFFFu : 0u;
+}
+
+__device__ __forceinline__ void sah_accum(uint32_t* rec, float3 lo, float3 hi, float4 c, bool shared_mem) {
+    (void)shared_mem;
+    atomicAdd(&rec[0], 1u);
+    atomicMin(&rec[1], float_flip(lo.x));
+    atomicMin(&rec[2], float_flip(lo.y));
+    atomicMin(&rec[3], float_flip(lo.z));
+    atomicMax(&rec[4], float_flip(hi.x));
+    atomicMax(&rec[5], float_flip(hi.y));
+    atomicMax(&rec[6], float_flip(hi.z));
+    atomicMin(&rec[7], float_flip(c.x));
+    atomicMin(&rec[8], float_flip(c.y));
+    atomicMin(&rec[9], float_flip(c.z));
+    atomicMax(&rec[10], float_flip(c.x));
+    atomicMax(&rec[11], float_flip(c.y));
+    atomicMax(&rec[12], float_flip(c.z));
+}
+
+// Bins of every active position; the task of the block's first position
+// (most of the block at the top levels) aggregates in shared memory.
+__global__ void k_sah_bin(const uint32_t* __restrict__ perm, const int* __restrict__ pos_task, uint32_t n,
+                          const SahTask* __restrict__ tasks, const float4* __restrict__ cen,
+                          const TriSlot* __restrict__ flat, uint32_t* __restrict__ bins) {
+    __shared__ uint32_t sb[SAH_BINS * SAH_REC];
+    __shared__ int t0s;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (threadIdx.x == 0) t0s = pos_task[min(blockIdx.x * blockDim.x, n - 1)];
+    for (int i = threadIdx.x; i < SAH_BINS * SAH_REC; i += blockDim.x) {
+        int k = i % SAH_REC;
+        sb[i] = (k == 0) ? 0u : ((k >= 1 && k <= 3) || (k >= 7 && k <= 9)) ? 0xFFFFFFFFu : 0u;
+    }
+    __syncthreads();
+    const int t0 = t0s;
+    if (p < n) {
+        const int t = pos_task[p];
+        if (t >= 0 && tasks[t].split != SAH_MEDIAN) {
+            const uint32_t prim = perm[p];
+            const TriSlot s = flat[prim];
+            const float3 lo = f3(fminf(fminf(s.v0.x, s.v1.x), s.v2.x), fminf(fminf(s.v0.y, s.v1.y), s.v2.y),
+                                 fminf(fminf(s.v0.z, s.v1.z), s.v2.z));
+            const float3 hi = f3(fmaxf(fmaxf(s.v0.x, s.v1.x), s.v2.x), fmaxf(fmaxf(s.v0.y, s.v1.y), s.v2.y),
+                                 fmaxf(fmaxf(s.v0.z, s.v1.z), s.v2.z));
+            const float4 c = cen[prim];
+            const uint32_t b = sah_bin(tasks[t], c);
+            if (t == t0) sah_accum(sb + b * SAH_REC, lo, hi, c, true);
+            else sah_accum(bins + ((size_t)t * SAH_BINS + b) * SAH_REC, lo, hi, c, false);
+        }
+    }
+    __syncthreads();
+    if (t0 >= 0 && tasks[t0].split != SAH_MEDIAN) {
+        for (int i = threadIdx.x; i < SAH_BINS; i += blockDim.x) {
+            const uint32_t* r = sb + i * SAH_REC;
+            if (r[0] == 0u) continue;
+            uint32_t* g = bins + ((size_t)t0 * SAH_BINS + i) * SAH_REC;
+            atomicAdd(&g[0], r[0]);
+            for (int k = 1; k <= 3; ++k) atomicMin(&g[k], r[k]);
+            for (int k = 4; k <= 6; ++k) atomicMax(&g[k], r[k]);
+            for (int k = 7; k <= 9; ++k) atomicMin(&g[k], r[k]);
+            for (int k = 10; k <= 12; ++k) atomicMax(&g[k], r[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ float half_area(float3 lo, float3 hi) {
+    float3 e = f3(fmaxf(hi.x - lo.x, 0.f), fmaxf(hi.y - lo.y, 0.f), fmaxf(hi.z - lo.z, 0.f));
+    return e.x * e.y + e.y * e.z + e.z * e.x;
+}
+
+// Sets the next-level task of one child: binning axis and mapping from its
+// centroid bounds.
+__device__ void sah_child_task(SahTask& c, uint32_t node, uint32_t first, uint32_t count, float3 clo, float3 chi,
+                               bool median) {
+    c.node = node;
+    c.first = first;
+    c.count = count;
+    float3 e = f3(chi.x - clo.x, chi.y - clo.y, chi.z - clo.z);
+    uint32_t ax = (e.x >= e.y && e.x >= e.z) ? 0u : (e.y >= e.z ? 1u : 2u);
+    float ext = ax == 0 ? e.x : (ax == 1 ? e.y : e.z);
+    c.axis = ax;
+    c.cmin = ax == 0 ? clo.x : (ax == 1 ? clo.y : clo.z);
+    c.cscale = ext > 0.f ? (float)SAH_BINS / ext : 0.f;
+    // all centroids on one point, below the SAH levels, or a range that the
+    // collapse turns into one leaf anyway (<= 3): split by position
+    c.split = (median || !(ext > 0.f) || count <= 3u) ? SAH_MEDIAN : 0u;
+    c.left_count = 0;
+    c.lcur = c.rcur = 0;
+    c.child_task[0] = c.child_task[1] = 0xFFFFFFFFu;
+}
+
+// One thread per task: choose the split, create the children.
+__global__ void k_sah_split(SahTask* __restrict__ tasks, uint32_t n_tasks, const uint32_t* __restrict__ bins,
+                            SahTask* __restrict__ next, uint32_t* __restrict__ n_next, uint32_t next_cap,
+                            uint32_t* __restrict__ node_alloc, uint32_t node_cap, Bvh2 b, uint32_t level,
+                            uint32_t* __restrict__ err) {
+    const uint32_t ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= n_tasks) return;
+    SahTask& T = tasks[ti];
+    uint32_t left = T.count / 2;  // median by position
+    float3 clo[2] = {f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)}, chi[2] = {f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)};
+    bool median = T.split == SAH_MEDIAN;
+    if (!median) {
+        const uint32_t* B = bins + (size_t)ti * SAH_BINS * SAH_REC;
+        float ra[SAH_BINS];  // area of bins [k, K)
+        uint32_t rc[SAH_BINS];
+        float3 lo = f3(3.4e38f, 3.4e38f, 3.4e38f), hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+        uint32_t cnt = 0;
+        for (int k = SAH_BINS - 1; k >= 0; --k) {
+            const uint32_t* r = B + k * SAH_REC;
+            if (r[0]) {
+                lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])), fminf(lo.z, float_unflip(r[3])));
+                hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])), fmaxf(hi.z, float_unflip(r[6])));
+                cnt += r[0];
+            }
+            ra[k] = cnt ? half_area(lo, hi) : 0.f;
+            rc[k] = cnt;
+        }
+        lo = f3(3.4e38f, 3.4e38f, 3.4e38f);
+        hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+        cnt = 0;
+        float best = 3.4e38f;
+        int bk = -1;
+        for (int k = 1; k < SAH_BINS; ++k) {
+            const uint32_t* r = B + (k - 1) * SAH_REC;
+            if (r[0]) {
+                lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])), fminf(lo.z, float_unflip(r[3])));
+                hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])), fmaxf(hi.z, float_unflip(r[6])));
+                cnt += r[0];
+            }
+            if (cnt == 0 || rc[k] == 0) continue;
+            float cost = (float)cnt * half_area(lo, hi) + (float)rc[k] * ra[k];
+            if (cost < best) {
+                best = cost;
+                bk = k;
+            }
+        }
+        if (bk < 0) {
+            median = true;
+        } else {
+            T.split = (uint32_t)bk;
+            left = 0;
+            float3 l0 = f3(3.4e38f, 3.4e38f, 3.4e38f), h0 = f3(-3.4e38f, -3.4e38f, -3.4e38f), l1 = l0, h1 = h0;
+            for (int k = 0; k < SAH_BINS; ++k) {
+                const uint32_t* r = B + k * SAH_REC;
+                if (!r[0]) continue;
+                float3 a = f3(float_unflip(r[7]), float_unflip(r[8]), float_unflip(r[9]));
+                float3 z = f3(float_unflip(r[10]), float_unflip(r[11]), float_unflip(r[12]));
+                if (k < bk) {
+                    left += r[0];
+                    l0 = f3(fminf(l0.x, a.x), fminf(l0.y, a.y), fminf(l0.z, a.z));
+                    h0 = f3(fmaxf(h0.x, z.x), fmaxf(h0.y, z.y), fmaxf(h0.z, z.z));
+                } else {
+                    l1 = f3(fminf(l1.x, a.x), fminf(l1.y, a.y), fminf(l1.z, a.z));
+                    h1 = f3(fmaxf(h1.x, z.x), fmaxf(h1.y, z.y), fmaxf(h1.z, z.z));
+                }
+            }
+            clo[0] = l0;
+            chi[0] = h0;
+            clo[1] = l1;
+            chi[1] = h1;
+        }
+    }
+    if (median) {
+        T.split = SAH_MEDIAN;
+        left = T.count / 2;
+        // centroid bounds are not tracked for position splits: the children
+        // keep splitting by position
+    }
+    T.left_count = left;
+    const uint32_t firsts[2] = {T.first, T.first + left}, counts[2] = {left, T.count - left};
+    uint32_t refs[2];
+    for (int c = 0; c < 2; ++c) {
+        if (counts[c] == 1u) {
+            refs[c] = LEAF | firsts[c];
+            b.lparent[firsts[c]] = T.node;
+            T.child_task[c] = 0xFFFFFFFFu;
+        } else {
+            uint32_t nd = atomicAdd(node_alloc, 1u);
+            uint32_t tn = atomicAdd(n_next, 1u);
+            if (nd >= node_cap || tn >= next_cap || counts[c] == 0u) {
+                atomicOr(err, ERR_QUEUE_OVERFLOW);
+                refs[c] = 0u;
+                T.child_task[c] = 0xFFFFFFFFu;
+                continue;
+            }
+            refs[c] = nd;
+            b.iparent[nd] = T.node;
+            T.child_task[c] = tn;
+            sah_child_task(next[tn], nd, firsts[c], counts[c], clo[c], chi[c], median || level + 1 >= SAH_MEDIAN_LEVEL);
+        }
+    }
+    b.inode[T.node] = make_uint4(refs[0], refs[1], T.first, T.first + T.count - 1u);
+}
+
+__global__ void k_sah_root(const uint32_t* __restrict__ bounds, uint32_t n, SahTask* __restrict__ t,
+                           int* __restrict__ pos_task, uint32_t* __restrict__ perm) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) {
+        float3 lo = f3(float_unflip(bounds[0]), float_unflip(bounds[1]), float_unflip(bounds[2]));
+        float3 hi = f3(float_unflip(bounds[3]), float_unflip(bounds[4]), float_unflip(bounds[5]));
+        sah_child_task(t[0], 0u, 0u, n, lo, hi, false);
+    }
+    if (p < n) {
+        pos_task[p] = 0;
+        perm[p] = p;
+    }
+}
+
+// Moves every active primitive into its child's range.
+__global__ void k_sah_partition(const uint32_t* __restrict__ perm, const int* __restrict__ pos_task, uint32_t n,
+                                SahTask* __restrict__ tasks, const float4* __restrict__ cen,
+                                uint32_t* __restrict__ perm2, int* __restrict__ pos_task2) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int t = pos_task[p];
+    const uint32_t prim = perm[p];
+    if (t < 0) {
+        perm2[p] = prim;
+        pos_task2[p] = -1;
+        return;
+    }
+    SahTask& T = tasks[t];
+    uint32_t side;
+    if (T.split == SAH_MEDIAN) side = (p - T.first) >= T.left_count ? 1u : 0u;
+    else side = sah_bin(T, cen[prim]) >= T.split ? 1u : 0u;
+    uint32_t np = side ? T.first + T.left_count + atomicAdd(&T.rcur, 1u) : T.first + atomicAdd(&T.lcur, 1u);
+    perm2[np] = prim;
+    pos_task2[np] = T.child_task[side] == 0xFFFFFFFFu ? -1 : (int)T.child_task[side];
+}
+
 __device__ __forceinline__ void ref_box(const Bvh2& b, uint32_t r, float3& lo, float3& hi) {
     float4 a, c;
     if (r & LEAF) {
@@ -315,8 +582,6 @@ __global__ void k_refit8(Node8* __restrict__ nodes, const TriSlot* __restrict__ 
     quantize_node(nlo, nhi, slo, shi, used, imask, nd, err);
     nodes[i] = nd;
 }
-
-__device__ __forceinline__ const InstFwd& fwd_of(const InstFwd* fwd, uint32_t i) { return fwd[i]; }
 
 // Leaf slots of moved instances, re-transformed from object space.
 __global__ void k_update_slots(TriSlot* __restrict__ tris, uint32_t n_tris, const uint32_t* __restrict__ tri_inst,
@@ -509,6 +774,8 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
     uint32_t *bounds = nullptr, *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr,
              *scratch = nullptr, *counters = nullptr, *err = nullptr;
     uint2 *qa = nullptr, *qb = nullptr;
+    SahTask* sah_tasks[2] = {nullptr, nullptr};
+    uint32_t* sah_bins = nullptr;
     Bvh2 b{};
     if (n == 0) return cudaSuccess;
     {
@@ -542,13 +809,53 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
         uint32_t grid = (n + B - 1) / B;
         k_flatten<<<grid, B, 0, st>>>(in.vtx, in.indices, in.mesh_infos, in.inst, in.fwd, in.n_inst, n, flat,
                                       out->tri_inst, cen, bounds);
-        k_morton<<<grid, B, 0, st>>>(cen, bounds, n, keys, vals);
-        out->kernel_launches += 2;
-        uint32_t *sk, *sv;
-        out->kernel_launches += sort_pairs(keys, vals, keys2, vals2, n, nullptr, 0, 30, scratch, st, &sk, &sv);
-        if (n > 1) {
-            k_karras<<<(n - 1 + B - 1) / B, B, 0, st>>>(sk, (int)n, b);
+        ++out->kernel_launches;
+        uint32_t* sv = nullptr;
+        if (in.builder == BVH_BUILDER_LBVH || n < 2) {
+            k_morton<<<grid, B, 0, st>>>(cen, bounds, n, keys, vals);
             ++out->kernel_launches;
+            uint32_t* sk;
+            out->kernel_launches += sort_pairs(keys, vals, keys2, vals2, n, nullptr, 0, 30, scratch, st, &sk, &sv);
+            if (n > 1) {
+                k_karras<<<(n - 1 + B - 1) / B, B, 0, st>>>(sk, (int)n, b);
+                ++out->kernel_launches;
+            }
+        } else {
+            // binned SAH, level by level (keys/vals/keys2/vals2 serve as the
+            // permutation and position -> task ping-pong buffers)
+            uint32_t *perm = keys, *perm2 = keys2;
+            int *pt = (int*)vals, *pt2 = (int*)vals2;
+            const uint32_t task_cap = n / 2 + 1;
+            CK(dalloc(&sah_tasks[0], task_cap));
+            CK(dalloc(&sah_tasks[1], task_cap));
+            CK(dalloc(&sah_bins, (size_t)task_cap * SAH_BINS * SAH_REC));
+            CK(cudaMemcpyAsync(counters, std::array<uint32_t, 4>{1u, 0u, 0u, 0u}.data(), 16, cudaMemcpyHostToDevice, st));
+            k_sah_root<<<grid, B, 0, st>>>(bounds, n, sah_tasks[0], pt, perm);
+            ++out->kernel_launches;
+            uint32_t n_tasks = 1, level = 0;
+            while (n_tasks > 0) {
+                uint32_t words = n_tasks * SAH_BINS * SAH_REC;
+                k_sah_init_bins<<<(words + 255) / 256, 256, 0, st>>>(sah_bins, words);
+                k_sah_bin<<<grid, B, 0, st>>>(perm, pt, n, sah_tasks[0], cen, flat, sah_bins);
+                CK(cudaMemsetAsync(counters + 2, 0, 4, st));
+                k_sah_split<<<(n_tasks + 127) / 128, 128, 0, st>>>(sah_tasks[0], n_tasks, sah_bins, sah_tasks[1],
+                                                                   counters + 2, task_cap, counters, n - 1, b, level,
+                                                                   err);
+                k_sah_partition<<<grid, B, 0, st>>>(perm, pt, n, sah_tasks[0], cen, perm2, pt2);
+                out->kernel_launches += 4;
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(&n_tasks, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                std::swap(perm, perm2);
+                std::swap(pt, pt2);
+                std::swap(sah_tasks[0], sah_tasks[1]);
+                if (n_tasks > task_cap || ++level > 4096) {
+                    if (msg) *msg = "binned SAH build did not converge";
+                    e = cudaErrorUnknown;
+                    goto done;
+                }
+            }
+            sv = perm;
         }
         k_refit<<<grid, B, 0, st>>>(flat, sv, (int)n, b);
         ++out->kernel_launches;
@@ -596,6 +903,9 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
         out->depth = depth;
     }
 done:
+    cudaFree(sah_tasks[0]);
+    cudaFree(sah_tasks[1]);
+    cudaFree(sah_bins);
     cudaFree(flat);
     cudaFree(cen);
     cudaFree(bounds);

@@ -29,6 +29,9 @@ struct LightInst {
     float4 params;
 };
 
+constexpr int BVH_BUILDER_SAH = 0;   // binned SAH, top-down (default)
+constexpr int BVH_BUILDER_LBVH = 1;  // Morton-ordered LBVH (Karras 2012)
+
 struct BvhInputs {
     const float4* vtx;        // device srt_vertex array (pos, normal)
     const uint32_t* indices;  // device global index buffer
@@ -37,6 +40,7 @@ struct BvhInputs {
     const InstFwd* fwd;       // device, one per instance
     uint32_t n_inst;
     uint32_t n_tris;          // flattened triangle count
+    int builder;              // BVH_BUILDER_*
 };
 
 struct BvhOutputs {

@@ -42,6 +42,7 @@ struct srt_ctx {
     // so handles may be destroyed in any order (e.g. by a garbage collector).
     int children = 0;
     bool closing = false;
+    int bvh_builder = 0;  // SRT_BVH_* for the scenes built next
 };
 
 namespace {
@@ -150,6 +151,12 @@ srt_status srt_ctx_destroy(srt_ctx* c) {
         return SRT_OK;
     }
     ctx_free(c);
+    return SRT_OK;
+}
+
+srt_status srt_ctx_set_bvh_builder(srt_ctx* c, int builder) {
+    if (!c || (builder != SRT_BVH_SAH && builder != SRT_BVH_LBVH)) return SRT_ERR_INVALID_ARG;
+    c->bvh_builder = builder;
     return SRT_OK;
 }
 
@@ -411,7 +418,8 @@ srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
     CUDA_TRY(c, upload(&s->lights, a->lights, 64ull * a->n_lights, 64ull * a->n_lights, st));
     CUDA_TRY(c, upload(&s->inst, inst.data(), sizeof(InstDev) * inst.size(), sizeof(InstDev) * inst.size(), st));
     CUDA_TRY(c, upload(&s->fwd, fwd.data(), sizeof(InstFwd) * fwd.size(), sizeof(InstFwd) * fwd.size(), st));
-    BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total};
+    BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total,
+                 c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH};
     std::string msg;
     cudaError_t e = build_bvh8(bi, st, &s->bvh, &msg);
     if (e != cudaSuccess) return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, "BVH build: " + msg);
