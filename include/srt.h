@@ -430,6 +430,13 @@ srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batc
  * (weights as given) and, when params_out/m_out/v_out are non-NULL, one Adam
  * step (gradients divided by n; step adam_step + 1). */
 srt_status srt_guide_test_forward(srt_ctx* ctx, const float* params, const float* x, uint32_t n, float* out);
+/* The same forward pass on the tcgen05 / tensor-memory kernel. */
+srt_status srt_guide_test_forward_tc(srt_ctx* ctx, const float* params, const float* x, uint32_t n, float* out);
+/* Inference kernel of a guiding renderer: mma.sync fragments or tcgen05 MMAs
+ * into tensor memory (same network, same results up to FP32 summation order). */
+#define SRT_GUIDE_INFER_MMA_SYNC 0
+#define SRT_GUIDE_INFER_TCGEN05  1
+srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind);
 srt_status srt_guide_test_mixture(srt_ctx* ctx, const float* raw, const float* omega, const float* u, uint32_t n,
                                   float* out);
 srt_status srt_guide_test_train(srt_ctx* ctx, const float* params, const float* adam_m, const float* adam_v,

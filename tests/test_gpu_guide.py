@@ -38,12 +38,13 @@ def _batch(rng, n):
     return x, om.astype(np.float32), pb, w
 
 
+@pytest.mark.parametrize("tcgen05", [False, True], ids=["mma_sync", "tcgen05"])
 @pytest.mark.parametrize("n,out_scale", [(1, 1.0), (37, 1.0), (4096, 10.0), (100_003, 1.0)])
-def test_forward_matches_oracle(srt, ctx, n, out_scale):
+def test_forward_matches_oracle(srt, ctx, n, out_scale, tcgen05):
     rng = np.random.default_rng(n)
     w = _weights(srt, 7 + n, out_scale)
     x, _, _, _ = _batch(rng, n)
-    y = srt.guide_forward(ctx, w, x)
+    y = srt.guide_forward(ctx, w, x, tcgen05=tcgen05)
     params = go.unpack(w)
     emu, _ = go.forward_bf16(params, x.astype(np.float64))
     ref, _ = go.forward(params, x.astype(np.float64))
@@ -235,3 +236,33 @@ def test_trained_guide_reduces_error(srt, ctx):
     e_plain = float(np.mean((plain - ref) ** 2 / (ref ** 2 + 0.01)))
     e_guided = float(np.mean((guided - ref) ** 2 / (ref ** 2 + 0.01)))
     assert e_guided * 1.15 < e_plain, (e_plain, e_guided)
+
+
+def test_tcgen05_and_mma_sync_inference_agree(srt, ctx):
+    """The two inference kernels (tcgen05 MMAs into tensor memory, and
+    mma.sync fragments) run the same frozen network: their raw outputs agree
+    to FP32 summation order, so the guided images agree up to the rare
+    sampling decision that flips."""
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b.build(ctx)
+    trained = _render(srt, ctx, scene, cam, 48, 32, srt.FLAG_GUIDING, 64)
+    ckpt = trained.guide_weights()
+    flags = srt.FLAG_GUIDING | srt.FLAG_GUIDE_FROZEN | srt.FLAG_FP64_ACCUM
+    out = []
+    for kind in (srt.GUIDE_INFER_TCGEN05, srt.GUIDE_INFER_MMA_SYNC):
+        p = srt.default_params(photons_per_frame=0, flags=flags)
+        r = srt.Renderer(ctx, scene, 48, 32, p)
+        r.set_guide_weights(ckpt)
+        r.set_guide_inference(kind)
+        ctl = srt.CameraController(*cam)
+        for f in range(64):
+            r.render(ctl.build_uniform(48 / 32, f))
+        a = r.read_accum64()
+        out.append(a[..., :3] / a[..., 3:4])
+        r.close()
+    tc, mma = out
+    close = np.all(np.abs(tc - mma) <= 1e-4 * np.maximum(np.abs(mma), 1e-3), axis=-1)
+    assert np.mean(close) > 0.9
+    assert tc.mean() == pytest.approx(mma.mean(), rel=5e-3)
+    trained.close()

@@ -123,6 +123,9 @@ PRESET_BATCH_RANDOM = 6
 BVH_SAH = 0
 BVH_LBVH = 1
 
+GUIDE_INFER_MMA_SYNC = 0
+GUIDE_INFER_TCGEN05 = 1
+
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
 
@@ -200,6 +203,8 @@ SIGNATURES = {
     "srt_renderer_guide_info": (_I, [_P, C.POINTER(_U32), C.POINTER(_U32)]),
     "srt_renderer_guide_configure": (_I, [_P, _F, _U32]),
     "srt_guide_test_forward": (_I, [_P, _P, _P, _U32, _P]),
+    "srt_guide_test_forward_tc": (_I, [_P, _P, _P, _U32, _P]),
+    "srt_renderer_guide_set_inference": (_I, [_P, _I]),
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
@@ -526,6 +531,10 @@ class Renderer:
         _check(lib().srt_renderer_guide_get_weights(self.h, ptr(out), len(out)), self.ctx.h)
         return out
 
+    def set_guide_inference(self, kind: int) -> None:
+        """GUIDE_INFER_MMA_SYNC or GUIDE_INFER_TCGEN05."""
+        _check(lib().srt_renderer_guide_set_inference(self.h, kind), self.ctx.h)
+
     def set_guide_weights(self, w: np.ndarray) -> None:
         a = np.ascontiguousarray(w, np.float32)
         _check(lib().srt_renderer_guide_set_weights(self.h, ptr(a), len(a)), self.ctx.h)
@@ -605,12 +614,13 @@ def guide_default_weights(seed: int = 1) -> np.ndarray:
     return out
 
 
-def guide_forward(ctx: Context, params: np.ndarray, x: np.ndarray) -> np.ndarray:
-    """Raw network outputs [n, 48] for inputs x [n, 10] (srt_guide_test_forward)."""
+def guide_forward(ctx: Context, params: np.ndarray, x: np.ndarray, tcgen05: bool = False) -> np.ndarray:
+    """Raw network outputs [n, 48] for inputs x [n, 10] (srt_guide_test_forward[_tc])."""
     w = np.ascontiguousarray(params, np.float32)
     a = np.ascontiguousarray(x, np.float32).reshape(-1, 10)
     out = np.zeros((len(a), 48), np.float32)
-    _check(lib().srt_guide_test_forward(ctx.h, ptr(w), ptr(a), len(a), ptr(out)), ctx.h)
+    fn = lib().srt_guide_test_forward_tc if tcgen05 else lib().srt_guide_test_forward
+    _check(fn(ctx.h, ptr(w), ptr(a), len(a), ptr(out)), ctx.h)
     return out
 
 

@@ -1261,7 +1261,8 @@ struct GuideScratch {
 };
 }  // namespace
 
-extern "C" srt_status srt_guide_test_forward(srt_ctx* c, const float* params, const float* x, uint32_t n, float* out) {
+namespace {
+srt_status guide_test_forward(srt_ctx* c, const float* params, const float* x, uint32_t n, float* out, int tc) {
     if (!c || !params || (n && (!x || !out))) return SRT_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (n == 0) return SRT_OK;
@@ -1272,10 +1273,35 @@ extern "C" srt_status srt_guide_test_forward(srt_ctx* c, const float* params, co
     CUDA_TRY(c, dev_alloc(&s.x, (size_t)n * G_IN));
     CUDA_TRY(c, dev_alloc(&s.y, (size_t)n * G_OUT));
     CUDA_TRY(c, cudaMemcpyAsync(s.x, x, (size_t)n * G_IN * 4, cudaMemcpyHostToDevice, c->stream));
-    launch_guide_test_forward(s.g.net, s.x, n, s.y, c->stream);
+    launch_guide_test_forward(s.g.net, s.x, n, s.y, tc, c->d_err, c->stream);
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaMemcpyAsync(out, s.y, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c, c->d_err);
+}
+}  // namespace
+
+extern "C" srt_status srt_guide_test_forward(srt_ctx* c, const float* params, const float* x, uint32_t n, float* out) {
+    return guide_test_forward(c, params, x, n, out, 0);
+}
+
+extern "C" srt_status srt_guide_test_forward_tc(srt_ctx* c, const float* params, const float* x, uint32_t n,
+                                                float* out) {
+    return guide_test_forward(c, params, x, n, out, 1);
+}
+
+extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind) {
+    if (!r || (kind != SRT_GUIDE_INFER_MMA_SYNC && kind != SRT_GUIDE_INFER_TCGEN05)) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->guide.tc = kind == SRT_GUIDE_INFER_TCGEN05 ? 1 : 0;
+    r->args.guide = r->guide;
+    if (r->graph) {  // the choice is baked into the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
     return SRT_OK;
 }
 

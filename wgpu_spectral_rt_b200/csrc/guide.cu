@@ -20,6 +20,7 @@
 
 #include "guide.cuh"
 #include "render_kernels.h"
+#include "umma.cuh"
 
 namespace srt {
 
@@ -143,6 +144,8 @@ struct Mix {
     float sel, sel_sig;
     float norm[G_LOBES];
     float lk[G_LOBES];
+    float c[G_LOBES];   // vMF normalisation kappa / (2 pi (1 - e^-2kappa))
+    float e2[G_LOBES];  // e^-2kappa
 };
 SRT_DEV void mixture(const float* r, Mix& m) {
     float mx = -3.4e38f;
@@ -157,6 +160,8 @@ SRT_DEV void mixture(const float* r, Mix& m) {
         m.mu[j] = v / n;
         m.lk[j] = r[5 * j + 3];
         m.kappa[j] = expf(clampf(r[5 * j + 3], G_KAPPA_LO, G_KAPPA_HI));
+        m.c[j] = m.kappa[j] / (2.0f * PI * (-expm1f(-2.0f * m.kappa[j])));
+        m.e2[j] = expf(-2.0f * m.kappa[j]);
         m.pi[j] = expf(r[5 * j + 4] - mx);
         sum += m.pi[j];
     }
@@ -168,9 +173,9 @@ SRT_DEV void mixture(const float* r, Mix& m) {
 SRT_DEV float vmf(float3 mu, float k, float3 w) {
     return k / (2.0f * PI * (-expm1f(-2.0f * k))) * expf(k * (dot(mu, w) - 1.0f));
 }
-// Sample a vMF lobe (Wenzel Jakob's stable form of Wood's method).
-SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
-    float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * k)) / k;
+// Sample a vMF lobe (Wenzel Jakob's stable form of Wood's method); e2 = e^-2k.
+SRT_DEV float3 vmf_sample_e2(float3 mu, float k, float e2, float u1, float u2) {
+    float w = 1.0f + logf(u1 + (1.0f - u1) * e2) / k;
     w = clampf(w, -1.0f, 1.0f);
     float r = sqrtf(fmaxf(0.0f, 1.0f - w * w));
     float sp, cp;
@@ -179,6 +184,9 @@ SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
     float3 b1 = normalize(cross(mu, t));
     float3 b2 = cross(mu, b1);
     return normalize(mu * w + b1 * (r * cp) + b2 * (r * sp));
+}
+SRT_DEV float3 vmf_sample(float3 mu, float k, float u1, float u2) {
+    return vmf_sample_e2(mu, k, expf(-2.0f * k), u1, u2);
 }
 
 // Copies a rows x cols bf16 matrix (rows contiguous in global memory) into
@@ -360,6 +368,63 @@ SRT_DEV void vertex_inputs(float3 p, float3 n, float3 wo, float lambda, float4 b
     x[9] = (lambda - LAMBDA_MIN) / LAMBDA_RANGE;
 }
 
+// Throughput, training record, Russian roulette and the next ray of guided
+// vertex v (path id) once its direction is drawn; the direction's sampling
+// pdf is sel q + (1 - sel) cos / pi.  Returns whether the path continues.
+SRT_DEV bool finish_vertex(const FrameArgs& a, uint32_t bounce, uint32_t frame, uint32_t v, uint32_t id, float4 p,
+                           float3 ffn, uint4 misc, uint32_t s, float3 dir, float sel, float q) {
+    const GuideArgs& G = a.guide;
+    const DevScene& S = a.scene;
+    const float4 wo4 = G.gv.wo[v], spec = G.gv.spec[v];
+    float4 thr = a.pb.thr[id];
+    const float3 hp = xyz(p);
+    float cosv = dot(ffn, dir);
+    uint32_t rec = 0u;  // record index + 1 (0: none)
+    bool alive = false;
+    if (cosv > 0.0f) {
+        float pb = cosv / PI;
+        float pdf = sel * q + (1.0f - sel) * pb;
+        float4 att = spec * (pb / pdf);  // (spec / pi) cos / pdf
+        thr = thr * att;
+        // training sample (a hashed subset of the vertices)
+        if (G.train) {
+            atomicAdd(&G.gc->candidates, 1u);
+            uint32_t h = pcg_hash(id ^ (bounce << 24) ^ (frame * 0x9E3779B9u)) & 0xFFFFu;
+            if (h < G.gc->threshold) {
+                uint32_t r = atomicAdd(&G.gc->records, 1u);
+                if (r < G.batch) {
+                    float x[G_IN];
+                    vertex_inputs(hp, ffn, xyz(wo4), p.w, S.bmin, S.binv, x);
+                    G.rec.x0[r] = f4(x[0], x[1], x[2], x[3]);
+                    G.rec.x1[r] = f4(x[4], x[5], x[6], x[7]);
+                    G.rec.x2[r] = f4(x[8], x[9], 0.f, 0.f);
+                    G.rec.w[r] = f4(dir.x, dir.y, dir.z, pdf);
+                    float fcos = (spec.x + spec.y + spec.z + spec.w) * 0.25f * pb;
+                    G.rec.b[r] = f4(pb, fcos, 0.f, 0.f);
+                    G.rec.thr[r] = thr;
+                    G.rec.rad[r] = splat4(__int_as_float(0x7FC00000));  // NaN: not reached yet
+                    G.rec.pid[r] = id;
+                    rec = r + 1u;
+                }
+            }
+        }
+        alive = true;
+        if (bounce > 3u) {
+            float pr = max4(thr);
+            if (rng_next(s) > pr) alive = false;
+            else thr = thr / pr;
+        }
+        if (bounce + 1u >= a.max_depth) alive = false;
+    }
+    if (alive) {
+        a.pb.thr[id] = thr;
+        a.pb.ray_o[id] = f4(hp.x, hp.y, hp.z, 0.0001f);
+        a.pb.ray_d[id] = f4(dir.x, dir.y, dir.z, 100.0f);
+    }
+    a.pb.misc[id] = make_uint4(s, misc.y, misc.z, rec);
+    return alive;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- inference
@@ -404,7 +469,7 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32
         HalfMix m;
         half_mixture(out + sl * 52, half, m);
         uint32_t id = 0, s = 0;
-        float4 p = splat4(0.f), nn = splat4(0.f), wo4 = splat4(0.f), spec = splat4(0.f), thr = splat4(0.f);
+        float4 p = splat4(0.f), nn = splat4(0.f);
         uint4 misc = make_uint4(0, 0, 0, 0);
         if (valid) {
             id = G.gv.id[v];
@@ -431,55 +496,7 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32
         if (use_guide) dir = gdir;
         const float q = half_pdf(m, dir);
         bool alive = false;
-        if (valid && half == 0) {
-            wo4 = G.gv.wo[v];
-            spec = G.gv.spec[v];
-            thr = a.pb.thr[id];
-            const float3 hp = xyz(p);
-            float cosv = dot(ffn, dir);
-            uint32_t rec = 0u;  // record index + 1 (0: none)
-            if (cosv > 0.0f) {
-                float pb = cosv / PI;
-                float pdf = m.sel * q + (1.0f - m.sel) * pb;
-                float4 att = spec * (pb / pdf);  // (spec / pi) cos / pdf
-                thr = thr * att;
-                // training sample (a hashed subset of the vertices)
-                if (G.train) {
-                    atomicAdd(&G.gc->candidates, 1u);
-                    uint32_t h = pcg_hash(id ^ (bounce << 24) ^ (frame * 0x9E3779B9u)) & 0xFFFFu;
-                    if (h < G.gc->threshold) {
-                        uint32_t r = atomicAdd(&G.gc->records, 1u);
-                        if (r < G.batch) {
-                            float x[G_IN];
-                            vertex_inputs(hp, ffn, xyz(wo4), p.w, S.bmin, S.binv, x);
-                            G.rec.x0[r] = f4(x[0], x[1], x[2], x[3]);
-                            G.rec.x1[r] = f4(x[4], x[5], x[6], x[7]);
-                            G.rec.x2[r] = f4(x[8], x[9], 0.f, 0.f);
-                            G.rec.w[r] = f4(dir.x, dir.y, dir.z, pdf);
-                            float fcos = (spec.x + spec.y + spec.z + spec.w) * 0.25f * pb;
-                            G.rec.b[r] = f4(pb, fcos, 0.f, 0.f);
-                            G.rec.thr[r] = thr;
-                            G.rec.rad[r] = splat4(__int_as_float(0x7FC00000));  // NaN: not reached yet
-                            G.rec.pid[r] = id;
-                            rec = r + 1u;
-                        }
-                    }
-                }
-                alive = true;
-                if (bounce > 3u) {
-                    float pr = max4(thr);
-                    if (rng_next(s) > pr) alive = false;
-                    else thr = thr / pr;
-                }
-                if (bounce + 1u >= a.max_depth) alive = false;
-            }
-            if (alive) {
-                a.pb.thr[id] = thr;
-                a.pb.ray_o[id] = f4(hp.x, hp.y, hp.z, 0.0001f);
-                a.pb.ray_d[id] = f4(dir.x, dir.y, dir.z, 100.0f);
-            }
-            a.pb.misc[id] = make_uint4(s, misc.y, misc.z, rec);
-        }
+        if (valid && half == 0) alive = finish_vertex(a, bounce, frame, v, id, p, ffn, misc, s, dir, m.sel, q);
         // push the survivors into the next bounce's queue
         uint32_t mask = __ballot_sync(0xFFFFFFFFu, alive);
         uint32_t slot_base = 0;
@@ -576,7 +593,7 @@ __global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) {
                 float wt = G.rec.weight[r] * inv_mean;
                 float vm[G_LOBES], q = 0.f;
                 for (int j = 0; j < G_LOBES; ++j) {
-                    vm[j] = vmf(m.mu[j], m.kappa[j], om);
+                    vm[j] = m.c[j] * expf(m.kappa[j] * (dot(m.mu[j], om) - 1.0f));
                     q += m.pi[j] * vm[j];
                 }
                 q = fmaxf(q, 1e-30f);
@@ -855,6 +872,337 @@ __global__ void k_guide_test_mixture(const float* __restrict__ raw, const float*
     }
 }
 
+// ---------------------------------------------------------------- tcgen05 inference
+// The same network on the fifth-generation tensor cores.  A block runs two
+// independent groups of 128 threads (warps 0-3 and 4-7); a group owns 128
+// vertices (M = 128 rows).  The encoded rows and each hidden layer's
+// activations live in the group's shared-memory A buffer in the K-major
+// core-matrix layout (umma.cuh), the weights (shared by both groups) as the
+// B operands (N = 64, or 48 for the output layer), and every layer is K / 16
+// tcgen05.mma instructions issued by one thread of the group into the
+// group's 128 x 64 FP32 accumulator in tensor memory.  Thread t reads row t
+// back (tcgen05.ld), adds the bias, applies ReLU and writes the bf16 row of
+// the next layer's A operand; after the output layer it holds its vertex's
+// 48 raw outputs in registers and samples its mixture alone.  While one
+// group waits for its MMAs the other runs its epilogue or mixture code.
+namespace {
+
+constexpr int TC_ROWS = 128;
+constexpr int TC_GROUPS = 2;
+constexpr uint32_t TC_TMEM_COLS = 64 * TC_GROUPS;
+constexpr uint32_t TC_WAIT_POLLS = 1u << 22;
+__host__ __device__ constexpr uint32_t tc_woff(int l) { return l == 0 ? 0u : 16384u + 8192u * (uint32_t)(l - 1); }
+constexpr uint32_t TC_A_BYTES = TC_ROWS * G_ENC * 2;
+__host__ __device__ constexpr uint32_t tc_aoff(int g) { return 47104u + TC_A_BYTES * (uint32_t)g; }
+constexpr uint32_t TC_B_OFF = tc_aoff(TC_GROUPS);
+constexpr uint32_t TC_BAR_OFF = TC_B_OFF + SB_ELEMS * 4;  // one mbarrier per group, then the TMEM base
+constexpr uint32_t TC_SMEM = TC_BAR_OFF + 8 * TC_GROUPS + 16;
+static_assert(tc_woff(4) + G_OUT * G_HID * 2 == tc_aoff(0), "tcgen05 weight layout");
+static_assert(tc_aoff(0) % 128 == 0 && TC_B_OFF % 16 == 0 && TC_BAR_OFF % 8 == 0, "tcgen05 shared-memory alignment");
+static_assert(2 * (TC_SMEM + 1024) <= 228 * 1024, "two blocks per SM");
+
+// Barrier of one 128-thread group (ids 1 and 2; 0 is the block barrier).
+SRT_DEV void group_sync(uint32_t id) { asm volatile("bar.sync %0, 128;\n" ::"r"(id) : "memory"); }
+// AND of `pred` over the group, also a barrier.
+SRT_DEV bool group_and(uint32_t id, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n"
+        ".reg .pred p, q;\n"
+        "setp.ne.u32 q, %1, 0;\n"
+        "bar.red.and.pred p, %2, 128, q;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id)
+        : "memory");
+    return r != 0u;
+}
+
+// Weights of all layers into the core-matrix layout (cp.async) and biases.
+SRT_DEV void load_weights_tc(const GuideNet& net, unsigned char* smem, float* sb) {
+    for (int l = 0; l < G_LAYERS; ++l) {
+        const int K = g_in(l), N = g_out(l), cpr = K / 8;
+        for (int i = threadIdx.x; i < N * cpr; i += blockDim.x) {
+            const int n = i / cpr, kc = i - n * cpr;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                             smem_u32(smem + tc_woff(l) + umma_offset((uint32_t)n, 8u * kc, (uint32_t)K))),
+                         "l"(net.wbf + g_woff(l) + n * K + 8 * kc));
+        }
+    }
+    int bo = 0;
+    for (int l = 0; l < G_LAYERS; ++l) {
+        for (int i = threadIdx.x; i < g_out(l); i += blockDim.x) sb[bo + i] = net.master[g_boff(l) + i];
+        bo += g_out(l);
+    }
+    cp_async_wait_all();
+    fence_async_smem();  // the tensor core reads them through the async proxy
+}
+
+// Row `row` of the A operand (K = 128): the frequency encoding of x, with the
+// octave recurrence of encode_half.
+SRT_DEV void encode_row_tc(const float* x, unsigned char* A, uint32_t row) {
+    uint32_t pk[G_ENC / 2];
+#pragma unroll
+    for (int d = 0; d < G_IN; ++d) {
+        float s, c;
+        sincospif(x[d], &s, &c);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            pk[6 * d + k] = pack2(s, c);  // features 12 d + 2 k (sin), + 1 (cos)
+            float s2 = __fmul_rn(__fmul_rn(2.0f, s), c);
+            float c2 = __fmaf_rn(c, c, -__fmul_rn(s, s));
+            s = s2;
+            c = c2;
+        }
+    }
+#pragma unroll
+    for (int i = 60; i < 64; ++i) pk[i] = 0u;
+#pragma unroll
+    for (int ch = 0; ch < G_ENC / 8; ++ch)
+        *reinterpret_cast<uint4*>(A + umma_offset(row, 8u * ch, G_ENC)) =
+            make_uint4(pk[4 * ch], pk[4 * ch + 1], pk[4 * ch + 2], pk[4 * ch + 3]);
+}
+
+// Bias + ReLU of 16 accumulator columns into 8 packed bf16 pairs.
+SRT_DEV void relu_pack16(const uint32_t (&r)[16], const float* bias, uint32_t* out) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        out[i] = pack2(fmaxf(__uint_as_float(r[2 * i]) + bias[2 * i], 0.f),
+                       fmaxf(__uint_as_float(r[2 * i + 1]) + bias[2 * i + 1], 0.f));
+}
+
+// A group of 128 threads: its A buffer, accumulator columns, mbarrier and
+// barrier id; `row` = the thread's row (and TMEM lane).
+struct TcGroup {
+    unsigned char* A;
+    uint32_t tmem;  // lane 0, the group's first column
+    uint64_t* mbar;
+    uint32_t bar;
+    uint32_t row;
+};
+
+// The five layers for the group's 128 rows (A holds the encoded rows, made
+// visible to the async proxy by the caller's fence + group barrier).  On
+// return `out` holds this thread's raw outputs.  False (for every thread of
+// the group) when a layer's MMAs did not complete within the wait limit;
+// `phase` then still names the phase that did not complete.
+SRT_DEV bool mlp_tc(const TcGroup& g, const unsigned char* smem, const float* sb, uint32_t& phase,
+                    float (&out)[G_OUT]) {
+    const uint32_t a_addr = smem_u32(g.A), w_addr = smem_u32(smem);
+    const uint32_t taddr = g.tmem + (((g.row >> 5) * 32u) << 16);
+#pragma unroll
+    for (int l = 0; l < G_LAYERS; ++l) {
+        const uint32_t K = (uint32_t)g_in(l), N = (uint32_t)g_out(l), SBO = K / 8u * 128u;
+        if (g.row == 0) {
+            tc_fence_after();
+            for (uint32_t s = 0; s < K / 16u; ++s)
+                umma_bf16(g.tmem, umma_desc(a_addr + 256u * s, 128u, SBO),
+                          umma_desc(w_addr + tc_woff(l) + 256u * s, 128u, SBO), umma_idesc_bf16(TC_ROWS, N), s);
+            umma_commit(g.mbar);
+        }
+        if (!group_and(g.bar, mbar_wait(g.mbar, phase, TC_WAIT_POLLS))) return false;
+        phase ^= 1u;
+        tc_fence_after();
+        const float* bias = sb + G_HID * l;
+        uint32_t r0[16], r1[16], r2[16];
+        tmem_ld16(taddr, r0);
+        tmem_ld16(taddr + 16u, r1);
+        tmem_ld16(taddr + 32u, r2);
+        if (l < G_LAYERS - 1) {
+            uint32_t r3[16];
+            tmem_ld16(taddr + 48u, r3);
+            tmem_wait16(r0);
+            tmem_wait16(r1);
+            tmem_wait16(r2);
+            tmem_wait16(r3);
+            uint32_t pk[32];
+            relu_pack16(r0, bias, pk);
+            relu_pack16(r1, bias + 16, pk + 8);
+            relu_pack16(r2, bias + 32, pk + 16);
+            relu_pack16(r3, bias + 48, pk + 24);
+#pragma unroll
+            for (int ch = 0; ch < G_HID / 8; ++ch)
+                *reinterpret_cast<uint4*>(g.A + umma_offset(g.row, 8u * ch, G_HID)) =
+                    make_uint4(pk[4 * ch], pk[4 * ch + 1], pk[4 * ch + 2], pk[4 * ch + 3]);
+            fence_async_smem();
+        } else {
+            tmem_wait16(r0);
+            tmem_wait16(r1);
+            tmem_wait16(r2);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                out[i] = __uint_as_float(r0[i]) + bias[i];
+                out[16 + i] = __uint_as_float(r1[i]) + bias[16 + i];
+                out[32 + i] = __uint_as_float(r2[i]) + bias[32 + i];
+            }
+        }
+        tc_fence_before();
+        group_sync(g.bar);
+    }
+    return true;
+}
+
+SRT_DEV float mix_pdf(const Mix& m, float3 w) {
+    float q = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) q += m.pi[j] * (m.c[j] * expf(m.kappa[j] * (dot(m.mu[j], w) - 1.0f)));
+    return q;
+}
+// Lobe j = first with u0 below the cumulative weight (the last lobe on
+// rounding), then a vMF direction from (u1, u2).
+SRT_DEV float3 mix_sample(const Mix& m, float u0, float u1, float u2) {
+    float acc = 0.f;
+    float3 mu = m.mu[G_LOBES - 1];
+    float k = m.kappa[G_LOBES - 1], e2 = m.e2[G_LOBES - 1];
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) {
+        acc += m.pi[j];
+        if (!found && u0 < acc) {
+            found = true;
+            mu = m.mu[j];
+            k = m.kappa[j];
+            e2 = m.e2[j];
+        }
+    }
+    return vmf_sample_e2(mu, k, e2, u1, u2);
+}
+
+// Block set-up (tensor-memory allocation, mbarriers, weights) and this
+// thread's group.
+SRT_DEV TcGroup tc_setup(unsigned char* smem, const GuideNet& net, float*& sb) {
+    sb = reinterpret_cast<float*>(smem + TC_B_OFF);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TC_BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_BAR_OFF + 8 * TC_GROUPS);
+    if ((threadIdx.x >> 5) == 0) {
+        tmem_alloc(tslot, TC_TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (threadIdx.x < TC_GROUPS) mbar_init(bars + threadIdx.x, 1);
+    load_weights_tc(net, smem, sb);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t grp = threadIdx.x / TC_ROWS;
+    TcGroup g;
+    g.A = smem + tc_aoff((int)grp);
+    g.tmem = *tslot + 64u * grp;
+    g.mbar = bars + grp;
+    g.bar = 1u + grp;
+    g.row = threadIdx.x % TC_ROWS;
+    return g;
+}
+// After a timed-out layer: record it and give the group's MMAs in flight one
+// more bounded wait; then (every path, whole block) free the tensor memory.
+SRT_DEV void tc_teardown(const TcGroup& g, bool ok, uint32_t phase, uint32_t* err) {
+    if (!ok) {
+        if (g.row == 0) atomicOr(err, ERR_MMA_TIMEOUT);
+        mbar_wait(g.mbar, phase, TC_WAIT_POLLS);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 0) tmem_dealloc(g.tmem, TC_TMEM_COLS);  // warp 0: group 0, base column
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_infer_tc(FrameArgs a, uint32_t bounce) {
+    const GuideArgs& G = a.guide;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const uint32_t n = G.gc->verts[bounce];
+    if (blockIdx.x * TC_ROWS * TC_GROUPS >= n) return;
+    float* sb;
+    const TcGroup grp = tc_setup(smem, G.net, sb);
+    const DevScene& S = a.scene;
+    const uint32_t frame = a.cam->frame_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t base = (blockIdx.x * TC_GROUPS + threadIdx.x / TC_ROWS) * TC_ROWS; base < n;
+         base += gridDim.x * TC_GROUPS * TC_ROWS) {
+        const uint32_t v = base + grp.row;
+        const bool valid = v < n;
+        float x[G_IN];
+        float4 p = splat4(0.f), nn = splat4(0.f);
+        if (valid) {
+            p = G.gv.p[v];
+            nn = G.gv.n[v];
+            float4 wo = G.gv.wo[v];
+            vertex_inputs(xyz(p), xyz(nn), xyz(wo), p.w, S.bmin, S.binv, x);
+        } else {
+            for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
+        }
+        encode_row_tc(x, grp.A, grp.row);
+        fence_async_smem();
+        group_sync(grp.bar);
+        float raw[G_OUT];
+        if (!mlp_tc(grp, smem, sb, phase, raw)) {
+            ok = false;
+            break;
+        }
+        bool alive = false;
+        uint32_t id = 0;
+        if (valid) {
+            Mix m;
+            mixture(raw, m);
+            id = G.gv.id[v];
+            const uint4 misc = a.pb.misc[id];
+            uint32_t s = misc.x;
+            const float3 ffn = xyz(nn);
+            float3 dir;
+            if (rng_next(s) < m.sel) {
+                const float u0 = rng_next(s), u1 = rng_next(s), u2 = rng_next(s);
+                dir = mix_sample(m, u0, u1, u2);
+            } else {
+                float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
+                if (length(d) < 0.001f) d = ffn;
+                dir = normalize(d);
+            }
+            alive = finish_vertex(a, bounce, frame, v, id, p, ffn, misc, s, dir, m.sel, mix_pdf(m, dir));
+        }
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, alive);
+        uint32_t slot_base = 0;
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            if ((int)lane == leader) slot_base = atomicAdd(&a.counters->paths[bounce + 1], (uint32_t)__popc(mask));
+            slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, leader);
+        }
+        if (alive) a.pb.queue[(bounce + 1) & 1][slot_base + __popc(mask & ((1u << lane) - 1u))] = id;
+    }
+    tc_teardown(grp, ok, phase, a.err);
+}
+
+// Forward pass of n samples on the tcgen05 path (inputs [n][10] -> raw outputs [n][48]).
+__global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_test_forward_tc(GuideNet net,
+                                                                                  const float* __restrict__ x,
+                                                                                  uint32_t n, float* __restrict__ y,
+                                                                                  uint32_t* err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* sb;
+    const TcGroup grp = tc_setup(smem, net, sb);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t base = (blockIdx.x * TC_GROUPS + threadIdx.x / TC_ROWS) * TC_ROWS; base < n;
+         base += gridDim.x * TC_GROUPS * TC_ROWS) {
+        const uint32_t r = base + grp.row;
+        float xi[G_IN];
+        for (int i = 0; i < G_IN; ++i) xi[i] = r < n ? x[(size_t)r * G_IN + i] : 0.f;
+        encode_row_tc(xi, grp.A, grp.row);
+        fence_async_smem();
+        group_sync(grp.bar);
+        float raw[G_OUT];
+        if (!mlp_tc(grp, smem, sb, phase, raw)) {
+            ok = false;
+            break;
+        }
+        if (r < n)
+            for (int i = 0; i < G_OUT; ++i) y[(size_t)r * G_OUT + i] = raw[i];
+    }
+    tc_teardown(grp, ok, phase, err);
+}
+
 // ---------------------------------------------------------------- launchers
 size_t guide_infer_smem() {
     return SW_ELEMS * 2 + SB_ELEMS * 4 + GWI * IN_BYTES;
@@ -871,12 +1219,17 @@ cudaError_t guide_configure() {
                                  (int)guide_infer_smem());
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_guide_fwdbwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_train_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_test_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     return e;
 }
 
 int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * 2;
-    k_guide_infer<<<grid, GWI * 32, guide_infer_smem(), st>>>(a, bounce);
+    if (a.guide.tc) k_guide_infer_tc<<<grid, TC_ROWS * TC_GROUPS, TC_SMEM, st>>>(a, bounce);
+    else k_guide_infer<<<grid, GWI * 32, guide_infer_smem(), st>>>(a, bounce);
     return 1;
 }
 
@@ -979,6 +1332,7 @@ cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
     g.lr = 1e-3f;
     g.train = 1;
     g.batch = G_BATCH_DEFAULT;
+    g.tc = 1;
     return e;
 }
 
@@ -1014,8 +1368,10 @@ cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m,
     return e;
 }
 
-int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, cudaStream_t st) {
-    k_guide_test_forward<<<64, GWI * 32, guide_infer_smem(), st>>>(net, x, n, y);
+int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, int tc, uint32_t* err,
+                              cudaStream_t st) {
+    if (tc) k_guide_test_forward_tc<<<128, TC_ROWS * TC_GROUPS, TC_SMEM, st>>>(net, x, n, y, err);
+    else k_guide_test_forward<<<64, GWI * 32, guide_infer_smem(), st>>>(net, x, n, y);
     return 1;
 }
 int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,

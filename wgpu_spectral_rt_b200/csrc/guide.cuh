@@ -100,6 +100,7 @@ struct GuideArgs {
     int train;               // run a training step after each frame
     float lr;
     uint32_t batch;          // training samples recorded per frame (<= G_REC_CAP)
+    int tc;                  // inference on tcgen05 / tensor memory (else mma.sync)
 };
 static_assert(G_NPARAMS % 8 == 0 && g_woff(1) % 8 == 0 && g_woff(2) % 8 == 0 && g_woff(3) % 8 == 0 &&
                   g_woff(4) % 8 == 0,
@@ -110,7 +111,9 @@ struct FrameArgs;
 cudaError_t guide_configure();  // raises the dynamic shared-memory limits once per device
 int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st);
 int launch_guide_train(const FrameArgs& a, cudaStream_t st);
-int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, cudaStream_t st);
+// tc: the tcgen05 kernel (err: device error word for an MMA wait that gave up).
+int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, int tc, uint32_t* err,
+                              cudaStream_t st);
 int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,
                               cudaStream_t st);
 // phase 0: forward + backward + weight gradients of gc->records records
