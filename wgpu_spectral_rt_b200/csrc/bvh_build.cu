@@ -204,34 +204,41 @@ __global__ void k_refit(const TriSlot* __restrict__ flat, const uint32_t* __rest
 // the bottom-up box pass and the 8-wide collapse are shared.
 constexpr int SAH_BINS = 16;
 constexpr int SAH_REC = 13;  // count, box lo/hi, centroid lo/hi (flipped floats)
+constexpr int SAH_TASK_WORDS = 3 * SAH_BINS * SAH_REC;  // bins of the three axes
 constexpr uint32_t SAH_MEDIAN = 0xFFFFFFFFu;
+constexpr uint32_t SAH_LOCAL = 0xFFFFFFFEu;  // binned by its split thread (small ranges)
+constexpr uint32_t SAH_SMALL = 64;           // ranges up to this size bin without atomics
 constexpr uint32_t SAH_MEDIAN_LEVEL = 48;
 
 struct SahTask {
     uint32_t node, first, count, axis;
-    float cmin, cscale;  // bin = (c - cmin) * cscale
+    float cmin[3], cscale[3];  // bin along axis a = (c_a - cmin[a]) * cscale[a]
+    uint32_t bin_slot;         // bins of this task (SAH tasks only)
     uint32_t split, left_count;
     uint32_t lcur, rcur;
     uint32_t child_task[2];  // next-level task of each child, 0xFFFFFFFF for a leaf
 };
 
-__device__ __forceinline__ uint32_t sah_bin(const SahTask& t, float4 c) {
-    float v = t.axis == 0 ? c.x : (t.axis == 1 ? c.y : c.z);
-    float f = (v - t.cmin) * t.cscale;
+__device__ __forceinline__ uint32_t sah_bin(const SahTask& t, float4 c, uint32_t ax) {
+    float v = ax == 0 ? c.x : (ax == 1 ? c.y : c.z);
+    float f = (v - t.cmin[ax]) * t.cscale[ax];
     int b = (int)f;
     return (uint32_t)min(max(b, 0), SAH_BINS - 1);
+}
+
+__device__ __forceinline__ uint32_t sah_init_word(uint32_t i) {
+    uint32_t k = i % SAH_REC;
+    // lo fields start at +inf (min of flipped), hi fields at 0
+    return (k == 0u) ? 0u : ((k >= 1 && k <= 3) || (k >= 7 && k <= 9)) ? 0xFFFFFFFFu : 0u;
 }
 
 __global__ void k_sah_init_bins(uint32_t* __restrict__ bins, uint32_t n_words) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_words) return;
-    uint32_t k = i % SAH_REC;
-    // lo fields start at +inf (min of flipped), hi fields at 0
-    bins[i] = (k == 0u) ? 0u : ((k >= 1 && k <= 3) || (k >= 7 && k <= 9)) ? 0xFFFFFFFFu : 0u;
+    bins[i] = sah_init_word(i);
 }
 
-__device__ __forceinline__ void sah_accum(uint32_t* rec, float3 lo, float3 hi, float4 c, bool shared_mem) {
-    (void)shared_mem;
+__device__ __forceinline__ void sah_accum(uint32_t* rec, float3 lo, float3 hi, float4 c) {
     atomicAdd(&rec[0], 1u);
     atomicMin(&rec[1], float_flip(lo.x));
     atomicMin(&rec[2], float_flip(lo.y));
@@ -247,24 +254,29 @@ __device__ __forceinline__ void sah_accum(uint32_t* rec, float3 lo, float3 hi, f
     atomicMax(&rec[12], float_flip(c.z));
 }
 
-// Bins of every active position; the task of the block's first position
-// (most of the block at the top levels) aggregates in shared memory.
+// Bins of every active position (of tasks larger than SAH_SMALL) along all
+// three axes; the tasks of the block's first and last positions (most of the
+// block) aggregate in shared memory.
 __global__ void k_sah_bin(const uint32_t* __restrict__ perm, const int* __restrict__ pos_task, uint32_t n,
                           const SahTask* __restrict__ tasks, const float4* __restrict__ cen,
                           const TriSlot* __restrict__ flat, uint32_t* __restrict__ bins) {
-    __shared__ uint32_t sb[SAH_BINS * SAH_REC];
-    __shared__ int t0s;
+    __shared__ uint32_t sb[2][SAH_TASK_WORDS];
+    __shared__ int ts[2];
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (threadIdx.x == 0) t0s = pos_task[min(blockIdx.x * blockDim.x, n - 1)];
-    for (int i = threadIdx.x; i < SAH_BINS * SAH_REC; i += blockDim.x) {
-        int k = i % SAH_REC;
-        sb[i] = (k == 0) ? 0u : ((k >= 1 && k <= 3) || (k >= 7 && k <= 9)) ? 0xFFFFFFFFu : 0u;
+    if (threadIdx.x == 0) {
+        ts[0] = pos_task[min(blockIdx.x * blockDim.x, n - 1)];
+        ts[1] = pos_task[min(blockIdx.x * blockDim.x + blockDim.x - 1, n - 1)];
+        if (ts[1] == ts[0]) ts[1] = -1;
+        for (int k = 0; k < 2; ++k)
+            if (ts[k] >= 0 && tasks[ts[k]].split != 0u) ts[k] = -1;
     }
+    for (int i = threadIdx.x; i < 2 * SAH_TASK_WORDS; i += blockDim.x)
+        sb[i / SAH_TASK_WORDS][i % SAH_TASK_WORDS] = sah_init_word((uint32_t)(i % SAH_TASK_WORDS));
     __syncthreads();
-    const int t0 = t0s;
     if (p < n) {
         const int t = pos_task[p];
-        if (t >= 0 && tasks[t].split != SAH_MEDIAN) {
+        if (t >= 0 && tasks[t].split == 0u) {
+            const SahTask& T = tasks[t];
             const uint32_t prim = perm[p];
             const TriSlot s = flat[prim];
             const float3 lo = f3(fminf(fminf(s.v0.x, s.v1.x), s.v2.x), fminf(fminf(s.v0.y, s.v1.y), s.v2.y),
@@ -272,22 +284,26 @@ __global__ void k_sah_bin(const uint32_t* __restrict__ perm, const int* __restri
             const float3 hi = f3(fmaxf(fmaxf(s.v0.x, s.v1.x), s.v2.x), fmaxf(fmaxf(s.v0.y, s.v1.y), s.v2.y),
                                  fmaxf(fmaxf(s.v0.z, s.v1.z), s.v2.z));
             const float4 c = cen[prim];
-            const uint32_t b = sah_bin(tasks[t], c);
-            if (t == t0) sah_accum(sb + b * SAH_REC, lo, hi, c, true);
-            else sah_accum(bins + ((size_t)t * SAH_BINS + b) * SAH_REC, lo, hi, c, false);
+            uint32_t* dst = t == ts[0] ? sb[0] : t == ts[1] ? sb[1] : bins + (size_t)T.bin_slot * SAH_TASK_WORDS;
+            for (uint32_t ax = 0; ax < 3; ++ax) {
+                if (!(T.cscale[ax] > 0.f)) continue;
+                sah_accum(dst + (ax * SAH_BINS + sah_bin(T, c, ax)) * SAH_REC, lo, hi, c);
+            }
         }
     }
     __syncthreads();
-    if (t0 >= 0 && tasks[t0].split != SAH_MEDIAN) {
-        for (int i = threadIdx.x; i < SAH_BINS; i += blockDim.x) {
-            const uint32_t* r = sb + i * SAH_REC;
+    for (int k = 0; k < 2; ++k) {
+        if (ts[k] < 0) continue;
+        uint32_t* G = bins + (size_t)tasks[ts[k]].bin_slot * SAH_TASK_WORDS;
+        for (int i = threadIdx.x; i < 3 * SAH_BINS; i += blockDim.x) {
+            const uint32_t* r = sb[k] + i * SAH_REC;
             if (r[0] == 0u) continue;
-            uint32_t* g = bins + ((size_t)t0 * SAH_BINS + i) * SAH_REC;
+            uint32_t* g = G + i * SAH_REC;
             atomicAdd(&g[0], r[0]);
-            for (int k = 1; k <= 3; ++k) atomicMin(&g[k], r[k]);
-            for (int k = 4; k <= 6; ++k) atomicMax(&g[k], r[k]);
-            for (int k = 7; k <= 9; ++k) atomicMin(&g[k], r[k]);
-            for (int k = 10; k <= 12; ++k) atomicMax(&g[k], r[k]);
+            for (int j = 1; j <= 3; ++j) atomicMin(&g[j], r[j]);
+            for (int j = 4; j <= 6; ++j) atomicMax(&g[j], r[j]);
+            for (int j = 7; j <= 9; ++j) atomicMin(&g[j], r[j]);
+            for (int j = 10; j <= 12; ++j) atomicMax(&g[j], r[j]);
         }
     }
 }
@@ -297,78 +313,130 @@ __device__ __forceinline__ float half_area(float3 lo, float3 hi) {
     return e.x * e.y + e.y * e.z + e.z * e.x;
 }
 
-// Sets the next-level task of one child: binning axis and mapping from its
-// centroid bounds.
+// Sets the next-level task of one child: bin mappings of the three axes from
+// its centroid bounds, and a bin slot when it will be binned.
 __device__ void sah_child_task(SahTask& c, uint32_t node, uint32_t first, uint32_t count, float3 clo, float3 chi,
-                               bool median) {
+                               bool median, uint32_t* bin_alloc, uint32_t bin_cap) {
     c.node = node;
     c.first = first;
     c.count = count;
-    float3 e = f3(chi.x - clo.x, chi.y - clo.y, chi.z - clo.z);
-    uint32_t ax = (e.x >= e.y && e.x >= e.z) ? 0u : (e.y >= e.z ? 1u : 2u);
-    float ext = ax == 0 ? e.x : (ax == 1 ? e.y : e.z);
-    c.axis = ax;
-    c.cmin = ax == 0 ? clo.x : (ax == 1 ? clo.y : clo.z);
-    c.cscale = ext > 0.f ? (float)SAH_BINS / ext : 0.f;
+    const float lo[3] = {clo.x, clo.y, clo.z}, ext[3] = {chi.x - clo.x, chi.y - clo.y, chi.z - clo.z};
+    bool any = false;
+    for (int a = 0; a < 3; ++a) {
+        c.cmin[a] = lo[a];
+        c.cscale[a] = ext[a] > 0.f ? (float)SAH_BINS / ext[a] : 0.f;
+        any = any || ext[a] > 0.f;
+    }
+    c.axis = 0;
     // all centroids on one point, below the SAH levels, or a range that the
     // collapse turns into one leaf anyway (<= 3): split by position
-    c.split = (median || !(ext > 0.f) || count <= 3u) ? SAH_MEDIAN : 0u;
+    c.split = (median || !any || count <= 3u) ? SAH_MEDIAN : (count <= SAH_SMALL ? SAH_LOCAL : 0u);
+    c.bin_slot = 0xFFFFFFFFu;
+    if (c.split == 0u) {
+        uint32_t slot = atomicAdd(bin_alloc, 1u);
+        if (slot < bin_cap) c.bin_slot = slot;
+        else c.split = SAH_MEDIAN;  // out of bin slots (cannot happen: n / 4 tasks of >= 4)
+    }
     c.left_count = 0;
     c.lcur = c.rcur = 0;
     c.child_task[0] = c.child_task[1] = 0xFFFFFFFFu;
 }
 
-// One thread per task: choose the split, create the children.
+// One thread per task: choose the split (axis and bin boundary of least
+// cost), create the children.
 __global__ void k_sah_split(SahTask* __restrict__ tasks, uint32_t n_tasks, const uint32_t* __restrict__ bins,
+                            const uint32_t* __restrict__ perm, const float4* __restrict__ cen,
+                            const TriSlot* __restrict__ flat,
                             SahTask* __restrict__ next, uint32_t* __restrict__ n_next, uint32_t next_cap,
-                            uint32_t* __restrict__ node_alloc, uint32_t node_cap, Bvh2 b, uint32_t level,
-                            uint32_t* __restrict__ err) {
+                            uint32_t* __restrict__ bin_alloc, uint32_t bin_cap, uint32_t* __restrict__ node_alloc,
+                            uint32_t node_cap, Bvh2 b, uint32_t level, uint32_t* __restrict__ err) {
     const uint32_t ti = blockIdx.x * blockDim.x + threadIdx.x;
     if (ti >= n_tasks) return;
     SahTask& T = tasks[ti];
     uint32_t left = T.count / 2;  // median by position
     float3 clo[2] = {f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)}, chi[2] = {f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)};
     bool median = T.split == SAH_MEDIAN;
-    if (!median) {
-        const uint32_t* B = bins + (size_t)ti * SAH_BINS * SAH_REC;
-        float ra[SAH_BINS];  // area of bins [k, K)
-        uint32_t rc[SAH_BINS];
-        float3 lo = f3(3.4e38f, 3.4e38f, 3.4e38f), hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
-        uint32_t cnt = 0;
-        for (int k = SAH_BINS - 1; k >= 0; --k) {
-            const uint32_t* r = B + k * SAH_REC;
-            if (r[0]) {
-                lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])), fminf(lo.z, float_unflip(r[3])));
-                hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])), fmaxf(hi.z, float_unflip(r[6])));
-                cnt += r[0];
+    uint32_t local[SAH_TASK_WORDS];  // the bins of a small range, filled here without atomics
+    const uint32_t* Bt = local;
+    if (T.split == 0u) Bt = bins + (size_t)T.bin_slot * SAH_TASK_WORDS;
+    if (T.split == SAH_LOCAL) {
+        for (int i = 0; i < SAH_TASK_WORDS; ++i) local[i] = sah_init_word((uint32_t)i);
+        for (uint32_t q = T.first; q < T.first + T.count; ++q) {
+            const uint32_t prim = perm[q];
+            const TriSlot s = flat[prim];
+            const float4 c = cen[prim];
+            const uint32_t f[12] = {float_flip(fminf(fminf(s.v0.x, s.v1.x), s.v2.x)),
+                                    float_flip(fminf(fminf(s.v0.y, s.v1.y), s.v2.y)),
+                                    float_flip(fminf(fminf(s.v0.z, s.v1.z), s.v2.z)),
+                                    float_flip(fmaxf(fmaxf(s.v0.x, s.v1.x), s.v2.x)),
+                                    float_flip(fmaxf(fmaxf(s.v0.y, s.v1.y), s.v2.y)),
+                                    float_flip(fmaxf(fmaxf(s.v0.z, s.v1.z), s.v2.z)),
+                                    float_flip(c.x), float_flip(c.y), float_flip(c.z),
+                                    float_flip(c.x), float_flip(c.y), float_flip(c.z)};
+            for (uint32_t ax = 0; ax < 3; ++ax) {
+                if (!(T.cscale[ax] > 0.f)) continue;
+                uint32_t* r = local + (ax * SAH_BINS + sah_bin(T, c, ax)) * SAH_REC;
+                r[0] += 1u;
+                for (int j = 0; j < 3; ++j) {
+                    r[1 + j] = min(r[1 + j], f[j]);
+                    r[4 + j] = max(r[4 + j], f[3 + j]);
+                    r[7 + j] = min(r[7 + j], f[6 + j]);
+                    r[10 + j] = max(r[10 + j], f[9 + j]);
+                }
             }
-            ra[k] = cnt ? half_area(lo, hi) : 0.f;
-            rc[k] = cnt;
         }
-        lo = f3(3.4e38f, 3.4e38f, 3.4e38f);
-        hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
-        cnt = 0;
+        T.split = 0u;
+    }
+    if (!median) {
         float best = 3.4e38f;
-        int bk = -1;
-        for (int k = 1; k < SAH_BINS; ++k) {
-            const uint32_t* r = B + (k - 1) * SAH_REC;
-            if (r[0]) {
-                lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])), fminf(lo.z, float_unflip(r[3])));
-                hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])), fmaxf(hi.z, float_unflip(r[6])));
-                cnt += r[0];
+        int bk = -1, bax = -1;
+        for (int ax = 0; ax < 3; ++ax) {
+            if (!(T.cscale[ax] > 0.f)) continue;
+            const uint32_t* B = Bt + ax * SAH_BINS * SAH_REC;
+            float ra[SAH_BINS];  // area of bins [k, K)
+            uint32_t rc[SAH_BINS];
+            float3 lo = f3(3.4e38f, 3.4e38f, 3.4e38f), hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+            uint32_t cnt = 0;
+            for (int k = SAH_BINS - 1; k >= 0; --k) {
+                const uint32_t* r = B + k * SAH_REC;
+                if (r[0]) {
+                    lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])),
+                            fminf(lo.z, float_unflip(r[3])));
+                    hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])),
+                            fmaxf(hi.z, float_unflip(r[6])));
+                    cnt += r[0];
+                }
+                ra[k] = cnt ? half_area(lo, hi) : 0.f;
+                rc[k] = cnt;
             }
-            if (cnt == 0 || rc[k] == 0) continue;
-            float cost = (float)cnt * half_area(lo, hi) + (float)rc[k] * ra[k];
-            if (cost < best) {
-                best = cost;
-                bk = k;
+            lo = f3(3.4e38f, 3.4e38f, 3.4e38f);
+            hi = f3(-3.4e38f, -3.4e38f, -3.4e38f);
+            cnt = 0;
+            for (int k = 1; k < SAH_BINS; ++k) {
+                const uint32_t* r = B + (k - 1) * SAH_REC;
+                if (r[0]) {
+                    lo = f3(fminf(lo.x, float_unflip(r[1])), fminf(lo.y, float_unflip(r[2])),
+                            fminf(lo.z, float_unflip(r[3])));
+                    hi = f3(fmaxf(hi.x, float_unflip(r[4])), fmaxf(hi.y, float_unflip(r[5])),
+                            fmaxf(hi.z, float_unflip(r[6])));
+                    cnt += r[0];
+                }
+                if (cnt == 0 || rc[k] == 0) continue;
+                float cost = (float)cnt * half_area(lo, hi) + (float)rc[k] * ra[k];
+                if (cost < best) {
+                    best = cost;
+                    bk = k;
+                    bax = ax;
+                }
             }
         }
         if (bk < 0) {
             median = true;
         } else {
+            T.axis = (uint32_t)bax;
             T.split = (uint32_t)bk;
             left = 0;
+            const uint32_t* B = Bt + bax * SAH_BINS * SAH_REC;
             float3 l0 = f3(3.4e38f, 3.4e38f, 3.4e38f), h0 = f3(-3.4e38f, -3.4e38f, -3.4e38f), l1 = l0, h1 = h0;
             for (int k = 0; k < SAH_BINS; ++k) {
                 const uint32_t* r = B + k * SAH_REC;
@@ -416,19 +484,21 @@ __global__ void k_sah_split(SahTask* __restrict__ tasks, uint32_t n_tasks, const
             refs[c] = nd;
             b.iparent[nd] = T.node;
             T.child_task[c] = tn;
-            sah_child_task(next[tn], nd, firsts[c], counts[c], clo[c], chi[c], median || level + 1 >= SAH_MEDIAN_LEVEL);
+            sah_child_task(next[tn], nd, firsts[c], counts[c], clo[c], chi[c], median || level + 1 >= SAH_MEDIAN_LEVEL,
+                           bin_alloc, bin_cap);
         }
     }
     b.inode[T.node] = make_uint4(refs[0], refs[1], T.first, T.first + T.count - 1u);
 }
 
 __global__ void k_sah_root(const uint32_t* __restrict__ bounds, uint32_t n, SahTask* __restrict__ t,
-                           int* __restrict__ pos_task, uint32_t* __restrict__ perm) {
+                           int* __restrict__ pos_task, uint32_t* __restrict__ perm, uint32_t* __restrict__ bin_alloc,
+                           uint32_t bin_cap) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p == 0) {
         float3 lo = f3(float_unflip(bounds[0]), float_unflip(bounds[1]), float_unflip(bounds[2]));
         float3 hi = f3(float_unflip(bounds[3]), float_unflip(bounds[4]), float_unflip(bounds[5]));
-        sah_child_task(t[0], 0u, 0u, n, lo, hi, false);
+        sah_child_task(t[0], 0u, 0u, n, lo, hi, false, bin_alloc, bin_cap);
     }
     if (p < n) {
         pos_task[p] = 0;
@@ -452,7 +522,7 @@ __global__ void k_sah_partition(const uint32_t* __restrict__ perm, const int* __
     SahTask& T = tasks[t];
     uint32_t side;
     if (T.split == SAH_MEDIAN) side = (p - T.first) >= T.left_count ? 1u : 0u;
-    else side = sah_bin(T, cen[prim]) >= T.split ? 1u : 0u;
+    else side = sah_bin(T, cen[prim], T.axis) >= T.split ? 1u : 0u;
     uint32_t np = side ? T.first + T.left_count + atomicAdd(&T.rcur, 1u) : T.first + atomicAdd(&T.lcur, 1u);
     perm2[np] = prim;
     pos_task2[np] = T.child_task[side] == 0xFFFFFFFFu ? -1 : (int)T.child_task[side];
@@ -826,26 +896,32 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
             uint32_t *perm = keys, *perm2 = keys2;
             int *pt = (int*)vals, *pt2 = (int*)vals2;
             const uint32_t task_cap = n / 2 + 1;
+            const uint32_t bin_cap = n / 4 + 1;  // tasks that bin hold >= 4 primitives
             CK(dalloc(&sah_tasks[0], task_cap));
             CK(dalloc(&sah_tasks[1], task_cap));
-            CK(dalloc(&sah_bins, (size_t)task_cap * SAH_BINS * SAH_REC));
+            CK(dalloc(&sah_bins, (size_t)bin_cap * SAH_TASK_WORDS));
+            // counters: node alloc, -, next tasks, bin slots of the next level
             CK(cudaMemcpyAsync(counters, std::array<uint32_t, 4>{1u, 0u, 0u, 0u}.data(), 16, cudaMemcpyHostToDevice, st));
-            k_sah_root<<<grid, B, 0, st>>>(bounds, n, sah_tasks[0], pt, perm);
+            k_sah_root<<<grid, B, 0, st>>>(bounds, n, sah_tasks[0], pt, perm, counters + 3, bin_cap);
             ++out->kernel_launches;
-            uint32_t n_tasks = 1, level = 0;
+            uint32_t n_tasks = 1, n_bins = 1, level = 0;
             while (n_tasks > 0) {
-                uint32_t words = n_tasks * SAH_BINS * SAH_REC;
-                k_sah_init_bins<<<(words + 255) / 256, 256, 0, st>>>(sah_bins, words);
+                uint32_t words = n_bins * SAH_TASK_WORDS;
+                if (words) k_sah_init_bins<<<(words + 255) / 256, 256, 0, st>>>(sah_bins, words);
                 k_sah_bin<<<grid, B, 0, st>>>(perm, pt, n, sah_tasks[0], cen, flat, sah_bins);
-                CK(cudaMemsetAsync(counters + 2, 0, 4, st));
-                k_sah_split<<<(n_tasks + 127) / 128, 128, 0, st>>>(sah_tasks[0], n_tasks, sah_bins, sah_tasks[1],
-                                                                   counters + 2, task_cap, counters, n - 1, b, level,
-                                                                   err);
+                CK(cudaMemsetAsync(counters + 2, 0, 8, st));
+                k_sah_split<<<(n_tasks + 127) / 128, 128, 0, st>>>(sah_tasks[0], n_tasks, sah_bins, perm, cen, flat,
+                                                                   sah_tasks[1],
+                                                                   counters + 2, task_cap, counters + 3, bin_cap,
+                                                                   counters, n - 1, b, level, err);
                 k_sah_partition<<<grid, B, 0, st>>>(perm, pt, n, sah_tasks[0], cen, perm2, pt2);
                 out->kernel_launches += 4;
                 CK(cudaGetLastError());
-                CK(cudaMemcpyAsync(&n_tasks, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+                uint32_t hc2[2];
+                CK(cudaMemcpyAsync(hc2, counters + 2, 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                n_tasks = hc2[0];
+                n_bins = std::min(hc2[1], bin_cap);
                 std::swap(perm, perm2);
                 std::swap(pt, pt2);
                 std::swap(sah_tasks[0], sah_tasks[1]);
