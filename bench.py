@@ -401,18 +401,24 @@ def main(argv=None):
     photons_all = photons * args.steps * world
     rays_all = (st["rays_closest"] + st["rays_shadow"] + st["rays_photon"]) * world
 
-    # ---- end to end through the C ABI with host buffers (camera in, RGBA8 out)
-    import numpy as np
-
-    ldr = np.zeros((h, w, 4), np.uint8)
+    # ---- end to end through the C ABI with host buffers: the camera uniform goes
+    # in from pinned memory each step, and each step's RGBA8 image comes back to
+    # pinned host memory (srt_read_ldr_async); the host waits for frame k's image
+    # after launching frame k + 1, and for the last one before the clock stops
     e2e_steps = 0 if args.no_e2e else max(8, args.steps // 4)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
+    checksum = 0
+    tickets = []
     t0 = time.perf_counter()
     for k in range(e2e_steps):
         r.render(cam_u(args.warmup + args.steps + k))
-        ldr[:] = r.read_ldr()
+        tickets.append(r.read_ldr_async())
+        if k >= 1:
+            checksum += int(r.ldr_wait(tickets[k - 1])[h // 2, w // 2, 0])
+    if e2e_steps:
+        checksum += int(r.ldr_wait(tickets[-1])[h // 2, w // 2, 0])
     t1 = time.perf_counter()
     te = torch.tensor([t1 - t0], dtype=torch.float64, device=f"cuda:{local_rank}")
     if dist:

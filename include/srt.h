@@ -322,6 +322,15 @@ srt_status srt_read_accum_f64(srt_renderer* r, double* rgba);
 /* Tonemapped RGBA8 storage texture (shader.wgsl:809-822), row 0 = bottom
  * row, `pitch` bytes per row (>= 4*width). */
 srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t pitch);
+/* Read-back without a stall (no reference counterpart): enqueues, after the
+ * frames rendered so far, a copy of the RGBA8 image (row 0 first, tightly
+ * packed) into one of two pinned host slots the renderer owns, and returns
+ * a ticket.  srt_ldr_wait(ticket) blocks until that copy has landed and
+ * points *pixels at it; the slot is reused by the second read_ldr_async
+ * after it, so a ticket is valid until then.  A frame loop that renders
+ * frame k+1 before waiting for frame k's ticket keeps the GPU busy. */
+srt_status srt_read_ldr_async(srt_renderer* r, uint32_t* ticket);
+srt_status srt_ldr_wait(srt_renderer* r, uint32_t ticket, const uint8_t** pixels);
 /* Engine::save_screenshot + ScreenshotSaver (engine.rs:191-244,
  * screenshot.rs:27-103): row flip, sRGB OETF of the 8-bit values, PNG file. */
 srt_status srt_save_screenshot(srt_renderer* r, const char* path);

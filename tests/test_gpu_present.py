@@ -79,3 +79,33 @@ def test_renderer_blit_and_splat(srt, ctx):
     np.testing.assert_array_equal(r.splat_photons(u, window), srt.photon_splat(ctx, photons, u, window))
     r.close()
     scene.close()
+
+
+@pytest.mark.gpu
+def test_async_ldr_readback(srt, ctx):
+    """srt_read_ldr_async + srt_ldr_wait return each frame's image (pinned
+    slots used in turn) while the next frame is already enqueued."""
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b.build(ctx)
+    w, h = 64, 48
+    p = srt.default_params(photons_per_frame=1 << 14)
+    ra, rs = srt.Renderer(ctx, scene, w, h, p), srt.Renderer(ctx, scene, w, h, p)
+    ctl = srt.CameraController(*cam)
+    tickets, got, want = [], [], []
+    for f in range(5):
+        u = ctl.build_uniform(w / h, f)
+        ra.render(u)
+        tickets.append(ra.read_ldr_async())
+        if f >= 1:
+            got.append(ra.ldr_wait(tickets[f - 1]).copy())
+        rs.render(u)
+        want.append(rs.read_ldr())
+    got.append(ra.ldr_wait(tickets[-1]).copy())
+    for g, x in zip(got, want):
+        np.testing.assert_array_equal(g, x)
+    with pytest.raises(srt.SrtError):
+        ra.ldr_wait(tickets[0])  # its slot has been reused
+    ra.close()
+    rs.close()
+    scene.close()

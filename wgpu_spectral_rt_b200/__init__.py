@@ -196,6 +196,8 @@ SIGNATURES = {
     "srt_scene_read_lights": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
     "srt_scene_read_bvh": (_I, [_P, _P, C.c_uint64, _P, C.c_uint64]),
     "srt_ctx_set_bvh_builder": (_I, [_P, _I]),
+    "srt_read_ldr_async": (_I, [_P, C.POINTER(_U32)]),
+    "srt_ldr_wait": (_I, [_P, _U32, C.POINTER(C.POINTER(C.c_uint8))]),
     "srt_guide_param_count": (_U32, []),
     "srt_guide_default_weights": (_I, [C.c_uint64, _P, _U32]),
     "srt_renderer_guide_get_weights": (_I, [_P, _P, _U32]),
@@ -492,6 +494,19 @@ class Renderer:
         out = np.zeros((self.target_height, self.target_width, 4), np.uint8)
         _check(lib().srt_read_ldr_rgba8(self.h, ptr(out), 4 * self.target_width), self.ctx.h)
         return out
+
+    def read_ldr_async(self) -> int:
+        """Enqueues a read-back of the current image into a pinned slot; returns its ticket."""
+        t = C.c_uint32()
+        _check(lib().srt_read_ldr_async(self.h, C.byref(t)), self.ctx.h)
+        return t.value
+
+    def ldr_wait(self, ticket: int) -> np.ndarray:
+        """The image of `ticket` once its copy has landed (a view of the pinned slot, valid
+        until the second read_ldr_async after it)."""
+        p = C.POINTER(C.c_uint8)()
+        _check(lib().srt_ldr_wait(self.h, ticket, C.byref(p)), self.ctx.h)
+        return np.ctypeslib.as_array(p, shape=(self.target_height, self.target_width, 4))
 
     def save_screenshot(self, path: str | os.PathLike):
         _check(lib().srt_save_screenshot(self.h, str(path).encode()), self.ctx.h)

@@ -630,6 +630,10 @@ struct srt_renderer {
     double ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // photon, -, closest, shade, shadow, finalize, raygen, guide training
     std::vector<cudaEvent_t> ev;
     GuideArgs guide{};  // SRT_FLAG_GUIDING only
+    // asynchronous RGBA8 read-back: two pinned slots used in turn
+    uint8_t* ldr_pinned[2] = {nullptr, nullptr};
+    cudaEvent_t ldr_ev[2] = {nullptr, nullptr};
+    uint32_t ldr_calls = 0;
 
     ~srt_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -639,6 +643,10 @@ struct srt_renderer {
         for (auto& e : ev) cudaEventDestroy(e);
         cudaFree(cam_dev);
         cudaFreeHost(cam_ring);
+        for (int k = 0; k < 2; ++k) {
+            cudaFreeHost(ldr_pinned[k]);
+            if (ldr_ev[k]) cudaEventDestroy(ldr_ev[k]);
+        }
         cudaFree(counters);
         cudaFree(stats);
         cudaFree(err);
@@ -980,6 +988,35 @@ extern "C" srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t
     CUDA_TRY(c, cudaMemcpy2DAsync(out, pitch, r->ldr, 4 * r->w, 4 * r->w, r->h, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_read_ldr_async(srt_renderer* r, uint32_t* ticket) {
+    if (!r || !ticket) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    const size_t bytes = (size_t)4 * r->w * r->h;
+    if (!r->ldr_pinned[0]) {
+        for (int k = 0; k < 2; ++k) {
+            CUDA_TRY(c, cudaMallocHost((void**)&r->ldr_pinned[k], bytes));
+            CUDA_TRY(c, cudaEventCreateWithFlags(&r->ldr_ev[k], cudaEventDisableTiming));
+        }
+    }
+    const uint32_t slot = r->ldr_calls & 1u;
+    CUDA_TRY(c, cudaEventSynchronize(r->ldr_ev[slot]));  // the slot's previous copy has landed
+    CUDA_TRY(c, cudaMemcpyAsync(r->ldr_pinned[slot], r->ldr, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaEventRecord(r->ldr_ev[slot], c->stream));
+    *ticket = r->ldr_calls++;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_ldr_wait(srt_renderer* r, uint32_t ticket, const uint8_t** pixels) {
+    if (!r || !pixels || !r->ldr_pinned[0] || ticket >= r->ldr_calls || ticket + 2u < r->ldr_calls)
+        return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaEventSynchronize(r->ldr_ev[ticket & 1u]));
+    *pixels = r->ldr_pinned[ticket & 1u];
+    return SRT_OK;
 }
 
 extern "C" srt_status srt_save_screenshot(srt_renderer* r, const char* path) {
