@@ -460,6 +460,27 @@ SRT_DEV uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xFFu; }
 SRT_DEV float qbyte(uint32_t w, uint32_t k) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | k)); }
 SRT_DEV float unbias(float a, float b) { return fmaf(-8388608.0f, a, b); }
 
+// Two fused multiply-adds: one packed fma.rn.f32x2 with SRT_TRAV_FMA2 (the
+// slab test of a child computes its near and far plane of an axis at once),
+// two scalar ones otherwise.  Both round each lane once, like fmaf.
+#ifndef SRT_TRAV_FMA2
+#define SRT_TRAV_FMA2 0
+#endif
+SRT_DEV float2 fma2(float2 a, float2 b, float2 c) {
+#if SRT_TRAV_FMA2
+    uint64_t x, y, z, r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b.x), "f"(b.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(z) : "f"(c.x), "f"(c.y));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(x), "l"(y), "l"(z));
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+#else
+    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+
 struct TravCounters {
     unsigned long long* nodes;
     unsigned long long* tris;
@@ -574,14 +595,14 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
         for (int i = 0; i < 8; ++i) {
             const uint32_t k = (uint32_t)(i & 3);
             uint32_t m = byte_of(i < 4 ? meta0 : meta1, k);
-            float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, k), ax, bx);
-            float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, k), ay, by);
-            float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, k), az, bz);
-            float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, k), ax, bx);
-            float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, k), ay, by);
-            float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, k), az, bz);
-            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
-            float tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest)) * robust;
+            const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
+                                   make_float2(ax, ax), make_float2(bx, bx));
+            const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
+                                   make_float2(ay, ay), make_float2(by, by));
+            const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
+                                   make_float2(az, az), make_float2(bz, bz));
+            float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, ray.tmin));
+            float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, tbest)) * robust;
             if (m != 0u && tn <= tf) {
                 uint32_t c = m >> 5;
                 if (c == 7u)
@@ -747,14 +768,14 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
     for (int i = 0; i < 8; ++i) {
         const uint32_t k = (uint32_t)(i & 3);
         uint32_t m = byte_of(i < 4 ? w1.z : w1.w, k);
-        float tnx = fmaf(qbyte(i < 4 ? nx0 : nx1, k), ax, bx);
-        float tny = fmaf(qbyte(i < 4 ? ny0 : ny1, k), ay, by);
-        float tnz = fmaf(qbyte(i < 4 ? nz0 : nz1, k), az, bz);
-        float tfx = fmaf(qbyte(i < 4 ? fx0 : fx1, k), ax, bx);
-        float tfy = fmaf(qbyte(i < 4 ? fy0 : fy1, k), ay, by);
-        float tfz = fmaf(qbyte(i < 4 ? fz0 : fz1, k), az, bz);
-        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, T.tmin));
-        float tf = fminf(fminf(tfx, tfy), fminf(tfz, T.tbest)) * robust;
+        const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
+                               make_float2(ax, ax), make_float2(bx, bx));
+        const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
+                               make_float2(ay, ay), make_float2(by, by));
+        const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
+                               make_float2(az, az), make_float2(bz, bz));
+        float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, T.tmin));
+        float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, T.tbest)) * robust;
         if (m != 0u && tn <= tf) {
             uint32_t c = m >> 5;
             if (c == 7u) hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
