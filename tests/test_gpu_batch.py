@@ -99,3 +99,78 @@ def test_handles_destroyed_in_any_order(srt):
     scene.close()
     batch.close()
     r.close()
+
+
+def _guided(srt, p, frozen):
+    p.flags |= srt.FLAG_GUIDING | (srt.FLAG_GUIDE_FROZEN if frozen else 0)
+    return p
+
+
+def test_batch_guided_matches_single_scene_renders(srt, ctx):
+    """Guided scenes of a batch have their Lambert continuations sampled by one
+    grouped tcgen05 launch per bounce, whose tiles load the network of their
+    own scene; with frozen networks (a different one per scene) the images
+    equal those of the same renderers rendered alone.  The middle scene is
+    plain (a mixed batch)."""
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    params = _params(srt)
+    params[0] = _guided(srt, params[0], True)
+    params[2] = _guided(srt, params[2], True)
+    weights = {0: srt.guide_default_weights(11), 2: srt.guide_default_weights(12)}
+    batch = srt.Batch(ctx, scenes, SIZES, params)
+    for i, w in weights.items():
+        batch.renderers[i].set_guide_weights(w)
+    frames = 3
+    for f in range(frames):
+        batch.render(_cams(ctls, f))
+    ctx.synchronize()
+    for i, (scene, (w, h)) in enumerate(zip(scenes, SIZES)):
+        r = srt.Renderer(ctx, scene, w, h, params[i])
+        if i in weights:
+            r.set_guide_weights(weights[i])
+        for f in range(frames):
+            r.render(ctls[i].build_uniform(w / h, f))
+        np.testing.assert_array_equal(batch.renderers[i].read_accum(), r.read_accum())
+        r.close()
+    batch.close()
+
+
+def test_batch_guided_training_matches_single_scene_training(srt, ctx):
+    """The grouped training step (targets, forward/backward, weight gradients,
+    Adam: one launch each for all guided scenes) moves every scene's network
+    as the single-renderer step does: after one frame the two updates agree
+    up to the summation order of the gradients (Adam's first step is
+    lr * g / (|g| + eps), so only parameters with |g| near eps may differ)."""
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    params = [_guided(srt, p, False) for p in _params(srt)]
+    lr = 1e-4
+    w0 = [srt.guide_default_weights(21 + i) for i in range(3)]
+    batch = srt.Batch(ctx, scenes, SIZES, params)
+    for i, x in enumerate(batch.renderers):
+        x.set_guide_weights(w0[i])
+        x.configure_guide(lr=lr)
+    batch.render(_cams(ctls, 0))
+    ctx.synchronize()
+    for i, (scene, (w, h)) in enumerate(zip(scenes, SIZES)):
+        r = srt.Renderer(ctx, scene, w, h, params[i])
+        r.set_guide_weights(w0[i])
+        r.configure_guide(lr=lr)
+        r.render(ctls[i].build_uniform(w / h, 0))
+        ref, got = r.guide_weights(), batch.renderers[i].guide_weights()
+        assert r.guide_info()["adam_steps"] == 1
+        assert batch.renderers[i].guide_info()["adam_steps"] == 1
+        moved = np.abs(ref - w0[i]) > 0.5 * lr
+        assert moved.mean() > 0.1
+        d = np.abs(got - ref)
+        assert d.max() <= 2 * lr + 1e-6
+        assert (d[moved] <= 1e-2 * lr).mean() > 0.99
+        r.close()
+    for f in range(1, 4):
+        batch.render(_cams(ctls, f))
+    ctx.synchronize()
+    for x in batch.renderers:
+        assert x.guide_info()["adam_steps"] == 4
+        assert np.all(np.isfinite(x.read_accum()))
+    batch.close()

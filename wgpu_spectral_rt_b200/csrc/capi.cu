@@ -701,10 +701,14 @@ struct srt_renderer {
         if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
         return n + launch_raygen(args, st);
     }
-    int record_shade(uint32_t b, cudaStream_t st) { return b < p.max_depth ? launch_bounce(args, b, st, 2) : 0; }
-    int record_end(cudaStream_t st) {
+    // guide = false: the guided continuation and the training step are left
+    // to the batch's grouped guide kernels
+    int record_shade(uint32_t b, cudaStream_t st, bool guide) {
+        return b < p.max_depth ? launch_bounce(args, b, st, guide ? 2 : 4) : 0;
+    }
+    int record_end(cudaStream_t st, bool guide) {
         int n = launch_finalize(args, st) + launch_frame_stats(args, st);
-        if (args.guiding) n += launch_guide_train(args, st);
+        if (args.guiding && guide) n += launch_guide_train(args, st);
         return n;
     }
     MultiTraceItem trace_item(uint32_t b, bool shadow) const {
@@ -728,6 +732,7 @@ struct srt_renderer {
         return it;
     }
     bool batch_owned = false;
+    uint32_t args_gen = 0;  // bumped when kernel arguments change outside a capture (a batch re-captures)
 };
 
 extern "C" srt_params srt_params_default(void) {
@@ -1276,6 +1281,7 @@ extern "C" srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, ui
     if (lr >= 0.0f) r->guide.lr = lr;
     if (batch > 0) r->guide.batch = batch;
     r->args.guide = r->guide;
+    r->args_gen += 1;
     if (r->graph) {  // both are kernel arguments of the captured frame
         cudaGraphExecDestroy(r->graph);
         r->graph = nullptr;
@@ -1335,6 +1341,7 @@ extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     r->guide.tc = kind == SRT_GUIDE_INFER_TCGEN05 ? 1 : 0;
     r->args.guide = r->guide;
+    r->args_gen += 1;
     if (r->graph) {  // the choice is baked into the captured frame
         cudaGraphExecDestroy(r->graph);
         r->graph = nullptr;
@@ -1521,7 +1528,9 @@ struct srt_batch {
     cudaEvent_t up_ev[2] = {};
     int up_i = 0;
     MultiTraceItem* items_dev = nullptr;  // [2 kinds][MAX_BOUNCES][MAX_BATCH]
-    uint32_t* fetch_dev = nullptr;        // [2 kinds][MAX_BOUNCES]
+    uint32_t* fetch_dev = nullptr;        // [3][MAX_BOUNCES]: closest-hit, shadow, guide chunk counters
+    FrameArgs* guide_items_dev = nullptr; // [MAX_BATCH] frame arguments of the guided renderers
+    std::vector<uint32_t> graph_gen;      // the renderers' args_gen at capture
     std::vector<cudaStream_t> side;
     cudaStream_t cap = nullptr;
     cudaEvent_t fork_ev = nullptr;
@@ -1547,6 +1556,7 @@ struct srt_batch {
         cudaFreeHost(cams_host);
         cudaFree(items_dev);
         cudaFree(fetch_dev);
+        cudaFree(guide_items_dev);
         for (srt_renderer* x : r) {
             if (x) {
                 x->batch_owned = false;
@@ -1558,6 +1568,8 @@ struct srt_batch {
 
     srt_status capture(const std::vector<uint8_t>& active) {
         srt_ctx* c = ctx;
+        // frames in flight read the item tables that are rewritten below
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
@@ -1573,6 +1585,17 @@ struct srt_batch {
                 items[((size_t)1 * MAX_BOUNCES + b) * MAX_BATCH + k] = r[act[k]]->trace_item(b, true);
             }
         CUDA_TRY(c, cudaMemcpy(items_dev, items.data(), items.size() * sizeof(MultiTraceItem), cudaMemcpyHostToDevice));
+        // guided renderers: their continuations and training steps run as
+        // grouped launches over all of them (their frame arguments are
+        // uploaded once the capture has recorded every per-renderer launch)
+        std::vector<srt_renderer*> guided;
+        uint32_t guide_depth = 0;
+        for (int k = 0; k < na; ++k)
+            if (r[act[k]]->args.guiding) {
+                guided.push_back(r[act[k]]);
+                guide_depth = std::max(guide_depth, r[act[k]]->p.max_depth);
+            }
+        const int ng = (int)guided.size();
         cudaGraph_t g;
         int n = 0;
         CUDA_TRY(c, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
@@ -1585,22 +1608,35 @@ struct srt_batch {
             }
             for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
         };
-        cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 2 * MAX_BOUNCES, cap);
+        cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 3 * MAX_BOUNCES, cap);
         fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_begin(s); });
         for (uint32_t b = 0; b < max_depth; ++b) {
             n += launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
                                     (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
-            fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s); });
+            fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
+            if (ng && b + 1 < guide_depth)
+                n += launch_guide_infer_multi(guide_items_dev, ng, b, fetch_dev + 2 * MAX_BOUNCES + b, c->sm_count,
+                                              cap);
             n += launch_trace_multi(items_dev + ((size_t)MAX_BOUNCES + b) * MAX_BATCH, na, 1, small_stack,
                                     fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
         }
-        fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_end(s); });
+        fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_end(s, false); });
+        if (ng) n += launch_guide_train_multi(guide_items_dev, ng, c->sm_count, cap);
         cudaError_t e = cudaStreamEndCapture(cap, &g);
         CUDA_TRY(c, e);
+        if (ng) {
+            std::vector<FrameArgs> gargs;
+            for (srt_renderer* x : guided) gargs.push_back(x->args);
+            e = cudaMemcpy(guide_items_dev, gargs.data(), ng * sizeof(FrameArgs), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) cudaGraphDestroy(g);
+            CUDA_TRY(c, e);
+        }
         e = cudaGraphInstantiate(&graph, g, 0);
         cudaGraphDestroy(g);
         CUDA_TRY(c, e);
         graph_active = active;
+        graph_gen.clear();
+        for (srt_renderer* x : r) graph_gen.push_back(x->args_gen);
         graph_launches = n;
         return SRT_OK;
     }
@@ -1615,7 +1651,9 @@ struct srt_batch {
         bool any = false;
         for (uint8_t a : active) any = any || a;
         if (!any) return SRT_OK;
-        if (!graph || active != graph_active) {
+        bool stale = graph_gen.size() != n;
+        for (size_t i = 0; i < n && !stale; ++i) stale = graph_gen[i] != r[i]->args_gen;
+        if (!graph || active != graph_active || stale) {
             srt_status s = capture(active);
             if (s != SRT_OK) return s;
         }
@@ -1652,7 +1690,8 @@ extern "C" srt_status srt_batch_create(srt_ctx* c, uint32_t n, srt_scene* const*
     CUDA_TRY(c, cudaMemset(B->cams_dev, 0, n * sizeof(srt_camera_uniform)));
     for (auto& e : B->up_ev) CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CUDA_TRY(c, dev_alloc(&B->items_dev, (size_t)2 * MAX_BOUNCES * MAX_BATCH));
-    CUDA_TRY(c, dev_alloc(&B->fetch_dev, (size_t)2 * MAX_BOUNCES));
+    CUDA_TRY(c, dev_alloc(&B->fetch_dev, (size_t)3 * MAX_BOUNCES));
+    CUDA_TRY(c, dev_alloc(&B->guide_items_dev, (size_t)MAX_BATCH));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
     CUDA_TRY(c, cudaEventCreateWithFlags(&B->fork_ev, cudaEventDisableTiming));
     B->side.assign(n, nullptr);

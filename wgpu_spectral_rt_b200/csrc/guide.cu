@@ -15,6 +15,7 @@
 // gradient product over the samples, and Adam on FP32 master weights.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -433,7 +434,7 @@ SRT_DEV bool finish_vertex(const FrameArgs& a, uint32_t bounce, uint32_t frame, 
 // Russian roulette, next queue; plus the recording of training samples.
 __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32_t bounce) {
     const GuideArgs& G = a.guide;
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
     unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
@@ -514,8 +515,9 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32
 // Per record: the radiance that arrived along the sampled direction and the
 // training weight F / p = L f cos / p.  Records whose path ended before its
 // next vertex carry no later radiance (L = 0).
-__global__ void k_guide_targets(FrameArgs a) {
+SRT_DEV void guide_targets(const FrameArgs& a) {
     const GuideArgs& G = a.guide;
+    if (!G.train) return;
     uint32_t n = min(G.gc->records, G.batch);
     float local = 0.f;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -539,13 +541,16 @@ __global__ void k_guide_targets(FrameArgs a) {
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xFFFFFFFFu, local, o);
     if ((threadIdx.x & 31) == 0 && local != 0.f) atomicAdd(&G.gc->weight_sum, local);
 }
+__global__ void k_guide_targets(FrameArgs a) { guide_targets(a); }
+// many renderers: blockIdx.y = item
+__global__ void k_guide_targets_multi(const FrameArgs* __restrict__ items) { guide_targets(items[blockIdx.y]); }
 
 // Forward + backward of 16 records per warp: stores the encoded inputs,
 // post-ReLU activations and per-layer deltas (bf16) for the weight-gradient
 // product.  Loss per sample (weight w normalised by the batch mean):
 //   -w log q(omega) for the lobes, -w log(sel q + (1 - sel) p_bsdf) for sel.
-__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) {
-    extern __shared__ __align__(16) unsigned char smem[];
+SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
+    extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     __nv_bfloat16* swt = sw + SW_ELEMS;
     float* sb = reinterpret_cast<float*>(swt + SWT_ELEMS);
@@ -693,13 +698,19 @@ __global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) {
         __syncwarp();
     }
 }
+__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) { guide_fwdbwd(G); }
+// many renderers (blockIdx.y = item), those that train
+__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd_multi(const FrameArgs* __restrict__ items) {
+    const GuideArgs& G = items[blockIdx.y].guide;
+    if (G.train) guide_fwdbwd(G);
+}
 
 // Weight gradients dW_l = sum_s delta_l[s]^T a_{l-1}[s] (and bias sums),
 // split over the samples; job (blockIdx.y): 0, 1 = layer 0 input halves,
 // 2..5 = layers 1..4.  8 warps: warp w owns output rows 16 (w & 3) .. + 15
 // and input columns 32 (w >> 2) .. + 31 of the 64 x 64 block.
 constexpr int WGRAD_BLOCKS = 64;  // sample splits per job
-__global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) {
+SRT_DEV void guide_wgrad(const GuideArgs& G) {
     __shared__ __align__(16) __nv_bfloat16 sd[32 * g_pad(G_HID)];
     __shared__ __align__(16) __nv_bfloat16 sa[32 * g_pad(G_HID)];
     const uint32_t n = min(G.gc->records, G.batch);
@@ -775,10 +786,16 @@ __global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) {
     }
     if (job != 1 && threadIdx.x < nout && bsum != 0.f) atomicAdd(G.net.grad + g_boff(l) + threadIdx.x, bsum);
 }
+__global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) { guide_wgrad(G); }
+// many renderers: blockIdx.z = item
+__global__ void __launch_bounds__(256) k_guide_wgrad_multi(const FrameArgs* __restrict__ items) {
+    const GuideArgs& G = items[blockIdx.z].guide;
+    if (G.train) guide_wgrad(G);
+}
 
 // Adam on the FP32 master weights (gradients are sums over the batch and
 // are divided by its size), then the bf16 copies; clears the gradients.
-__global__ void k_guide_adam(GuideArgs G) {
+SRT_DEV void guide_adam(const GuideArgs& G) {
     const uint32_t n = min(G.gc->records, G.batch);
     if (n == 0) return;
     const float inv = 1.0f / (float)n;
@@ -804,10 +821,16 @@ __global__ void k_guide_adam(GuideArgs G) {
         }
     }
 }
+__global__ void k_guide_adam(GuideArgs G) { guide_adam(G); }
+// many renderers: blockIdx.y = item
+__global__ void k_guide_adam_multi(const FrameArgs* __restrict__ items) {
+    const GuideArgs& G = items[blockIdx.y].guide;
+    if (G.train) guide_adam(G);
+}
 
 // Next frame's recording threshold (of 65536) so that about 90 % of the
 // training batch fills; counts the Adam step; clears the per-frame counters.
-__global__ void k_guide_frame_end(GuideArgs G, int trained) {
+SRT_DEV void guide_frame_end(const GuideArgs& G, int trained) {
     GuideCounters* gc = G.gc;
     if (threadIdx.x < 32) gc->verts[threadIdx.x] = 0u;
     if (threadIdx.x != 0) return;
@@ -821,12 +844,18 @@ __global__ void k_guide_frame_end(GuideArgs G, int trained) {
     gc->candidates = 0u;
     gc->weight_sum = 0.f;
 }
+__global__ void k_guide_frame_end(GuideArgs G, int trained) { guide_frame_end(G, trained); }
+// many renderers: one block per item
+__global__ void k_guide_frame_end_multi(const FrameArgs* __restrict__ items) {
+    const GuideArgs& G = items[blockIdx.x].guide;
+    guide_frame_end(G, G.train);
+}
 
 // ---------------------------------------------------------------- test kernels
 // Forward pass of n samples (inputs [n][10]) -> raw outputs [n][48].
 __global__ void __launch_bounds__(GWI * 32, 2) k_guide_test_forward(GuideNet net, const float* __restrict__ x,
                                                                     uint32_t n, float* __restrict__ y) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
     unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
@@ -900,6 +929,10 @@ constexpr uint32_t TC_SMEM = TC_BAR_OFF + 8 * TC_GROUPS + 16;
 static_assert(tc_woff(4) + G_OUT * G_HID * 2 == tc_aoff(0), "tcgen05 weight layout");
 static_assert(tc_aoff(0) % 128 == 0 && TC_B_OFF % 16 == 0 && TC_BAR_OFF % 8 == 0, "tcgen05 shared-memory alignment");
 static_assert(2 * (TC_SMEM + 1024) <= 228 * 1024, "two blocks per SM");
+// the grouped kernel: rows per chunk, and its chunk table after the single-renderer layout
+constexpr uint32_t TC_CHUNK = TC_ROWS * TC_GROUPS;
+constexpr uint32_t TC_SMEM_MULTI = TC_SMEM + 4 * (MAX_BATCH + 1) + 8;
+static_assert(TC_SMEM % 4 == 0 && 2 * (TC_SMEM_MULTI + 1024) <= 228 * 1024, "grouped kernel: two blocks per SM");
 
 // Barrier of one 128-thread group (ids 1 and 2; 0 is the block barrier).
 SRT_DEV void group_sync(uint32_t id) { asm volatile("bar.sync %0, 128;\n" ::"r"(id) : "memory"); }
@@ -1069,9 +1102,9 @@ SRT_DEV float3 mix_sample(const Mix& m, float u0, float u1, float u2) {
     return vmf_sample_e2(mu, k, e2, u1, u2);
 }
 
-// Block set-up (tensor-memory allocation, mbarriers, weights) and this
-// thread's group.
-SRT_DEV TcGroup tc_setup(unsigned char* smem, const GuideNet& net, float*& sb) {
+// Block set-up (tensor-memory allocation, mbarriers, the weights of `net`
+// unless null) and this thread's group.
+SRT_DEV TcGroup tc_setup(unsigned char* smem, const GuideNet* net, float*& sb) {
     sb = reinterpret_cast<float*>(smem + TC_B_OFF);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TC_BAR_OFF);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_BAR_OFF + 8 * TC_GROUPS);
@@ -1080,7 +1113,7 @@ SRT_DEV TcGroup tc_setup(unsigned char* smem, const GuideNet& net, float*& sb) {
         tmem_relinquish();
     }
     if (threadIdx.x < TC_GROUPS) mbar_init(bars + threadIdx.x, 1);
-    load_weights_tc(net, smem, sb);
+    if (net) load_weights_tc(*net, smem, sb);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -1108,70 +1141,133 @@ SRT_DEV void tc_teardown(const TcGroup& g, bool ok, uint32_t phase, uint32_t* er
 
 }  // namespace
 
+// One 128-row tile of guided vertices (rows base .. base + 127 of n) of the
+// renderer `a`: encoding, the network on the tensor cores, mixture
+// sampling, the vertex continuation and the push into the next queue.
+// False when the network's MMAs did not complete (nothing was written).
+SRT_DEV bool infer_tile_tc(const FrameArgs& a, uint32_t bounce, const TcGroup& grp, const unsigned char* smem,
+                           const float* sb, uint32_t base, uint32_t n, uint32_t& phase) {
+    const GuideArgs& G = a.guide;
+    const DevScene& S = a.scene;
+    const uint32_t frame = a.cam->frame_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t v = base + grp.row;
+    const bool valid = v < n;
+    float x[G_IN];
+    float4 p = splat4(0.f), nn = splat4(0.f);
+    if (valid) {
+        p = G.gv.p[v];
+        nn = G.gv.n[v];
+        float4 wo = G.gv.wo[v];
+        vertex_inputs(xyz(p), xyz(nn), xyz(wo), p.w, S.bmin, S.binv, x);
+    } else {
+        for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
+    }
+    encode_row_tc(x, grp.A, grp.row);
+    fence_async_smem();
+    group_sync(grp.bar);
+    float raw[G_OUT];
+    if (!mlp_tc(grp, smem, sb, phase, raw)) return false;
+    bool alive = false;
+    uint32_t id = 0;
+    if (valid) {
+        Mix m;
+        mixture(raw, m);
+        id = G.gv.id[v];
+        const uint4 misc = a.pb.misc[id];
+        uint32_t s = misc.x;
+        const float3 ffn = xyz(nn);
+        float3 dir;
+        if (rng_next(s) < m.sel) {
+            const float u0 = rng_next(s), u1 = rng_next(s), u2 = rng_next(s);
+            dir = mix_sample(m, u0, u1, u2);
+        } else {
+            float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
+            if (length(d) < 0.001f) d = ffn;
+            dir = normalize(d);
+        }
+        alive = finish_vertex(a, bounce, frame, v, id, p, ffn, misc, s, dir, m.sel, mix_pdf(m, dir));
+    }
+    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, alive);
+    uint32_t slot_base = 0;
+    if (mask) {
+        const int leader = __ffs(mask) - 1;
+        if ((int)lane == leader) slot_base = atomicAdd(&a.counters->paths[bounce + 1], (uint32_t)__popc(mask));
+        slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, leader);
+    }
+    if (alive) a.pb.queue[(bounce + 1) & 1][slot_base + __popc(mask & ((1u << lane) - 1u))] = id;
+    return true;
+}
+
 __global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_infer_tc(FrameArgs a, uint32_t bounce) {
     const GuideArgs& G = a.guide;
     extern __shared__ __align__(1024) unsigned char smem[];
     const uint32_t n = G.gc->verts[bounce];
     if (blockIdx.x * TC_ROWS * TC_GROUPS >= n) return;
     float* sb;
-    const TcGroup grp = tc_setup(smem, G.net, sb);
-    const DevScene& S = a.scene;
-    const uint32_t frame = a.cam->frame_count;
-    const uint32_t lane = threadIdx.x & 31u;
+    const TcGroup grp = tc_setup(smem, &G.net, sb);
     uint32_t phase = 0;
     bool ok = true;
     for (uint32_t base = (blockIdx.x * TC_GROUPS + threadIdx.x / TC_ROWS) * TC_ROWS; base < n;
          base += gridDim.x * TC_GROUPS * TC_ROWS) {
-        const uint32_t v = base + grp.row;
-        const bool valid = v < n;
-        float x[G_IN];
-        float4 p = splat4(0.f), nn = splat4(0.f);
-        if (valid) {
-            p = G.gv.p[v];
-            nn = G.gv.n[v];
-            float4 wo = G.gv.wo[v];
-            vertex_inputs(xyz(p), xyz(nn), xyz(wo), p.w, S.bmin, S.binv, x);
-        } else {
-            for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
-        }
-        encode_row_tc(x, grp.A, grp.row);
-        fence_async_smem();
-        group_sync(grp.bar);
-        float raw[G_OUT];
-        if (!mlp_tc(grp, smem, sb, phase, raw)) {
+        if (!infer_tile_tc(a, bounce, grp, smem, sb, base, n, phase)) {
             ok = false;
             break;
         }
-        bool alive = false;
-        uint32_t id = 0;
-        if (valid) {
-            Mix m;
-            mixture(raw, m);
-            id = G.gv.id[v];
-            const uint4 misc = a.pb.misc[id];
-            uint32_t s = misc.x;
-            const float3 ffn = xyz(nn);
-            float3 dir;
-            if (rng_next(s) < m.sel) {
-                const float u0 = rng_next(s), u1 = rng_next(s), u2 = rng_next(s);
-                dir = mix_sample(m, u0, u1, u2);
-            } else {
-                float3 d = ffn + random_unit_vector(s);  // shader.wgsl:462-466
-                if (length(d) < 0.001f) d = ffn;
-                dir = normalize(d);
-            }
-            alive = finish_vertex(a, bounce, frame, v, id, p, ffn, misc, s, dir, m.sel, mix_pdf(m, dir));
-        }
-        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, alive);
-        uint32_t slot_base = 0;
-        if (mask) {
-            const int leader = __ffs(mask) - 1;
-            if ((int)lane == leader) slot_base = atomicAdd(&a.counters->paths[bounce + 1], (uint32_t)__popc(mask));
-            slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, leader);
-        }
-        if (alive) a.pb.queue[(bounce + 1) & 1][slot_base + __popc(mask & ((1u << lane) - 1u))] = id;
     }
     tc_teardown(grp, ok, phase, a.err);
+}
+
+// Guided vertices of many renderers (the batched renderer) in one persistent
+// launch: a virtual queue concatenates every item's vertices of this bounce,
+// each item padded to whole chunks of TC_CHUNK rows; a block draws chunks
+// from *fetch (zeroed per frame), loads the network of the chunk's item when
+// it differs from the one it holds, and its two groups run the chunk's two
+// 128-row tiles.  Items whose path depth ends at this bounce take no chunk.
+__global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2)
+    k_guide_infer_tc_multi(const FrameArgs* __restrict__ items, int n_items, uint32_t bounce,
+                           uint32_t* __restrict__ fetch) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint32_t* pre = reinterpret_cast<uint32_t*>(smem + TC_SMEM);  // chunk offset of each item, then the total
+    volatile uint32_t* slot = pre + MAX_BATCH + 1;                 // the chunk drawn, by iteration parity
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < n_items; ++i) {
+            pre[i] = acc;
+            const FrameArgs& a = items[i];
+            const uint32_t n = bounce + 1u < a.max_depth ? a.guide.gc->verts[bounce] : 0u;
+            acc += (n + TC_CHUNK - 1u) / TC_CHUNK;
+        }
+        pre[n_items] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = pre[n_items];
+    if (blockIdx.x >= total) return;
+    float* sb;
+    const TcGroup grp = tc_setup(smem, nullptr, sb);
+    const uint32_t g = threadIdx.x / TC_ROWS;
+    int cur = -1;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t it = 0;; ++it) {
+        if (threadIdx.x == 0) slot[it & 1u] = atomicAdd(fetch, 1u);
+        // the barrier also ends every group's previous tile (weights free to reload)
+        if (__syncthreads_or(!ok)) break;
+        const uint32_t c = slot[it & 1u];
+        if (c >= total) break;
+        int k = 0;
+        while (k + 1 < n_items && pre[k + 1] <= c) ++k;
+        const FrameArgs& a = items[k];
+        if (k != cur) {
+            load_weights_tc(a.guide.net, smem, sb);
+            __syncthreads();
+            cur = k;
+        }
+        const uint32_t n = a.guide.gc->verts[bounce];
+        const uint32_t base = (c - pre[k]) * TC_CHUNK + g * TC_ROWS;
+        if (base < n && !infer_tile_tc(a, bounce, grp, smem, sb, base, n, phase)) ok = false;
+    }
+    tc_teardown(grp, ok, phase, items[cur < 0 ? 0 : cur].err);
 }
 
 // Forward pass of n samples on the tcgen05 path (inputs [n][10] -> raw outputs [n][48]).
@@ -1181,7 +1277,7 @@ __global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_test_forward_t
                                                                                   uint32_t* err) {
     extern __shared__ __align__(1024) unsigned char smem[];
     float* sb;
-    const TcGroup grp = tc_setup(smem, net, sb);
+    const TcGroup grp = tc_setup(smem, &net, sb);
     uint32_t phase = 0;
     bool ok = true;
     for (uint32_t base = (blockIdx.x * TC_GROUPS + threadIdx.x / TC_ROWS) * TC_ROWS; base < n;
@@ -1223,6 +1319,12 @@ cudaError_t guide_configure() {
         e = cudaFuncSetAttribute(k_guide_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_guide_test_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_infer_tc_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_SMEM_MULTI);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_fwdbwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)guide_train_smem());
     return e;
 }
 
@@ -1254,6 +1356,27 @@ int launch_guide_train(const FrameArgs& a, cudaStream_t st) {
     }
     k_guide_frame_end<<<1, 32, 0, st>>>(g, g.train);
     return n + 1;
+}
+
+int launch_guide_infer_multi(const FrameArgs* items, int n_items, uint32_t bounce, uint32_t* fetch, int sm_count,
+                             cudaStream_t st) {
+    if (n_items <= 0) return 0;
+    const uint32_t grid = (uint32_t)(sm_count > 0 ? sm_count : 148) * 2;
+    k_guide_infer_tc_multi<<<grid, TC_ROWS * TC_GROUPS, TC_SMEM_MULTI, st>>>(items, n_items, bounce, fetch);
+    return 1;
+}
+
+int launch_guide_train_multi(const FrameArgs* items, int n_items, int sm_count, cudaStream_t st) {
+    if (n_items <= 0) return 0;
+    const uint32_t sm = (uint32_t)(sm_count > 0 ? sm_count : 148);
+    const uint32_t per = std::max(8u, 2u * sm / (uint32_t)n_items);  // forward/backward blocks per item
+    const uint32_t n = (uint32_t)n_items;
+    k_guide_targets_multi<<<dim3(std::max(8u, 4u * sm / n), n), 256, 0, st>>>(items);
+    k_guide_fwdbwd_multi<<<dim3(per, n), GWT * 32, guide_train_smem(), st>>>(items);
+    k_guide_wgrad_multi<<<dim3(WGRAD_BLOCKS, 6, n), 256, 0, st>>>(items);
+    k_guide_adam_multi<<<dim3((G_NPARAMS + 255) / 256, n), 256, 0, st>>>(items);
+    k_guide_frame_end_multi<<<n, 32, 0, st>>>(items);
+    return 5;
 }
 
 int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st) {

@@ -111,6 +111,13 @@ struct FrameArgs;
 cudaError_t guide_configure();  // raises the dynamic shared-memory limits once per device
 int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st);
 int launch_guide_train(const FrameArgs& a, cudaStream_t st);
+// Many renderers at once (device array of their frame arguments, the batched
+// renderer): the guided vertices of one bounce in one persistent tcgen05
+// launch (fetch: a zeroed chunk counter), and one training step of every
+// item (those with train set) in five grouped launches.
+int launch_guide_infer_multi(const FrameArgs* items, int n_items, uint32_t bounce, uint32_t* fetch, int sm_count,
+                             cudaStream_t st);
+int launch_guide_train_multi(const FrameArgs* items, int n_items, int sm_count, cudaStream_t st);
 // tc: the tcgen05 kernel (err: device error word for an MMA wait that gave up).
 int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, int tc, uint32_t* err,
                               cudaStream_t st);

@@ -668,11 +668,11 @@ int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stag
     int launches = 0;
     uint32_t grid = blocks_for((uint64_t)a.width * a.height, TRACE_BLOCK);
     if (stage == 0 || stage == 1) launches += launch_trace_closest(a, bounce, st);
-    if (stage == 0 || stage == 2) {
+    if (stage == 0 || stage == 2 || stage == 4) {
         if (a.guiding) k_shade<true><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         else k_shade<false><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         ++launches;
-        if (a.guiding && bounce + 1 < a.max_depth) launches += launch_guide_infer(a, bounce, st);
+        if (a.guiding && stage != 4 && bounce + 1 < a.max_depth) launches += launch_guide_infer(a, bounce, st);
         if (a.ray_sort && bounce + 1 < a.max_depth) {
             // 4 passes: the sorted queue lands back in the queue buffer
             uint32_t *sk, *sv;

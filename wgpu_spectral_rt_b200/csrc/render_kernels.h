@@ -103,7 +103,8 @@ struct FrameArgs {
 int launch_photon_pass(FrameArgs& a, cudaStream_t st);
 // Camera paths: raygen, then per bounce trace / shade / shadow; finalize.
 int launch_raygen(const FrameArgs& a, cudaStream_t st);
-int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stage /* 0 all, 1 trace, 2 shade, 3 shadow */);
+int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st,
+                  int stage /* 0 all, 1 trace, 2 shade, 3 shadow, 4 shade without the guided continuation */);
 int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st);  // trace_kernels.cu
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);   // trace_kernels.cu
 // Closest hit for the rays named by queue[0 .. *count) (queue NULL: 0 .. *count),
