@@ -28,7 +28,7 @@ namespace srt {
 namespace {
 
 constexpr int GWI = 8;  // warps per block of the inference kernels (2 blocks per SM)
-constexpr int GWT = 4;  // warps per block of the training forward/backward kernel
+constexpr int GWT = 8;  // warps per block of the training forward/backward kernel (1 block per SM)
 // Per-warp staging of the inference kernels: the encoded rows (16 x 136
 // bf16); the raw outputs (16 x 52 fp32) reuse the same bytes once the
 // first layer has taken its A fragments.
@@ -58,6 +58,12 @@ SRT_DEV uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
 }
+// pack2 of max(lo, 0), max(hi, 0): the conversion applies the ReLU itself.
+SRT_DEV uint32_t pack2_relu(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
 SRT_DEV float2 unpack2(uint32_t u) {
     __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162*>(&u);
     return __bfloat1622float2(v);
@@ -74,6 +80,12 @@ SRT_DEV void load_b2(uint32_t (&b)[4], const __nv_bfloat16* W, int stride, int n
     int t = threadIdx.x & 31;
     const __nv_bfloat16* p = W + (n0 + (t & 7) + 8 * (t >> 4)) * stride + k0 + 8 * ((t >> 3) & 1);
     ldsm4(b, p);
+}
+// The same fragments from B stored [k][n] row-major (transposing loads).
+SRT_DEV void load_b2t(uint32_t (&b)[4], const __nv_bfloat16* B, int stride, int n0, int k0) {
+    int t = threadIdx.x & 31;
+    const __nv_bfloat16* p = B + (k0 + (t & 7) + 8 * ((t >> 3) & 1)) * stride + n0 + 8 * (t >> 4);
+    ldsm4t(b, p);
 }
 
 // One dense layer for the warp's 16 samples: c = a W^T + bias.
@@ -105,10 +117,10 @@ template <int N>
 SRT_DEV void relu_to_a(const float (&c)[N / 8][4], uint32_t (&a)[N / 16][4]) {
 #pragma unroll
     for (int s = 0; s < N / 16; ++s) {
-        a[s][0] = pack2(fmaxf(c[2 * s][0], 0.f), fmaxf(c[2 * s][1], 0.f));
-        a[s][1] = pack2(fmaxf(c[2 * s][2], 0.f), fmaxf(c[2 * s][3], 0.f));
-        a[s][2] = pack2(fmaxf(c[2 * s + 1][0], 0.f), fmaxf(c[2 * s + 1][1], 0.f));
-        a[s][3] = pack2(fmaxf(c[2 * s + 1][2], 0.f), fmaxf(c[2 * s + 1][3], 0.f));
+        a[s][0] = pack2_relu(c[2 * s][0], c[2 * s][1]);
+        a[s][1] = pack2_relu(c[2 * s][2], c[2 * s][3]);
+        a[s][2] = pack2_relu(c[2 * s + 1][0], c[2 * s + 1][1]);
+        a[s][3] = pack2_relu(c[2 * s + 1][2], c[2 * s + 1][3]);
     }
 }
 
@@ -268,7 +280,7 @@ SRT_DEV float half_pdf(const HalfMix& m, float3 w) {
 
 // Loads all layer weights (bf16, padded rows) and biases into shared memory.
 // Every weight block starts on a 16-byte boundary (g_woff(l) is a multiple of 8).
-SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb, bool transposed, __nv_bfloat16* swt) {
+SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb) {
     int off = 0;
     for (int l = 0; l < G_LAYERS; ++l) {
         copy_rows(sw + off, net.wbf + g_woff(l), g_out(l), g_in(l));
@@ -279,27 +291,14 @@ SRT_DEV void load_weights(const GuideNet& net, __nv_bfloat16* sw, float* sb, boo
         for (int i = threadIdx.x; i < g_out(l); i += blockDim.x) sb[bo + i] = net.master[g_boff(l) + i];
         bo += g_out(l);
     }
-    if (transposed) {  // W^T [in][out] of layers 1..4 for the backward pass
-        int o2 = 0;
-        for (int l = 1; l < G_LAYERS; ++l) {
-            copy_rows(swt + o2, net.wtbf + g_woff(l), g_in(l), g_out(l));
-            o2 += g_in(l) * g_pad(g_out(l));
-        }
-    }
     cp_async_wait_all();
 }
 constexpr int SW_ELEMS = G_HID * g_pad(G_ENC) + 3 * G_HID * g_pad(G_HID) + G_OUT * g_pad(G_HID);
-constexpr int SWT_ELEMS = 3 * G_HID * g_pad(G_HID) + G_HID * g_pad(G_OUT);
 constexpr int SB_ELEMS = 4 * G_HID + G_OUT;
 SRT_DEV const __nv_bfloat16* wl(const __nv_bfloat16* sw, int l) {
     int off = 0;
     for (int i = 0; i < l; ++i) off += g_out(i) * g_pad(g_in(i));
     return sw + off;
-}
-SRT_DEV const __nv_bfloat16* wtl(const __nv_bfloat16* swt, int l) {  // l = 1..4
-    int off = 0;
-    for (int i = 1; i < l; ++i) off += g_in(i) * g_pad(g_out(i));
-    return swt + off;
 }
 SRT_DEV const float* bl(const float* sb, int l) { return sb + l * G_HID; }
 
@@ -443,7 +442,7 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32
     float* out = reinterpret_cast<float*>(in);
     const uint32_t n = G.gc->verts[bounce];
     if (blockIdx.x * GWI * 16 >= n) return;
-    load_weights(G.net, sw, sb, false, nullptr);
+    load_weights(G.net, sw, sb);
     __syncthreads();
     const DevScene& S = a.scene;
     const uint32_t frame = a.cam->frame_count;
@@ -552,8 +551,7 @@ __global__ void k_guide_targets_multi(const FrameArgs* __restrict__ items) { gui
 SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
-    __nv_bfloat16* swt = sw + SW_ELEMS;
-    float* sb = reinterpret_cast<float*>(swt + SWT_ELEMS);
+    float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
     unsigned char* wbase = reinterpret_cast<unsigned char*>(sb + SB_ELEMS);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int per_warp = 16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2;
@@ -563,7 +561,7 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
     __nv_bfloat16* d4 = reinterpret_cast<__nv_bfloat16*>(out + 16 * 52);
     const uint32_t n = min(G.gc->records, G.batch);
     if (blockIdx.x * GWT * 16 >= n) return;
-    load_weights(G.net, sw, sb, true, swt);
+    load_weights(G.net, sw, sb);
     __syncthreads();
     const float inv_mean = G.gc->weight_sum > 0.f ? (float)n / G.gc->weight_sum : 0.f;
     const int g = lane >> 2, cq = lane & 3;
@@ -651,13 +649,13 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
             float c[8][4];
 #pragma unroll
             for (int j = 0; j < 8; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
-            const __nv_bfloat16* WT = wtl(swt, l + 1);  // [in = 64][out = K]
+            const __nv_bfloat16* W = wl(sw, l + 1);  // [out = K][in = 64]: B[k][n] = W[k][n]
 #pragma unroll
             for (int s = 0; s < K / 16; ++s) {
 #pragma unroll
                 for (int j = 0; j < 8; j += 2) {
                     uint32_t b[4];
-                    load_b2(b, WT, g_pad(K), 8 * j, 16 * s);
+                    load_b2t(b, W, g_pad(G_HID), 8 * j, 16 * s);
                     mma16816(c[j], da[s], b[0], b[1]);
                     mma16816(c[j + 1], da[s], b[2], b[3]);
                 }
@@ -812,13 +810,7 @@ SRT_DEV void guide_adam(const GuideArgs& G) {
         G.net.master[i] = w;
         int l = 0;
         while (l < 4 && i >= g_woff(l + 1)) ++l;
-        int k = i - g_woff(l);
-        if (k < g_in(l) * g_out(l)) {
-            __nv_bfloat16 h = __float2bfloat16_rn(w);
-            G.net.wbf[i] = h;
-            int o = k / g_in(l), in = k - o * g_in(l);
-            G.net.wtbf[g_woff(l) + in * g_out(l) + o] = h;
-        }
+        if (i - g_woff(l) < g_in(l) * g_out(l)) G.net.wbf[i] = __float2bfloat16_rn(w);
     }
 }
 __global__ void k_guide_adam(GuideArgs G) { guide_adam(G); }
@@ -862,7 +854,7 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_test_forward(GuideNet net
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __nv_bfloat16* in = reinterpret_cast<__nv_bfloat16*>(wbase + warp * IN_BYTES);
     float* out = reinterpret_cast<float*>(in);
-    load_weights(net, sw, sb, false, nullptr);
+    load_weights(net, sw, sb);
     __syncthreads();
     for (uint32_t base = (blockIdx.x * GWI + warp) * 16; base < n; base += gridDim.x * GWI * 16) {
         uint32_t r = base + (lane & 15);
@@ -1001,8 +993,7 @@ SRT_DEV void encode_row_tc(const float* x, unsigned char* A, uint32_t row) {
 SRT_DEV void relu_pack16(const uint32_t (&r)[16], const float* bias, uint32_t* out) {
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        out[i] = pack2(fmaxf(__uint_as_float(r[2 * i]) + bias[2 * i], 0.f),
-                       fmaxf(__uint_as_float(r[2 * i + 1]) + bias[2 * i + 1], 0.f));
+        out[i] = pack2_relu(__uint_as_float(r[2 * i]) + bias[2 * i], __uint_as_float(r[2 * i + 1]) + bias[2 * i + 1]);
 }
 
 // A group of 128 threads: its A buffer, accumulator columns, mbarrier and
@@ -1304,7 +1295,7 @@ size_t guide_infer_smem() {
     return SW_ELEMS * 2 + SB_ELEMS * 4 + GWI * IN_BYTES;
 }
 size_t guide_train_smem() {
-    return (SW_ELEMS + SWT_ELEMS) * 2 + SB_ELEMS * 4 +
+    return SW_ELEMS * 2 + SB_ELEMS * 4 +
            GWT * (16 * g_pad(G_ENC) * 2 + 4 * 16 * g_pad(G_HID) * 2 + 16 * 52 * 4 + 16 * g_pad(G_OUT) * 2);
 }
 
@@ -1424,7 +1415,6 @@ cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
     };
     chk(galloc(&g.net.master, G_NPARAMS));
     chk(galloc(&g.net.wbf, G_NPARAMS));
-    chk(galloc(&g.net.wtbf, G_NPARAMS));
     chk(galloc(&g.net.adam_m, G_NPARAMS));
     chk(galloc(&g.net.adam_v, G_NPARAMS));
     chk(galloc(&g.net.grad, G_NPARAMS));
@@ -1460,7 +1450,7 @@ cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
 }
 
 void guide_free(GuideArgs& g) {
-    void* bufs[] = {g.net.master, g.net.wbf, g.net.wtbf, g.net.adam_m, g.net.adam_v, g.net.grad,
+    void* bufs[] = {g.net.master, g.net.wbf, g.net.adam_m, g.net.adam_v, g.net.grad,
                     g.gv.p, g.gv.n, g.gv.wo, g.gv.spec, g.gv.id, g.rec.x0, g.rec.x1, g.rec.x2, g.rec.w, g.rec.b,
                     g.rec.thr, g.rec.rad, g.rec.pid, g.rec.weight, g.rec.act, g.rec.delta, g.gc};
     for (void* b : bufs) cudaFree(b);
@@ -1469,18 +1459,13 @@ void guide_free(GuideArgs& g) {
 
 cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m, const float* adam_v,
                          uint32_t adam_step) {
-    std::vector<__nv_bfloat16> wbf(G_NPARAMS, __float2bfloat16_rn(0.0f)), wtbf(G_NPARAMS, __float2bfloat16_rn(0.0f));
+    std::vector<__nv_bfloat16> wbf(G_NPARAMS, __float2bfloat16_rn(0.0f));
     for (int l = 0; l < G_LAYERS; ++l)
-        for (int o = 0; o < g_out(l); ++o)
-            for (int i = 0; i < g_in(l); ++i) {
-                __nv_bfloat16 h = __float2bfloat16_rn(params[g_woff(l) + o * g_in(l) + i]);
-                wbf[g_woff(l) + o * g_in(l) + i] = h;
-                wtbf[g_woff(l) + i * g_out(l) + o] = h;
-            }
+        for (int k = 0; k < g_in(l) * g_out(l); ++k)
+            wbf[g_woff(l) + k] = __float2bfloat16_rn(params[g_woff(l) + k]);
     std::vector<float> zero(G_NPARAMS, 0.0f);
     cudaError_t e = cudaMemcpy(g.net.master, params, G_NPARAMS * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(g.net.wbf, wbf.data(), G_NPARAMS * 2, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(g.net.wtbf, wtbf.data(), G_NPARAMS * 2, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(g.net.adam_m, adam_m ? adam_m : zero.data(), G_NPARAMS * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)

@@ -44,7 +44,6 @@ __host__ __device__ constexpr int g_pad(int n) { return n + 8; }
 struct GuideNet {
     float* master;          // G_NPARAMS fp32
     __nv_bfloat16* wbf;     // bf16 weights, same flat offsets (biases unused)
-    __nv_bfloat16* wtbf;    // bf16 transposed weights [in][out] per layer, flat at g_woff
     float* adam_m;          // G_NPARAMS
     float* adam_v;          // G_NPARAMS
     float* grad;            // G_NPARAMS fp32 accumulators (zeroed by the Adam step)
