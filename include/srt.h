@@ -448,6 +448,10 @@ srt_status srt_guide_test_forward_tc(srt_ctx* ctx, const float* params, const fl
 srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind);
 srt_status srt_guide_test_mixture(srt_ctx* ctx, const float* raw, const float* omega, const float* u, uint32_t n,
                                   float* out);
+/* The same for the mixture functions of the tcgen05 inference kernel (fast
+ * exponentials, logarithms, reciprocal square roots and division). */
+srt_status srt_guide_test_mixture_tc(srt_ctx* ctx, const float* raw, const float* omega, const float* u, uint32_t n,
+                                     float* out);
 srt_status srt_guide_test_train(srt_ctx* ctx, const float* params, const float* adam_m, const float* adam_v,
                                 uint32_t adam_step, float lr, const float* x, const float* omega,
                                 const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,

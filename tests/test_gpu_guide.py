@@ -61,7 +61,8 @@ def test_forward_matches_oracle(srt, ctx, n, out_scale, tcgen05):
     assert np.all(y[:, 41:] == y[:, 41:])  # finite padding outputs
 
 
-def test_mixture_pdf_and_samples_match_oracle(srt, ctx):
+@pytest.mark.parametrize("tc", [False, True], ids=["mma_sync", "tcgen05"])
+def test_mixture_pdf_and_samples_match_oracle(srt, ctx, tc):
     rng = np.random.default_rng(11)
     n = 20_000
     raw = rng.normal(0, 1.5, (n, 48)).astype(np.float32)
@@ -69,7 +70,7 @@ def test_mixture_pdf_and_samples_match_oracle(srt, ctx):
     om = rng.normal(size=(n, 3))
     om /= np.linalg.norm(om, axis=1, keepdims=True)
     u = rng.uniform(0, 1, (n, 3)).astype(np.float32)
-    out = srt.guide_mixture(ctx, raw, om.astype(np.float32), u)
+    out = srt.guide_mixture(ctx, raw, om.astype(np.float32), u, tcgen05=tc)
     mu, kappa, pi, _, _ = go.mixture(raw.astype(np.float64))
     q = (pi * go.vmf_pdf(mu, kappa, om[:, None, :].astype(np.float32).astype(np.float64))).sum(1)
     # exp(kappa (mu.w - 1)) with kappa up to e^7: fp32 dot products carry ~1e-4
@@ -81,7 +82,8 @@ def test_mixture_pdf_and_samples_match_oracle(srt, ctx):
     assert np.mean(cos > 1 - 1e-4) > 0.999
 
 
-def test_mixture_sampling_statistics(srt, ctx):
+@pytest.mark.parametrize("tc", [False, True], ids=["mma_sync", "tcgen05"])
+def test_mixture_sampling_statistics(srt, ctx, tc):
     rng = np.random.default_rng(12)
     n = 200_000
     raw = np.zeros((n, 48), np.float32)
@@ -91,7 +93,7 @@ def test_mixture_sampling_statistics(srt, ctx):
     kappa = 20.0
     raw[:, 3] = math.log(kappa)
     om = np.tile(np.array([0.0, 0.0, 1.0], np.float32), (n, 1))
-    out = srt.guide_mixture(ctx, raw, om, rng.uniform(0, 1, (n, 3)).astype(np.float32))
+    out = srt.guide_mixture(ctx, raw, om, rng.uniform(0, 1, (n, 3)).astype(np.float32), tcgen05=tc)
     mu = np.array([0.3, -0.5, 0.8]) / np.linalg.norm([0.3, -0.5, 0.8])
     mean_cos = (out[:, 1:] @ mu).mean()
     assert mean_cos == pytest.approx(1 / math.tanh(kappa) - 1 / kappa, abs=2e-3)

@@ -208,6 +208,7 @@ SIGNATURES = {
     "srt_guide_test_forward_tc": (_I, [_P, _P, _P, _U32, _P]),
     "srt_renderer_guide_set_inference": (_I, [_P, _I]),
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
+    "srt_guide_test_mixture_tc": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
 
@@ -639,13 +640,15 @@ def guide_forward(ctx: Context, params: np.ndarray, x: np.ndarray, tcgen05: bool
     return out
 
 
-def guide_mixture(ctx: Context, raw: np.ndarray, omega: np.ndarray, u: np.ndarray) -> np.ndarray:
-    """[n, 4]: mixture pdf at omega and a direction sampled with u (srt_guide_test_mixture)."""
+def guide_mixture(ctx: Context, raw: np.ndarray, omega: np.ndarray, u: np.ndarray, tcgen05: bool = False) -> np.ndarray:
+    """[n, 4]: mixture pdf at omega and a direction sampled with u (srt_guide_test_mixture; tcgen05: the
+    mixture functions of the tcgen05 inference kernel, srt_guide_test_mixture_tc)."""
     r = np.ascontiguousarray(raw, np.float32).reshape(-1, 48)
     o = np.ascontiguousarray(omega, np.float32).reshape(-1, 3)
     uu = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
     out = np.zeros((len(r), 4), np.float32)
-    _check(lib().srt_guide_test_mixture(ctx.h, ptr(r), ptr(o), ptr(uu), len(r), ptr(out)), ctx.h)
+    fn = lib().srt_guide_test_mixture_tc if tcgen05 else lib().srt_guide_test_mixture
+    _check(fn(ctx.h, ptr(r), ptr(o), ptr(uu), len(r), ptr(out)), ctx.h)
     return out
 
 

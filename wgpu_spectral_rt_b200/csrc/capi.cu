@@ -1349,8 +1349,9 @@ extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind
     return SRT_OK;
 }
 
-extern "C" srt_status srt_guide_test_mixture(srt_ctx* c, const float* raw, const float* omega, const float* u,
-                                             uint32_t n, float* out) {
+namespace {
+srt_status guide_test_mixture(srt_ctx* c, const float* raw, const float* omega, const float* u, uint32_t n,
+                              float* out, int tc) {
     if (!c || (n && (!raw || !omega || !u || !out))) return SRT_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     if (n == 0) return SRT_OK;
@@ -1363,11 +1364,22 @@ extern "C" srt_status srt_guide_test_mixture(srt_ctx* c, const float* raw, const
     CUDA_TRY(c, cudaMemcpyAsync(d_raw, raw, (size_t)n * G_OUT * 4, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(d_om, omega, (size_t)n * 12, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(d_u, u, (size_t)n * 12, cudaMemcpyHostToDevice, c->stream));
-    launch_guide_test_mixture(d_raw, d_om, d_u, n, s.y, c->stream);
+    launch_guide_test_mixture(d_raw, d_om, d_u, n, s.y, tc, c->stream);
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaMemcpyAsync(out, s.y, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SRT_OK;
+}
+}  // namespace
+
+extern "C" srt_status srt_guide_test_mixture(srt_ctx* c, const float* raw, const float* omega, const float* u,
+                                             uint32_t n, float* out) {
+    return guide_test_mixture(c, raw, omega, u, n, out, 0);
+}
+
+extern "C" srt_status srt_guide_test_mixture_tc(srt_ctx* c, const float* raw, const float* omega, const float* u,
+                                                uint32_t n, float* out) {
+    return guide_test_mixture(c, raw, omega, u, n, out, 1);
 }
 
 extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, const float* adam_m, const float* adam_v,

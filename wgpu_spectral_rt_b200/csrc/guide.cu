@@ -183,6 +183,50 @@ SRT_DEV void mixture(const float* r, Mix& m) {
     m.sel_sig = 1.0f / (1.0f + expf(-r[40]));
     m.sel = G_SEL_LO + G_SEL_SPAN * m.sel_sig;
 }
+// The mixture with the hardware's fast approximations (the tcgen05 inference
+// path and training): exponentials and logarithms through ex2 / lg2 (__expf,
+// __logf), reciprocal square roots for normalisation, approximate division.
+// Their relative errors (~1e-6) are far below the noise of one sample, and
+// sampling and pdf evaluation use the same functions.
+SRT_DEV void mixture_fast(const float* r, Mix& m) {
+    float mx = -3.4e38f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) mx = fmaxf(mx, r[5 * j + 4]);
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) {
+        const float3 v = f3(r[5 * j], r[5 * j + 1], r[5 * j + 2]);
+        const float d2 = dot(v, v);
+        const float inv = rsqrtf(fmaxf(d2, 1e-24f));
+        m.norm[j] = d2 * inv;
+        m.mu[j] = v * inv;
+        m.lk[j] = r[5 * j + 3];
+        const float k = __expf(clampf(r[5 * j + 3], G_KAPPA_LO, G_KAPPA_HI));
+        const float e2 = __expf(-2.0f * k);
+        m.kappa[j] = k;
+        m.e2[j] = e2;
+        m.c[j] = __fdividef(k, 2.0f * PI * (1.0f - e2));
+        m.pi[j] = __expf(r[5 * j + 4] - mx);
+        sum += m.pi[j];
+    }
+    const float isum = __fdividef(1.0f, sum);
+#pragma unroll
+    for (int j = 0; j < G_LOBES; ++j) m.pi[j] *= isum;
+    m.sel_sig = __fdividef(1.0f, 1.0f + __expf(-r[40]));
+    m.sel = G_SEL_LO + G_SEL_SPAN * m.sel_sig;
+}
+SRT_DEV float3 normalize_fast(float3 a) { return a * rsqrtf(dot(a, a)); }
+SRT_DEV float3 vmf_sample_fast(float3 mu, float k, float e2, float u1, float u2) {
+    float w = 1.0f + __fdividef(__logf(u1 + (1.0f - u1) * e2), k);
+    w = clampf(w, -1.0f, 1.0f);
+    const float r = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    float sp, cp;
+    sincospif(2.0f * u2, &sp, &cp);
+    const float3 t = fabsf(mu.x) > 0.9f ? f3(0.f, 1.f, 0.f) : f3(1.f, 0.f, 0.f);
+    const float3 b1 = normalize_fast(cross(mu, t));
+    const float3 b2 = cross(mu, b1);
+    return normalize_fast(mu * w + b1 * (r * cp) + b2 * (r * sp));
+}
 SRT_DEV float vmf(float3 mu, float k, float3 w) {
     return k / (2.0f * PI * (-expm1f(-2.0f * k))) * expf(k * (dot(mu, w) - 1.0f));
 }
@@ -590,32 +634,33 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
             if (r < n) {
                 const float* raw = out + lane * 52;
                 Mix m;
-                mixture(raw, m);
+                mixture_fast(raw, m);
                 float4 w4 = G.rec.w[r], b4 = G.rec.b[r];
                 float3 om = xyz(w4);
                 float wt = G.rec.weight[r] * inv_mean;
                 float vm[G_LOBES], q = 0.f;
                 for (int j = 0; j < G_LOBES; ++j) {
-                    vm[j] = m.c[j] * expf(m.kappa[j] * (dot(m.mu[j], om) - 1.0f));
+                    vm[j] = m.c[j] * __expf(m.kappa[j] * (dot(m.mu[j], om) - 1.0f));
                     q += m.pi[j] * vm[j];
                 }
                 q = fmaxf(q, 1e-30f);
+                const float iq = 1.0f / q;
                 for (int j = 0; j < G_LOBES; ++j) {
-                    float gam = m.pi[j] * vm[j] / q;
+                    float gam = m.pi[j] * vm[j] * iq;
                     gr[5 * j + 4] = wt * (m.pi[j] - gam);
                     float k = m.kappa[j];
                     float mw = dot(m.mu[j], om);
                     float dl = 1.0f / k - 2.0f / expm1f(2.0f * k) + mw - 1.0f;
                     bool inside = m.lk[j] > G_KAPPA_LO && m.lk[j] < G_KAPPA_HI;
                     gr[5 * j + 3] = inside ? -wt * gam * dl * k : 0.f;
-                    float3 gd = (om - m.mu[j] * mw) * (-wt * gam * k / m.norm[j]);
+                    float3 gd = (om - m.mu[j] * mw) * __fdividef(-wt * gam * k, m.norm[j]);
                     gr[5 * j] = gd.x;
                     gr[5 * j + 1] = gd.y;
                     gr[5 * j + 2] = gd.z;
                 }
                 float pb = b4.x;
                 float pmix = fmaxf(m.sel * q + (1.0f - m.sel) * pb, 1e-30f);
-                gr[40] = -wt * (q - pb) / pmix * G_SEL_SPAN * m.sel_sig * (1.0f - m.sel_sig);
+                gr[40] = __fdividef(-wt * (q - pb), pmix) * G_SEL_SPAN * m.sel_sig * (1.0f - m.sel_sig);
             }
             for (int i = 0; i < G_OUT; i += 2)
                 *reinterpret_cast<uint32_t*>(d4 + lane * g_pad(G_OUT) + i) = pack2(gr[i], gr[i + 1]);
@@ -1070,7 +1115,7 @@ SRT_DEV bool mlp_tc(const TcGroup& g, const unsigned char* smem, const float* sb
 SRT_DEV float mix_pdf(const Mix& m, float3 w) {
     float q = 0.f;
 #pragma unroll
-    for (int j = 0; j < G_LOBES; ++j) q += m.pi[j] * (m.c[j] * expf(m.kappa[j] * (dot(m.mu[j], w) - 1.0f)));
+    for (int j = 0; j < G_LOBES; ++j) q += m.pi[j] * (m.c[j] * __expf(m.kappa[j] * (dot(m.mu[j], w) - 1.0f)));
     return q;
 }
 // Lobe j = first with u0 below the cumulative weight (the last lobe on
@@ -1090,7 +1135,7 @@ SRT_DEV float3 mix_sample(const Mix& m, float u0, float u1, float u2) {
             e2 = m.e2[j];
         }
     }
-    return vmf_sample_e2(mu, k, e2, u1, u2);
+    return vmf_sample_fast(mu, k, e2, u1, u2);
 }
 
 // Block set-up (tensor-memory allocation, mbarriers, the weights of `net`
@@ -1163,7 +1208,7 @@ SRT_DEV bool infer_tile_tc(const FrameArgs& a, uint32_t bounce, const TcGroup& g
     uint32_t id = 0;
     if (valid) {
         Mix m;
-        mixture(raw, m);
+        mixture_fast(raw, m);
         id = G.gv.id[v];
         const uint4 misc = a.pb.misc[id];
         uint32_t s = misc.x;
@@ -1259,6 +1304,22 @@ __global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2)
         if (base < n && !infer_tile_tc(a, bounce, grp, smem, sb, base, n, phase)) ok = false;
     }
     tc_teardown(grp, ok, phase, items[cur < 0 ? 0 : cur].err);
+}
+
+// The tcgen05 path's mixture: pdf at omega and a direction sampled with u, one sample per thread.
+__global__ void k_guide_test_mixture_tc(const float* __restrict__ raw, const float* __restrict__ omega,
+                                        const float* __restrict__ u, uint32_t n, float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float r[G_OUT];
+    for (int k = 0; k < G_OUT; ++k) r[k] = raw[(size_t)i * G_OUT + k];
+    Mix m;
+    mixture_fast(r, m);
+    const float3 d = mix_sample(m, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+    out[4 * i] = mix_pdf(m, f3(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2]));
+    out[4 * i + 1] = d.x;
+    out[4 * i + 2] = d.y;
+    out[4 * i + 3] = d.z;
 }
 
 // Forward pass of n samples on the tcgen05 path (inputs [n][10] -> raw outputs [n][48]).
@@ -1483,7 +1544,11 @@ int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, f
     return 1;
 }
 int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,
-                              cudaStream_t st) {
+                              int tc, cudaStream_t st) {
+    if (tc) {
+        k_guide_test_mixture_tc<<<(n + 127) / 128, 128, 0, st>>>(raw, omega, u, n, out);
+        return 1;
+    }
     k_guide_test_mixture<<<(n + 63) / 64, 128, 0, st>>>(raw, omega, u, n, out);  // 16 samples per warp
     return 1;
 }

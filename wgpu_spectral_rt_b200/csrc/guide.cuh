@@ -120,7 +120,8 @@ int launch_guide_train_multi(const FrameArgs* items, int n_items, int sm_count, 
 // tc: the tcgen05 kernel (err: device error word for an MMA wait that gave up).
 int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, int tc, uint32_t* err,
                               cudaStream_t st);
-int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out,
+// tc: the mixture functions of the tcgen05 inference kernel (else the mma.sync kernel's lane-pair form)
+int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out, int tc,
                               cudaStream_t st);
 // phase 0: forward + backward + weight gradients of gc->records records
 // (gc->weight_sum set by the caller); phase 1: one Adam step.
