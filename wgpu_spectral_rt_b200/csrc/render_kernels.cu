@@ -12,6 +12,15 @@
 #include "radix_sort.cuh"
 #include "render_kernels.h"
 
+// Resident blocks of TRACE_BLOCK threads per SM the shading kernels are
+// compiled for.  8 caps them at 64 registers (the unbounded build takes 87,
+// 108 with guiding, and runs 20 warps per SM): the spills stay in L1 and the
+// doubled warp count hides the photon-gather latency better (measured shading
+// per frame: config 2 1.98 -> 1.79 ms, the guiding scene 2.94 -> 2.58 ms).
+#ifndef SRT_SHADE_MIN_BLOCKS
+#define SRT_SHADE_MIN_BLOCKS 8
+#endif
+
 namespace srt {
 
 namespace {
@@ -143,7 +152,7 @@ __global__ void k_photon_emit(FrameArgs a) {
 // One bounce of the photon loop after its closest-hit query
 // (photon_emit.wgsl:227-330).  Material type 5 (no reference counterpart)
 // reflects with the probability of the film's Airy reflectance, else absorbs.
-__global__ void __launch_bounds__(TRACE_BLOCK) k_photon_shade(FrameArgs a, uint32_t bounce) {
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_photon_shade(FrameArgs a, uint32_t bounce) {
     uint32_t n = a.counters->photon_paths[bounce];
     if (blockIdx.x * blockDim.x >= n) return;
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,7 +363,7 @@ SRT_DEV LightSample sample_light(const DevScene& S, float3 hp, float4 wl, uint32
 // (shader.wgsl:568-700).
 // GUIDE: Lambert continuations are left to k_guide_infer (guide.cu).
 template <bool GUIDE>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_shade(FrameArgs a, uint32_t bounce) {
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(FrameArgs a, uint32_t bounce) {
     uint32_t n = a.counters->paths[bounce];
     if (blockIdx.x * blockDim.x >= n) return;
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
