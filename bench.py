@@ -321,6 +321,23 @@ def guided_section(seconds=3.0, ref_spp=4096):
             "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"]}
 
 
+def batched_guided_section(seconds=2.0, ref_spp=256):
+    """C5 reduced (full-size study: wgpu_spectral_rt_b200.batch_guide_study): 16 seeded scenes, each
+    with its own online-trained network, in one batched renderer (grouped guide launches) vs the
+    plain batched renderer at equal time, per-scene relMSE against FP64 plain references."""
+    from wgpu_spectral_rt_b200 import batch_guide_study
+
+    d = batch_guide_study.study(n_scenes=16, resolutions=(64, 128, 256, 512), photons=(0.25e6, 4e6),
+                                max_depth=12, ref_spp=ref_spp, seconds=seconds)
+    return {"workload": (f"C5 reduced: 16 scenes ({min(d['triangles'])}..{max(d['triangles'])} triangles), "
+                         f"viewports 64^2..512^2, 0.25M..4M photons, depth 12, one network per scene; "
+                         f"reference {ref_spp} iterations FP64, {seconds} s per arm"),
+            "ms_per_iteration_plain": d["plain"]["ms_per_iteration"],
+            "ms_per_iteration_guided": d["guided"]["ms_per_iteration"],
+            "geomean_relmse_ratio_plain_over_guided": round(d["geomean_ratio_plain_over_guided"], 3),
+            "scenes_improved": d["scenes_improved"]}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,6 +354,7 @@ def main(argv=None):
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the C3 batched-renderer section")
     ap.add_argument("--no-guided", action="store_true", help="skip the C4 guided-vs-plain section")
+    ap.add_argument("--no-batched-guided", action="store_true", help="skip the C5 batched-guiding section")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -466,6 +484,9 @@ def main(argv=None):
     guided = None
     if rank == 0 and world == 1 and not args.no_guided:
         guided = guided_section()
+    batched_guided = None
+    if rank == 0 and world == 1 and not args.no_batched_guided:
+        batched_guided = batched_guided_section()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -491,6 +512,7 @@ def main(argv=None):
             "roofline": roof,
             "batched": batched,
             "guided": guided,
+            "batched_guided": batched_guided,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
