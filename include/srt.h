@@ -433,6 +433,10 @@ srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_steps, uint32
 /* Adam learning rate (default 1e-3; < 0 keeps it) and training samples
  * recorded per frame (default 65536, at most 262144; 0 keeps it). */
 srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batch);
+/* Adam steps per frame (1..16, default 1): the frame's training records are
+ * split into `steps` consecutive sub-batches, one forward/backward, gradient
+ * and Adam step each. */
+srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t steps);
 /* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
  * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),
  * sampled direction).  train: loss gradients summed over n samples
@@ -509,7 +513,8 @@ srt_status srt_batch_render(srt_batch* b, const srt_camera_uniform* cams, const 
 srt_status srt_batch_get_tuning(const srt_batch* b, srt_batch_tuning* out);
 srt_status srt_batch_set_tuning(srt_batch* b, const srt_batch_tuning* t);
 /* Times `iterations` iterations of every candidate (blocks per SM x chunk),
- * keeps the fastest, then clears every scene's accumulation and statistics. */
+ * keeps the fastest, then clears every scene's accumulation and statistics;
+ * guided scenes get back the network and Adam state they had before. */
 srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform* cams, uint32_t iterations,
                               srt_batch_tuning* out);
 

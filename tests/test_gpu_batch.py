@@ -174,3 +174,24 @@ def test_batch_guided_training_matches_single_scene_training(srt, ctx):
         assert x.guide_info()["adam_steps"] == 4
         assert np.all(np.isfinite(x.read_accum()))
     batch.close()
+
+
+def test_batch_autotune_leaves_guided_networks_untouched(srt, ctx):
+    """The tuning frames train nothing: a guided scene's weights and Adam step
+    count are the same before and after srt_batch_autotune."""
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    params = [_guided(srt, p, False) for p in _params(srt)]
+    batch = srt.Batch(ctx, scenes, SIZES, params)
+    batch.render(_cams(ctls, 0))  # one trained iteration first
+    ctx.synchronize()
+    before = [(x.guide_weights(), x.guide_info()["adam_steps"]) for x in batch.renderers]
+    assert all(steps == 1 for _, steps in before)
+    batch.autotune(_cams(ctls, 1), iterations=1)
+    for x, (w, steps) in zip(batch.renderers, before):
+        np.testing.assert_array_equal(x.guide_weights(), w)
+        assert x.guide_info()["adam_steps"] == steps
+    batch.render(_cams(ctls, 2))
+    ctx.synchronize()
+    assert all(x.guide_info()["adam_steps"] == 2 for x in batch.renderers)
+    batch.close()

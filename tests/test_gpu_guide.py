@@ -187,6 +187,42 @@ def test_guided_render_is_unbiased(srt, ctx):
     guided.close()
 
 
+def test_several_adam_steps_per_frame(srt, ctx):
+    """srt_renderer_guide_set_steps: each frame's records split into strided
+    sub-batches, one Adam step each; in a batch, scenes keep their own count."""
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b.build(ctx)
+    w, h, frames = 48, 32, 6
+    ctl = srt.CameraController(*cam)
+    one = srt.Renderer(ctx, scene, w, h, srt.default_params(photons_per_frame=1 << 14, flags=srt.FLAG_GUIDING))
+    four = srt.Renderer(ctx, scene, w, h, srt.default_params(photons_per_frame=1 << 14, flags=srt.FLAG_GUIDING))
+    four.set_guide_steps(4)
+    for f in range(frames):
+        one.render(ctl.build_uniform(w / h, f))
+        four.render(ctl.build_uniform(w / h, f))
+    ctx.synchronize()
+    assert one.guide_info()["adam_steps"] == frames
+    assert four.guide_info()["adam_steps"] == 4 * frames
+    w1, w4 = one.guide_weights(), four.guide_weights()
+    w0 = srt.guide_default_weights(1)
+    assert np.all(np.isfinite(w4))
+    # Adam moves a parameter by at most ~lr per step: four steps per frame move further
+    assert np.abs(w4 - w0).max() > 1.5 * np.abs(w1 - w0).max()
+    with pytest.raises(srt.SrtError):
+        one.set_guide_steps(0)
+    one.close()
+    four.close()
+    params = [srt.default_params(photons_per_frame=1 << 14, flags=srt.FLAG_GUIDING) for _ in range(2)]
+    batch = srt.Batch(ctx, [scene, scene], [(w, h), (32, 32)], params)
+    batch.renderers[1].set_guide_steps(3)
+    for f in range(2):
+        batch.render([ctl.build_uniform(w / h, f), ctl.build_uniform(1.0, f)])
+    ctx.synchronize()
+    assert [x.guide_info()["adam_steps"] for x in batch.renderers] == [2, 6]
+    batch.close()
+
+
 def test_frozen_guide_is_deterministic_and_restores(srt, ctx):
     b = srt.SceneBuilder()
     cam = b.add_preset(srt.PRESET_CORNELL_BOX)

@@ -209,6 +209,7 @@ SIGNATURES = {
     "srt_renderer_guide_set_inference": (_I, [_P, _I]),
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_mixture_tc": (_I, [_P, _P, _P, _P, _U32, _P]),
+    "srt_renderer_guide_set_steps": (_I, [_P, _U32]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
 
@@ -559,6 +560,10 @@ class Renderer:
         steps, thr = C.c_uint32(), C.c_uint32()
         _check(lib().srt_renderer_guide_info(self.h, C.byref(steps), C.byref(thr)), self.ctx.h)
         return {"adam_steps": steps.value, "record_threshold": thr.value}
+
+    def set_guide_steps(self, steps: int) -> None:
+        """Adam steps per frame, each on a consecutive 1/steps of the frame's training records."""
+        _check(lib().srt_renderer_guide_set_steps(self.h, steps), self.ctx.h)
 
     def configure_guide(self, lr: float | None = None, batch: int | None = None) -> None:
         """Adam learning rate and training samples recorded per frame."""

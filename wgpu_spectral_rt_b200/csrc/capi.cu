@@ -1289,6 +1289,22 @@ extern "C" srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, ui
     return SRT_OK;
 }
 
+extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t steps) {
+    if (!r || steps < 1 || steps > 16) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->guide.steps = steps;
+    r->args.guide = r->guide;
+    r->args_gen += 1;
+    if (r->graph) {  // the step count shapes the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return SRT_OK;
+}
+
 namespace {
 struct GuideScratch {
     GuideArgs g{};
@@ -1601,11 +1617,12 @@ struct srt_batch {
         // grouped launches over all of them (their frame arguments are
         // uploaded once the capture has recorded every per-renderer launch)
         std::vector<srt_renderer*> guided;
-        uint32_t guide_depth = 0;
+        uint32_t guide_depth = 0, guide_steps = 1;
         for (int k = 0; k < na; ++k)
             if (r[act[k]]->args.guiding) {
                 guided.push_back(r[act[k]]);
                 guide_depth = std::max(guide_depth, r[act[k]]->p.max_depth);
+                guide_steps = std::max(guide_steps, r[act[k]]->args.guide.steps);
             }
         const int ng = (int)guided.size();
         cudaGraph_t g;
@@ -1633,7 +1650,7 @@ struct srt_batch {
                                     fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
         }
         fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_end(s, false); });
-        if (ng) n += launch_guide_train_multi(guide_items_dev, ng, c->sm_count, cap);
+        if (ng) n += launch_guide_train_multi(guide_items_dev, ng, guide_steps, c->sm_count, cap);
         cudaError_t e = cudaStreamEndCapture(cap, &g);
         CUDA_TRY(c, e);
         if (ng) {
@@ -1782,6 +1799,18 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
     CUDA_TRY(c, cudaEventCreate(&e1));
     srt_batch_tuning best{8, 32, 3.4e38f, 0};
     srt_status st = SRT_OK;
+    // guided scenes train during the tuning frames: their networks and Adam
+    // state are saved here and put back afterwards
+    std::vector<void*> saved(b->r.size(), nullptr);
+    for (size_t i = 0; i < b->r.size(); ++i)
+        if (b->r[i]->args.guiding) {
+            cudaError_t e = cudaMalloc(&saved[i], guide_state_bytes());
+            if (e == cudaSuccess) e = guide_state_copy(b->r[i]->guide, saved[i], true, c->stream);
+            if (e != cudaSuccess) {
+                for (void* p : saved) cudaFree(p);
+                return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, cudaGetErrorString(e));
+            }
+        }
     for (uint32_t bp : bps)
         for (uint32_t ch : chunks) {
             srt_batch_tuning t{bp, ch, 0.0f, 0};
@@ -1805,7 +1834,15 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    cudaError_t restored = cudaSuccess;
+    for (size_t i = 0; i < b->r.size(); ++i)
+        if (saved[i]) {
+            if (restored == cudaSuccess) restored = guide_state_copy(b->r[i]->guide, saved[i], false, c->stream);
+        }
+    cudaStreamSynchronize(c->stream);
+    for (void* p : saved) cudaFree(p);
     if (st != SRT_OK) return st;
+    CUDA_TRY(c, restored);
     uint32_t n_cand = best.candidates;
     srt_batch_set_tuning(b, &best);
     b->tune.ms_per_iteration = best.ms_per_iteration;

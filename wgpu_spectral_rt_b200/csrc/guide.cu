@@ -558,6 +558,20 @@ __global__ void __launch_bounds__(GWI * 32, 2) k_guide_infer(FrameArgs a, uint32
 // Per record: the radiance that arrived along the sampled direction and the
 // training weight F / p = L f cos / p.  Records whose path ended before its
 // next vertex carry no later radiance (L = 0).
+// The records of training step `step` (of G.steps this frame): records
+// step, step + steps, step + 2 steps, ...  Records are stored in the order
+// their vertices were shaded (by bounce, then roughly by pixel), so strided
+// sub-batches each sample the whole frame.
+struct StepRecs {
+    uint32_t count, first, stride;
+};
+SRT_DEV StepRecs step_recs(const GuideArgs& G, int step) {
+    const uint32_t n = min(G.gc->records, G.batch);
+    const uint32_t k = max(G.steps, 1u), f = (uint32_t)step;
+    return StepRecs{n > f ? (n - f + k - 1u) / k : 0u, f, k};
+}
+SRT_DEV uint32_t rec_at(const StepRecs& sr, uint32_t j) { return sr.first + j * sr.stride; }
+
 SRT_DEV void guide_targets(const FrameArgs& a) {
     const GuideArgs& G = a.guide;
     if (!G.train) return;
@@ -592,7 +606,7 @@ __global__ void k_guide_targets_multi(const FrameArgs* __restrict__ items) { gui
 // post-ReLU activations and per-layer deltas (bf16) for the weight-gradient
 // product.  Loss per sample (weight w normalised by the batch mean):
 //   -w log q(omega) for the lobes, -w log(sel q + (1 - sel) p_bsdf) for sel.
-SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
+SRT_DEV void guide_fwdbwd(const GuideArgs& G, int step) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
     float* sb = reinterpret_cast<float*>(sw + SW_ELEMS);
@@ -603,17 +617,19 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
     __nv_bfloat16* act = in + 16 * g_pad(G_ENC);
     float* out = reinterpret_cast<float*>(act + 4 * 16 * g_pad(G_HID));
     __nv_bfloat16* d4 = reinterpret_cast<__nv_bfloat16*>(out + 16 * 52);
-    const uint32_t n = min(G.gc->records, G.batch);
+    const uint32_t n_all = min(G.gc->records, G.batch);
+    const StepRecs sr = step_recs(G, step);
+    const uint32_t n = sr.count;  // this step's records, by index j (record rec_at(sr, j))
     if (blockIdx.x * GWT * 16 >= n) return;
     load_weights(G.net, sw, sb);
     __syncthreads();
-    const float inv_mean = G.gc->weight_sum > 0.f ? (float)n / G.gc->weight_sum : 0.f;
+    const float inv_mean = G.gc->weight_sum > 0.f ? (float)n_all / G.gc->weight_sum : 0.f;
     const int g = lane >> 2, cq = lane & 3;
     for (uint32_t base = (blockIdx.x * GWT + warp) * 16; base < n; base += gridDim.x * GWT * 16) {
         {
-            uint32_t r = base + (lane & 15);
+            const uint32_t j = base + (lane & 15), r = rec_at(sr, j);
             float x[G_IN];
-            if (r < n) {
+            if (j < n) {
                 float4 x0 = G.rec.x0[r], x1 = G.rec.x1[r], x2 = G.rec.x2[r];
                 x[0] = x0.x; x[1] = x0.y; x[2] = x0.z; x[3] = x0.w;
                 x[4] = x1.x; x[5] = x1.y; x[6] = x1.z; x[7] = x1.w;
@@ -628,10 +644,10 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
         __syncwarp();
         // output gradient, one lane per sample
         if (lane < 16) {
-            uint32_t r = base + lane;
+            const uint32_t j = base + lane, r = rec_at(sr, j);
             float gr[G_OUT];
             for (int i = 0; i < G_OUT; ++i) gr[i] = 0.f;
-            if (r < n) {
+            if (j < n) {
                 const float* raw = out + lane * 52;
                 Mix m;
                 mixture_fast(raw, m);
@@ -669,8 +685,8 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
         // store inputs, activations and the output delta for the weight gradients
         for (int e = lane; e < 16 * (G_ACT_STRIDE / 8); e += 32) {
             int row = e / (G_ACT_STRIDE / 8), ch = e % (G_ACT_STRIDE / 8);
-            uint32_t r = base + row;
-            if (r >= n) continue;
+            if (base + row >= n) continue;
+            const uint32_t r = rec_at(sr, base + row);
             const __nv_bfloat16* src = ch < 16 ? in + row * g_pad(G_ENC) + 8 * ch
                                                : act + ((ch - 16) / 8) * 16 * g_pad(G_HID) + row * g_pad(G_HID) +
                                                      8 * ((ch - 16) % 8);
@@ -679,8 +695,8 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
         }
         for (int e = lane; e < 16 * (G_OUT / 8); e += 32) {
             int row = e / (G_OUT / 8), ch = e % (G_OUT / 8);
-            uint32_t r = base + row;
-            if (r >= n) continue;
+            if (base + row >= n) continue;
+            const uint32_t r = rec_at(sr, base + row);
             *reinterpret_cast<uint4*>(G.rec.delta + (size_t)r * G_DELTA_STRIDE + g_delta_off(4) + 8 * ch) =
                 *reinterpret_cast<const uint4*>(d4 + row * g_pad(G_OUT) + 8 * ch);
         }
@@ -724,15 +740,16 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
                 da[s][2] = pack2(c[2 * s + 1][0], c[2 * s + 1][1]);
                 da[s][3] = pack2(c[2 * s + 1][2], c[2 * s + 1][3]);
             }
-            uint32_t r0 = base + g, r1 = base + g + 8;
+            const bool ok0 = base + g < n, ok1 = base + g + 8 < n;
+            const uint32_t r0 = rec_at(sr, base + g), r1 = rec_at(sr, base + g + 8);
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 __nv_bfloat16* d0 = G.rec.delta + g_delta_off(l) + 16 * s + 2 * cq;
-                if (r0 < n) {
+                if (ok0) {
                     *reinterpret_cast<uint32_t*>(d0 + (size_t)r0 * G_DELTA_STRIDE) = da[s][0];
                     *reinterpret_cast<uint32_t*>(d0 + (size_t)r0 * G_DELTA_STRIDE + 8) = da[s][2];
                 }
-                if (r1 < n) {
+                if (ok1) {
                     *reinterpret_cast<uint32_t*>(d0 + (size_t)r1 * G_DELTA_STRIDE) = da[s][1];
                     *reinterpret_cast<uint32_t*>(d0 + (size_t)r1 * G_DELTA_STRIDE + 8) = da[s][3];
                 }
@@ -741,11 +758,11 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G) {
         __syncwarp();
     }
 }
-__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G) { guide_fwdbwd(G); }
-// many renderers (blockIdx.y = item), those that train
-__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd_multi(const FrameArgs* __restrict__ items) {
+__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd(GuideArgs G, int step) { guide_fwdbwd(G, step); }
+// many renderers (blockIdx.y = item), those that train and take this step
+__global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd_multi(const FrameArgs* __restrict__ items, int step) {
     const GuideArgs& G = items[blockIdx.y].guide;
-    if (G.train) guide_fwdbwd(G);
+    if (G.train && (uint32_t)step < G.steps) guide_fwdbwd(G, step);
 }
 
 // Weight gradients dW_l = sum_s delta_l[s]^T a_{l-1}[s] (and bias sums),
@@ -753,10 +770,11 @@ __global__ void __launch_bounds__(GWT * 32) k_guide_fwdbwd_multi(const FrameArgs
 // 2..5 = layers 1..4.  8 warps: warp w owns output rows 16 (w & 3) .. + 15
 // and input columns 32 (w >> 2) .. + 31 of the 64 x 64 block.
 constexpr int WGRAD_BLOCKS = 64;  // sample splits per job
-SRT_DEV void guide_wgrad(const GuideArgs& G) {
+SRT_DEV void guide_wgrad(const GuideArgs& G, int step) {
     __shared__ __align__(16) __nv_bfloat16 sd[32 * g_pad(G_HID)];
     __shared__ __align__(16) __nv_bfloat16 sa[32 * g_pad(G_HID)];
-    const uint32_t n = min(G.gc->records, G.batch);
+    const StepRecs sr = step_recs(G, step);
+    const uint32_t n = sr.count;
     const int job = blockIdx.y;
     const int l = job <= 1 ? 0 : job - 1;
     const int in0 = job == 1 ? 64 : 0;
@@ -775,9 +793,9 @@ SRT_DEV void guide_wgrad(const GuideArgs& G) {
         // stage 32 samples: deltas (out columns) and activations (input columns)
         {
             int row = threadIdx.x >> 3, ch = threadIdx.x & 7;
-            uint32_t r = s + row;
+            const uint32_t r = rec_at(sr, s + row);
             uint4 dv = make_uint4(0, 0, 0, 0), av = make_uint4(0, 0, 0, 0);
-            if (r < s1) {
+            if (s + row < s1) {
                 if (8 * ch < nout)
                     dv = *reinterpret_cast<const uint4*>(G.rec.delta + (size_t)r * G_DELTA_STRIDE + g_delta_off(l) + 8 * ch);
                 av = *reinterpret_cast<const uint4*>(G.rec.act + (size_t)r * G_ACT_STRIDE + g_act_off(l - 1) + in0 + 8 * ch);
@@ -829,20 +847,20 @@ SRT_DEV void guide_wgrad(const GuideArgs& G) {
     }
     if (job != 1 && threadIdx.x < nout && bsum != 0.f) atomicAdd(G.net.grad + g_boff(l) + threadIdx.x, bsum);
 }
-__global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G) { guide_wgrad(G); }
+__global__ void __launch_bounds__(256) k_guide_wgrad(GuideArgs G, int step) { guide_wgrad(G, step); }
 // many renderers: blockIdx.z = item
-__global__ void __launch_bounds__(256) k_guide_wgrad_multi(const FrameArgs* __restrict__ items) {
+__global__ void __launch_bounds__(256) k_guide_wgrad_multi(const FrameArgs* __restrict__ items, int step) {
     const GuideArgs& G = items[blockIdx.z].guide;
-    if (G.train) guide_wgrad(G);
+    if (G.train && (uint32_t)step < G.steps) guide_wgrad(G, step);
 }
 
 // Adam on the FP32 master weights (gradients are sums over the batch and
 // are divided by its size), then the bf16 copies; clears the gradients.
-SRT_DEV void guide_adam(const GuideArgs& G) {
-    const uint32_t n = min(G.gc->records, G.batch);
+SRT_DEV void guide_adam(const GuideArgs& G, int step) {
+    const uint32_t n = step_recs(G, step).count;
     if (n == 0) return;
     const float inv = 1.0f / (float)n;
-    const float t = (float)(G.gc->adam_step + 1u);
+    const float t = (float)(G.gc->adam_step + 1u + (uint32_t)step);
     const float b1t = 1.0f - powf(0.9f, t), b2t = 1.0f - powf(0.999f, t);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G_NPARAMS; i += gridDim.x * blockDim.x) {
         float gr = G.net.grad[i] * inv;
@@ -858,11 +876,11 @@ SRT_DEV void guide_adam(const GuideArgs& G) {
         if (i - g_woff(l) < g_in(l) * g_out(l)) G.net.wbf[i] = __float2bfloat16_rn(w);
     }
 }
-__global__ void k_guide_adam(GuideArgs G) { guide_adam(G); }
+__global__ void k_guide_adam(GuideArgs G, int step) { guide_adam(G, step); }
 // many renderers: blockIdx.y = item
-__global__ void k_guide_adam_multi(const FrameArgs* __restrict__ items) {
+__global__ void k_guide_adam_multi(const FrameArgs* __restrict__ items, int step) {
     const GuideArgs& G = items[blockIdx.y].guide;
-    if (G.train) guide_adam(G);
+    if (G.train && (uint32_t)step < G.steps) guide_adam(G, step);
 }
 
 // Next frame's recording threshold (of 65536) so that about 90 % of the
@@ -876,7 +894,7 @@ SRT_DEV void guide_frame_end(const GuideArgs& G, int trained) {
         double t = 65536.0 * 0.9 * (double)G.batch / (double)c;
         gc->threshold = (uint32_t)fmin(65536.0, fmax(1.0, t));
     }
-    if (trained && gc->records > 0u) gc->adam_step += 1u;
+    if (trained && gc->records > 0u) gc->adam_step += max(G.steps, 1u);
     gc->records = 0u;
     gc->candidates = 0u;
     gc->weight_sum = 0.f;
@@ -1389,12 +1407,17 @@ int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
 
 namespace {
 int launch_train_steps(const GuideArgs& g, int sm, int adam, cudaStream_t st) {
-    k_guide_fwdbwd<<<sm, GWT * 32, guide_train_smem(), st>>>(g);
-    dim3 wg(WGRAD_BLOCKS, 6);
-    k_guide_wgrad<<<wg, 256, 0, st>>>(g);
-    if (!adam) return 2;
-    k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g);
-    return 3;
+    int n = 0;
+    for (int k = 0; k < (int)std::max(g.steps, 1u); ++k) {
+        k_guide_fwdbwd<<<sm, GWT * 32, guide_train_smem(), st>>>(g, k);
+        dim3 wg(WGRAD_BLOCKS, 6);
+        k_guide_wgrad<<<wg, 256, 0, st>>>(g, k);
+        n += 2;
+        if (!adam) continue;
+        k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g, k);
+        ++n;
+    }
+    return n;
 }
 }  // namespace
 
@@ -1418,22 +1441,27 @@ int launch_guide_infer_multi(const FrameArgs* items, int n_items, uint32_t bounc
     return 1;
 }
 
-int launch_guide_train_multi(const FrameArgs* items, int n_items, int sm_count, cudaStream_t st) {
+int launch_guide_train_multi(const FrameArgs* items, int n_items, uint32_t max_steps, int sm_count,
+                             cudaStream_t st) {
     if (n_items <= 0) return 0;
     const uint32_t sm = (uint32_t)(sm_count > 0 ? sm_count : 148);
     const uint32_t per = std::max(8u, 2u * sm / (uint32_t)n_items);  // forward/backward blocks per item
     const uint32_t n = (uint32_t)n_items;
     k_guide_targets_multi<<<dim3(std::max(8u, 4u * sm / n), n), 256, 0, st>>>(items);
-    k_guide_fwdbwd_multi<<<dim3(per, n), GWT * 32, guide_train_smem(), st>>>(items);
-    k_guide_wgrad_multi<<<dim3(WGRAD_BLOCKS, 6, n), 256, 0, st>>>(items);
-    k_guide_adam_multi<<<dim3((G_NPARAMS + 255) / 256, n), 256, 0, st>>>(items);
+    int launches = 2;
+    for (int k = 0; k < (int)std::max(max_steps, 1u); ++k) {
+        k_guide_fwdbwd_multi<<<dim3(per, n), GWT * 32, guide_train_smem(), st>>>(items, k);
+        k_guide_wgrad_multi<<<dim3(WGRAD_BLOCKS, 6, n), 256, 0, st>>>(items, k);
+        k_guide_adam_multi<<<dim3((G_NPARAMS + 255) / 256, n), 256, 0, st>>>(items, k);
+        launches += 3;
+    }
     k_guide_frame_end_multi<<<n, 32, 0, st>>>(items);
-    return 5;
+    return launches;
 }
 
 int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st) {
     if (phase == 0) return launch_train_steps(g, 148, 0, st);
-    k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g);
+    k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g, 0);
     return 1;
 }
 
@@ -1470,6 +1498,7 @@ void guide_default_params(uint64_t seed, float* out) {
 
 cudaError_t guide_alloc(GuideArgs& g, size_t n_verts) {
     g = GuideArgs{};
+    g.steps = 1;
     cudaError_t e = cudaSuccess;
     auto chk = [&](cudaError_t r) {
         if (e == cudaSuccess) e = r;
@@ -1516,6 +1545,22 @@ void guide_free(GuideArgs& g) {
                     g.rec.thr, g.rec.rad, g.rec.pid, g.rec.weight, g.rec.act, g.rec.delta, g.gc};
     for (void* b : bufs) cudaFree(b);
     g = GuideArgs{};
+}
+
+size_t guide_state_bytes() { return (size_t)G_NPARAMS * (4 * 3 + 2) + sizeof(GuideCounters); }
+
+cudaError_t guide_state_copy(GuideArgs& g, void* buf, bool save, cudaStream_t st) {
+    unsigned char* b = static_cast<unsigned char*>(buf);
+    void* parts[] = {g.net.master, g.net.adam_m, g.net.adam_v, g.net.wbf, g.gc};
+    const size_t sizes[] = {(size_t)G_NPARAMS * 4, (size_t)G_NPARAMS * 4, (size_t)G_NPARAMS * 4, (size_t)G_NPARAMS * 2,
+                            sizeof(GuideCounters)};
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 5 && e == cudaSuccess; ++i) {
+        e = save ? cudaMemcpyAsync(b, parts[i], sizes[i], cudaMemcpyDeviceToDevice, st)
+                 : cudaMemcpyAsync(parts[i], b, sizes[i], cudaMemcpyDeviceToDevice, st);
+        b += sizes[i];
+    }
+    return e;
 }
 
 cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m, const float* adam_v,

@@ -99,6 +99,7 @@ struct GuideArgs {
     int train;               // run a training step after each frame
     float lr;
     uint32_t batch;          // training samples recorded per frame (<= G_REC_CAP)
+    uint32_t steps;          // Adam steps per frame, each on a consecutive 1/steps of the records
     int tc;                  // inference on tcgen05 / tensor memory (else mma.sync)
 };
 static_assert(G_NPARAMS % 8 == 0 && g_woff(1) % 8 == 0 && g_woff(2) % 8 == 0 && g_woff(3) % 8 == 0 &&
@@ -116,7 +117,8 @@ int launch_guide_train(const FrameArgs& a, cudaStream_t st);
 // item (those with train set) in five grouped launches.
 int launch_guide_infer_multi(const FrameArgs* items, int n_items, uint32_t bounce, uint32_t* fetch, int sm_count,
                              cudaStream_t st);
-int launch_guide_train_multi(const FrameArgs* items, int n_items, int sm_count, cudaStream_t st);
+int launch_guide_train_multi(const FrameArgs* items, int n_items, uint32_t max_steps, int sm_count,
+                             cudaStream_t st);
 // tc: the tcgen05 kernel (err: device error word for an MMA wait that gave up).
 int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, float* y, int tc, uint32_t* err,
                               cudaStream_t st);
@@ -124,7 +126,7 @@ int launch_guide_test_forward(const GuideNet& net, const float* x, uint32_t n, f
 int launch_guide_test_mixture(const float* raw, const float* omega, const float* u, uint32_t n, float* out, int tc,
                               cudaStream_t st);
 // phase 0: forward + backward + weight gradients of gc->records records
-// (gc->weight_sum set by the caller); phase 1: one Adam step.
+// (gc->weight_sum set by the caller; g.steps = 1); phase 1: one Adam step.
 int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st);
 
 // Host side: deterministic default weights (G_NPARAMS floats), device
@@ -133,6 +135,10 @@ int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st);
 void guide_default_params(uint64_t seed, float* out);
 cudaError_t guide_alloc(GuideArgs& g, size_t n_verts);
 void guide_free(GuideArgs& g);
+// The trainable state (FP32 and bf16 weights, Adam moments, counters) to or
+// from a device buffer of guide_state_bytes() (stream-ordered copies).
+size_t guide_state_bytes();
+cudaError_t guide_state_copy(GuideArgs& g, void* buf, bool save, cudaStream_t st);
 cudaError_t guide_upload(GuideArgs& g, const float* params, const float* adam_m, const float* adam_v,
                          uint32_t adam_step);
 
