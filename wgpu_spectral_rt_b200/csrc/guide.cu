@@ -412,6 +412,24 @@ SRT_DEV void vertex_inputs(float3 p, float3 n, float3 wo, float lambda, float4 b
     x[9] = (lambda - LAMBDA_MIN) / LAMBDA_RANGE;
 }
 
+// Warp-aggregated counter updates from the lanes that execute the call
+// together (one atomic per warp instead of one per lane; every guided vertex
+// counts itself, so per-lane atomics on one address would queue in L2):
+// agg_add adds the lanes' count, agg_slot also hands each lane its own slot.
+SRT_DEV void agg_add(uint32_t* ctr) {
+    const uint32_t m = __activemask();
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(m) - 1)) atomicAdd(ctr, (uint32_t)__popc(m));
+}
+SRT_DEV uint32_t agg_slot(uint32_t* ctr) {
+    const uint32_t m = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == (uint32_t)leader) base = atomicAdd(ctr, (uint32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
 // Throughput, training record, Russian roulette and the next ray of guided
 // vertex v (path id) once its direction is drawn; the direction's sampling
 // pdf is sel q + (1 - sel) cos / pi.  Returns whether the path continues.
@@ -432,10 +450,10 @@ SRT_DEV bool finish_vertex(const FrameArgs& a, uint32_t bounce, uint32_t frame, 
         thr = thr * att;
         // training sample (a hashed subset of the vertices)
         if (G.train) {
-            atomicAdd(&G.gc->candidates, 1u);
+            agg_add(&G.gc->candidates);
             uint32_t h = pcg_hash(id ^ (bounce << 24) ^ (frame * 0x9E3779B9u)) & 0xFFFFu;
             if (h < G.gc->threshold) {
-                uint32_t r = atomicAdd(&G.gc->records, 1u);
+                uint32_t r = agg_slot(&G.gc->records);
                 if (r < G.batch) {
                     float x[G_IN];
                     vertex_inputs(hp, ffn, xyz(wo4), p.w, S.bmin, S.binv, x);
