@@ -604,6 +604,11 @@ extern "C" srt_status srt_scene_info(const srt_scene* s, uint64_t* n_tris, uint6
 }
 
 // ====================================================================== renderer
+// Frames enqueue independent stages on two branches (srt_renderer::record_overlapped).
+#ifndef SRT_FRAME_OVERLAP
+#define SRT_FRAME_OVERLAP 1
+#endif
+
 struct srt_renderer {
     srt_ctx* ctx = nullptr;
     srt_scene* scene = nullptr;
@@ -623,6 +628,8 @@ struct srt_renderer {
     double4* accum64 = nullptr;
     uchar4* ldr = nullptr;
     cudaStream_t cap_stream = nullptr;
+    cudaStream_t side_stream = nullptr;  // the second branch of an overlapped frame
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaGraphExec_t graph = nullptr;
     int launches_per_frame = 0;
     uint32_t frame_count = 0;
@@ -638,6 +645,9 @@ struct srt_renderer {
     ~srt_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (side_stream) cudaStreamDestroy(side_stream);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
         for (auto& e : ring_ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : ev) cudaEventDestroy(e);
@@ -660,8 +670,9 @@ struct srt_renderer {
     }
 
     // Enqueues one frame (after the camera upload).  stage timing: events
-    // between stages (only when `timed`).
+    // between stages (only when `timed`, which keeps every stage in order).
     int record(cudaStream_t st, bool timed) {
+        if (!timed && SRT_FRAME_OVERLAP) return record_overlapped(st);
         int n = 0;
         size_t e = 0;
         auto mark = [&]() {
@@ -690,6 +701,48 @@ struct srt_renderer {
         mark();
         if (args.guiding) n += launch_guide_train(args, st);
         mark();
+        return n;
+    }
+
+    // The same frame with independent stages side by side (two branches that
+    // fork from and join `st`): the camera rays and their first closest hits
+    // beside the photon pass (neither reads the other's buffers; shading
+    // joins them), and after each shading step the shadow rays of bounce b
+    // beside the closest hits of bounce b + 1 (the shadow rays add to the
+    // path radiance, which the shading of b + 1 reads after the join; the
+    // closest hits read and write only rays, queues and hits).  The results
+    // are those of the serial order.
+    int record_overlapped(cudaStream_t st) {
+        int n = 0;
+        cudaStream_t s2 = side_stream;
+        auto fork = [&]() {
+            cudaEventRecord(fork_ev, st);
+            cudaStreamWaitEvent(s2, fork_ev, 0);
+        };
+        auto join = [&]() {
+            cudaEventRecord(join_ev, s2);
+            cudaStreamWaitEvent(st, join_ev, 0);
+        };
+        cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
+        fork();
+        n += launch_raygen(args, s2);
+        n += launch_bounce(args, 0, s2, 1);
+        if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
+        join();
+        for (uint32_t b = 0; b < p.max_depth; ++b) {
+            n += launch_bounce(args, b, st, 2);
+            if (b + 1 < p.max_depth) {
+                fork();
+                n += launch_bounce(args, b, s2, 3);
+                n += launch_bounce(args, b + 1, st, 1);
+                join();
+            } else {
+                n += launch_bounce(args, b, st, 3);
+            }
+        }
+        n += launch_finalize(args, st);
+        n += launch_frame_stats(args, st);
+        if (args.guiding) n += launch_guide_train(args, st);
         return n;
     }
 
@@ -882,6 +935,9 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     r->ev.resize(n_events);
     for (auto& e : r->ev) CUDA_TRY(c, cudaEventCreate(&e));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&r->side_stream, cudaStreamNonBlocking));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&r->fork_ev, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&r->join_ev, cudaEventDisableTiming));
     if (env_fault("launch")) return fail(c, SRT_ERR_CUDA, "injected launch failure");
     ctx_retain(c);
     *out = r.release();
