@@ -1619,6 +1619,8 @@ struct srt_batch {
     cudaStream_t cap = nullptr;
     cudaEvent_t fork_ev = nullptr;
     std::vector<cudaEvent_t> join_ev;
+    cudaStream_t ovl = nullptr;  // shadow rays of bounce b beside the closest hits of b + 1
+    cudaEvent_t ovl_fork = nullptr, ovl_join = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::vector<uint8_t> graph_active;
     int graph_launches = 0;
@@ -1632,6 +1634,9 @@ struct srt_batch {
             if (s) cudaStreamDestroy(s);
         if (cap) cudaStreamDestroy(cap);
         if (fork_ev) cudaEventDestroy(fork_ev);
+        if (ovl) cudaStreamDestroy(ovl);
+        if (ovl_fork) cudaEventDestroy(ovl_fork);
+        if (ovl_join) cudaEventDestroy(ovl_join);
         for (auto e : join_ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : up_ev)
@@ -1695,15 +1700,32 @@ struct srt_batch {
         };
         cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 3 * MAX_BOUNCES, cap);
         fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_begin(s); });
+        auto closest = [&](uint32_t b, cudaStream_t s) {
+            return launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
+                                      (int)tune.blocks_per_sm, tune.chunk, c->sm_count, s);
+        };
+        auto shadow = [&](uint32_t b, cudaStream_t s) {
+            return launch_trace_multi(items_dev + ((size_t)MAX_BOUNCES + b) * MAX_BATCH, na, 1, small_stack,
+                                      fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count,
+                                      s);
+        };
+        n += closest(0, cap);
         for (uint32_t b = 0; b < max_depth; ++b) {
-            n += launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
-                                    (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
             fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
             if (ng && b + 1 < guide_depth)
                 n += launch_guide_infer_multi(guide_items_dev, ng, b, fetch_dev + 2 * MAX_BOUNCES + b, c->sm_count,
                                               cap);
-            n += launch_trace_multi(items_dev + ((size_t)MAX_BOUNCES + b) * MAX_BATCH, na, 1, small_stack,
-                                    fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count, cap);
+            if (b + 1 < max_depth) {
+                // independent: the shadow rays add to the radiance, the closest hits read rays and queues
+                cudaEventRecord(ovl_fork, cap);
+                cudaStreamWaitEvent(ovl, ovl_fork, 0);
+                n += shadow(b, ovl);
+                n += closest(b + 1, cap);
+                cudaEventRecord(ovl_join, ovl);
+                cudaStreamWaitEvent(cap, ovl_join, 0);
+            } else {
+                n += shadow(b, cap);
+            }
         }
         fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_end(s, false); });
         if (ng) n += launch_guide_train_multi(guide_items_dev, ng, guide_steps, c->sm_count, cap);
@@ -1779,6 +1801,9 @@ extern "C" srt_status srt_batch_create(srt_ctx* c, uint32_t n, srt_scene* const*
     CUDA_TRY(c, dev_alloc(&B->guide_items_dev, (size_t)MAX_BATCH));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
     CUDA_TRY(c, cudaEventCreateWithFlags(&B->fork_ev, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&B->ovl, cudaStreamNonBlocking));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&B->ovl_fork, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&B->ovl_join, cudaEventDisableTiming));
     B->side.assign(n, nullptr);
     B->join_ev.assign(n, nullptr);
     for (uint32_t i = 0; i < n; ++i) {
