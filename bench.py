@@ -160,7 +160,7 @@ def build_scene(srt, ctx, preset_name: str, seed: int = 0):
 def cpu_baseline(srt, b, cam, w, h, params, seconds_target=15.0, threads=0):
     """The CPU oracle on a bounded sample of one frame (row subset + the same share of photons)."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import binding as orc  # the checker, used here as the timed CPU baseline
+    import binding as orc  # the oracle, timed here as the CPU baseline
 
     t0 = time.perf_counter()
     o = orc.OracleScene(b.arrays())

@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, as the checker.  The product package never
+CPU-baseline leg of bench.py, to check the CUDA path.  The product package never
 imports it.
 """
 from __future__ import annotations

@@ -1,6 +1,6 @@
 """FP64 CPU oracle of the neural path-guiding network (numpy).
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA guiding kernels.  The
+TEST INFRASTRUCTURE ONLY: the oracle for the CUDA guiding kernels.  The
 reference has no path guiding; this restates the project's own definition of
 the network, the vMF mixture and the training loss in float64, so that the
 GPU's forward outputs, mixture pdfs, loss gradients and Adam steps can be

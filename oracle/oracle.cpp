@@ -1,7 +1,7 @@
 // oracle.cpp — CPU oracle of the spectral path-tracing path.
 //
 // TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and the
-// CPU-baseline leg of bench.py as the checker.  The product library never
+// CPU-baseline leg of bench.py, to check the CUDA path.  The product library never
 // links or calls it.
 //
 // Every shading function restates the reference WGSL in FP32 with the same

@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
  * calls this code; only the tests, the smoke check and the benchmark's CPU
- * baseline leg do, as the checker.
+ * baseline leg do, to check the CUDA path against it.
  *
  * The oracle restates the reference's WGSL hot path in C++ FP32 (same
  * operation order, same RNG consumption order), with closest-hit / any-hit

@@ -1,6 +1,6 @@
 """CPU restatement of the reference's two raster steps (numpy, float32).
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA presentation kernels.
+TEST INFRASTRUCTURE ONLY: the oracle for the CUDA presentation kernels.
 
 * Letterbox blit: renderer/blit_pass.rs:114-154 (scale of the quad from the
   target and window aspect ratios), shaders/blit.wgsl:7-34 (a quad over
