@@ -231,7 +231,7 @@ srt_status srt_scene_builder_add_instance(srt_scene_builder* b, uint32_t mesh_id
 /* builder.rs:101-129: adds the instance and one world-space srt_light per triangle */
 srt_status srt_scene_builder_add_light_instance(srt_scene_builder* b, uint32_t mesh_id, uint32_t mat_id,
                                                 const float transform[16], const float params[4]);
-/* Counts and read-only views of the builder's host arrays (for checkers and
+/* Counts and read-only views of the builder's host arrays (for CPU comparisons and
  * for srt_scene_build).  Pointers stay valid until the builder changes. */
 typedef struct srt_scene_arrays {
     const srt_vertex* vertices;     uint32_t n_vertices;
