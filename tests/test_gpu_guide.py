@@ -250,9 +250,13 @@ def test_guiding_rejects_ray_sort(srt, ctx):
 
 def test_trained_guide_reduces_error(srt, ctx):
     """What the guide gains: on a room lit only through a small ceiling spot,
-    guided path tracing (learning online from frame 0) reaches a lower relMSE
+    guided path tracing (learning online from frame 0) reaches a lower error
     than plain path tracing at the same sample count, against a 16384-spp FP64
-    reference on decorrelated sample streams."""
+    reference on decorrelated sample streams.  The per-pixel relative squared
+    error is heavy-tailed (a few firefly pixels carry up to half of the mean,
+    so the mean moves between runs of the online training), so the test
+    compares its median (measured gain 1.9x) and its mean without the worst
+    1 % of pixels (measured gain 1.25-1.55x)."""
     b = srt.SceneBuilder()
     cam = b.add_preset(srt.PRESET_INDIRECT_ROOM)
     scene = b.build(ctx)
@@ -271,9 +275,14 @@ def test_trained_guide_reduces_error(srt, ctx):
     ref = run(0, 16384, seed=0x5EED0001)
     plain = run(0, 1024)
     guided = run(srt.FLAG_GUIDING, 1024)
-    e_plain = float(np.mean((plain - ref) ** 2 / (ref ** 2 + 0.01)))
-    e_guided = float(np.mean((guided - ref) ** 2 / (ref ** 2 + 0.01)))
-    assert e_guided * 1.15 < e_plain, (e_plain, e_guided)
+    def errors(x):
+        e = np.sort(np.mean((x - ref) ** 2 / (ref ** 2 + 0.01), axis=-1).ravel())
+        return float(np.median(e)), float(e[:int(0.99 * e.size)].mean())
+
+    med_p, trim_p = errors(plain)
+    med_g, trim_g = errors(guided)
+    assert med_g * 1.4 < med_p, (med_p, med_g)
+    assert trim_g * 1.1 < trim_p, (trim_p, trim_g)
 
 
 def test_tcgen05_and_mma_sync_inference_agree(srt, ctx):
