@@ -746,14 +746,13 @@ struct srt_renderer {
         return n;
     }
 
-    // The same frame in three parts for the batched renderer, which traces
-    // the rays of all its scenes in shared launches between them.
-    int record_begin(cudaStream_t st) {
-        int n = 0;
-        cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
-        if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
-        return n + launch_raygen(args, st);
+    // The same frame in parts for the batched renderer, which traces the
+    // rays of all its scenes in shared launches between them.
+    void record_clear(cudaStream_t st) { cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st); }
+    int record_photons(cudaStream_t st) {
+        return p.photons_per_frame > 0 && scene->n_lights > 0 ? launch_photon_pass(args, st) : 0;
     }
+    int record_raygen(cudaStream_t st) { return launch_raygen(args, st); }
     // guide = false: the guided continuation and the training step are left
     // to the batch's grouped guide kernels
     int record_shade(uint32_t b, cudaStream_t st, bool guide) {
@@ -1699,7 +1698,7 @@ struct srt_batch {
             for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
         };
         cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 3 * MAX_BOUNCES, cap);
-        fork_join([](srt_renderer* x, cudaStream_t s) { return x->record_begin(s); });
+        for (int k = 0; k < na; ++k) r[act[k]]->record_clear(cap);
         auto closest = [&](uint32_t b, cudaStream_t s) {
             return launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
                                       (int)tune.blocks_per_sm, tune.chunk, c->sm_count, s);
@@ -1709,7 +1708,17 @@ struct srt_batch {
                                       fetch_dev + MAX_BOUNCES + b, (int)tune.blocks_per_sm, tune.chunk, c->sm_count,
                                       s);
         };
+        // the scenes' photon passes on their branches, beside the camera rays
+        // and their first closest hits (shading, after the join, reads both)
+        cudaEventRecord(fork_ev, cap);
+        for (int k = 0; k < na; ++k) {
+            cudaStreamWaitEvent(side[k], fork_ev, 0);
+            n += r[act[k]]->record_photons(side[k]);
+            cudaEventRecord(join_ev[k], side[k]);
+        }
+        for (int k = 0; k < na; ++k) n += r[act[k]]->record_raygen(cap);
         n += closest(0, cap);
+        for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
         for (uint32_t b = 0; b < max_depth; ++b) {
             fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
             if (ng && b + 1 < guide_depth)
