@@ -339,6 +339,19 @@ srt_status srt_save_screenshot(srt_renderer* r, const char* path);
  * with the rows flipped and the sRGB OETF applied to the 8-bit values. */
 srt_status srt_screenshot_write(const char* path, const uint8_t* rgba, uint32_t width, uint32_t height,
                                 uint32_t pitch);
+/* The same two steps with the PNG encoding on a worker thread, as the
+ * reference's engine does with its screenshot channel (engine.rs:39-45,
+ * :242): srt_save_screenshot_async reads the image back (synchronously, like
+ * Engine::save_screenshot) and queues the encoding and the file write;
+ * srt_screenshot_write_async copies `rgba` and queues the same.  Jobs run in
+ * order on one library-owned thread.  srt_screenshot_flush blocks until every
+ * queued write is done and returns in *failed_writes (may be NULL) how many
+ * failed since the previous flush.  Queued writes finish before the process
+ * exits. */
+srt_status srt_save_screenshot_async(srt_renderer* r, const char* path);
+srt_status srt_screenshot_write_async(const char* path, const uint8_t* rgba, uint32_t width, uint32_t height,
+                                      uint32_t pitch);
+srt_status srt_screenshot_flush(uint32_t* failed_writes);
 srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out);
 srt_status srt_renderer_reset_stats(srt_renderer* r);
 /* The photon set of the last frame in emission order (photon_emit.wgsl

@@ -167,6 +167,25 @@ def test_screenshot_flip_and_srgb(srt, tmp_path):
     assert np.array_equal(got, exp)
 
 
+def test_screenshot_worker_writes_the_same_files(srt, tmp_path):
+    """srt_screenshot_write_async: PNGs encoded on the library's worker thread are
+    byte-identical to the synchronous writer's; the caller's buffer may change
+    right after the call; a failed write is counted once by the next flush."""
+    rng = np.random.default_rng(1)
+    imgs = [rng.integers(0, 256, (9 + k, 6 + 2 * k, 4), dtype=np.uint8) for k in range(4)]
+    for k, img in enumerate(imgs):
+        srt.screenshot_write(tmp_path / f"sync{k}.png", img)
+        srt.screenshot_write_async(tmp_path / f"async{k}.png", img)
+        img[:] = 0  # the job holds its own copy
+    srt.screenshot_write_async(tmp_path / "no_such_dir" / "x.png", imgs[0])
+    assert srt.screenshot_flush() == 1
+    assert srt.screenshot_flush() == 0
+    for k in range(4):
+        assert (tmp_path / f"async{k}.png").read_bytes() == (tmp_path / f"sync{k}.png").read_bytes()
+    with pytest.raises(srt.SrtError):
+        srt.screenshot_write_async(tmp_path / "bad.png", np.zeros((0, 4, 4), np.uint8))
+
+
 def test_invalid_arguments_fail_cleanly(srt):
     L = srt.lib()
     assert L.srt_scene_builder_add_instance(None, 0, 0, None) == 1

@@ -324,6 +324,9 @@ def test_accumulation_reset_and_stats(srt, ctx, config1, tmp_path):
     assert st["frames"] == 5 and st["paths"] == 5 * w * h and st["rays_closest"] > st["paths"]
     r.save_screenshot(tmp_path / "s.png")
     assert (tmp_path / "s.png").stat().st_size > 100
+    r.save_screenshot_async(tmp_path / "a.png")  # read back now, encoded on the worker thread
+    assert srt.screenshot_flush() == 0
+    assert (tmp_path / "a.png").read_bytes() == (tmp_path / "s.png").read_bytes()
     r.close()
 
 

@@ -172,6 +172,9 @@ SIGNATURES = {
     "srt_read_ldr_rgba8": (_I, [_P, _P, _U32]),
     "srt_save_screenshot": (_I, [_P, C.c_char_p]),
     "srt_screenshot_write": (_I, [C.c_char_p, _P, _U32, _U32, _U32]),
+    "srt_save_screenshot_async": (_I, [_P, C.c_char_p]),
+    "srt_screenshot_write_async": (_I, [C.c_char_p, _P, _U32, _U32, _U32]),
+    "srt_screenshot_flush": (_I, [_P]),
     "srt_renderer_get_stats": (_I, [_P, C.POINTER(Stats)]),
     "srt_renderer_reset_stats": (_I, [_P]),
     "srt_renderer_read_photons": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
@@ -513,6 +516,11 @@ class Renderer:
     def save_screenshot(self, path: str | os.PathLike):
         _check(lib().srt_save_screenshot(self.h, str(path).encode()), self.ctx.h)
 
+    def save_screenshot_async(self, path: str | os.PathLike):
+        """Reads the image back now; the PNG is encoded and written on the library's worker thread
+        (screenshot_flush waits for it)."""
+        _check(lib().srt_save_screenshot_async(self.h, str(path).encode()), self.ctx.h)
+
     def stats(self) -> dict:
         s = Stats()
         _check(lib().srt_renderer_get_stats(self.h, C.byref(s)), self.ctx.h)
@@ -589,6 +597,20 @@ def screenshot_write(path, rgba: np.ndarray) -> None:
     a = np.ascontiguousarray(rgba, np.uint8)
     h, w = a.shape[:2]
     _check(lib().srt_screenshot_write(str(path).encode(), ptr(a), w, h, 4 * w))
+
+
+def screenshot_write_async(path, rgba: np.ndarray) -> None:
+    """screenshot_write on the library's worker thread (the pixels are copied before this returns)."""
+    a = np.ascontiguousarray(rgba, np.uint8)
+    h, w = a.shape[:2]
+    _check(lib().srt_screenshot_write_async(str(path).encode(), ptr(a), w, h, 4 * w))
+
+
+def screenshot_flush() -> int:
+    """Waits for every queued screenshot write; returns how many failed since the previous flush."""
+    n = C.c_uint32()
+    _check(lib().srt_screenshot_flush(C.byref(n)))
+    return n.value
 
 
 def photon_grid_build(ctx: Context, photons: np.ndarray, frame: int, cell: float = 0.02, hash_bits: int = 22):

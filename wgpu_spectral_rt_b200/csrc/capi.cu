@@ -1090,6 +1090,20 @@ extern "C" srt_status srt_save_screenshot(srt_renderer* r, const char* path) {
     return SRT_OK;
 }
 
+extern "C" srt_status srt_save_screenshot_async(srt_renderer* r, const char* path) {
+    if (!r || !path) return SRT_ERR_INVALID_ARG;
+    uint32_t pitch = (4 * r->w + 255u) & ~255u;  // utils/wgpu.rs:53-58
+    std::vector<uint8_t> buf((size_t)pitch * r->h);
+    srt_status s = srt_read_ldr_rgba8(r, buf.data(), pitch);
+    if (s != SRT_OK) return s;
+    try {
+        screenshot_enqueue(path, std::move(buf), r->w, r->h, pitch);
+    } catch (const std::exception& e) {
+        return fail(r->ctx, SRT_ERR_OOM, std::string("screenshot worker: ") + e.what());
+    }
+    return SRT_OK;
+}
+
 extern "C" srt_status srt_screenshot_write(const char* path, const uint8_t* rgba, uint32_t w, uint32_t h,
                                            uint32_t pitch) {
     if (!path || !rgba || w == 0 || h == 0 || pitch < 4 * w) return SRT_ERR_INVALID_ARG;

@@ -63,4 +63,8 @@ void camera_build_uniform(const float pos[3], float yaw, float pitch, float aspe
 // screenshot.rs:27-103: padded RGBA8 rows (row 0 = bottom) -> PNG with the
 // rows flipped and the sRGB OETF applied to the 8-bit values.
 bool write_screenshot_png(const std::string& path, const uint8_t* rgba, uint32_t w, uint32_t h, uint32_t pitch);
+// The same on the library's screenshot worker thread (screenshot_worker.cpp):
+// the job owns `rgba`; srt_screenshot_flush waits for it.
+void screenshot_enqueue(const std::string& path, std::vector<uint8_t>&& rgba, uint32_t w, uint32_t h,
+                        uint32_t pitch);
 uint8_t srgb_oetf_u8(uint8_t c);
