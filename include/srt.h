@@ -319,6 +319,13 @@ srt_status srt_reset_accumulation(srt_renderer* r);
 srt_status srt_read_accum_f32(srt_renderer* r, float* rgba);
 /* FP64 accumulation (SRT_FLAG_FP64_ACCUM): width*height double4. */
 srt_status srt_read_accum_f64(srt_renderer* r, double* rgba);
+/* Resume of an accumulation (no reference counterpart; the reference keeps
+ * its sums only in GPU memory): loads w*h RGBA FP64 sums in the layout
+ * srt_read_accum_f64 returns into the FP64 accumulation, and their FP32
+ * roundings into the FP32 one.  A later frame whose camera uniform carries
+ * frame_count N > 0 adds to them, so a long render read back after N frames
+ * continues where it stopped.  Requires SRT_FLAG_FP64_ACCUM. */
+srt_status srt_write_accum_f64(srt_renderer* r, const double* rgba);
 /* Tonemapped RGBA8 storage texture (shader.wgsl:809-822), row 0 = bottom
  * row, `pitch` bytes per row (>= 4*width). */
 srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t pitch);
@@ -442,6 +449,18 @@ srt_status srt_guide_default_weights(uint64_t seed, float* out, uint32_t n);
 /* Checkpoint / restore of a guiding renderer's FP32 weights (restore resets Adam). */
 srt_status srt_renderer_guide_get_weights(srt_renderer* r, float* out, uint32_t n);
 srt_status srt_renderer_guide_set_weights(srt_renderer* r, const float* w, uint32_t n);
+/* Checkpoint / resume of the whole training state: FP32 weights and the two
+ * Adam moments (srt_guide_param_count() floats each) and the Adam step count.
+ * set_state puts all of it back, so training continues where it stopped. */
+/* Failure-path test: one block waits on a device barrier that never
+ * completes, giving up after `polls` polls (1..2^20) like the tensor-core
+ * kernels' bounded waits; returns SRT_ERR_TIMEOUT, and the context stays
+ * usable. */
+srt_status srt_test_wait_timeout(srt_ctx* ctx, uint32_t polls);
+srt_status srt_renderer_guide_get_state(srt_renderer* r, float* params, float* adam_m, float* adam_v,
+                                        uint32_t* adam_step);
+srt_status srt_renderer_guide_set_state(srt_renderer* r, const float* params, const float* adam_m,
+                                        const float* adam_v, uint32_t adam_step);
 srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_steps, uint32_t* record_threshold);
 /* Adam learning rate (default 1e-3; < 0 keeps it) and training samples
  * recorded per frame (default 65536, at most 262144; 0 keeps it). */

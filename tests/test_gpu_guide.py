@@ -223,6 +223,34 @@ def test_several_adam_steps_per_frame(srt, ctx):
     batch.close()
 
 
+def test_guide_training_state_checkpoint(srt, ctx):
+    """srt_renderer_guide_get_state / set_state: weights, Adam moments and step
+    count move to a new renderer unchanged, and its training counts on from
+    there."""
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b.build(ctx)
+    w, h = 48, 32
+    trained = _render(srt, ctx, scene, cam, w, h, srt.FLAG_GUIDING, 8)
+    st = trained.guide_state()
+    assert st["adam_step"] == 8 and np.any(st["adam_m"] != 0) and np.all(st["adam_v"] >= 0)
+    np.testing.assert_array_equal(st["params"], trained.guide_weights())
+    r = _render(srt, ctx, scene, cam, w, h, srt.FLAG_GUIDING, 0)
+    r.set_guide_state(st)
+    back = r.guide_state()
+    for k in ("params", "adam_m", "adam_v"):
+        np.testing.assert_array_equal(back[k], st[k])
+    assert back["adam_step"] == 8 and r.guide_info()["adam_steps"] == 8
+    ctl = srt.CameraController(*cam)
+    for f in range(8, 10):
+        r.render(ctl.build_uniform(w / h, f))
+    ctx.synchronize()
+    assert r.guide_info()["adam_steps"] == 10
+    assert np.all(np.isfinite(r.guide_weights()))
+    trained.close()
+    r.close()
+
+
 def test_frozen_guide_is_deterministic_and_restores(srt, ctx):
     b = srt.SceneBuilder()
     cam = b.add_preset(srt.PRESET_CORNELL_BOX)

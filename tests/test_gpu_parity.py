@@ -341,3 +341,43 @@ def test_graph_and_direct_launch_agree(srt, ctx, config1):
         outs.append(r.read_accum())
         r.close()
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
+def test_accumulation_resume_continues_bit_for_bit(srt, ctx, cornell):
+    """srt_write_accum_f64: FP64 sums read back after 5 frames and loaded into a
+    new renderer continue, frame for frame, exactly as the uninterrupted render."""
+    b, scene, o, cam = cornell
+    w, h = 32, 24
+    p = srt.default_params(photons_per_frame=1 << 14, flags=srt.FLAG_FP64_ACCUM)
+    r = srt.Renderer(ctx, scene, w, h, p)
+    for f in range(5):
+        r.render(_cam(srt, cam, w, h, f))
+    saved = r.read_accum64()
+    for f in range(5, 9):
+        r.render(_cam(srt, cam, w, h, f))
+    full = r.read_accum64()
+    r2 = srt.Renderer(ctx, scene, w, h, p)
+    r2.write_accum64(saved)
+    np.testing.assert_array_equal(r2.read_accum64(), saved)
+    for f in range(5, 9):
+        r2.render(_cam(srt, cam, w, h, f))
+    np.testing.assert_array_equal(r2.read_accum64(), full)
+    assert np.all(r2.read_accum()[..., 3] == 9)
+    plain = srt.Renderer(ctx, scene, w, h, srt.default_params(photons_per_frame=1 << 14))
+    with pytest.raises(srt.SrtError):
+        plain.write_accum64(saved)  # no FP64 accumulation to load into
+    for x in (r, r2, plain):
+        x.close()
+
+
+def test_bounded_wait_timeout_is_reported_and_context_survives(srt, ctx, cornell):
+    """A device wait that cannot complete gives up after its poll limit; the
+    host gets SRT_ERR_TIMEOUT and the context keeps working."""
+    with pytest.raises(srt.SrtError) as e:
+        srt.wait_timeout_check(ctx, 1000)
+    assert e.value.status == 4  # SRT_ERR_TIMEOUT
+    b, scene, o, cam = cornell
+    r = srt.Renderer(ctx, scene, 16, 16, srt.default_params(photons_per_frame=1 << 12))
+    r.render(_cam(srt, cam, 16, 16, 0))
+    assert np.all(r.read_accum()[..., 3] == 1)
+    r.close()

@@ -213,6 +213,10 @@ SIGNATURES = {
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_mixture_tc": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_renderer_guide_set_steps": (_I, [_P, _U32]),
+    "srt_renderer_guide_get_state": (_I, [_P, _P, _P, _P, _P]),
+    "srt_renderer_guide_set_state": (_I, [_P, _P, _P, _P, _U32]),
+    "srt_write_accum_f64": (_I, [_P, _P]),
+    "srt_test_wait_timeout": (_I, [_P, _U32]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
 
@@ -495,6 +499,14 @@ class Renderer:
         _check(lib().srt_read_accum_f64(self.h, ptr(out)), self.ctx.h)
         return out
 
+    def write_accum64(self, sums: np.ndarray) -> None:
+        """Loads FP64 sums [h, w, 4] (as read_accum64 returns them) to resume an accumulation; the next
+        frame must carry the frame count the sums were read at."""
+        a = np.ascontiguousarray(sums, np.float64)
+        if a.shape != (self.target_height, self.target_width, 4):
+            raise ValueError(f"expected shape {(self.target_height, self.target_width, 4)}, got {a.shape}")
+        _check(lib().srt_write_accum_f64(self.h, ptr(a)), self.ctx.h)
+
     def read_ldr(self) -> np.ndarray:
         out = np.zeros((self.target_height, self.target_width, 4), np.uint8)
         _check(lib().srt_read_ldr_rgba8(self.h, ptr(out), 4 * self.target_width), self.ctx.h)
@@ -555,6 +567,22 @@ class Renderer:
         out = np.zeros(guide_param_count(), np.float32)
         _check(lib().srt_renderer_guide_get_weights(self.h, ptr(out), len(out)), self.ctx.h)
         return out
+
+    def guide_state(self) -> dict:
+        """Checkpoint of the guide's training state: weights, Adam moments and step count."""
+        n = guide_param_count()
+        p, m, v = (np.zeros(n, np.float32) for _ in range(3))
+        step = C.c_uint32()
+        _check(lib().srt_renderer_guide_get_state(self.h, ptr(p), ptr(m), ptr(v), C.byref(step)), self.ctx.h)
+        return {"params": p, "adam_m": m, "adam_v": v, "adam_step": step.value}
+
+    def set_guide_state(self, state: dict) -> None:
+        p, m, v = (np.ascontiguousarray(state[k], np.float32) for k in ("params", "adam_m", "adam_v"))
+        n = guide_param_count()
+        if not (p.size == m.size == v.size == n):
+            raise ValueError(f"expected {n} values per array")
+        _check(lib().srt_renderer_guide_set_state(self.h, ptr(p), ptr(m), ptr(v), int(state["adam_step"])),
+               self.ctx.h)
 
     def set_guide_inference(self, kind: int) -> None:
         """GUIDE_INFER_MMA_SYNC or GUIDE_INFER_TCGEN05."""
@@ -655,6 +683,11 @@ def guide_default_weights(seed: int = 1) -> np.ndarray:
     out = np.zeros(guide_param_count(), np.float32)
     _check(lib().srt_guide_default_weights(seed, ptr(out), len(out)))
     return out
+
+
+def wait_timeout_check(ctx: Context, polls: int = 1000) -> None:
+    """Runs a device wait that cannot complete (bounded by `polls`); raises SrtError with SRT_ERR_TIMEOUT."""
+    _check(lib().srt_test_wait_timeout(ctx.h, polls), ctx.h)
 
 
 def guide_forward(ctx: Context, params: np.ndarray, x: np.ndarray, tcgen05: bool = False) -> np.ndarray:

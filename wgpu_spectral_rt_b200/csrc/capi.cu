@@ -17,6 +17,7 @@
 #include "host_scene.h"
 #include "radix_sort.cuh"
 #include "render_kernels.h"
+#include "umma.cuh"
 
 using namespace srt;
 
@@ -90,6 +91,10 @@ srt_status check_device_error(srt_ctx* c, uint32_t* d_err) {
     if (h != 0u) {
         CUDA_TRY(c, cudaMemsetAsync(d_err, 0, 4, c->stream));
         char buf[96];
+        if (h & ERR_MMA_TIMEOUT) {  // a bounded wait gave up; the context stays usable
+            std::snprintf(buf, sizeof buf, "a bounded device wait gave up (error word 0x%x)", h);
+            return fail(c, SRT_ERR_TIMEOUT, buf);
+        }
         std::snprintf(buf, sizeof buf, "device check failed (error word 0x%x)", h);
         return fail(c, SRT_ERR_DEVICE_ASSERT, buf);
     }
@@ -1042,6 +1047,21 @@ extern "C" srt_status srt_read_accum_f64(srt_renderer* r, double* rgba) {
     return check_device_error(c, r->err);
 }
 
+extern "C" srt_status srt_write_accum_f64(srt_renderer* r, const double* rgba) {
+    if (!r || !rgba) return SRT_ERR_INVALID_ARG;
+    if (!r->accum64) return fail(r->ctx, SRT_ERR_INVALID_ARG, "renderer created without SRT_FLAG_FP64_ACCUM");
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    const size_t np = (size_t)r->w * r->h;
+    std::vector<float4> f(np);
+    for (size_t i = 0; i < np; ++i)
+        f[i] = make_float4((float)rgba[4 * i], (float)rgba[4 * i + 1], (float)rgba[4 * i + 2], (float)rgba[4 * i + 3]);
+    CUDA_TRY(c, cudaMemcpyAsync(r->accum64, rgba, np * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(r->accum, f.data(), np * sizeof(float4), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SRT_OK;
+}
+
 extern "C" srt_status srt_read_ldr_rgba8(srt_renderer* r, uint8_t* out, uint32_t pitch) {
     if (!r || !out || pitch < 4 * r->w) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
@@ -1325,6 +1345,42 @@ extern "C" srt_status srt_renderer_guide_set_weights(srt_renderer* r, const floa
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     CUDA_TRY(c, guide_upload(r->guide, w, nullptr, nullptr, 0));
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_test_wait_timeout(srt_ctx* c, uint32_t polls) {
+    if (!c || polls == 0 || polls > (1u << 20)) return SRT_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    launch_test_wait_timeout(polls, c->d_err, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    return check_device_error(c, c->d_err);
+}
+
+extern "C" srt_status srt_renderer_guide_get_state(srt_renderer* r, float* params, float* adam_m, float* adam_v,
+                                                   uint32_t* adam_step) {
+    if (!r || !params || !adam_m || !adam_v || !adam_step) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    GuideCounters gc;
+    const size_t bytes = (size_t)G_NPARAMS * 4;
+    CUDA_TRY(c, cudaMemcpyAsync(params, r->guide.net.master, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(adam_m, r->guide.net.adam_m, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(adam_v, r->guide.net.adam_v, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(&gc, r->guide.gc, sizeof gc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    *adam_step = gc.adam_step;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_set_state(srt_renderer* r, const float* params, const float* adam_m,
+                                                   const float* adam_v, uint32_t adam_step) {
+    if (!r || !params || !adam_m || !adam_v) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, guide_upload(r->guide, params, adam_m, adam_v, adam_step));
     return SRT_OK;
 }
 

@@ -1358,6 +1358,18 @@ __global__ void k_guide_test_mixture_tc(const float* __restrict__ raw, const flo
     out[4 * i + 3] = d.z;
 }
 
+// A wait that cannot complete, for the failure-path test: an mbarrier that
+// expects one arrival and never gets it.  The bounded wait gives up after
+// `polls` polls and records ERR_MMA_TIMEOUT, as the inference kernels' MMA
+// waits do; nothing stays in flight.
+__global__ void k_test_wait_timeout(uint32_t polls, uint32_t* err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    const bool done = mbar_wait(&bar, 0, polls);
+    if (!done && threadIdx.x == 0) atomicOr(err, ERR_MMA_TIMEOUT);
+}
+
 // Forward pass of n samples on the tcgen05 path (inputs [n][10] -> raw outputs [n][48]).
 __global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_test_forward_tc(GuideNet net,
                                                                                   const float* __restrict__ x,
@@ -1475,6 +1487,11 @@ int launch_guide_train_multi(const FrameArgs* items, int n_items, uint32_t max_s
     }
     k_guide_frame_end_multi<<<n, 32, 0, st>>>(items);
     return launches;
+}
+
+int launch_test_wait_timeout(uint32_t polls, uint32_t* err, cudaStream_t st) {
+    k_test_wait_timeout<<<1, 32, 0, st>>>(polls, err);
+    return 1;
 }
 
 int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st) {

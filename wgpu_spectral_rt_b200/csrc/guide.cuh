@@ -128,6 +128,8 @@ int launch_guide_test_mixture(const float* raw, const float* omega, const float*
 // phase 0: forward + backward + weight gradients of gc->records records
 // (gc->weight_sum set by the caller; g.steps = 1); phase 1: one Adam step.
 int launch_guide_test_train(const GuideArgs& g, int phase, cudaStream_t st);
+// One block waiting on an mbarrier that never completes, `polls` polls at most.
+int launch_test_wait_timeout(uint32_t polls, uint32_t* err, cudaStream_t st);
 
 // Host side: deterministic default weights (G_NPARAMS floats), device
 // buffers for n_verts guided vertices per bounce and G_REC_CAP records, and
