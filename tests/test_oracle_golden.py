@@ -142,3 +142,23 @@ def test_bsdf_lambert_and_limits(orc):
             break
     else:
         pytest.fail("no refraction sampled")
+
+
+def test_lambert_directions_are_cosine_distributed(orc):
+    """The Lambert continuation normalize(n + unit vector) (shader.wgsl:462-466)
+    is cosine-weighted about n: E[cos] = 2/3, E[cos^2] = 1/2, azimuth uniform;
+    its attenuation is the reflectance spectrum, the same for every sample."""
+    n_s = 40_000
+    rows = [_bsdf_row([0, 0, -1], [0, 0, 1], [0.5, 0.4, 0.3, 1, 0, 0, 0, 0], True, [450, 550, 650, 750],
+                      [1, 1, 1, 1], 7919 * k + 1) for k in range(n_s)]
+    out = orc.device_math(6, np.array(rows, np.float32)).astype(np.float64)
+    c = out[:, 2]
+    assert np.all(c > -1e-6) and np.all(out[:, 7] == 0)
+    tol = 4 / math.sqrt(n_s)
+    assert abs(c.mean() - 2 / 3) < tol * 0.25
+    assert abs((c ** 2).mean() - 0.5) < tol * 0.3
+    phi = np.arctan2(out[:, 1], out[:, 0])
+    hist, _ = np.histogram(phi, bins=8, range=(-math.pi, math.pi))
+    assert np.all(np.abs(hist / n_s - 1 / 8) < 0.01)
+    att = out[:, 3:7]
+    assert np.all(att == att[0]) and np.all((att[0] > 0) & (att[0] <= 0.99))
