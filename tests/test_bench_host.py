@@ -56,3 +56,12 @@ def test_batched_workload_is_seeded_and_in_range():
     assert all(w == h and w in (256, 512, 1024, 2048) for w, h in sizes)
     assert all(1e6 <= p <= 16e6 for p in photons)
     assert _workload(16, (256, 512), (1e6, 2e6), 778) != a
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    """Under torchrun only rank 0 times the reference; the other ranks print nothing and exit 0."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "3"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip() == ""
