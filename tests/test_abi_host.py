@@ -194,3 +194,19 @@ def test_invalid_arguments_fail_cleanly(srt):
         b.add_instance(3, 0, np.eye(4))  # no such mesh
     with pytest.raises(srt.SrtError):
         b.add_mesh(np.zeros((3, 8), np.float32), [0, 1, 5])  # index out of range
+
+
+def test_missing_native_library_fails_loudly(tmp_path):
+    """Without the CUDA library the package raises on first use; there is no
+    CPU fallback for the product path."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import wgpu_spectral_rt_b200 as srt\n"
+            "try:\n    srt.Context(0)\nexcept RuntimeError as e:\n    print('raised:', e)\n")
+    env = dict(os.environ, SRT_LIB_PATH=str(tmp_path / "missing.so"), PYTHONPATH=root)
+    p = subprocess.run([sys.executable, "-c", code], env=env, cwd=tmp_path, capture_output=True, text=True,
+                       timeout=120)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.startswith("raised: native library missing")
