@@ -210,3 +210,14 @@ def test_missing_native_library_fails_loudly(tmp_path):
                        timeout=120)
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.startswith("raised: native library missing")
+
+
+def test_no_device_is_reported_as_a_status(srt):
+    """On a machine without a CUDA device, context creation returns
+    SRT_ERR_NO_DEVICE instead of aborting (skipped where a GPU is present)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(srt.SrtError) as e:
+        srt.Context(0)
+    assert e.value.status == 6  # SRT_ERR_NO_DEVICE
