@@ -400,13 +400,21 @@ srt_status srt_photon_grid_build(srt_ctx* ctx, const srt_photon* photons, uint32
  * legacy default stream) of the current device.  No context is needed.
  * Temporary storage comes from one fixed __device__ array in the library
  * (16.5 MiB, held by every GPU that loads the library until exit); n above
- * SRT_GRID_NOALLOC_MAX_PHOTONS returns SRT_ERR_CAPACITY.
+ * SRT_GRID_NOALLOC_MAX_PHOTONS returns SRT_ERR_CAPACITY.  Alignment:
+ * photons 16 bytes, keys_out and ranges_out 8 bytes; a misaligned pointer
+ * returns SRT_ERR_INVALID_ARG before any device work.  n = 0 only clears
+ * ranges_out.
  *
  * The first call on a device looks up that array's device address (once per
  * device, with the device current); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller.  Asynchronous: synchronise `stream`
- * before reading the outputs. */
+ * capture.  The address belongs to the CUDA context that was current at the
+ * lookup: a call under another context of the same device (after
+ * cudaDeviceReset, or one made current through the driver API) looks it up
+ * again, so make such a call outside stream capture too.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  Launch failures are reported from each launch's own status; an
+ * error that an unrelated earlier call left pending is neither reported nor
+ * cleared.  Asynchronous: synchronise `stream` before reading the outputs. */
 #define SRT_GRID_NOALLOC_MAX_PHOTONS (1u << 20)
 srt_status srt_photon_grid_build_noalloc(void* stream, const srt_photon* photons, uint32_t n, uint32_t frame_count,
                                          float cell_size, uint32_t hash_bits, uint64_t* keys_out,

@@ -221,3 +221,26 @@ def test_no_device_is_reported_as_a_status(srt):
     with pytest.raises(srt.SrtError) as e:
         srt.Context(0)
     assert e.value.status == 6  # SRT_ERR_NO_DEVICE
+
+
+def test_noalloc_grid_refuses_bad_arguments_before_device_work(srt):
+    """srt_photon_grid_build_noalloc checks its arguments before it touches a
+    device: a misaligned photon, key or range pointer (the kernels read
+    photons as 16-byte vectors and write 8-byte keys and ranges), a count
+    above the fixed scratch capacity and an invalid cell size are refused with
+    a status.  The pointers below are never dereferenced."""
+    L = srt.lib()
+    f = L.srt_photon_grid_build_noalloc
+    aligned = C.c_void_p(1 << 20)
+    st = f(None, C.c_void_p(aligned.value + 8), 10, 0, 0.02, 22, None, None)
+    assert srt.STATUS[st] == "INVALID_ARG"
+    st = f(None, aligned, 10, 0, 0.02, 22, C.c_void_p(aligned.value + 4), None)
+    assert srt.STATUS[st] == "INVALID_ARG"
+    st = f(None, aligned, 10, 0, 0.02, 22, None, C.c_void_p(aligned.value + 2))
+    assert srt.STATUS[st] == "INVALID_ARG"
+    st = f(None, aligned, (1 << 20) + 1, 0, 0.02, 22, None, None)
+    assert srt.STATUS[st] == "CAPACITY"
+    st = f(None, aligned, 10, 0, 0.0, 22, None, None)
+    assert srt.STATUS[st] == "INVALID_ARG"
+    st = f(None, None, 10, 0, 0.02, 22, None, None)
+    assert srt.STATUS[st] == "INVALID_ARG"
