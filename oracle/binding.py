@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
         L.orc_photon_grid_build.argtypes = [P, U32, U32, C.c_float, U32, P, P]
         L.orc_photon_gather.argtypes = [P, U32, P, U32, U32, P, P]
         L.orc_render_frame.argtypes = [P, P, U32, U32, P, U32, U32, P, P, P, P, C.c_int]
+        L.orc_render_frame_photons.argtypes = [P, P, U32, U32, P, P, U32, U32, U32, P, P, P, P, C.c_int]
+        L.orc_tri_probe.argtypes = [P, P, P, U32, P, P]
         L.orc_max_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -82,15 +84,31 @@ class OracleScene:
         c = lib().orc_photon_emit(self.h, n_photons, frame, max_bounces, _p(out), _p(em), threads)
         return out[:c].copy(), em[:c].copy()
 
+    def tri_probe(self, rays: np.ndarray, prims: np.ndarray):
+        """FP64 (t where each ray's line meets the plane of triangle prims[i],
+        distance from that point to the triangle's boundary: > 0 inside)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        pr = np.ascontiguousarray(prims, np.uint32)
+        t = np.zeros(len(r), np.float64)
+        e = np.zeros(len(r), np.float64)
+        lib().orc_tri_probe(self.h, _p(r), _p(pr), len(r), _p(t), _p(e))
+        return t, e
+
     def render_frame(self, cam, w: int, h: int, params, accum: np.ndarray | None = None, row_stride=1, row_phase=0,
-                     want_ldr=True, want_radiance=False, threads: int = 0):
+                     want_ldr=True, want_radiance=False, threads: int = 0, photons: np.ndarray | None = None):
+        """One frame; `photons` (n x 8 float32) replaces the oracle's own photon pass."""
         if accum is None:
             accum = np.zeros((h, w, 4), np.float32)
         ldr = np.zeros((h, w, 4), np.uint8) if want_ldr else None
         rad = np.zeros((h, w, 4), np.float32) if want_radiance else None
         stats = np.zeros(5, np.uint64)
-        lib().orc_render_frame(self.h, C.byref(cam), w, h, C.byref(params), row_stride, row_phase, _p(accum),
-                               _p(ldr), _p(rad), _p(stats), threads)
+        if photons is None:
+            lib().orc_render_frame(self.h, C.byref(cam), w, h, C.byref(params), row_stride, row_phase, _p(accum),
+                                   _p(ldr), _p(rad), _p(stats), threads)
+        else:
+            ph = np.ascontiguousarray(photons, np.float32).reshape(-1, 8)
+            lib().orc_render_frame_photons(self.h, C.byref(cam), w, h, C.byref(params), _p(ph), len(ph), row_stride,
+                                           row_phase, _p(accum), _p(ldr), _p(rad), _p(stats), threads)
         return accum, ldr, rad, stats
 
     def close(self):

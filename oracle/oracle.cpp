@@ -600,10 +600,10 @@ struct Hit {
     double t;
     uint32_t prim;
     double u, v;
-    double t2;  // best t among other triangles (brute force only)
+    double t2;  // best t among other triangles (brute force, or the BVH with want_t2)
 };
 
-Hit closest(const orc_scene* s, const DRay& r, bool brute, bool any) {
+Hit closest(const orc_scene* s, const DRay& r, bool brute, bool any, bool want_t2 = false) {
     Hit h{false, std::numeric_limits<double>::infinity(), 0xFFFFFFFFu, 0, 0, std::numeric_limits<double>::infinity()};
     if (brute) {
         size_t n = s->tinst.size();
@@ -631,7 +631,9 @@ Hit closest(const orc_scene* s, const DRay& r, bool brute, bool any) {
     stack[sp++] = 0;
     while (sp > 0) {
         const orc_scene::Node& nd = s->nodes[stack[--sp]];
-        double tcur = h.hit ? h.t : r.tmax;
+        // with want_t2, boxes are culled at the second-best t so that the
+        // nearest hit of any other triangle is found too
+        double tcur = h.hit ? (want_t2 ? std::min(h.t2, r.tmax) : h.t) : r.tmax;
         if (!box_hit(nd, r, inv, tcur)) continue;
         if (nd.leaf) {
             for (uint32_t k = 0; k < nd.right; ++k) {
@@ -643,7 +645,12 @@ Hit closest(const orc_scene* s, const DRay& r, bool brute, bool any) {
                     h.prim = 0;
                     return h;
                 }
-                if (!h.hit || t < h.t || (t == h.t && i < h.prim)) h = {true, t, i, u, v, h.t2};
+                if (!h.hit || t < h.t || (t == h.t && i < h.prim)) {
+                    if (h.hit) h.t2 = std::min(h.t2, h.t);
+                    h = {true, t, i, u, v, h.t2};
+                } else {
+                    h.t2 = std::min(h.t2, t);
+                }
             }
         } else {
             if (sp + 2 > 128) continue;
@@ -1084,12 +1091,60 @@ void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit,
         Hit h{};
         h.hit = false;
         h.t2 = std::numeric_limits<double>::infinity();
-        if (r.dir[0] != 0.f || r.dir[1] != 0.f || r.dir[2] != 0.f) h = closest(s, d, brute != 0, any_hit != 0);
+        if (r.dir[0] != 0.f || r.dir[1] != 0.f || r.dir[2] != 0.f)
+            h = closest(s, d, brute != 0, any_hit != 0, t_second != nullptr);
         if (t_out) t_out[i] = h.hit ? h.t : std::numeric_limits<double>::infinity();
         if (prim_out) prim_out[i] = h.hit ? h.prim : 0xFFFFFFFFu;
         if (u_out) u_out[i] = h.hit ? h.u : 0.0;
         if (v_out) v_out[i] = h.hit ? h.v : 0.0;
-        if (t_second) t_second[i] = brute ? h.t2 : std::numeric_limits<double>::infinity();
+        if (t_second) t_second[i] = h.t2;
+    }
+}
+
+// Where the line of each ray meets the plane of the given flattened triangle
+// (FP64, world space): the ray parameter t there and the distance from that
+// point to the triangle's boundary (the nearest of its three edge segments),
+// positive inside the triangle and negative outside.  A ray that passes
+// within a small distance of a triangle's boundary is one whose hit or miss
+// of that triangle FP32 arithmetic can decide either way.  prim = 0xFFFFFFFF
+// or a ray parallel to the plane gives t = inf and distance = inf.
+void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prims, uint32_t n, double* t_out,
+                   double* edge_out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        const double inf = std::numeric_limits<double>::infinity();
+        t_out[i] = inf;
+        edge_out[i] = inf;
+        uint32_t p = prims[i];
+        if (p >= s->tinst.size()) continue;
+        const double* v = &s->tv[9 * (size_t)p];
+        const srt_ray& r = rays[i];
+        double o[3] = {r.origin[0], r.origin[1], r.origin[2]}, d[3] = {r.dir[0], r.dir[1], r.dir[2]};
+        double e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+        double e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+        double nrm[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        double den = nrm[0] * d[0] + nrm[1] * d[1] + nrm[2] * d[2];
+        if (den == 0.0) continue;
+        double t = (nrm[0] * (v[0] - o[0]) + nrm[1] * (v[1] - o[1]) + nrm[2] * (v[2] - o[2])) / den;
+        double x[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+        // inside test by the signs of the edge normals' dot products
+        bool inside = true;
+        double dist = inf;
+        for (int k = 0; k < 3; ++k) {
+            const double* a = v + 3 * k;
+            const double* b = v + 3 * ((k + 1) % 3);
+            double ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+            double ax[3] = {x[0] - a[0], x[1] - a[1], x[2] - a[2]};
+            double c[3] = {ab[1] * ax[2] - ab[2] * ax[1], ab[2] * ax[0] - ab[0] * ax[2], ab[0] * ax[1] - ab[1] * ax[0]};
+            if (c[0] * nrm[0] + c[1] * nrm[1] + c[2] * nrm[2] < 0.0) inside = false;
+            double l2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+            double f = l2 > 0.0 ? (ax[0] * ab[0] + ax[1] * ab[1] + ax[2] * ab[2]) / l2 : 0.0;
+            f = std::min(1.0, std::max(0.0, f));
+            double q[3] = {ax[0] - f * ab[0], ax[1] - f * ab[1], ax[2] - f * ab[2]};
+            dist = std::min(dist, std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]));
+        }
+        t_out[i] = t;
+        edge_out[i] = inside ? dist : -dist;
     }
 }
 
@@ -1213,6 +1268,14 @@ void orc_photon_gather(const srt_photon* photons, uint32_t n, const float* q, ui
 void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
                       const srt_params* params, uint32_t row_stride, uint32_t row_phase, float* accum, uint8_t* ldr,
                       float* radiance_out, uint64_t* stats_out, int n_threads) {
+    orc_render_frame_photons(s, cam, w, h, params, nullptr, 0, row_stride, row_phase, accum, ldr, radiance_out,
+                             stats_out, n_threads);
+}
+
+void orc_render_frame_photons(const orc_scene* s, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
+                              const srt_params* params, const srt_photon* photons_in, uint32_t n_photons_in,
+                              uint32_t row_stride, uint32_t row_phase, float* accum, uint8_t* ldr,
+                              float* radiance_out, uint64_t* stats_out, int n_threads) {
 #ifdef _OPENMP
     if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
@@ -1222,7 +1285,12 @@ void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_
     Grid grid;
     bool have_grid = params->photons_per_frame > 0;
     uint32_t stored = 0;
-    if (have_grid) {
+    if (have_grid && photons_in) {
+        // the given photon set (e.g. another implementation's photon pass)
+        stored = n_photons_in;
+        std::vector<uint64_t> keys;
+        grid_build(photons_in, stored, frame, params->cell_size, params->hash_bits, keys, &grid);
+    } else if (have_grid) {
         uint32_t np = params->photons_per_frame;
         std::vector<Emitted> em(np);
         uint64_t ph_rays = 0;

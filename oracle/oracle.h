@@ -35,11 +35,18 @@ void orc_scene_destroy(orc_scene* s);
 uint64_t orc_scene_num_tris(const orc_scene* s);
 
 /* FP64 queries.  brute = 1 tests every triangle, otherwise an FP64 BVH.
- * Closest: (t, prim, u, v) lexicographic min over (t, prim); t_second is the
- * smallest t of any OTHER triangle hit (inf if none), used to detect ties.
+ * Closest: (t, prim, u, v) lexicographic min over (t, prim); t_second (may be
+ * NULL) is the smallest t of any OTHER triangle hit (inf if none), used to
+ * detect ties, in both modes.
  * Any-hit (any_hit = 1): prim = 0 hit / 0xFFFFFFFF miss. */
 void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit, int brute,
                double* t_out, uint32_t* prim_out, double* u_out, double* v_out, double* t_second);
+
+/* FP64: for ray i and flattened triangle prims[i], the ray parameter where
+ * the ray's line meets the triangle's plane and the distance from that point
+ * to the triangle's boundary (positive inside, negative outside). */
+void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prims, uint32_t n, double* t_out,
+                   double* edge_out);
 
 /* Same op codes and record layouts as srt_test_device_math. */
 int orc_device_math(int op, uint32_t n, const void* in, void* out, const void* aux);
@@ -69,6 +76,14 @@ void orc_photon_gather(const srt_photon* photons, uint32_t n, const float* queri
 void orc_render_frame(const orc_scene* s, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
                       const srt_params* params, uint32_t row_stride, uint32_t row_phase,
                       float* accum, uint8_t* ldr, float* radiance_out, uint64_t* stats_out, int n_threads);
+
+/* The same frame with the photon pass replaced by a given photon set
+ * (photons_in, n_photons_in, e.g. read back from the GPU's photon pass), so
+ * that camera paths can be compared on identical photon maps. */
+void orc_render_frame_photons(const orc_scene* s, const srt_camera_uniform* cam, uint32_t w, uint32_t h,
+                              const srt_params* params, const srt_photon* photons_in, uint32_t n_photons_in,
+                              uint32_t row_stride, uint32_t row_phase, float* accum, uint8_t* ldr,
+                              float* radiance_out, uint64_t* stats_out, int n_threads);
 
 int orc_max_threads(void);
 

@@ -74,3 +74,60 @@ def relmse(x, ref):
     x = np.asarray(x, np.float64)
     ref = np.asarray(ref, np.float64)
     return float(np.mean((x - ref) ** 2 / (ref ** 2 + 0.01)))
+
+
+MISS = 0xFFFFFFFF
+# Named exclusion set of the closest-hit comparison.  The GPU answers in FP32
+# (world-space vertices rounded once, watertight edge functions) and the
+# oracle in FP64, so a ray whose hit or miss of a triangle FP32 rounding can
+# decide either way is not a disagreement:
+#   tie    another triangle is hit within |dt| < 1e-6 of the nearest (the
+#          north-star rule)
+#   edge   the ray passes within EDGE_REL * scale of the boundary of the
+#          oracle's hit triangle or of the GPU's (FP64 distance, world units;
+#          scale = max(1, |origin|inf, |hit point|inf), the magnitude of the
+#          FP32 coordinates involved)
+#   range  the oracle's hit lies within RANGE_REL * scale of tmin or tmax
+EDGE_REL = 2.0 ** -19
+RANGE_REL = 2.0 ** -19
+
+
+def closest_hit_parity(scene, oracle, rays, brute=True, hits=None):
+    """Compares GPU closest hits with the FP64 oracle on `rays` [n, 8].
+    Returns a dict with the masks and counts; `bad` are disagreements outside
+    the named exclusion set (must be empty)."""
+    g = scene.trace(rays) if hits is None else hits
+    t, prim, u, v, t2 = oracle.trace(rays, brute=brute)
+    pg = g["prim"]
+    hit_o, hit_g = prim != MISS, pg != MISS
+    o = rays[:, 0:3].astype(np.float64)
+    d = rays[:, 4:7].astype(np.float64)
+    tt = np.where(hit_o, t, np.where(hit_g, g["t"].astype(np.float64), 0.0))
+    x = o + tt[:, None] * d
+    scale = np.maximum(1.0, np.maximum(np.abs(o).max(1), np.abs(x).max(1)))
+    with np.errstate(invalid="ignore"):
+        tie = hit_o & (np.abs(t2 - t) < 1e-6)
+    _, e_o = oracle.tri_probe(rays, prim)
+    _, e_g = oracle.tri_probe(rays, pg)
+    edge = (np.abs(e_o) < EDGE_REL * scale) | (np.abs(e_g) < EDGE_REL * scale)
+    rng_ = hit_o & ((np.abs(t - rays[:, 3]) < RANGE_REL * scale) | (np.abs(t - rays[:, 7]) < RANGE_REL * scale))
+    excluded = tie | edge | rng_
+    mismatch = pg != prim
+    both = hit_o & hit_g & (pg == prim)
+    dt = np.abs(g["t"][both].astype(np.float64) - t[both]) / np.maximum(1.0, t[both])
+    return {"n": len(rays), "hits": int(hit_o.sum()), "mismatch": int(mismatch.sum()),
+            "excluded": int(excluded.sum()), "tie": int(tie.sum()), "edge": int(edge.sum()),
+            "range": int(rng_.sum()), "mismatch_excluded": int((mismatch & excluded).sum()),
+            "bad": np.nonzero(mismatch & ~excluded)[0], "max_rel_dt": float(dt.max()) if dt.size else 0.0,
+            # the largest boundary distances among the disagreements (how tight EDGE_REL could be)
+            "mismatch_edge_rel": np.sort(np.minimum(np.abs(e_o), np.abs(e_g))[mismatch] / scale[mismatch])[-8:],
+            "g": g, "t": t, "prim": prim}
+
+
+def report(name, d):
+    """One line of parity statistics (shown with pytest -s or -rP)."""
+    keys = ("n", "hits", "mismatch", "mismatch_excluded", "excluded", "tie", "edge", "range", "max_rel_dt")
+    print(f"[parity] {name}: " + ", ".join(f"{k}={d[k]}" for k in keys if k in d)
+          + (f", bad={len(d['bad'])}" if "bad" in d else "")
+          + (f", mismatch_edge_rel_max={list(np.round(d['mismatch_edge_rel'], 9))}" if "mismatch_edge_rel" in d else ""),
+          flush=True)

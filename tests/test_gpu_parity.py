@@ -8,9 +8,10 @@ Tolerances:
                                          reach zero by cancellation (CIE lobes, film
                                          reflectance); unit directions compare by
                                          absolute difference
-  closest-hit triangle ids               exact, except ties |dt| < 1e-6 and
-                                         rays grazing an edge (oracle barycentric
-                                         within 1e-6 of the boundary)
+  closest-hit triangle ids               exact, except the named exclusion set of
+                                         tests/conftest.py: ties |dt| < 1e-6, rays
+                                         passing within EDGE_REL * scale of a
+                                         triangle boundary, hits at the range ends
   whole frames                           per-pixel agreement of >= 97 % of the
                                          pixels within 1e-3 relative, and an image
                                          relMSE below 1e-4 against the oracle
@@ -22,7 +23,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import random_rays, rel_err, relmse
+from conftest import closest_hit_parity, random_rays, rel_err, relmse, report
 
 pytestmark = pytest.mark.gpu
 
@@ -90,6 +91,9 @@ def _bsdf_cases(n, rng):
     return np.array(rows, np.float32)
 
 
+GRAZING = 1e-2
+
+
 def test_sample_bsdf(ctx, srt, orc):
     rows = _bsdf_cases(40000, np.random.default_rng(4))
     g = srt.device_math(ctx, 6, rows)
@@ -101,11 +105,22 @@ def test_sample_bsdf(ctx, srt, orc):
     ok = same_rng & same_branch & (o[:, 7] == 0)
     # ...sampled unit directions agree to 1e-5 absolute...
     assert np.abs(g[ok, :3] - o[ok, :3]).max() < 1e-5
-    # ...and the weights within 1e-5 relative, except where a grazing angle
-    # amplifies the ulp differences of the transcendental functions
-    err = rel_err(g[ok, 3:7], o[ok, 3:7], floor=1e-6).max(1)
-    assert np.quantile(err, 0.999) < 1e-5
-    assert err.max() < 1e-3
+    # ...and the weights within 1e-5 relative outside the grazing set: the
+    # incident or the sampled direction within GRAZING of the tangent plane
+    # (|cos| < GRAZING), where the 1/cos factors amplify the last-ulp
+    # differences of the GPU's and the host's transcendental functions
+    err = rel_err(g[:, 3:7], o[:, 3:7], floor=1e-6).max(1)
+    nrm = rows[:, 3:6].astype(np.float64)
+    cos_i = np.abs((rows[:, 0:3] * nrm).sum(1))
+    cos_o = np.abs((o[:, 0:3] * nrm).sum(1))
+    grazing = np.minimum(cos_i, cos_o) < GRAZING
+    sel = ok & ~grazing
+    worst = np.argsort(-np.where(sel, err, 0))[:6]
+    print(f"[parity] bsdf: n={len(rows)}, compared={int(sel.sum())}, grazing={int((ok & grazing).sum())}, "
+          f"max err={err[sel].max():.3e}; worst (type, cos_i, cos_o, err): "
+          + "; ".join(f"({rows[k, 10]:.0f}, {cos_i[k]:.2e}, {cos_o[k]:.2e}, {err[k]:.2e})" for k in worst), flush=True)
+    assert err[sel].max() < 1e-5
+    assert err[ok & grazing].max() < 1e-2
 
 
 def test_grid_hash_bit_exact(ctx, srt, orc):
@@ -216,29 +231,17 @@ def cornell(srt, orc, ctx):
     o.close()
 
 
-def _closest_parity(scene, oracle, rays):
-    g = scene.trace(rays)
-    t, prim, u, v, t2 = oracle.trace(rays, brute=True)
-    hit_g = g["prim"] != 0xFFFFFFFF
-    hit_o = prim != 0xFFFFFFFF
-    edge = np.minimum(np.minimum(u, v), 1 - u - v) < 1e-6
-    with np.errstate(invalid="ignore"):
-        tie = np.abs(t2 - t) < 1e-6
-    excluded = (edge | tie) & hit_o
-    agree = (g["prim"] == prim) | excluded
-    # grazing misses: the oracle hit lies within 1e-6 (barycentric) of an edge
-    agree |= (~hit_o & ~hit_g)
-    return agree, hit_g, hit_o, g, t
-
-
 @pytest.mark.parametrize("which", ["config1", "cornell"])
 def test_closest_hit_ids(request, which):
+    """Exact triangle ids outside the named exclusion set (ties, rays within
+    EDGE_REL * scale of a triangle boundary, hits at the ends of the range;
+    tests/conftest.py)."""
     b, scene, o, _ = request.getfixturevalue(which)
     rays = random_rays(40000, np.random.default_rng(11), spread=0.9)
-    agree, hit_g, hit_o, g, t = _closest_parity(scene, o, rays)
-    assert agree.mean() > 0.9995, (agree.mean(), np.nonzero(~agree)[0][:10])
-    both = hit_g & hit_o
-    assert np.abs(g["t"][both] - t[both]).max() < 1e-4
+    d = closest_hit_parity(scene, o, rays, brute=True)
+    report(which, d)
+    assert len(d["bad"]) == 0, d["bad"][:10]
+    assert d["max_rel_dt"] < 1e-5
 
 
 def test_any_hit(config1):
