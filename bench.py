@@ -21,8 +21,8 @@ Mrays/s are reported beside it.
               counting build over the same frames) / its mean CUDA-event
               duration, against the measured HBM copy bandwidth
   cpu_baseline  the CPU oracle (C++ restatement of the reference shader
-              math, OpenMP over all host threads) on a bounded sample of the
-              same frame: a row subset and the matching share of photons
+              math, OpenMP over all host threads) on one whole frame of the
+              same workload, with the oracle's own scene generator
 
 Multi-GPU: the path does not shard across GPUs (one frame is one GPU's
 work); --gpus N under torchrun runs N replicas, each rendering its own
@@ -32,7 +32,9 @@ max over ranks of the timed region ("scaling": "weak").
 --impl reference times the reference's CPU implementation of the path — the
 oracle port (the reference itself is Rust + WGSL on a Vulkan ray-query
 device and cannot run here) — with all host threads, on the same workload
-and metric; rank 0 only.
+and metric, one whole frame per timed step; rank 0 only.  It builds its
+scene and camera with the oracle's own generator and loads nothing of the
+GPU package.
 """
 from __future__ import annotations
 
@@ -47,6 +49,8 @@ import tempfile
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -55,6 +59,8 @@ CONFIGS = {
     "config2": ("PRESET_CONFIG2", 1920, 1080, 12, 1 << 22),
     "config1": ("PRESET_CONFIG1", 256, 256, 8, 1 << 18),
 }
+# srt_preset values (include/srt.h), for the CPU legs that do not load the GPU package
+PRESET_IDS = {"PRESET_CONFIG1": 2, "PRESET_CONFIG2": 3}
 
 
 def _peaks():
@@ -157,90 +163,92 @@ def build_scene(srt, ctx, preset_name: str, seed: int = 0):
     return b, scene, cam
 
 
-def cpu_baseline(srt, b, cam, w, h, params, seconds_target=15.0, threads=0):
-    """The CPU oracle on a bounded sample of one frame (row subset + the same share of photons)."""
+def _oracle():
     sys.path.insert(0, str(ROOT / "oracle"))
-    import binding as orc  # the oracle, timed here as the CPU baseline
+    import binding as orc  # the oracle: timed as the CPU baseline, never part of the GPU path
 
+    return orc
+
+
+def _cpu_frame(orc, o, preset_cam, w, h, depth, photons, frame, fraction=1):
+    """One frame of the oracle port (all host threads): rows y % fraction == 0
+    and 1/fraction of the photons (fraction 1 = the whole frame).  Returns
+    (seconds, stats [paths, closest rays, shadow rays, emitted, stored])."""
+    pos, yaw, pitch = preset_cam
+    u = orc.camera_uniform(pos, yaw, pitch, w / h, frame)
+    p = orc.default_params(max_depth=depth, photons_per_frame=max(1, photons // fraction),
+                           photon_norm_count=float(photons))
+    t = time.perf_counter()
+    _, _, _, st = o.render_frame(u, w, h, p, row_stride=fraction, row_phase=0, want_ldr=False)
+    return time.perf_counter() - t, st
+
+
+def cpu_baseline(cfg, frames=1):
+    """The CPU oracle (the reference's shader math restated in C++, OpenMP over
+    all host threads) on whole frames of the same workload: its own scene
+    generator and camera, the same sampling as the reference arm's steps."""
+    orc = _oracle()
+    preset, w, h, depth, photons = cfg
     t0 = time.perf_counter()
-    o = orc.OracleScene(b.arrays())
+    scn = orc.Preset(PRESET_IDS[preset], 0)
+    o = orc.OracleScene(scn.arrays())
     build_s = time.perf_counter() - t0
-    pos, yaw, pitch = cam
-    u = srt.camera_uniform(pos, yaw, pitch, w / h, 0)
-    # calibrate on a tiny sample, then size the sample to ~seconds_target
-    stride = 64
-    frac = 1.0 / stride
-
-    def run(stride):
-        p = srt.Params.from_buffer_copy(params)
-        p.photon_norm_count = float(params.photons_per_frame)
-        p.photons_per_frame = max(1, int(params.photons_per_frame // stride))
-        t = time.perf_counter()
-        _, _, _, st = o.render_frame(u, w, h, p, row_stride=stride, row_phase=0, want_ldr=False, threads=threads)
-        return time.perf_counter() - t, st
-
-    dt, st = run(stride)
-    while dt < seconds_target / 4 and stride > 1:
-        stride = max(1, stride // 4)
-        dt, st = run(stride)
-    frac = 1.0 / stride
-    paths = int(st[0])
-    value = paths / dt / 1e6
-    o.close()
-    return {
-        "value": round(value, 4), "unit": "Mpaths/s", "cores": orc.max_threads() if threads <= 0 else threads,
-        "kind": "port",
-        "sample": (f"1/{stride} of the rows ({paths} paths) and 1/{stride} of the photons "
-                   f"({int(params.photons_per_frame // stride)}) of one {w}x{h} frame; {dt:.1f} s; "
-                   f"oracle scene build {build_s:.1f} s not timed"),
-        "rays_closest": int(st[1]), "rays_shadow": int(st[2]), "seconds": round(dt, 3), "fraction": frac,
+    _cpu_frame(orc, o, scn.camera, w, h, depth, photons, 0, fraction=16)  # warm-up (page-in, thread pool)
+    dt_total, paths, st_sum = 0.0, 0, np.zeros(5, np.uint64)
+    for f in range(frames):
+        dt, st = _cpu_frame(orc, o, scn.camera, w, h, depth, photons, 1 + f)
+        dt_total += dt
+        paths += int(st[0])
+        st_sum += st
+    value = paths / dt_total / 1e6
+    out = {
+        "value": round(value, 4), "unit": "Mpaths/s", "cores": orc.max_threads(), "kind": "port",
+        "sample": (f"{frames} whole {w}x{h} frame(s) ({paths} paths, {photons} photons each), "
+                   f"{dt_total:.1f} s; oracle scene generator + FP64 BVH build {build_s:.1f} s not timed"),
+        "rays_closest": int(st_sum[1]), "rays_shadow": int(st_sum[2]), "seconds": round(dt_total, 3),
     }
+    o.close()
+    scn.close()
+    return out
 
 
 def run_reference(args, cfg, rank, world):
-    """--impl reference: the CPU port of the reference path, all host threads, rank 0 only."""
+    """--impl reference: the CPU port of the reference path (the oracle, with
+    its own scene generator and camera; nothing of the GPU package is loaded),
+    all host threads, rank 0 only.  A timed step is one whole frame of the
+    workload; the untimed warm-up steps render 1/16 of a frame."""
     if rank != 0:
         return 0
-    import wgpu_spectral_rt_b200 as srt
-
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import binding as orc
-
+    orc = _oracle()
     preset, w, h, depth, photons = cfg
-    b = srt.SceneBuilder()
-    cam = b.add_preset(getattr(srt, preset), 0)
-    o = orc.OracleScene(b.arrays())
-    params = srt.default_params(max_depth=depth, photons_per_frame=photons)
-    pos, yaw, pitch = cam
-    # each step: 1/stride of the rows and of the photons of frame k; stride sized so a step is ~1-2 s
-    stride = args.ref_stride
+    scn = orc.Preset(PRESET_IDS[preset], 0)
+    o = orc.OracleScene(scn.arrays())
+    n_tris = o.n_tris
+    for k in range(args.warmup):
+        _cpu_frame(orc, o, scn.camera, w, h, depth, photons, k, fraction=16)
     total_paths, t_total = 0, 0.0
-    for k in range(args.warmup + args.steps):
-        u = srt.camera_uniform(pos, yaw, pitch, w / h, k)
-        p = srt.Params.from_buffer_copy(params)
-        p.photon_norm_count = float(photons)
-        p.photons_per_frame = max(1, photons // stride)
-        t = time.perf_counter()
-        _, _, _, st = o.render_frame(u, w, h, p, row_stride=stride, row_phase=k % stride, want_ldr=False)
-        dt = time.perf_counter() - t
-        if k >= args.warmup:
-            total_paths += int(st[0])
-            t_total += dt
+    for k in range(args.steps):
+        dt, st = _cpu_frame(orc, o, scn.camera, w, h, depth, photons, args.warmup + k)
+        total_paths += int(st[0])
+        t_total += dt
     value = total_paths / t_total / 1e6
     cores = orc.max_threads()
     line = {
         "metric": "Mpaths/s", "value": round(value, 4), "unit": "Mpaths/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_total / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, seeded)",
         "impl": "reference",
-        "config": {"workload": f"{args.config}: {w}x{h}, depth {depth}, {photons} photons/frame, 1 spp per step",
+        "config": {"workload": (f"{args.config}: {n_tris} triangles, {w}x{h}, depth {depth}, {photons} "
+                                f"photons/frame, 1 spp per step"),
                    "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": round(value, 4), "unit": "Mpaths/s", "cores": cores, "kind": "port",
-                         "sample": f"per step 1/{stride} of the rows and of the photons of one frame"},
+                         "sample": (f"per timed step one whole {w}x{h} frame ({photons} photons); warm-up steps "
+                                    f"1/16 of a frame")},
         "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     o.close()
+    scn.close()
     return 0
 
 
@@ -348,8 +356,6 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=0)
     ap.add_argument("--height", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--ref-stride", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the C3 batched-renderer section")
@@ -490,7 +496,7 @@ def main(argv=None):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(srt, b, cam, w, h, params, seconds_target=args.cpu_seconds)
+        cpu = cpu_baseline(cfg)
     if rank == 0:
         clocks = clk.summary()
         line = {

@@ -18,6 +18,45 @@ LIB_PATH = HERE / "liboracle.so"
 _lib = None
 
 
+# Record layouts of include/srt.h, declared here so that the oracle runs
+# without the product package.
+class CameraUniform(C.Structure):  # srt_camera_uniform (camera.rs:4-13), 272 B
+    _fields_ = [("view_inverse", C.c_float * 16), ("proj_inverse", C.c_float * 16), ("view", C.c_float * 16),
+                ("proj", C.c_float * 16), ("frame_count", C.c_uint32), ("pad", C.c_uint32 * 3)]
+
+
+class Params(C.Structure):  # srt_params, 52 B
+    _fields_ = [("max_depth", C.c_uint32), ("photons_per_frame", C.c_uint32), ("hash_bits", C.c_uint32),
+                ("photon_max_bounces", C.c_uint32), ("gather_cap", C.c_uint32), ("flags", C.c_uint32),
+                ("cell_size", C.c_float), ("gather_radius0", C.c_float), ("radius_exponent", C.c_float),
+                ("spectral_radius", C.c_float), ("photon_norm_count", C.c_float), ("block_size", C.c_uint32),
+                ("seed", C.c_uint32)]
+
+
+class SceneArrays(C.Structure):  # srt_scene_arrays
+    _fields_ = [("vertices", C.c_void_p), ("n_vertices", C.c_uint32), ("indices", C.c_void_p),
+                ("n_indices", C.c_uint32), ("mesh_infos", C.c_void_p), ("n_meshes", C.c_uint32),
+                ("materials", C.c_void_p), ("n_materials", C.c_uint32), ("instances", C.c_void_p),
+                ("n_instances", C.c_uint32), ("lights", C.c_void_p), ("n_lights", C.c_uint32)]
+
+
+assert C.sizeof(CameraUniform) == 272 and C.sizeof(Params) == 52
+
+
+def default_params(**kw) -> Params:
+    """The reference's constants: MAX_DEPTH 12 (renderer/compute_pass.rs:26),
+    MAX_PHOTONS 2^20 (renderer/mod.rs:18), HASH_SIZE 2^22 (:19), 5 photon
+    bounces (photon_emit.wgsl:219), 64 gathered photons (shader.wgsl:312),
+    CELL_SIZE 0.02 (:275), radius 0.02 * (frame + 1)^-0.15 (:302-303),
+    spectral radius 20 nm (:279)."""
+    p = Params(max_depth=12, photons_per_frame=1 << 20, hash_bits=22, photon_max_bounces=5, gather_cap=64,
+               flags=0, cell_size=0.02, gather_radius0=0.02, radius_exponent=-0.15, spectral_radius=20.0,
+               photon_norm_count=0.0, block_size=0, seed=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
 def build() -> Path:
     """Compiles the oracle with its Makefile (g++ -fopenmp)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
@@ -48,6 +87,11 @@ def lib() -> C.CDLL:
         L.orc_render_frame_photons.argtypes = [P, P, U32, U32, P, P, U32, U32, U32, P, P, P, P, C.c_int]
         L.orc_tri_probe.argtypes = [P, P, P, U32, P, P]
         L.orc_max_threads.restype = C.c_int
+        L.orc_preset_create.restype = P
+        L.orc_preset_create.argtypes = [C.c_int, U32]
+        L.orc_preset_destroy.argtypes = [P]
+        L.orc_preset_arrays.argtypes = [P, P, P]
+        L.orc_camera_uniform.argtypes = [P, C.c_float, C.c_float, C.c_float, U32, P]
         _lib = L
     return _lib
 
@@ -56,11 +100,57 @@ def _p(a: np.ndarray | None):
     return C.c_void_p(a.ctypes.data) if a is not None else None
 
 
+class Preset:
+    """A preset scene from the oracle's own generator (scenes.cpp): arrays()
+    gives an srt_scene_arrays view of it, camera = ([x, y, z], yaw, pitch)."""
+
+    def __init__(self, preset: int, seed: int = 0):
+        self.h = lib().orc_preset_create(preset, seed)
+        if not self.h:
+            raise ValueError(f"unknown preset {preset}")
+        self._arrays = SceneArrays()
+        cam = (C.c_float * 5)()
+        lib().orc_preset_arrays(self.h, C.byref(self._arrays), cam)
+        self.camera = ([cam[0], cam[1], cam[2]], cam[3], cam[4])
+
+    def arrays(self) -> SceneArrays:
+        return self._arrays
+
+    def n_triangles(self) -> int:
+        a = self._arrays
+        ends = []
+        mi = np.ctypeslib.as_array(C.cast(a.mesh_infos, C.POINTER(C.c_uint32)), (a.n_meshes, 4))
+        inst = np.ctypeslib.as_array(C.cast(a.instances, C.POINTER(C.c_uint32)), (a.n_instances, 20))
+        for m in range(a.n_meshes):
+            ends.append(int(mi[m + 1, 1]) if m + 1 < a.n_meshes else a.n_indices)
+        return int(sum((ends[k] - int(mi[k, 1])) // 3 for k in inst[:, 0]))
+
+    def close(self):
+        if self.h:
+            lib().orc_preset_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def camera_uniform(pos, yaw: float, pitch: float, aspect: float, frame: int) -> CameraUniform:
+    """camera.rs:178-194 (the oracle's restatement)."""
+    u = CameraUniform()
+    p = (C.c_float * 3)(*pos)
+    lib().orc_camera_uniform(p, yaw, pitch, aspect, frame, C.byref(u))
+    return u
+
+
 class OracleScene:
     """FP64 ray queries + FP32 shading restatement over one scene's arrays."""
 
     def __init__(self, arrays):
-        # arrays: a wgpu_spectral_rt_b200.SceneArrays (pointers into host memory)
+        # arrays: an srt_scene_arrays structure (the product's SceneBuilder.arrays()
+        # or Preset.arrays()), pointers into host memory that outlive this call
         self.h = lib().orc_scene_create(C.byref(arrays))
 
     @property

@@ -87,6 +87,17 @@ void orc_render_frame_photons(const orc_scene* s, const srt_camera_uniform* cam,
 
 int orc_max_threads(void);
 
+/* The oracle's own scene generator (scenes.cpp): the arrays and camera
+ * {x, y, z, yaw, pitch} of a preset (srt_preset), built without the product
+ * library.  orc_preset_arrays points into the preset, which owns them. */
+typedef struct orc_preset orc_preset;
+orc_preset* orc_preset_create(int preset, uint32_t seed);
+void orc_preset_destroy(orc_preset* s);
+void orc_preset_arrays(const orc_preset* s, srt_scene_arrays* out, float camera[5]);
+/* camera.rs:178-194 with closed-form inverses */
+void orc_camera_uniform(const float pos[3], float yaw, float pitch, float aspect, uint32_t frame,
+                        srt_camera_uniform* out);
+
 #ifdef __cplusplus
 }
 #endif

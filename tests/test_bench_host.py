@@ -17,13 +17,22 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def test_reference_arm_prints_one_contract_line():
+    """One JSON line of the contract, from the oracle alone: the GPU package
+    and its native library are never loaded by the reference arm."""
     env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
-    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "3"],
-                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    code = ("import sys, bench\n"
+            "rc = bench.main(['--impl', 'reference', '--steps', '1', '--warmup', '3'])\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(int('wgpu_spectral_rt_b200' in sys.modules), int('libsrt_b200' in maps), "
+            "int('liboracle' in maps), file=sys.stderr)\n"
+            "sys.exit(rc)\n")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stderr.strip().splitlines()[-1] == "0 0 1"  # no GPU package, no libsrt_b200.so, the oracle
     lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
     d = json.loads(lines[0])
+    assert "1568780 triangles" in d["config"]["workload"]
     assert d["impl"] == "reference" and d["metric"] == "Mpaths/s" and d["unit"] == "Mpaths/s"
     assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1 and d["warmup"] == 3
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] in ("port", "reference")

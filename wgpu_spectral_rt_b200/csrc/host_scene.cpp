@@ -556,8 +556,12 @@ bool preset_fill(srt_scene_builder* b, int preset, uint32_t seed, float cam[5]) 
             uint32_t red = b->add_material(mat(0.65f, 0.05f, 0.05f, 1, 0, 0, 0, 0));
             uint32_t green = b->add_material(mat(0.12f, 0.45f, 0.15f, 1, 0, 0, 0, 0));
             uint32_t white = b->add_material(mat(0.73f, 0.73f, 0.73f, 1, 0, 0, 0, 0));
-            uint32_t stone = b->add_material(mat(0.3f + 0.5f * rnd(), 0.3f + 0.5f * rnd(), 0.3f + 0.5f * rnd(), 1, 0,
-                                                 0, 0, 0));
+            // draws are sequenced explicitly: the evaluation order of function
+            // arguments is unspecified in C++
+            const float sr = 0.3f + 0.5f * rnd();
+            const float sg = 0.3f + 0.5f * rnd();
+            const float sb = 0.3f + 0.5f * rnd();
+            uint32_t stone = b->add_material(mat(sr, sg, sb, 1, 0, 0, 0, 0));
             uint32_t plane = add_geom(b, geom_plane);
             cornell_walls(b, plane, white, red, green);
             float lp[4] = {0.0f, 6500.0f, 2.0f, 0.0f};
@@ -581,15 +585,21 @@ bool preset_fill(srt_scene_builder* b, int preset, uint32_t seed, float cam[5]) 
             for (int k = 0; used + per_ball <= budget && k < 512; ++k, used += per_ball) {
                 float kind = rnd();
                 uint32_t m;
-                if (kind < 0.4f) m = b->add_material(mat(0.9f, 0.8f, 0.7f, 1, 1, 0.05f + 0.45f * rnd(), 0, 0));
-                else if (kind < 0.8f)
-                    m = b->add_material(mat(1, 1, 1, 0.05f + 0.45f * rnd(), 5, 200.0f + 600.0f * rnd(), 1.33f, 1.5f));
-                else m = b->add_material(mat(1, 1, 1, 1, 2, 0, 1.5f, 0.0042f));
-                float r = 0.05f + 0.1f * rnd();
-                b->add_instance(ball, m,
-                                mat4_mul(mat4_translation(-0.85f + 1.7f * rnd(), -1.0f + r + 1.2f * rnd(),
-                                                          -0.85f + 1.7f * rnd()),
-                                         mat4_scale(2 * r, 2 * r, 2 * r)));
+                if (kind < 0.4f) {
+                    const float rough = 0.05f + 0.45f * rnd();
+                    m = b->add_material(mat(0.9f, 0.8f, 0.7f, 1, 1, rough, 0, 0));
+                } else if (kind < 0.8f) {
+                    const float alpha = 0.05f + 0.45f * rnd();
+                    const float film = 200.0f + 600.0f * rnd();
+                    m = b->add_material(mat(1, 1, 1, alpha, 5, film, 1.33f, 1.5f));
+                } else {
+                    m = b->add_material(mat(1, 1, 1, 1, 2, 0, 1.5f, 0.0042f));
+                }
+                const float r = 0.05f + 0.1f * rnd();
+                const float px = -0.85f + 1.7f * rnd();
+                const float py = -1.0f + r + 1.2f * rnd();
+                const float pz = -0.85f + 1.7f * rnd();
+                b->add_instance(ball, m, mat4_mul(mat4_translation(px, py, pz), mat4_scale(2 * r, 2 * r, 2 * r)));
             }
             return true;
         }
