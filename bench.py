@@ -481,6 +481,22 @@ def main(argv=None):
                                         "ms_trace_shadow", "ms_finalize")}}
         if traffic is not None:
             roof["traffic_note"] = tnote
+        # per bounce: rays, algorithmic GB/s of the closest-hit launch, and the
+        # share of closest-hit time spent in the launches past the first four
+        bt, bc = rt.bounce_stats(), rc.bounce_stats()
+        per = []
+        for k in range(depth):
+            rays_k = float(bc["rays"][0][k]) / nf
+            bytes_k = (float(bc["rays"][0][k]) * 48 + float(bc["nodes"][0][k]) * 80 + float(bc["tris"][0][k]) * 48) / nf
+            ms_k = float(bt["ms"][0][k]) / nf
+            per.append({"bounce": k, "rays": round(rays_k), "ms": round(ms_k, 4),
+                        "gbs": round(bytes_k / (ms_k * 1e-3) / 1e9, 1) if ms_k > 0 else None,
+                        "nodes_per_ray": round(float(bc["nodes"][0][k]) / max(1.0, float(bc["rays"][0][k])), 2),
+                        "shadow_rays": round(float(bc["rays"][1][k]) / nf),
+                        "shadow_ms": round(float(bt["ms"][1][k]) / nf, 4)})
+        roof["per_bounce_closest"] = per
+        tail = sum(x["ms"] for x in per[4:])
+        roof["tail_share"] = round(tail / max(1e-9, sum(x["ms"] for x in per)), 3)
         rt.close()
         rc.close()
 

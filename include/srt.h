@@ -184,6 +184,20 @@ typedef struct srt_stats {
     double ms_guide_train;      /* SRT_FLAG_STAGE_TIMING + SRT_FLAG_GUIDING: training step times */
 } srt_stats;
 
+/* Per-bounce statistics of a renderer's frames since the last
+ * srt_renderer_reset_stats (diagnostics of the wavefront; no reference
+ * counterpart).  Index [kind][bounce], kind 0 camera closest-hit rays, 1 shadow
+ * rays, 2 photon rays: rays traced; with SRT_FLAG_COUNT_VISITS the BVH8 nodes
+ * visited and triangles tested; with SRT_FLAG_STAGE_TIMING the traversal time
+ * (CUDA events) of the closest-hit (ms[0]) and shadow (ms[1]) launches. */
+#define SRT_MAX_BOUNCE_STATS 32
+typedef struct srt_bounce_stats {
+    uint64_t rays[3][SRT_MAX_BOUNCE_STATS];
+    uint64_t nodes[3][SRT_MAX_BOUNCE_STATS];
+    uint64_t tris[3][SRT_MAX_BOUNCE_STATS];
+    double ms[2][SRT_MAX_BOUNCE_STATS];
+} srt_bounce_stats;
+
 typedef struct srt_ctx srt_ctx;
 typedef struct srt_scene srt_scene;
 typedef struct srt_scene_builder srt_scene_builder;
@@ -360,6 +374,7 @@ srt_status srt_screenshot_write_async(const char* path, const uint8_t* rgba, uin
                                       uint32_t pitch);
 srt_status srt_screenshot_flush(uint32_t* failed_writes);
 srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out);
+srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_stats* out);
 srt_status srt_renderer_reset_stats(srt_renderer* r);
 /* The photon set of the last frame in emission order (photon_emit.wgsl
  * storage): copies min(count, capacity) photons to `out` (may be NULL) and

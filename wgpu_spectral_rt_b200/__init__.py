@@ -91,6 +91,11 @@ class Stats(C.Structure):
                 ("ms_guide_train", C.c_double)]
 
 
+class BounceStats(C.Structure):  # srt_bounce_stats
+    _fields_ = [("rays", (C.c_uint64 * 32) * 3), ("nodes", (C.c_uint64 * 32) * 3), ("tris", (C.c_uint64 * 32) * 3),
+                ("ms", (C.c_double * 32) * 2)]
+
+
 class SceneArrays(C.Structure):
     _fields_ = [("vertices", C.POINTER(Vertex)), ("n_vertices", C.c_uint32),
                 ("indices", C.POINTER(C.c_uint32)), ("n_indices", C.c_uint32),
@@ -176,6 +181,7 @@ SIGNATURES = {
     "srt_screenshot_write_async": (_I, [C.c_char_p, _P, _U32, _U32, _U32]),
     "srt_screenshot_flush": (_I, [_P]),
     "srt_renderer_get_stats": (_I, [_P, C.POINTER(Stats)]),
+    "srt_renderer_get_bounce_stats": (_I, [_P, C.POINTER(BounceStats)]),
     "srt_renderer_reset_stats": (_I, [_P]),
     "srt_renderer_read_photons": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
     "srt_trace_rays": (_I, [_P, _P, _U32, _P, _I]),
@@ -538,6 +544,14 @@ class Renderer:
         _check(lib().srt_renderer_get_stats(self.h, C.byref(s)), self.ctx.h)
         return {f: (list(getattr(s, f)) if f in ("nodes_visited", "tris_tested") else getattr(s, f))
                 for f, _ in Stats._fields_}
+
+    def bounce_stats(self) -> dict:
+        """Per-bounce arrays [kind][bounce] (kind 0 camera closest, 1 shadow, 2 photon): rays, nodes, tris;
+        ms [0 closest, 1 shadow][bounce] (SRT_FLAG_STAGE_TIMING)."""
+        s = BounceStats()
+        _check(lib().srt_renderer_get_bounce_stats(self.h, C.byref(s)), self.ctx.h)
+        return {"rays": np.array(s.rays, np.uint64), "nodes": np.array(s.nodes, np.uint64),
+                "tris": np.array(s.tris, np.uint64), "ms": np.array(s.ms, np.float64)}
 
     def reset_stats(self):
         _check(lib().srt_renderer_reset_stats(self.h), self.ctx.h)

@@ -640,6 +640,7 @@ struct srt_renderer {
     uint32_t frame_count = 0;
     uint64_t frames = 0, launches = 0, photons_emitted = 0, trace_launches = 0;
     double ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // photon, -, closest, shade, shadow, finalize, raygen, guide training
+    double ms_bounce[2][MAX_BOUNCES + 1] = {};  // closest-hit and shadow traversal per bounce
     std::vector<cudaEvent_t> ev;
     GuideArgs guide{};  // SRT_FLAG_GUIDING only
     // asynchronous RGBA8 read-back: two pinned slots used in turn
@@ -997,9 +998,12 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
             r->ms[6] += el(1, 2);
             for (uint32_t b = 0; b < r->p.max_depth; ++b) {
                 size_t base = 2 + 3 * b;
-                r->ms[2] += el(base, base + 1);
+                const double tc = el(base, base + 1), ts = el(base + 2, base + 3);
+                r->ms[2] += tc;
                 r->ms[3] += el(base + 1, base + 2);
-                r->ms[4] += el(base + 2, base + 3);
+                r->ms[4] += ts;
+                r->ms_bounce[0][b] += tc;
+                r->ms_bounce[1][b] += ts;
             }
             r->ms[5] += el(2 + 3 * r->p.max_depth, 3 + 3 * r->p.max_depth);
             r->ms[7] += el(3 + 3 * r->p.max_depth, 4 + 3 * r->p.max_depth);
@@ -1144,10 +1148,11 @@ extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
     out->rays_photon = d.photon_rays;
     out->photons_emitted = r->photons_emitted;
     out->photons_stored = d.photons_stored;
-    for (int k = 0; k < 3; ++k) {
-        out->nodes_visited[k] = d.nodes_visited[k];
-        out->tris_tested[k] = d.tris_tested[k];
-    }
+    for (int k = 0; k < 3; ++k)
+        for (int b = 0; b <= MAX_BOUNCES; ++b) {
+            out->nodes_visited[k] += d.nodes_bounce[k][b];
+            out->tris_tested[k] += d.tris_bounce[k][b];
+        }
     out->ms_photon_pass = r->ms[0];
     out->ms_trace_closest = r->ms[2];
     out->ms_shade = r->ms[3];
@@ -1160,12 +1165,33 @@ extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
     return check_device_error(c, r->err);
 }
 
+extern "C" srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_stats* out) {
+    if (!r || !out) return SRT_ERR_INVALID_ARG;
+    static_assert(SRT_MAX_BOUNCE_STATS == MAX_BOUNCES + 1, "per-bounce arrays");
+    srt_ctx* c = r->ctx;
+    DevStats d;
+    CUDA_TRY(c, cudaMemcpyAsync(&d, r->stats, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    std::memset(out, 0, sizeof *out);
+    for (int k = 0; k < 3; ++k)
+        for (int b = 0; b <= MAX_BOUNCES; ++b) {
+            out->rays[k][b] = d.rays_bounce[k][b];
+            out->nodes[k][b] = d.nodes_bounce[k][b];
+            out->tris[k][b] = d.tris_bounce[k][b];
+        }
+    for (int k = 0; k < 2; ++k)
+        for (int b = 0; b <= MAX_BOUNCES; ++b) out->ms[k][b] = r->ms_bounce[k][b];
+    return check_device_error(c, r->err);
+}
+
 extern "C" srt_status srt_renderer_reset_stats(srt_renderer* r) {
     if (!r) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     CUDA_TRY(c, cudaMemsetAsync(r->stats, 0, sizeof(DevStats), c->stream));
     r->frames = r->launches = r->photons_emitted = r->trace_launches = 0;
     for (double& m : r->ms) m = 0.0;
+    for (auto& row : r->ms_bounce)
+        for (double& m : row) m = 0.0;
     return SRT_OK;
 }
 

@@ -512,13 +512,18 @@ __global__ void k_frame_stats(FrameArgs a) {
     for (uint32_t i = 0; i < a.max_depth; ++i) {
         c += a.counters->paths[i];
         s += a.counters->shadow[i];
+        a.stats->rays_bounce[TRAV_CLOSEST][i] += a.counters->paths[i];
+        a.stats->rays_bounce[TRAV_SHADOW][i] += a.counters->shadow[i];
     }
     a.stats->closest_rays += c;
     a.stats->shadow_rays += s;
     a.stats->paths += a.counters->paths[0];
     unsigned long long pr = 0;
     if (a.photons_per_frame > 0u)
-        for (uint32_t i = 0; i < a.photon_max_bounces; ++i) pr += a.counters->photon_paths[i];
+        for (uint32_t i = 0; i < a.photon_max_bounces; ++i) {
+            pr += a.counters->photon_paths[i];
+            a.stats->rays_bounce[TRAV_PHOTON][i] += a.counters->photon_paths[i];
+        }
     a.stats->photon_rays += pr;
 }
 
@@ -629,7 +634,7 @@ int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
                            &dir_keys, &order);
     a.ph.sorted_vals = order;  // bounce-0 queue (read by k_photon_shade at bounce 0)
     for (uint32_t b = 0; b < a.photon_max_bounces; ++b) {
-        launches += launch_trace_queue(a.scene, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b],
+        launches += launch_trace_queue(a.scene, b, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b],
                                        &a.counters->fetch[TRAV_PHOTON][b], n, a.ph.ray_o, a.ph.ray_d, a.ph.hit,
                                        TRAV_PHOTON, a.count_visits, a.err, a.stats, a.sm_count, st);
         k_photon_shade<<<blocks_for(n, TRACE_BLOCK), TRACE_BLOCK, 0, st>>>(a, b);

@@ -30,8 +30,11 @@ struct DevStats {
     unsigned long long photon_rays;    // photon-pass closest-hit rays
     unsigned long long photons_stored;
     unsigned long long paths;
-    unsigned long long nodes_visited[3];  // by ray kind: TRAV_CLOSEST, TRAV_SHADOW, TRAV_PHOTON
-    unsigned long long tris_tested[3];
+    // by ray kind (TRAV_CLOSEST, TRAV_SHADOW, TRAV_PHOTON) and bounce;
+    // node visits and triangle tests with SRT_FLAG_COUNT_VISITS only
+    unsigned long long rays_bounce[3][MAX_BOUNCES + 1];
+    unsigned long long nodes_bounce[3][MAX_BOUNCES + 1];
+    unsigned long long tris_bounce[3][MAX_BOUNCES + 1];
 };
 
 constexpr int TRAV_CLOSEST = 0, TRAV_SHADOW = 1, TRAV_PHOTON = 2;
@@ -110,8 +113,8 @@ int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);  
 // Closest hit for the rays named by queue[0 .. *count) (queue NULL: 0 .. *count),
 // max_n bounding *count; traversal statistics go to slot `kind` (TRAV_*).
 // `fetch` is a zeroed counter the persistent warps draw queue positions from.
-int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t* fetch,
-                       uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
+int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue, const uint32_t* count,
+                       uint32_t* fetch, uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
                        uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st);  // trace_kernels.cu
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     k_trace(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
             const float4* __restrict__ ro, const float4* __restrict__ rd, float4* __restrict__ hit,
             const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c, float4* __restrict__ rad,
-            uint32_t* err, DevStats* stats, int kind) {
+            uint32_t* err, DevStats* stats, int kind, int bounce) {
     extern __shared__ uint2 stack_smem[];
     uint32_t q = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t n = *count;
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     Ray ray{xyz(o), xyz(d), o.w, d.w};
     float t = 0.f, u = 0.f, v = 0.f;
     uint32_t prim;
-    TravCounters tc{&stats->nodes_visited[kind], &stats->tris_tested[kind]};
+    TravCounters tc{&stats->nodes_bounce[kind][bounce], &stats->tris_bounce[kind][bounce]};
     bool h = traverse<ANY, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
     if (ANY) {
         // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     k_trace_pt(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
                uint32_t* __restrict__ fetch, const float4* __restrict__ ro, const float4* __restrict__ rd,
                float4* __restrict__ hit, const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
-               float4* __restrict__ rad, uint32_t* err, DevStats* stats, int kind) {
+               float4* __restrict__ rad, uint32_t* err, DevStats* stats, int kind, int bounce) {
     extern __shared__ uint2 stack_smem[];
     uint2* stack = stack_smem + threadIdx.x;
     const uint32_t n = *count;
@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
         }
     }
     if (COUNT) {
-        atomicAdd(&stats->nodes_visited[kind], (unsigned long long)n_nodes);
-        atomicAdd(&stats->tris_tested[kind], (unsigned long long)n_tris);
+        atomicAdd(&stats->nodes_bounce[kind][bounce], (unsigned long long)n_nodes);
+        atomicAdd(&stats->tris_bounce[kind][bounce], (unsigned long long)n_tris);
     }
 }
 
@@ -224,6 +224,7 @@ struct TraceLaunch {
     DevStats* stats;
     int kind;
     int sm_count;
+    int bounce;
 };
 
 template <bool ANY, bool COUNT, int STACK>
@@ -234,10 +235,10 @@ void launch_one(const TraceLaunch& L, cudaStream_t st) {
         grid = std::min(grid, std::max(1u, blocks_for(L.max_n, TRACE_BLOCK)));
         k_trace_pt<ANY, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(L.s, L.queue, L.count, L.fetch, L.ro, L.rd,
                                                                       L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats,
-                                                                      L.kind);
+                                                                      L.kind, L.bounce);
     } else {
         k_trace<ANY, COUNT, STACK><<<blocks_for(L.max_n, TRACE_BLOCK), TRACE_BLOCK, smem, st>>>(
-            L.s, L.queue, L.count, L.ro, L.rd, L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats, L.kind);
+            L.s, L.queue, L.count, L.ro, L.rd, L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats, L.kind, L.bounce);
     }
 }
 
@@ -261,7 +262,7 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     TraceLaunch L{a.scene, a.pb.queue[bounce & 1], &a.counters->paths[bounce],
                   bounce == 0 ? nullptr : &a.counters->fetch[TRAV_CLOSEST][bounce],
                   a.width * a.height, a.pb.ray_o, a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats,
-                  TRAV_CLOSEST, a.sm_count};
+                  TRAV_CLOSEST, a.sm_count, (int)bounce};
     launch_kind<false>(L, a.count_visits, st);
     return 1;
 }
@@ -274,19 +275,20 @@ int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
                       ? &a.counters->fetch[TRAV_SHADOW][bounce]
                       : nullptr,
                   a.width * a.height, a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad, a.err, a.stats,
-                  TRAV_SHADOW, a.sm_count};
+                  TRAV_SHADOW, a.sm_count, (int)bounce};
     launch_kind<true>(L, a.count_visits, st);
     return 1;
 }
 
-int launch_trace_queue(const DevScene& s, const uint32_t* queue, const uint32_t* count, uint32_t* fetch,
-                       uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
-                       uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st) {
+int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue, const uint32_t* count,
+                       uint32_t* fetch, uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind,
+                       int count_visits, uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st) {
     if (max_n == 0) return 0;
     // photon rays arrive direction-sorted: one ray per thread keeps that order
     // (persistent refill measured slower, 3.35 vs 3.15 ms per photon pass)
     (void)fetch;
-    TraceLaunch L{s, queue, count, nullptr, max_n, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind, sm_count};
+    TraceLaunch L{s, queue, count, nullptr, max_n, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind, sm_count,
+                  (int)bounce};
     launch_kind<false>(L, count_visits, st);
     return 1;
 }
