@@ -225,6 +225,12 @@ int srt_ctx_sm_count(const srt_ctx* ctx);
 #define SRT_BVH_SAH  0
 #define SRT_BVH_LBVH 1
 srt_status srt_ctx_set_bvh_builder(srt_ctx* ctx, int builder);
+/* Children per BVH node (2..8, default 8) for the scenes built next: the
+ * collapse stops expanding a node at `width` children; nodes keep the 8-slot
+ * compressed format, so the same traversal runs every width.  Like the
+ * builder, the width changes speed, never results.  No reference
+ * counterpart (the driver builds the reference's BLAS/TLAS). */
+srt_status srt_ctx_set_bvh_width(srt_ctx* ctx, uint32_t width);
 
 /* ------------------------------------------------------------------------ */
 /* Scene API: SceneBuilder (src/scene/builder.rs:47-267).                     */

@@ -205,6 +205,7 @@ SIGNATURES = {
     "srt_scene_read_lights": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
     "srt_scene_read_bvh": (_I, [_P, _P, C.c_uint64, _P, C.c_uint64]),
     "srt_ctx_set_bvh_builder": (_I, [_P, _I]),
+    "srt_ctx_set_bvh_width": (_I, [_P, _U32]),
     "srt_read_ldr_async": (_I, [_P, C.POINTER(_U32)]),
     "srt_ldr_wait": (_I, [_P, _U32, C.POINTER(C.POINTER(C.c_uint8))]),
     "srt_guide_param_count": (_U32, []),
@@ -293,6 +294,10 @@ class Context:
     def set_bvh_builder(self, builder: int) -> None:
         """BVH_SAH (default) or BVH_LBVH for the scenes built next."""
         _check(lib().srt_ctx_set_bvh_builder(self.h, builder), self.h)
+
+    def set_bvh_width(self, width: int) -> None:
+        """Children per BVH node (2..8, default 8) for the scenes built next."""
+        _check(lib().srt_ctx_set_bvh_width(self.h, width), self.h)
 
     def synchronize(self):
         _check(lib().srt_ctx_synchronize(self.h), self.h)

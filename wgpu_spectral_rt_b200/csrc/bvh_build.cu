@@ -706,7 +706,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
                            uint32_t* __restrict__ n_out, Node8* __restrict__ nodes, uint32_t* __restrict__ node_alloc,
                            uint32_t node_cap, TriSlot* __restrict__ tris_out, uint32_t* __restrict__ tri_alloc,
                            uint32_t tri_cap, const TriSlot* __restrict__ flat, const uint32_t* __restrict__ sorted_tri,
-                           uint32_t* __restrict__ err) {
+                           uint32_t* __restrict__ err, int width) {
     uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_in) return;
     uint2 q = qin[e];
@@ -721,7 +721,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         refs[1] = nd.y;
         nc = 2;
     }
-    while (nc < 8) {
+    while (nc < width) {
         int best = -1;
         float best_area = -1.0f;
         for (int c = 0; c < nc; ++c) {
@@ -948,7 +948,8 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
         while (n_in > 0) {
             CK(cudaMemsetAsync(counters + 2, 0, 4, st));
             k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(b, qa, n_in, qb, counters + 2, out->nodes, counters,
-                                                           node_cap, out->tris, counters + 1, n, flat, sv, err);
+                                                           node_cap, out->tris, counters + 1, n, flat, sv, err,
+                                                           in.width < 2 ? 2 : (in.width > 8 ? 8 : in.width));
             ++out->kernel_launches;
             ++depth;
             CK(cudaGetLastError());

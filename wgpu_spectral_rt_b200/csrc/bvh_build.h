@@ -41,6 +41,7 @@ struct BvhInputs {
     uint32_t n_inst;
     uint32_t n_tris;          // flattened triangle count
     int builder;              // BVH_BUILDER_*
+    int width = 8;            // children per node, 2..8 (nodes keep the 8-slot format)
 };
 
 struct BvhOutputs {

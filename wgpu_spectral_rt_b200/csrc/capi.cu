@@ -44,6 +44,7 @@ struct srt_ctx {
     int children = 0;
     bool closing = false;
     int bvh_builder = 0;  // SRT_BVH_* for the scenes built next
+    int bvh_width = 8;    // children per BVH node for the scenes built next
 };
 
 namespace {
@@ -162,6 +163,12 @@ srt_status srt_ctx_destroy(srt_ctx* c) {
 srt_status srt_ctx_set_bvh_builder(srt_ctx* c, int builder) {
     if (!c || (builder != SRT_BVH_SAH && builder != SRT_BVH_LBVH)) return SRT_ERR_INVALID_ARG;
     c->bvh_builder = builder;
+    return SRT_OK;
+}
+
+srt_status srt_ctx_set_bvh_width(srt_ctx* c, uint32_t width) {
+    if (!c || width < 2 || width > 8) return SRT_ERR_INVALID_ARG;
+    c->bvh_width = (int)width;
     return SRT_OK;
 }
 
@@ -424,7 +431,7 @@ srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
     CUDA_TRY(c, upload(&s->inst, inst.data(), sizeof(InstDev) * inst.size(), sizeof(InstDev) * inst.size(), st));
     CUDA_TRY(c, upload(&s->fwd, fwd.data(), sizeof(InstFwd) * fwd.size(), sizeof(InstFwd) * fwd.size(), st));
     BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total,
-                 c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH};
+                 c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH, c->bvh_width};
     std::string msg;
     cudaError_t e = build_bvh8(bi, st, &s->bvh, &msg);
     if (e != cudaSuccess) return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, "BVH build: " + msg);
