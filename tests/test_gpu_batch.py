@@ -62,6 +62,39 @@ def test_batch_matches_single_scene_renders(srt, ctx):
     batch.close()
 
 
+def test_batch_scene_matches_oracle(srt, orc, ctx):
+    """One scene of a batch (config 1, 96x64) against the CPU oracle frame by
+    frame, on the photon set the batch's photon pass produced: the same
+    per-pixel agreement as single-scene frames."""
+    from conftest import rel_err, relmse
+
+    sc = _scenes(srt, ctx)
+    scenes, ctls = [s for s, _ in sc], [c for _, c in sc]
+    params = _params(srt)
+    batch = srt.Batch(ctx, scenes, SIZES, params)
+    k = 1
+    w, h = SIZES[k]
+    b = srt.SceneBuilder()
+    b.add_preset(srt.PRESET_CONFIG1)
+    o = orc.OracleScene(b.arrays())
+    acc_o = np.zeros((h, w, 4), np.float32)
+    frames = 2
+    for f in range(frames):
+        cams = _cams(ctls, f)
+        batch.render(cams)
+        ph = batch.renderers[k].read_photons()
+        acc_o, _, _, _ = o.render_frame(cams[k], w, h, params[k], acc_o, want_ldr=False, photons=ph)
+    acc_g = batch.renderers[k].read_accum()
+    e = rel_err(acc_g[..., :3], acc_o[..., :3], floor=1e-3)
+    pix_ok = (e < 1e-3).all(-1)
+    rm = relmse(acc_g[..., :3] / frames, acc_o[..., :3] / frames)
+    print(f"[parity] batch scene {k}: pixels agreeing {pix_ok.mean():.5f}, relMSE {rm:.3e}", flush=True)
+    assert pix_ok.mean() >= 0.99
+    assert rm < 1e-4
+    batch.close()
+    o.close()
+
+
 def test_batch_autotune(srt, ctx):
     sc = _scenes(srt, ctx)
     scenes, ctls = [s for s, _ in sc], [c for _, c in sc]

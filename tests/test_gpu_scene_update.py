@@ -130,3 +130,40 @@ def test_update_rejects_bad_input(srt, ctx):
     with pytest.raises(srt.SrtError):
         s.update_instances([CUBE], np.zeros((1, 16), np.float32))  # singular
     s.close()
+
+
+@pytest.mark.parametrize("preset", [0, 1, 2, 4, 5])
+def test_gpu_light_expansion_matches_oracle_expansion(srt, orc, ctx, preset):
+    """The device expansion of light instances (builder.rs:101-129) against the
+    oracle's own restatement of the builder (oracle/scenes.cpp), bit for bit."""
+    b = srt.SceneBuilder()
+    b.add_preset(preset)
+    scene = b.build(ctx)
+    mine = orc.Preset(preset)
+    a = mine.arrays()
+    import ctypes as C
+
+    ref = np.ctypeslib.as_array(C.cast(a.lights, C.POINTER(C.c_float)), shape=(a.n_lights, 16)).copy()
+    np.testing.assert_array_equal(scene.read_lights(), ref)
+    scene.close()
+    mine.close()
+
+
+def test_moved_scene_hits_match_the_oracle(srt, orc, ctx):
+    """After srt_scene_update_instances, the moved scene's closest hits against
+    the FP64 oracle's brute force over the moved scene's arrays: exact outside
+    the named exclusion set."""
+    from conftest import closest_hit_parity, report
+
+    _, moved = _build(srt, ctx, **T0)
+    moved.update_instances([LIGHT, CUBE], np.stack([_colmajor(T1["light_t"]), _colmajor(T1["cube_t"])]))
+    b1, _unused = _build(srt, ctx, **T1)
+    o = orc.OracleScene(b1.arrays())
+    rays = _rays(40_000, 6)
+    d = closest_hit_parity(moved, o, rays, brute=True)
+    report("moved scene", d)
+    assert len(d["bad"]) == 0
+    assert d["max_rel_dt"] < 1e-5
+    _unused.close()
+    moved.close()
+    o.close()

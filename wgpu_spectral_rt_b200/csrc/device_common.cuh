@@ -487,6 +487,64 @@ struct TravCounters {
     unsigned long long* tris;
 };
 
+// Asynchronous 16-byte copies global -> shared (cp.async, L1-cached): a
+// lane starts fetching the next node into its shared-memory slot, tests
+// the pending triangles meanwhile, then waits for its own copies.
+SRT_DEV void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+SRT_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+SRT_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Node idx into this lane's slot: 5 chunks, chunk k at nbuf[k * stride].
+SRT_DEV void fetch_node_async(const DevScene& S, uint32_t idx, uint4* nbuf, int stride) {
+    const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) cp_async16(nbuf + k * stride, np + k);
+    cp_async_commit();
+}
+
+// Child slab tests of one node (words w0..w4) for a ray with inverse
+// direction idir and octant oct: the node's hit internal children (bits
+// 24..31, ordered by octant) | imask, and its hit triangle bits.
+SRT_DEV void node_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, uint4 w4, float3 o, float3 idir, uint32_t oct,
+                           float tmin, float tbest, uint2& g, uint2& tg) {
+    float sx = __uint_as_float((w0.w & 0xFFu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
+          sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    uint32_t imask = w0.w >> 24;
+    float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;
+    float bx = unbias(ax, (__uint_as_float(w0.x) - o.x) * idir.x), by = unbias(ay, (__uint_as_float(w0.y) - o.y) * idir.y),
+          bz = unbias(az, (__uint_as_float(w0.z) - o.z) * idir.z);
+    uint32_t nx0 = (oct & 1u) ? w3.z : w2.x, nx1 = (oct & 1u) ? w3.w : w2.y;
+    uint32_t fx0 = (oct & 1u) ? w2.x : w3.z, fx1 = (oct & 1u) ? w2.y : w3.w;
+    uint32_t ny0 = (oct & 2u) ? w4.x : w2.z, ny1 = (oct & 2u) ? w4.y : w2.w;
+    uint32_t fy0 = (oct & 2u) ? w2.z : w4.x, fy1 = (oct & 2u) ? w2.w : w4.y;
+    uint32_t nz0 = (oct & 4u) ? w4.z : w3.x, nz1 = (oct & 4u) ? w4.w : w3.y;
+    uint32_t fz0 = (oct & 4u) ? w3.x : w4.z, fz1 = (oct & 4u) ? w3.y : w4.w;
+    const float robust = 1.0000004f;
+    uint32_t hits = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t k = (uint32_t)(i & 3);
+        uint32_t m = byte_of(i < 4 ? w1.z : w1.w, k);
+        const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
+                               make_float2(ax, ax), make_float2(bx, bx));
+        const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
+                               make_float2(ay, ay), make_float2(by, by));
+        const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
+                               make_float2(az, az), make_float2(bz, bz));
+        float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, tmin));
+        float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, tbest)) * robust;
+        if (m != 0u && tn <= tf) {
+            uint32_t c = m >> 5;
+            if (c == 7u) hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
+            else hits |= ((1u << c) - 1u) << (m & 31u);
+        }
+    }
+    g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
+    tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+}
+
 // Stack-based traversal of the compressed BVH8.  A node group holds the
 // hit internal children of one node (bits 24..31 of .y, ordered so that the
 // highest bit is the nearest child for this ray octant) plus the node's
@@ -495,9 +553,9 @@ struct TravCounters {
 // minimum of (t, flattened triangle id), independent of traversal order.
 // `stack` is this thread's slice of shared memory, stride `stride` entries,
 // STACK entries deep (at least the tree depth: one entry per level).
-template <bool ANY, bool COUNT, int STACK = TRAV_STACK>
+template <bool ANY, bool COUNT, int STACK = TRAV_STACK, bool PF = false>
 SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, float& t_out, uint32_t& prim_out,
-                      float& u_out, float& v_out, uint32_t* err, TravCounters cnt) {
+                      float& u_out, float& v_out, uint32_t* err, TravCounters cnt, uint4* nbuf = nullptr) {
     prim_out = MISS;
     if (S.n_nodes == 0u) return false;
     if (!(ray.d.x != 0.0f || ray.d.y != 0.0f || ray.d.z != 0.0f)) return false;
@@ -518,6 +576,37 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
     uint2 g = make_uint2(0u, (1u << (24 + (0u ^ (oct ^ 7u)))) | 1u);
     uint2 tg = make_uint2(0u, 0u);
     while (true) {
+        // ---- with PF: pick the next node and start fetching it before the
+        // triangle tests of the last node (the same visiting order)
+        bool have = true;
+        if (PF) {
+            if ((g.y & 0xFF000000u) == 0u) {
+                if (sp == 0) have = false;
+                else {
+                    --sp;
+                    g = stack[sp * stride];
+                }
+            }
+            if (have) {
+                int bit = 31 - __clz(g.y & 0xFF000000u);
+                g.y &= ~(1u << bit);
+                uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
+                uint32_t idx = g.x + __popc(g.y & ((1u << slot) - 1u) & 0xFFu);
+                if (g.y & 0xFF000000u) {
+                    if (sp >= STACK) {
+                        atomicOr(err, ERR_STACK_OVERFLOW);
+                        break;
+                    }
+                    stack[sp * stride] = g;
+                    ++sp;
+                }
+                if (idx >= S.n_nodes) {
+                    atomicOr(err, ERR_BAD_INDEX);
+                    break;
+                }
+                fetch_node_async(S, idx, nbuf, stride);
+            }
+        }
         // ---- triangles of the last node
         while (tg.y != 0u) {
             int b = __ffs(tg.y) - 1;
@@ -531,6 +620,7 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
             if (intersect_tri(r, sh, xyz(a0), xyz(a1), xyz(a2), t, u, v)) {
                 uint32_t id = __float_as_uint(a0.w);
                 if (ANY) {
+                    if (PF) cp_async_wait_all();  // no copy into the slot outlives the ray
                     t_out = t;
                     prim_out = id;
                     if (COUNT) {
@@ -548,6 +638,14 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
                     }
                 }
             }
+        }
+        if (PF) {
+            if (!have) break;
+            cp_async_wait_all();
+            if (COUNT) ++n_nodes;
+            node_children(nbuf[0], nbuf[stride], nbuf[2 * stride], nbuf[3 * stride], nbuf[4 * stride], ray.o, idir, oct,
+                          ray.tmin, tbest, g, tg);
+            continue;
         }
         // ---- next node
         if ((g.y & 0xFF000000u) == 0u) {
@@ -675,10 +773,41 @@ SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, floa
 }
 
 // Returns true when the ray is finished (for ANY: T.best != MISS on a hit).
-template <bool ANY, int STACK>
+template <bool ANY, int STACK, bool PF = false>
 SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
-                       uint32_t& n_tris) {
+                       uint32_t& n_tris, uint4* nbuf = nullptr) {
     const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
+    bool have = true;
+    if (PF) {
+        // pick the next node and start fetching it; the triangle tests below
+        // run while the copy is in flight (same visiting order)
+        if ((T.g.y & 0xFF000000u) == 0u) {
+            if (T.sp == 0) have = false;
+            else {
+                --T.sp;
+                T.g = stack[T.sp * stride];
+            }
+        }
+        if (have) {
+            int bit = 31 - __clz(T.g.y & 0xFF000000u);
+            T.g.y &= ~(1u << bit);
+            uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
+            uint32_t idx = T.g.x + __popc(T.g.y & ((1u << slot) - 1u) & 0xFFu);
+            if (T.g.y & 0xFF000000u) {
+                if (T.sp >= STACK) {
+                    atomicOr(err, ERR_STACK_OVERFLOW);
+                    return true;
+                }
+                stack[T.sp * stride] = T.g;
+                ++T.sp;
+            }
+            if (idx >= S.n_nodes) {
+                atomicOr(err, ERR_BAD_INDEX);
+                return true;
+            }
+            fetch_node_async(S, idx, nbuf, stride);
+        }
+    }
 #if SRT_TRAV_ONE_TRI_PER_STEP
     // one item per step: a triangle if one is pending, else a node, so a lane
     // with a long triangle list does not hold up the lanes visiting nodes
@@ -712,6 +841,7 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         if (!(t >= T.tmin && t <= T.tbest)) continue;
         uint32_t id = __float_as_uint(a0.w);
         if (ANY) {
+            if (PF && have) cp_async_wait_all();  // no copy into the slot outlives the ray
             T.best = id;
             T.tbest = t;
             return true;
@@ -726,6 +856,14 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
 #if SRT_TRAV_ONE_TRI_PER_STEP
     if (tri_step) return false;
 #endif
+    if (PF) {
+        if (!have) return true;
+        cp_async_wait_all();
+        ++n_nodes;
+        node_children(nbuf[0], nbuf[stride], nbuf[2 * stride], nbuf[3 * stride], nbuf[4 * stride], T.o, T.idir, oct,
+                      T.tmin, T.tbest, T.g, T.tg);
+        return false;
+    }
     if ((T.g.y & 0xFF000000u) == 0u) {
         if (T.sp == 0) return true;
         --T.sp;

@@ -33,9 +33,28 @@
 #define SRT_SHADOW_PERSISTENT_FROM 0
 #endif
 
+// Fetch the next node with cp.async into shared memory while the pending
+// triangle tests run (k_trace and k_trace_pt).
+#ifndef SRT_TRAV_PREFETCH
+#define SRT_TRAV_PREFETCH 0
+#endif
+
 namespace srt {
 
 namespace {
+
+constexpr bool kPrefetch = SRT_TRAV_PREFETCH != 0;
+
+// Dynamic shared memory of a traversal block: the stacks, then (prefetch)
+// 5 x uint4 node slots per thread.
+template <int STACK>
+constexpr size_t trace_smem() {
+    return sizeof(uint2) * STACK * TRACE_BLOCK + (kPrefetch ? sizeof(uint4) * 5 * TRACE_BLOCK : 0);
+}
+template <int STACK>
+SRT_DEV uint4* node_slots(uint2* smem) {
+    return reinterpret_cast<uint4*>(smem + STACK * TRACE_BLOCK) + threadIdx.x;
+}
 
 // One ray per thread, one launch over the whole queue.
 template <bool ANY, bool COUNT, int STACK>
@@ -54,7 +73,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     float t = 0.f, u = 0.f, v = 0.f;
     uint32_t prim;
     TravCounters tc{&stats->nodes_bounce[kind][bounce], &stats->tris_bounce[kind][bounce]};
-    bool h = traverse<ANY, COUNT, STACK>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err, tc);
+    bool h = traverse<ANY, COUNT, STACK, kPrefetch>(S, ray, stack_smem + threadIdx.x, TRACE_BLOCK, t, prim, u, v, err,
+                                                    tc, kPrefetch ? node_slots<STACK>(stack_smem) : nullptr);
     if (ANY) {
         // shadow ray: unoccluded -> add its contribution (shader.wgsl:659-669)
         if (!h) {
@@ -114,7 +134,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
             if (exhausted) break;
             continue;
         }
-        if (active && trav_step<ANY, STACK>(S, T, stack, TRACE_BLOCK, err, n_nodes, n_tris)) {
+        if (active && trav_step<ANY, STACK, kPrefetch>(S, T, stack, TRACE_BLOCK, err, n_nodes, n_tris,
+                                                       kPrefetch ? node_slots<STACK>(stack_smem) : nullptr)) {
             active = false;
             if (ANY) {
                 if (T.best == MISS) {
@@ -229,7 +250,7 @@ struct TraceLaunch {
 
 template <bool ANY, bool COUNT, int STACK>
 void launch_one(const TraceLaunch& L, cudaStream_t st) {
-    size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
+    size_t smem = trace_smem<STACK>();
     if (SRT_TRACE_PERSISTENT && L.fetch) {
         uint32_t grid = (uint32_t)(L.sm_count > 0 ? L.sm_count : 148) * SRT_TRACE_MIN_BLOCKS;
         grid = std::min(grid, std::max(1u, blocks_for(L.max_n, TRACE_BLOCK)));
