@@ -252,17 +252,43 @@ def run_reference(args, cfg, rank, world):
     return 0
 
 
-def batched_section(srt, ctx, stream, n_scenes=32, iters=3, seed=12345):
-    """C3: n seeded scenes (triangle budgets log-uniform in [1e4, 2e6], square
-    viewports of 256..1024, 1M..8M photons each), one iteration = 1 spp of
-    every scene; batched renderer after autotuning vs the same scenes rendered
-    one after another with single-scene renderers."""
-    import numpy as np
+def _pcg(v: int) -> int:
+    state = (v * 747796405 + 2891336453) & 0xFFFFFFFF
+    word = (((state >> ((state >> 28) + 4)) ^ state) * 277803737) & 0xFFFFFFFF
+    return ((word >> 22) ^ word) & 0xFFFFFFFF
+
+
+def batch_seeds(n: int, base: int = 0) -> list[int]:
+    """Seeds of the seeded batch scene (PRESET_BATCH_RANDOM) whose triangle
+    budgets fall one into each of n equal strata of log [1e4, 2e6].  The
+    preset draws its budget from the seed as exp(log 1e4 + u log 200), u the
+    first draw of its PCG stream (pcg(pcg(seed * 747796405 + 2891336453)) /
+    2^32), so the stratified choice spans the configured range (up to the 2M
+    triangles of the largest scenes) instead of leaving its ends to chance."""
+    chosen: list[int | None] = [None] * n
+    seed = base
+    while any(c is None for c in chosen):
+        u = _pcg(_pcg((seed * 747796405 + 2891336453) & 0xFFFFFFFF)) / 4294967296.0
+        k = min(n - 1, int(u * n))
+        if chosen[k] is None:
+            chosen[k] = seed
+        seed += 1
+    return [int(c) for c in chosen]
+
+
+def batched_section(srt, ctx, stream, n_scenes=32, seed=12345):
+    """C3: n seeded scenes with triangle budgets stratified over log [1e4, 2e6],
+    square viewports of 256..1024, 1M..8M photons and 16..256 spp each
+    (log-uniform): the batched renderer (after autotuning) renders every scene
+    to its own spp count, scenes dropping out of the iterations as they finish;
+    against the same scenes rendered one after another with single-scene
+    renderers."""
     import torch
 
     rng = np.random.default_rng(seed)
-    scenes, ctls, sizes, params = [], [], [], []
-    for s in range(n_scenes):
+    seeds = batch_seeds(n_scenes)
+    scenes, ctls, sizes, params, spp = [], [], [], [], []
+    for s in seeds:
         b = srt.SceneBuilder()
         cam = b.add_preset(srt.PRESET_BATCH_RANDOM, s)
         scenes.append(b.build(ctx))
@@ -271,47 +297,61 @@ def batched_section(srt, ctx, stream, n_scenes=32, iters=3, seed=12345):
         sizes.append((r, r))
         ph = int(round(float(np.exp(rng.uniform(np.log(1e6), np.log(8e6))))))
         params.append(srt.default_params(photons_per_frame=ph, seed=s))
+        spp.append(int(round(float(np.exp(rng.uniform(np.log(16), np.log(256)))))))
     tris = [sc.info()["triangles"] for sc in scenes]
-    paths = sum(w * h for w, h in sizes)
-    photons = sum(p.photons_per_frame for p in params)
+    paths = sum(w * h * k for (w, h), k in zip(sizes, spp))
+    photons = sum(p.photons_per_frame * k for p, k in zip(params, spp))
+    iters = max(spp)
 
     def cams(f):
         return [c.build_uniform(w / h, f) for c, (w, h) in zip(ctls, sizes)]
 
-    def timed(fn, k):
+    def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        for f in range(k):
-            fn(f)
+        fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / k
+        return e0.elapsed_time(e1)
 
     singles = [srt.Renderer(ctx, sc, w, h, p) for sc, (w, h), p in zip(scenes, sizes, params)]
+    for i, r in enumerate(singles):  # warm-up: graph capture
+        r.render(ctls[i].build_uniform(sizes[i][0] / sizes[i][1], 0))
 
-    def seq(f):
-        cs = cams(f)
+    def seq():
         for i, r in enumerate(singles):
-            r.render(cs[i])
+            w, h = sizes[i]
+            for f in range(spp[i]):
+                r.render(ctls[i].build_uniform(w / h, f))
 
-    seq(0)
-    ms_seq = timed(lambda f: seq(f + 1), iters)
+    ms_seq = timed(seq)
     for r in singles:
         r.close()
     batch = srt.Batch(ctx, scenes, sizes, params)
     tune = batch.autotune(cams(0), iterations=1)
     batch.render(cams(0))
-    ms_batch = timed(lambda f: batch.render(cams(f + 1)), iters)
+    for k in range(1, 8):  # warm-up of the active sets near the end
+        batch.render(cams(0), active=[k * 32 <= x for x in spp])
+    for r in batch.renderers:
+        r.reset_accumulation()
+
+    def run():
+        for f in range(iters):
+            batch.render(cams(f), active=[f < x for x in spp])
+
+    ms_batch = timed(run)
+    frames = [r.stats()["frames"] for r in batch.renderers]
     batch.close()
     for sc in scenes:
         sc.close()
-    return {"workload": (f"C3: {n_scenes} seeded scenes, {min(tris)}..{max(tris)} triangles, viewports "
-                         f"256^2..1024^2, {paths} paths and {photons} photons per iteration, depth 12"),
-            "iterations": iters, "ms_per_iteration": round(ms_batch, 3),
+    return {"workload": (f"C3: {n_scenes} seeded scenes (budgets stratified over log [1e4, 2e6]), "
+                         f"{min(tris)}..{max(tris)} triangles, viewports 256^2..1024^2, {min(spp)}..{max(spp)} spp "
+                         f"per scene ({sum(spp)} scene-frames), {paths} paths and {photons} photons in all, depth 12"),
+            "iterations": iters, "ms_total": round(ms_batch, 2),
             "mpaths_per_s": round(paths / ms_batch / 1e3, 2), "mphotons_per_s": round(photons / ms_batch / 1e3, 2),
-            "sequential_ms_per_iteration": round(ms_seq, 3), "speedup_vs_sequential": round(ms_seq / ms_batch, 3),
-            "tuning": tune}
+            "sequential_ms_total": round(ms_seq, 2), "speedup_vs_sequential": round(ms_seq / ms_batch, 3),
+            "frames_rendered_match_spp": frames[: len(spp)] == spp, "tuning": tune}
 
 
 def guided_section(seconds=3.0, ref_spp=4096):
