@@ -220,6 +220,7 @@ SIGNATURES = {
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_mixture_tc": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_renderer_guide_set_steps": (_I, [_P, _U32]),
+    "srt_renderer_guide_set_bounces": (_I, [_P, _U32]),
     "srt_renderer_guide_get_state": (_I, [_P, _P, _P, _P, _P]),
     "srt_renderer_guide_set_state": (_I, [_P, _P, _P, _P, _U32]),
     "srt_write_accum_f64": (_I, [_P, _P]),
@@ -619,6 +620,10 @@ class Renderer:
     def set_guide_steps(self, steps: int) -> None:
         """Adam steps per frame, each on a consecutive 1/steps of the frame's training records."""
         _check(lib().srt_renderer_guide_set_steps(self.h, steps), self.ctx.h)
+
+    def set_guide_bounces(self, bounces: int) -> None:
+        """Guide the Lambert continuations of bounces < `bounces` only (later ones sample the cosine lobe)."""
+        _check(lib().srt_renderer_guide_set_bounces(self.h, bounces), self.ctx.h)
 
     def configure_guide(self, lr: float | None = None, batch: int | None = None) -> None:
         """Adam learning rate and training samples recorded per frame."""

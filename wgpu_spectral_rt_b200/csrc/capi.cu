@@ -941,6 +941,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
         CUDA_TRY(c, guide_upload(r->guide, w.data(), nullptr, nullptr, 0));
         r->guide.train = (p.flags & SRT_FLAG_GUIDE_FROZEN) ? 0 : 1;
         a.guiding = 1;
+        a.guide_bounces = MAX_BOUNCES + 1;  // every bounce
         a.guide = r->guide;
     }
     size_t n_events = 5 + 3 * (size_t)p.max_depth;
@@ -1457,6 +1458,21 @@ extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t ste
     r->args.guide = r->guide;
     r->args_gen += 1;
     if (r->graph) {  // the step count shapes the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces) {
+    if (!r || bounces < 1) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
+    r->args_gen += 1;
+    if (r->graph) {  // the guided bounces shape the captured frame
         cudaGraphExecDestroy(r->graph);
         r->graph = nullptr;
     }

@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(Fra
                         shadow = true;
                     }
                     a.pb.rad[id] = rad;
-                    if (GUIDE && bounce + 1u < a.max_depth) {
+                    if (GUIDE && bounce + 1u < a.max_depth && bounce < a.guide_bounces) {
                         guided = true;
                         g_p = f4(hp.x, hp.y, hp.z, wl.x);
                         g_n = f4(ffn.x, ffn.y, ffn.z, 0.f);
@@ -686,7 +686,8 @@ int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stag
         if (a.guiding) k_shade<true><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         else k_shade<false><<<grid, TRACE_BLOCK, 0, st>>>(a, bounce);
         ++launches;
-        if (a.guiding && stage != 4 && bounce + 1 < a.max_depth) launches += launch_guide_infer(a, bounce, st);
+        if (a.guiding && stage != 4 && bounce + 1 < a.max_depth && bounce < a.guide_bounces)
+            launches += launch_guide_infer(a, bounce, st);
         if (a.ray_sort && bounce + 1 < a.max_depth) {
             // 4 passes: the sorted queue lands back in the queue buffer
             uint32_t *sk, *sv;

@@ -99,6 +99,7 @@ struct FrameArgs {
     int sm_count;  // persistent traversal grid = sm_count * blocks per SM
     uint32_t seed; // added to the per-frame seeds of camera paths and photons (0: reference streams)
     int guiding;   // Lambert continuations sampled by the guide (k_guide_infer)
+    uint32_t guide_bounces;  // guided Lambert vertices: bounces < guide_bounces (later ones sample the cosine)
     GuideArgs guide;
 };
 

@@ -94,7 +94,13 @@ def _time_to_reach(curve, target):
 
 
 def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16, photons=1 << 20, ref_spp=65536,
-          seconds=20.0, lr=None, batch=None):
+          seconds=20.0, lr=None, batch=None, guide_bounces=None):
+    """Runs the study.  The reference is rendered as two halves on decorrelated
+    streams; their difference estimates the reference's own noise, which every
+    measured relMSE contains as a constant floor (E (x - ref)^2 = E (x - mu)^2
+    + Var ref for independent x and ref).  The time fraction is reported on
+    the raw curves and on the curves with that floor subtracted
+    ("time_fraction_ref_noise_subtracted"), which a short reference needs."""
     ctx = srt.Context(0)
     b = srt.SceneBuilder()
     cam = b.add_preset(preset)
@@ -106,13 +112,19 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
            "batch": batch if batch else 65536, "seconds": seconds}
 
     t0 = time.perf_counter()
-    ref_r = _renderer(ctx, scene, width, height, 0, max_depth, photons, REF_SEED)
-    for f0 in range(0, ref_spp, 256):
-        _render(ctx, ref_r, ctl, aspect, f0, min(256, ref_spp - f0))
-    ref = _mean_rgb(ref_r)
-    ref_r.close()
-    out["reference"] = {"frames": ref_spp, "seconds": round(time.perf_counter() - t0, 2),
-                        "accumulation": "fp64", "seed": REF_SEED}
+    halves = []
+    for k in range(2):
+        ref_r = _renderer(ctx, scene, width, height, 0, max_depth, photons, REF_SEED + k)
+        n = ref_spp // 2
+        for f0 in range(0, n, 256):
+            _render(ctx, ref_r, ctl, aspect, f0, min(256, n - f0))
+        halves.append(_mean_rgb(ref_r))
+        ref_r.close()
+    ref = 0.5 * (halves[0] + halves[1])
+    # Var(A - B) = 4 Var(ref) for halves A, B of the reference: its noise floor
+    floor = float(np.mean((halves[0] - halves[1]) ** 2 / (ref ** 2 + 0.01))) / 4.0
+    out["reference"] = {"frames": 2 * (ref_spp // 2), "seconds": round(time.perf_counter() - t0, 2),
+                        "accumulation": "fp64", "seed": REF_SEED, "noise_floor_relmse": floor}
 
     for name, flags in (("plain", 0), ("guided", srt.FLAG_GUIDING)):
         # warm-up (library load, graph capture) on a throwaway renderer
@@ -122,6 +134,8 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
         r = _renderer(ctx, scene, width, height, flags, max_depth, photons)
         if flags:
             r.configure_guide(lr, batch)
+            if guide_bounces:
+                r.set_guide_bounces(guide_bounces)
         frames, el, curve = _arm(ctx, r, ctl, aspect, seconds, ref)
         out[name] = {"frames": frames, "seconds": round(el, 3), "ms_per_frame": round(1e3 * el / frames, 4),
                      "relmse": curve[-1][2], "curve": curve}
@@ -133,6 +147,13 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
     out["guided_time_to_plain_relmse"] = t_g
     out["time_fraction"] = (t_g / out["plain"]["seconds"]) if t_g is not None else None
     out["relmse_ratio_plain_over_guided"] = target / max(out["guided"]["relmse"], 1e-30)
+    # the same with the reference's noise floor taken out of both curves
+    sub = [(t, f, e - floor) for t, f, e in out["guided"]["curve"]]
+    t_s = _time_to_reach(sub, target - floor) if target > floor else None
+    out["time_fraction_ref_noise_subtracted"] = (t_s / out["plain"]["seconds"]) if t_s is not None else None
+    out["relmse_ratio_ref_noise_subtracted"] = ((target - floor) / max(out["guided"]["relmse"] - floor, 1e-30)
+                                                if target > floor else None)
+    out["guide_bounces"] = guide_bounces
     scene.close()
     ctx.close()
     return out
@@ -149,9 +170,10 @@ def main():
     ap.add_argument("--seconds", type=float, default=20.0)
     ap.add_argument("--lr", type=float, default=None)
     ap.add_argument("--batch", type=int, default=None, help="training samples per frame")
+    ap.add_argument("--guide-bounces", type=int, default=None, help="guide bounces < N only (default all)")
     a = ap.parse_args()
     print(json.dumps(study(a.preset, a.width, a.height, a.max_depth, a.photons, a.ref_spp, a.seconds, a.lr,
-                           a.batch)))
+                           a.batch, a.guide_bounces)))
 
 
 if __name__ == "__main__":
