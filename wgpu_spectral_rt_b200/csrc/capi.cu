@@ -642,6 +642,12 @@ struct srt_renderer {
     cudaStream_t cap_stream = nullptr;
     cudaStream_t side_stream = nullptr;  // the second branch of an overlapped frame
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // guiding: the previous frame's training steps run on a third branch of
+    // the next overlapped frame (beside its photon pass and first closest
+    // hits); train_pending = the last frame's steps have not run yet
+    cudaStream_t train_stream = nullptr;
+    cudaEvent_t tfork_ev = nullptr, tjoin_ev = nullptr;
+    bool train_pending = false;
     cudaGraphExec_t graph = nullptr;
     int launches_per_frame = 0;
     uint32_t frame_count = 0;
@@ -661,6 +667,9 @@ struct srt_renderer {
         if (side_stream) cudaStreamDestroy(side_stream);
         if (fork_ev) cudaEventDestroy(fork_ev);
         if (join_ev) cudaEventDestroy(join_ev);
+        if (train_stream) cudaStreamDestroy(train_stream);
+        if (tfork_ev) cudaEventDestroy(tfork_ev);
+        if (tjoin_ev) cudaEventDestroy(tjoin_ev);
         for (auto& e : ring_ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : ev) cudaEventDestroy(e);
@@ -737,11 +746,23 @@ struct srt_renderer {
             cudaStreamWaitEvent(st, join_ev, 0);
         };
         cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
+        const bool deferred = args.guiding != 0;
+        if (deferred) {
+            // the previous frame's Adam steps and frame-end bookkeeping: they
+            // read that frame's training records and write the network, which
+            // nothing before this frame's shading touches (none on the first
+            // frame: no records)
+            cudaEventRecord(tfork_ev, st);
+            cudaStreamWaitEvent(train_stream, tfork_ev, 0);
+            n += launch_guide_steps(args, train_stream);
+            cudaEventRecord(tjoin_ev, train_stream);
+        }
         fork();
         n += launch_raygen(args, s2);
         n += launch_bounce(args, 0, s2, 1);
         if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
         join();
+        if (deferred) cudaStreamWaitEvent(st, tjoin_ev, 0);
         for (uint32_t b = 0; b < p.max_depth; ++b) {
             n += launch_bounce(args, b, st, 2);
             if (b + 1 < p.max_depth) {
@@ -755,8 +776,18 @@ struct srt_renderer {
         }
         n += launch_finalize(args, st);
         n += launch_frame_stats(args, st);
-        if (args.guiding) n += launch_guide_train(args, st);
+        // the training weights read this frame's path radiance: before the
+        // next frame's camera rays reset it; the steps run in the next frame
+        if (deferred) n += launch_guide_targets(args, st);
         return n;
+    }
+
+    // Runs training steps that a frame left to the next one (before the
+    // guide's state is read or changed from the host).
+    int flush_training(cudaStream_t st) {
+        if (!train_pending) return 0;
+        train_pending = false;
+        return launch_guide_steps(args, st);
     }
 
     // The same frame in parts for the batched renderer, which traces the
@@ -951,6 +982,9 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     CUDA_TRY(c, cudaStreamCreateWithFlags(&r->side_stream, cudaStreamNonBlocking));
     CUDA_TRY(c, cudaEventCreateWithFlags(&r->fork_ev, cudaEventDisableTiming));
     CUDA_TRY(c, cudaEventCreateWithFlags(&r->join_ev, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&r->train_stream, cudaStreamNonBlocking));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&r->tfork_ev, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&r->tjoin_ev, cudaEventDisableTiming));
     if (env_fault("launch")) return fail(c, SRT_ERR_CUDA, "injected launch failure");
     ctx_retain(c);
     *out = r.release();
@@ -1017,6 +1051,8 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
             r->ms[7] += el(3 + 3 * r->p.max_depth, 4 + 3 * r->p.max_depth);
         }
     }
+    // an overlapped guided frame leaves its training steps to the next frame
+    r->train_pending = r->args.guiding && !timed && SRT_FRAME_OVERLAP;
     r->trace_launches += r->p.max_depth;
     r->frames += 1;
     r->photons_emitted += r->p.photons_per_frame;
@@ -1362,10 +1398,23 @@ extern "C" srt_status srt_guide_default_weights(uint64_t seed, float* out, uint3
     return SRT_OK;
 }
 
+namespace {
+// Pending training steps of the last frame run before the host reads or
+// changes the guide's state, so it sees every frame's step.
+srt_status guide_flush(srt_renderer* r) {
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    r->launches += (uint64_t)r->flush_training(c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    return SRT_OK;
+}
+}  // namespace
+
 extern "C" srt_status srt_renderer_guide_get_weights(srt_renderer* r, float* out, uint32_t n) {
     if (!r || !out || n != (uint32_t)G_NPARAMS) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaMemcpyAsync(out, r->guide.net.master, n * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1376,6 +1425,7 @@ extern "C" srt_status srt_renderer_guide_set_weights(srt_renderer* r, const floa
     if (!r || !w || n != (uint32_t)G_NPARAMS) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     CUDA_TRY(c, guide_upload(r->guide, w, nullptr, nullptr, 0));
@@ -1395,6 +1445,7 @@ extern "C" srt_status srt_renderer_guide_get_state(srt_renderer* r, float* param
     if (!r || !params || !adam_m || !adam_v || !adam_step) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     GuideCounters gc;
     const size_t bytes = (size_t)G_NPARAMS * 4;
@@ -1412,6 +1463,7 @@ extern "C" srt_status srt_renderer_guide_set_state(srt_renderer* r, const float*
     if (!r || !params || !adam_m || !adam_v) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     CUDA_TRY(c, guide_upload(r->guide, params, adam_m, adam_v, adam_step));
@@ -1422,6 +1474,7 @@ extern "C" srt_status srt_renderer_guide_info(srt_renderer* r, uint32_t* adam_st
     if (!r) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     GuideCounters gc;
     CUDA_TRY(c, cudaMemcpyAsync(&gc, r->guide.gc, sizeof gc, cudaMemcpyDeviceToHost, c->stream));
@@ -1435,6 +1488,7 @@ extern "C" srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, ui
     if (!r || !(lr < 1.0f) || batch > G_REC_CAP) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     if (lr >= 0.0f) r->guide.lr = lr;
@@ -1452,6 +1506,7 @@ extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t ste
     if (!r || steps < 1 || steps > 16) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     r->guide.steps = steps;
@@ -1468,6 +1523,7 @@ extern "C" srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t b
     if (!r || bounces < 1) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
@@ -1527,6 +1583,7 @@ extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind
     if (!r || (kind != SRT_GUIDE_INFER_MMA_SYNC && kind != SRT_GUIDE_INFER_TCGEN05)) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     r->guide.tc = kind == SRT_GUIDE_INFER_TCGEN05 ? 1 : 0;

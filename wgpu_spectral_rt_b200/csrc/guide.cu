@@ -1452,13 +1452,20 @@ int launch_train_steps(const GuideArgs& g, int sm, int adam, cudaStream_t st) {
 }  // namespace
 
 int launch_guide_train(const FrameArgs& a, cudaStream_t st) {
+    return launch_guide_targets(a, st) + launch_guide_steps(a, st);
+}
+
+int launch_guide_targets(const FrameArgs& a, cudaStream_t st) {
+    if (!a.guide.train) return 0;
+    const int sm = a.sm_count > 0 ? a.sm_count : 148;
+    k_guide_targets<<<sm * 4, 256, 0, st>>>(a);
+    return 1;
+}
+
+int launch_guide_steps(const FrameArgs& a, cudaStream_t st) {
     const GuideArgs& g = a.guide;
-    int sm = a.sm_count > 0 ? a.sm_count : 148;
-    int n = 0;
-    if (g.train) {
-        k_guide_targets<<<sm * 4, 256, 0, st>>>(a);
-        n = 1 + launch_train_steps(g, sm, 1, st);
-    }
+    const int sm = a.sm_count > 0 ? a.sm_count : 148;
+    int n = g.train ? launch_train_steps(g, sm, 1, st) : 0;
     k_guide_frame_end<<<1, 32, 0, st>>>(g, g.train);
     return n + 1;
 }

@@ -111,6 +111,12 @@ struct FrameArgs;
 cudaError_t guide_configure();  // raises the dynamic shared-memory limits once per device
 int launch_guide_infer(const FrameArgs& a, uint32_t bounce, cudaStream_t st);
 int launch_guide_train(const FrameArgs& a, cudaStream_t st);
+// The two halves of launch_guide_train: the training weights of the frame's
+// records (reads the frame's path radiance; before the next frame's camera
+// rays), then the Adam steps and the frame-end bookkeeping (before the next
+// frame's shading).
+int launch_guide_targets(const FrameArgs& a, cudaStream_t st);
+int launch_guide_steps(const FrameArgs& a, cudaStream_t st);
 // Many renderers at once (device array of their frame arguments, the batched
 // renderer): the guided vertices of one bounce in one persistent tcgen05
 // launch (fetch: a zeroed chunk counter), and one training step of every
