@@ -351,7 +351,9 @@ def batched_section(srt, ctx, stream, n_scenes=32, seed=12345):
             "iterations": iters, "ms_total": round(ms_batch, 2),
             "mpaths_per_s": round(paths / ms_batch / 1e3, 2), "mphotons_per_s": round(photons / ms_batch / 1e3, 2),
             "sequential_ms_total": round(ms_seq, 2), "speedup_vs_sequential": round(ms_seq / ms_batch, 3),
-            "frames_rendered_match_spp": frames[: len(spp)] == spp, "tuning": tune}
+            "frames_rendered_match_spp": frames[: len(spp)] == spp, "tuning": tune,
+            "grid_cell": "0.02, fixed: the cell size changes the photon density estimate (the image), so it is not "
+                         "a speed knob of the compatible renderer"}
 
 
 def guided_section(seconds=3.0, ref_spp=4096):

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SRT_ABI_VERSION 3u
+#define SRT_ABI_VERSION 4u
 
 /* Status codes.  Replaces unwrap()/panic! and wgpu::SurfaceError
  * (src/app.rs:70-77, src/wgpu_ctx.rs:36-42). */
@@ -231,6 +231,11 @@ srt_status srt_ctx_set_bvh_builder(srt_ctx* ctx, int builder);
  * builder, the width changes speed, never results.  No reference
  * counterpart (the driver builds the reference's BLAS/TLAS). */
 srt_status srt_ctx_set_bvh_width(srt_ctx* ctx, uint32_t width);
+/* Rebuilds a scene's tree with `width` children per node (same builder).
+ * Waits for the device; renderers and batches using the scene pick up the
+ * new tree at their next frame (they capture their frame again). */
+srt_status srt_scene_rebuild_bvh(srt_scene* s, uint32_t width);
+srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width);
 
 /* ------------------------------------------------------------------------ */
 /* Scene API: SceneBuilder (src/scene/builder.rs:47-267).                     */
@@ -562,6 +567,8 @@ typedef struct srt_batch_tuning {
     uint32_t chunk;          /* rays a warp draws from the shared queue at once (32..1024, x32) */
     float ms_per_iteration;  /* autotune: time of one iteration with this choice */
     uint32_t candidates;     /* autotune: configurations timed */
+    uint32_t bvh_width;      /* autotune: children per node of the scenes' trees it kept (it times the
+                                other of 8 and 4 by rebuilding the trees; 0 = widths differ, not tuned) */
 } srt_batch_tuning;
 /* n <= 64 scenes; params: n entries (NULL: defaults); no STAGE_TIMING,
  * COUNT_VISITS or RAY_SORT flag in a batch. */

@@ -34,7 +34,7 @@ def test_every_declared_symbol_is_exported(srt):
 
 
 def test_abi_version_and_record_sizes(srt):
-    assert srt.lib().srt_abi_version() == 3
+    assert srt.lib().srt_abi_version() == 4
     assert srt.guide_param_count() == 23856
     assert C.sizeof(srt.CameraUniform) == 272 and C.sizeof(srt.Vertex) == 32 and C.sizeof(srt.Light) == 64
 

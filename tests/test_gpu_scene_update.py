@@ -167,3 +167,28 @@ def test_moved_scene_hits_match_the_oracle(srt, orc, ctx):
     _unused.close()
     moved.close()
     o.close()
+
+
+def test_tree_rebuild_mid_render_keeps_frames_bit_identical(srt, ctx):
+    """srt_scene_rebuild_bvh between frames (4 children per node, then 8
+    again): the renderer captures its frame again on the new tree and the
+    image equals that of a renderer whose scene was never rebuilt."""
+    b = srt.SceneBuilder()
+    cam = b.add_preset(srt.PRESET_CONFIG1)
+    s1, s2 = b.build(ctx), b.build(ctx)
+    w, h = 40, 32
+    p = srt.default_params(photons_per_frame=1 << 15)
+    r1, r2 = srt.Renderer(ctx, s1, w, h, p), srt.Renderer(ctx, s2, w, h, p)
+    ctl = srt.CameraController(*cam)
+    for f in range(6):
+        if f == 2:
+            s1.rebuild_bvh(4)
+            assert s1.info()["width"] == 4 and s1.info()["nodes"] > s2.info()["nodes"]
+        if f == 4:
+            s1.rebuild_bvh(8)
+        u = ctl.build_uniform(w / h, f)
+        r1.render(u)
+        r2.render(u)
+    np.testing.assert_array_equal(r1.read_accum(), r2.read_accum())
+    for x in (r1, r2, s1, s2):
+        x.close()

@@ -78,7 +78,7 @@ class Params(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_uint32), ("chunk", C.c_uint32), ("ms_per_iteration", C.c_float),
-                ("candidates", C.c_uint32)]
+                ("candidates", C.c_uint32), ("bvh_width", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -158,6 +158,8 @@ SIGNATURES = {
     "srt_scene_build": (_I, [_P, C.POINTER(SceneArrays), C.POINTER(_P)]),
     "srt_scene_destroy": (_I, [_P]),
     "srt_scene_info": (_I, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(_U32)]),
+    "srt_scene_rebuild_bvh": (_I, [_P, _U32]),
+    "srt_scene_bvh_width": (_I, [_P, C.POINTER(_U32)]),
     "srt_geometry_plane": (_I, [C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
     "srt_geometry_cube": (_I, [C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
     "srt_geometry_icosphere": (_I, [_U32, C.POINTER(Vertex), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)]),
@@ -410,9 +412,14 @@ class Scene:
         self.ctx, self.h = ctx, h
 
     def info(self) -> dict:
-        t, n, d = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        t, n, d, w = C.c_uint64(), C.c_uint64(), C.c_uint32(), C.c_uint32()
         _check(lib().srt_scene_info(self.h, C.byref(t), C.byref(n), C.byref(d)), self.ctx.h)
-        return {"triangles": t.value, "nodes": n.value, "depth": d.value}
+        _check(lib().srt_scene_bvh_width(self.h, C.byref(w)), self.ctx.h)
+        return {"triangles": t.value, "nodes": n.value, "depth": d.value, "width": w.value}
+
+    def rebuild_bvh(self, width: int) -> None:
+        """Rebuilds the tree with `width` children per node (renderers pick it up at their next frame)."""
+        _check(lib().srt_scene_rebuild_bvh(self.h, width), self.ctx.h)
 
     def trace(self, rays: np.ndarray, any_hit: bool = False) -> np.ndarray:
         """rays: float32 [n, 8] (origin, tmin, dir, tmax) -> hits structured (t, prim, u, v)."""

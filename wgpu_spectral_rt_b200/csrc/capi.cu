@@ -7,6 +7,7 @@
 // engine's screenshot readback (src/engine.rs:191-244).
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -318,6 +319,11 @@ struct srt_scene {
     uint8_t* moved = nullptr;
     float4* refit_aux = nullptr;
     uint32_t* refit_err = nullptr;
+    // tree rebuilds: renderers compare gen with the one they captured
+    uint32_t gen = 0;
+    int builder = BVH_BUILDER_SAH;
+    int width = 8;
+    uint32_t n_inst = 0;
     ~srt_scene() {
         cudaFree(light_insts);
         cudaFree(moved);
@@ -432,6 +438,9 @@ srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
     CUDA_TRY(c, upload(&s->fwd, fwd.data(), sizeof(InstFwd) * fwd.size(), sizeof(InstFwd) * fwd.size(), st));
     BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total,
                  c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH, c->bvh_width};
+    s->builder = bi.builder;
+    s->width = bi.width;
+    s->n_inst = a->n_instances;
     std::string msg;
     cudaError_t e = build_bvh8(bi, st, &s->bvh, &msg);
     if (e != cudaSuccess) return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, "BVH build: " + msg);
@@ -615,6 +624,55 @@ extern "C" srt_status srt_scene_info(const srt_scene* s, uint64_t* n_tris, uint6
     return SRT_OK;
 }
 
+extern "C" srt_status srt_scene_rebuild_bvh(srt_scene* s, uint32_t width) {
+    if (!s || width < 2 || width > 8) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    CUDA_TRY(c, cudaDeviceSynchronize());  // no frame of any renderer still reads the old tree
+    BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, s->n_inst, (uint32_t)s->n_tris, s->builder,
+                 (int)width};
+    BvhOutputs nb{};
+    std::string msg;
+    cudaError_t e = build_bvh8(bi, st, &nb, &msg);
+    if (e == cudaSuccess && nb.depth > (uint32_t)TRAV_STACK) {
+        e = cudaErrorInvalidValue;
+        msg = "BVH deeper than the traversal stack";
+    }
+    if (e != cudaSuccess) {
+        cudaFree(nb.nodes);
+        cudaFree(nb.tris);
+        cudaFree(nb.tri_inst);
+        return fail(c, e == cudaErrorMemoryAllocation ? SRT_ERR_OOM : SRT_ERR_CUDA, "BVH rebuild: " + msg);
+    }
+    cudaFree(s->bvh.nodes);
+    cudaFree(s->bvh.tris);
+    cudaFree(s->bvh.tri_inst);
+    s->bvh = nb;
+    // refit scratch is sized by the node count: allocated again on the next update
+    cudaFree(s->moved);
+    cudaFree(s->refit_aux);
+    cudaFree(s->refit_err);
+    s->moved = nullptr;
+    s->refit_aux = nullptr;
+    s->refit_err = nullptr;
+    s->width = (int)width;
+    DevScene& d = s->dev;
+    d.tri_inst = s->bvh.tri_inst;
+    d.nodes = s->bvh.nodes;
+    d.tris = s->bvh.tris;
+    d.n_nodes = s->bvh.n_nodes;
+    d.depth = s->bvh.depth;
+    s->gen += 1;
+    return SRT_OK;
+}
+
+extern "C" srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width) {
+    if (!s || !width) return SRT_ERR_INVALID_ARG;
+    *width = (uint32_t)s->width;
+    return SRT_OK;
+}
+
 // ====================================================================== renderer
 // Frames enqueue independent stages on two branches (srt_renderer::record_overlapped).
 #ifndef SRT_FRAME_OVERLAP
@@ -624,6 +682,19 @@ extern "C" srt_status srt_scene_info(const srt_scene* s, uint64_t* n_tris, uint6
 struct srt_renderer {
     srt_ctx* ctx = nullptr;
     srt_scene* scene = nullptr;
+    uint32_t scene_gen = 0;  // scene->gen when args.scene was taken
+
+    // After a tree rebuild of the scene: new tree pointers, a new capture.
+    void refresh_scene() {
+        if (scene_gen == scene->gen) return;
+        scene_gen = scene->gen;
+        args.scene = scene->dev;
+        args_gen += 1;
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+    }
     uint32_t w = 0, h = 0;
     srt_params p{};
     FrameArgs args{};
@@ -935,6 +1006,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     }
     FrameArgs& a = r->args;
     a.scene = s->dev;
+    r->scene_gen = s->gen;
     a.cam = r->cam_dev;
     a.width = w;
     a.height = h;
@@ -1005,6 +1077,7 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
     if (!r || !cam || r->batch_owned) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     cudaSetDevice(c->device);
+    r->refresh_scene();
     cudaStream_t st = c->stream;
     int slot = r->ring_i++ & 3;
     CUDA_TRY(c, cudaEventSynchronize(r->ring_ev[slot]));
@@ -1799,7 +1872,7 @@ struct srt_batch {
     cudaGraphExec_t graph = nullptr;
     std::vector<uint8_t> graph_active;
     int graph_launches = 0;
-    srt_batch_tuning tune{8, 32, 0.0f, 0};
+    srt_batch_tuning tune{8, 32, 0.0f, 0, 8};
     uint32_t max_depth = 0;
     bool small_stack = true;
 
@@ -1838,6 +1911,10 @@ struct srt_batch {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
         }
+        // the deepest tree sets the traversal stack (trees may have been rebuilt)
+        small_stack = true;
+        for (srt_renderer* x : r)
+            if (x->args.scene.depth > (uint32_t)TRAV_STACK_SMALL) small_stack = false;
         std::vector<int> act;
         for (size_t i = 0; i < r.size(); ++i)
             if (active[i]) act.push_back((int)i);
@@ -1943,6 +2020,7 @@ struct srt_batch {
         bool any = false;
         for (uint8_t a : active) any = any || a;
         if (!any) return SRT_OK;
+        for (srt_renderer* x : r) x->refresh_scene();  // trees rebuilt since the capture
         bool stale = graph_gen.size() != n;
         for (size_t i = 0; i < n && !stale; ++i) stale = graph_gen[i] != r[i]->args_gen;
         if (!graph || active != graph_active || stale) {
@@ -2063,7 +2141,7 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
     cudaEvent_t e0, e1;
     CUDA_TRY(c, cudaEventCreate(&e0));
     CUDA_TRY(c, cudaEventCreate(&e1));
-    srt_batch_tuning best{8, 32, 3.4e38f, 0};
+    srt_batch_tuning best{8, 32, 3.4e38f, 0, 0};
     srt_status st = SRT_OK;
     // guided scenes train during the tuning frames: their networks and Adam
     // state are saved here and put back afterwards
@@ -2079,7 +2157,7 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
         }
     for (uint32_t bp : bps)
         for (uint32_t ch : chunks) {
-            srt_batch_tuning t{bp, ch, 0.0f, 0};
+            srt_batch_tuning t{bp, ch, 0.0f, 0, 0};
             srt_batch_set_tuning(b, &t);
             st = b->render(cams, nullptr);  // capture + warm-up
             if (st != SRT_OK) break;
@@ -2098,6 +2176,49 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
                 best.ms_per_iteration = ms;
             }
         }
+    // BVH node width: the scenes' trees rebuilt with 4 children per node and
+    // timed with the best traversal setting; kept if faster, else rebuilt at
+    // their width.  The tree changes speed, never results.
+    best.bvh_width = 0;
+    {
+        std::vector<srt_scene*> sc;
+        for (srt_renderer* x : b->r)
+            if (std::find(sc.begin(), sc.end(), x->scene) == sc.end()) sc.push_back(x->scene);
+        uint32_t w0 = (uint32_t)sc[0]->width;
+        bool uniform = true;
+        for (srt_scene* x : sc) uniform = uniform && (uint32_t)x->width == w0;
+        best.bvh_width = uniform ? w0 : 0;
+        const uint32_t alt = w0 == 8u ? 4u : 8u;
+        if (st == SRT_OK && uniform) {
+            for (srt_scene* x : sc)
+                if (st == SRT_OK) st = srt_scene_rebuild_bvh(x, alt);
+            srt_batch_tuning t{best.blocks_per_sm, best.chunk, 0.0f, 0, 0};
+            srt_batch_set_tuning(b, &t);
+            if (st == SRT_OK) st = b->render(cams, nullptr);
+            float ms = 3.4e38f;
+            if (st == SRT_OK) {
+                cudaEventRecord(e0, c->stream);
+                for (uint32_t i = 0; i < iterations && st == SRT_OK; ++i) st = b->render(cams, nullptr);
+                cudaEventRecord(e1, c->stream);
+                if (st == SRT_OK) {
+                    cudaEventSynchronize(e1);
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms /= (float)iterations;
+                }
+            }
+            best.candidates += 1;
+            if (st == SRT_OK && ms < best.ms_per_iteration) {
+                best.ms_per_iteration = ms;
+                best.bvh_width = alt;
+            } else {
+                for (srt_scene* x : sc)
+                    if ((uint32_t)x->width != w0) {
+                        srt_status s2 = srt_scene_rebuild_bvh(x, w0);
+                        if (st == SRT_OK) st = s2;
+                    }
+            }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaError_t restored = cudaSuccess;
@@ -2113,6 +2234,7 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
     srt_batch_set_tuning(b, &best);
     b->tune.ms_per_iteration = best.ms_per_iteration;
     b->tune.candidates = n_cand;
+    b->tune.bvh_width = best.bvh_width;
     // the tuning frames are not part of any image
     for (srt_renderer* x : b->r) {
         srt_status s = srt_reset_accumulation(x);
