@@ -482,6 +482,12 @@ SRT_DEV float2 fma2(float2 a, float2 b, float2 c) {
 #endif
 }
 
+// Child bookkeeping of a node visit in one pass after the slab tests
+// (SRT_TRAV_LEAN) instead of per child.
+#ifndef SRT_TRAV_LEAN
+#define SRT_TRAV_LEAN 0
+#endif
+
 struct TravCounters {
     unsigned long long* nodes;
     unsigned long long* tris;
@@ -522,6 +528,41 @@ SRT_DEV void node_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, uint4 w4, flo
     uint32_t nz0 = (oct & 4u) ? w4.z : w3.x, nz1 = (oct & 4u) ? w4.w : w3.y;
     uint32_t fz0 = (oct & 4u) ? w3.x : w4.z, fz1 = (oct & 4u) ? w3.y : w4.w;
     const float robust = 1.0000004f;
+#if SRT_TRAV_LEAN
+    // the child loop only collects which slots are hit; the octant order of
+    // the internal children and the leaves' triangle bits follow once per node
+    uint32_t hitmask = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t k = (uint32_t)(i & 3);
+        const uint32_t m = byte_of(i < 4 ? w1.z : w1.w, k);
+        const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
+                               make_float2(ax, ax), make_float2(bx, bx));
+        const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
+                               make_float2(ay, ay), make_float2(by, by));
+        const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
+                               make_float2(az, az), make_float2(bz, bz));
+        const float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, tmin));
+        const float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, tbest)) * robust;
+        hitmask |= (m != 0u && tn <= tf) ? (1u << i) : 0u;
+    }
+    // internal children: slot i -> bit i ^ (oct ^ 7) (three conditional swaps)
+    uint32_t ib = hitmask & imask;
+    const uint32_t x = oct ^ 7u;
+    ib = (x & 1u) ? (((ib & 0x55u) << 1) | ((ib >> 1) & 0x55u)) : ib;
+    ib = (x & 2u) ? (((ib & 0x33u) << 2) | ((ib >> 2) & 0x33u)) : ib;
+    ib = (x & 4u) ? (((ib & 0x0Fu) << 4) | ((ib >> 4) & 0x0Fu)) : ib;
+    // leaves: their triangles' bits
+    uint32_t lb = hitmask & ~imask, tris = 0u;
+    while (lb != 0u) {
+        const uint32_t i = (uint32_t)(__ffs(lb) - 1);
+        lb &= lb - 1u;
+        const uint32_t m = ((i < 4u ? w1.z : w1.w) >> (8u * (i & 3u))) & 0xFFu;
+        tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+    }
+    g = make_uint2(w1.x, (ib << 24) | imask);
+    tg = make_uint2(w1.y, tris);
+#else
     uint32_t hits = 0u;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -543,6 +584,7 @@ SRT_DEV void node_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, uint4 w4, flo
     }
     g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
     tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+#endif
 }
 
 // Stack-based traversal of the compressed BVH8.  A node group holds the
@@ -566,7 +608,6 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
                      1.0f / (fabsf(ray.d.y) > eps ? ray.d.y : copysignf(eps, ray.d.y)),
                      1.0f / (fabsf(ray.d.z) > eps ? ray.d.z : copysignf(eps, ray.d.z)));
     uint32_t oct = (ray.d.x < 0.f ? 1u : 0u) | (ray.d.y < 0.f ? 2u : 0u) | (ray.d.z < 0.f ? 4u : 0u);
-    const float robust = 1.0000004f;  // conservative far-plane scaling of the slab test
     float tbest = ray.tmax;
     uint32_t best = MISS;
     float bu = 0.f, bv = 0.f;
@@ -672,46 +713,7 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
         const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
         uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
         if (COUNT) ++n_nodes;
-        float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-        float sx = __uint_as_float((w0.w & 0xFFu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
-              sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-        uint32_t imask = w0.w >> 24;
-        float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;
-        float bx = unbias(ax, (px - ray.o.x) * idir.x), by = unbias(ay, (py - ray.o.y) * idir.y),
-              bz = unbias(az, (pz - ray.o.z) * idir.z);
-        // near/far quantised planes per axis by ray octant
-        uint32_t lx0 = w2.x, lx1 = w2.y, ly0 = w2.z, ly1 = w2.w, lz0 = w3.x, lz1 = w3.y;
-        uint32_t hx0 = w3.z, hx1 = w3.w, hy0 = w4.x, hy1 = w4.y, hz0 = w4.z, hz1 = w4.w;
-        uint32_t nx0 = (oct & 1u) ? hx0 : lx0, nx1 = (oct & 1u) ? hx1 : lx1;
-        uint32_t fx0 = (oct & 1u) ? lx0 : hx0, fx1 = (oct & 1u) ? lx1 : hx1;
-        uint32_t ny0 = (oct & 2u) ? hy0 : ly0, ny1 = (oct & 2u) ? hy1 : ly1;
-        uint32_t fy0 = (oct & 2u) ? ly0 : hy0, fy1 = (oct & 2u) ? ly1 : hy1;
-        uint32_t nz0 = (oct & 4u) ? hz0 : lz0, nz1 = (oct & 4u) ? hz1 : lz1;
-        uint32_t fz0 = (oct & 4u) ? lz0 : hz0, fz1 = (oct & 4u) ? lz1 : hz1;
-        uint32_t meta0 = w1.z, meta1 = w1.w;
-        uint32_t hits = 0u;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const uint32_t k = (uint32_t)(i & 3);
-            uint32_t m = byte_of(i < 4 ? meta0 : meta1, k);
-            const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
-                                   make_float2(ax, ax), make_float2(bx, bx));
-            const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
-                                   make_float2(ay, ay), make_float2(by, by));
-            const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
-                                   make_float2(az, az), make_float2(bz, bz));
-            float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, ray.tmin));
-            float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, tbest)) * robust;
-            if (m != 0u && tn <= tf) {
-                uint32_t c = m >> 5;
-                if (c == 7u)
-                    hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
-                else
-                    hits |= ((1u << c) - 1u) << (m & 31u);
-            }
-        }
-        g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
-        tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+        node_children(w0, w1, w2, w3, w4, ray.o, idir, oct, ray.tmin, tbest, g, tg);
     }
     if (COUNT) {
         atomicAdd(cnt.nodes, (unsigned long long)n_nodes);
@@ -888,41 +890,7 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
     const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
     uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
     ++n_nodes;
-    float sxs = __uint_as_float((w0.w & 0xFFu) << 23), sys = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
-          szs = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
-    uint32_t imask = w0.w >> 24;
-    float ax = sxs * T.idir.x, ay = sys * T.idir.y, az = szs * T.idir.z;
-    float bx = unbias(ax, (__uint_as_float(w0.x) - T.o.x) * T.idir.x),
-          by = unbias(ay, (__uint_as_float(w0.y) - T.o.y) * T.idir.y),
-          bz = unbias(az, (__uint_as_float(w0.z) - T.o.z) * T.idir.z);
-    uint32_t nx0 = (oct & 1u) ? w3.z : w2.x, nx1 = (oct & 1u) ? w3.w : w2.y;
-    uint32_t fx0 = (oct & 1u) ? w2.x : w3.z, fx1 = (oct & 1u) ? w2.y : w3.w;
-    uint32_t ny0 = (oct & 2u) ? w4.x : w2.z, ny1 = (oct & 2u) ? w4.y : w2.w;
-    uint32_t fy0 = (oct & 2u) ? w2.z : w4.x, fy1 = (oct & 2u) ? w2.w : w4.y;
-    uint32_t nz0 = (oct & 4u) ? w4.z : w3.x, nz1 = (oct & 4u) ? w4.w : w3.y;
-    uint32_t fz0 = (oct & 4u) ? w3.x : w4.z, fz1 = (oct & 4u) ? w3.y : w4.w;
-    const float robust = 1.0000004f;
-    uint32_t hits = 0u;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const uint32_t k = (uint32_t)(i & 3);
-        uint32_t m = byte_of(i < 4 ? w1.z : w1.w, k);
-        const float2 tx = fma2(make_float2(qbyte(i < 4 ? nx0 : nx1, k), qbyte(i < 4 ? fx0 : fx1, k)),
-                               make_float2(ax, ax), make_float2(bx, bx));
-        const float2 ty = fma2(make_float2(qbyte(i < 4 ? ny0 : ny1, k), qbyte(i < 4 ? fy0 : fy1, k)),
-                               make_float2(ay, ay), make_float2(by, by));
-        const float2 tz = fma2(make_float2(qbyte(i < 4 ? nz0 : nz1, k), qbyte(i < 4 ? fz0 : fz1, k)),
-                               make_float2(az, az), make_float2(bz, bz));
-        float tn = fmaxf(fmaxf(tx.x, ty.x), fmaxf(tz.x, T.tmin));
-        float tf = fminf(fminf(tx.y, ty.y), fminf(tz.y, T.tbest)) * robust;
-        if (m != 0u && tn <= tf) {
-            uint32_t c = m >> 5;
-            if (c == 7u) hits |= 1u << (24 + ((uint32_t)i ^ (oct ^ 7u)));
-            else hits |= ((1u << c) - 1u) << (m & 31u);
-        }
-    }
-    T.g = make_uint2(w1.x, (hits & 0xFF000000u) | imask);
-    T.tg = make_uint2(w1.y, hits & 0x00FFFFFFu);
+    node_children(w0, w1, w2, w3, w4, T.o, T.idir, oct, T.tmin, T.tbest, T.g, T.tg);
     return false;
 }
 
