@@ -85,7 +85,7 @@ def lib() -> C.CDLL:
         L.orc_photon_gather.argtypes = [P, U32, P, U32, U32, P, P]
         L.orc_render_frame.argtypes = [P, P, U32, U32, P, U32, U32, P, P, P, P, C.c_int]
         L.orc_render_frame_photons.argtypes = [P, P, U32, U32, P, P, U32, U32, U32, P, P, P, P, C.c_int]
-        L.orc_tri_probe.argtypes = [P, P, P, U32, P, P]
+        L.orc_tri_probe.argtypes = [P, P, P, U32, P, P, P]
         L.orc_max_threads.restype = C.c_int
         L.orc_preset_create.restype = P
         L.orc_preset_create.argtypes = [C.c_int, U32]
@@ -174,15 +174,17 @@ class OracleScene:
         c = lib().orc_photon_emit(self.h, n_photons, frame, max_bounces, _p(out), _p(em), threads)
         return out[:c].copy(), em[:c].copy()
 
-    def tri_probe(self, rays: np.ndarray, prims: np.ndarray):
+    def tri_probe(self, rays: np.ndarray, prims: np.ndarray, with_cos: bool = False):
         """FP64 (t where each ray's line meets the plane of triangle prims[i],
-        distance from that point to the triangle's boundary: > 0 inside)."""
+        distance from that point to the triangle's boundary: > 0 inside[, |cos|
+        of the angle between the ray and the plane's normal])."""
         r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         pr = np.ascontiguousarray(prims, np.uint32)
         t = np.zeros(len(r), np.float64)
         e = np.zeros(len(r), np.float64)
-        lib().orc_tri_probe(self.h, _p(r), _p(pr), len(r), _p(t), _p(e))
-        return t, e
+        c = np.zeros(len(r), np.float64)
+        lib().orc_tri_probe(self.h, _p(r), _p(pr), len(r), _p(t), _p(e), _p(c))
+        return (t, e, c) if with_cos else (t, e)
 
     def render_frame(self, cam, w: int, h: int, params, accum: np.ndarray | None = None, row_stride=1, row_phase=0,
                      want_ldr=True, want_radiance=False, threads: int = 0, photons: np.ndarray | None = None):

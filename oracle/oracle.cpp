@@ -1106,15 +1106,18 @@ void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit,
 // point to the triangle's boundary (the nearest of its three edge segments),
 // positive inside the triangle and negative outside.  A ray that passes
 // within a small distance of a triangle's boundary is one whose hit or miss
-// of that triangle FP32 arithmetic can decide either way.  prim = 0xFFFFFFFF
-// or a ray parallel to the plane gives t = inf and distance = inf.
+// of that triangle FP32 arithmetic can decide either way.  cos_out (may be
+// NULL): |cos| of the angle between the ray and the plane's normal (the
+// point's uncertainty along the ray grows as 1 / cos).  prim = 0xFFFFFFFF
+// or a ray parallel to the plane gives t = inf, distance = inf and cos = 0.
 void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prims, uint32_t n, double* t_out,
-                   double* edge_out) {
+                   double* edge_out, double* cos_out) {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
         const double inf = std::numeric_limits<double>::infinity();
         t_out[i] = inf;
         edge_out[i] = inf;
+        if (cos_out) cos_out[i] = 0.0;
         uint32_t p = prims[i];
         if (p >= s->tinst.size()) continue;
         const double* v = &s->tv[9 * (size_t)p];
@@ -1145,6 +1148,11 @@ void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prim
         }
         t_out[i] = t;
         edge_out[i] = inside ? dist : -dist;
+        if (cos_out) {
+            double nl = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+            double dl = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            cos_out[i] = std::fabs(den) / (nl * dl);
+        }
     }
 }
 

@@ -43,10 +43,11 @@ void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit,
                double* t_out, uint32_t* prim_out, double* u_out, double* v_out, double* t_second);
 
 /* FP64: for ray i and flattened triangle prims[i], the ray parameter where
- * the ray's line meets the triangle's plane and the distance from that point
- * to the triangle's boundary (positive inside, negative outside). */
+ * the ray's line meets the triangle's plane, the distance from that point
+ * to the triangle's boundary (positive inside, negative outside) and
+ * (cos_out, may be NULL) |cos| of the angle between ray and plane normal. */
 void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prims, uint32_t n, double* t_out,
-                   double* edge_out);
+                   double* edge_out, double* cos_out);
 
 /* Same op codes and record layouts as srt_test_device_math. */
 int orc_device_math(int op, uint32_t n, const void* in, void* out, const void* aux);

@@ -83,11 +83,14 @@ MISS = 0xFFFFFFFF
 # decide either way is not a disagreement:
 #   tie    another triangle is hit within |dt| < 1e-6 of the nearest (the
 #          north-star rule)
-#   edge   the ray passes within EDGE_REL * scale of the boundary of the
-#          oracle's hit triangle or of the GPU's (FP64 distance, world units;
-#          scale = max(1, |origin|inf, |hit point|inf), the magnitude of the
-#          FP32 coordinates involved)
+#   edge   the ray passes within EDGE_REL * scale * (1 + 1 / |cos|) of the
+#          boundary of the oracle's hit triangle or of the GPU's (FP64 distance
+#          in world units; scale = max(1, |origin|inf, |hit point|inf), the
+#          magnitude of the FP32 coordinates involved; cos = cosine between
+#          the ray and the triangle's normal: a plane position uncertain by d
+#          moves the hit point d / |cos| along a grazing ray)
 #   range  the oracle's hit lies within RANGE_REL * scale of tmin or tmax
+# Hit distances of agreeing ids: |dt| <= 1e-5 t + EDGE_REL * scale / |cos|.
 EDGE_REL = 2.0 ** -19
 RANGE_REL = 2.0 ** -19
 
@@ -107,26 +110,31 @@ def closest_hit_parity(scene, oracle, rays, brute=True, hits=None):
     scale = np.maximum(1.0, np.maximum(np.abs(o).max(1), np.abs(x).max(1)))
     with np.errstate(invalid="ignore"):
         tie = hit_o & (np.abs(t2 - t) < 1e-6)
-    _, e_o = oracle.tri_probe(rays, prim)
-    _, e_g = oracle.tri_probe(rays, pg)
-    edge = (np.abs(e_o) < EDGE_REL * scale) | (np.abs(e_g) < EDGE_REL * scale)
+    _, e_o, c_o = oracle.tri_probe(rays, prim, with_cos=True)
+    _, e_g, c_g = oracle.tri_probe(rays, pg, with_cos=True)
+    with np.errstate(divide="ignore"):
+        slack_o = EDGE_REL * scale * (1.0 + 1.0 / np.maximum(c_o, 1e-12))
+        slack_g = EDGE_REL * scale * (1.0 + 1.0 / np.maximum(c_g, 1e-12))
+    edge = (np.abs(e_o) < slack_o) | (np.abs(e_g) < slack_g)
     rng_ = hit_o & ((np.abs(t - rays[:, 3]) < RANGE_REL * scale) | (np.abs(t - rays[:, 7]) < RANGE_REL * scale))
     excluded = tie | edge | rng_
     mismatch = pg != prim
     both = hit_o & hit_g & (pg == prim)
-    dt = np.abs(g["t"][both].astype(np.float64) - t[both]) / np.maximum(1.0, t[both])
+    # |dt| relative to its bound 1e-5 t + EDGE_REL scale / |cos| (<= 1 passes)
+    dt = np.abs(g["t"][both].astype(np.float64) - t[both]) / (
+        1e-5 * np.maximum(1.0, t[both]) + EDGE_REL * scale[both] / np.maximum(c_o[both], 1e-12))
     return {"n": len(rays), "hits": int(hit_o.sum()), "mismatch": int(mismatch.sum()),
             "excluded": int(excluded.sum()), "tie": int(tie.sum()), "edge": int(edge.sum()),
             "range": int(rng_.sum()), "mismatch_excluded": int((mismatch & excluded).sum()),
-            "bad": np.nonzero(mismatch & ~excluded)[0], "max_rel_dt": float(dt.max()) if dt.size else 0.0,
-            # the largest boundary distances among the disagreements (how tight EDGE_REL could be)
-            "mismatch_edge_rel": np.sort(np.minimum(np.abs(e_o), np.abs(e_g))[mismatch] / scale[mismatch])[-8:],
+            "bad": np.nonzero(mismatch & ~excluded)[0], "max_dt_over_bound": float(dt.max()) if dt.size else 0.0,
+            # the largest boundary distances among the disagreements, in units of the slack
+            "mismatch_edge_rel": np.sort(np.minimum(np.abs(e_o) / slack_o, np.abs(e_g) / slack_g)[mismatch])[-8:],
             "g": g, "t": t, "prim": prim}
 
 
 def report(name, d):
     """One line of parity statistics (shown with pytest -s or -rP)."""
-    keys = ("n", "hits", "mismatch", "mismatch_excluded", "excluded", "tie", "edge", "range", "max_rel_dt")
+    keys = ("n", "hits", "mismatch", "mismatch_excluded", "excluded", "tie", "edge", "range", "max_dt_over_bound")
     print(f"[parity] {name}: " + ", ".join(f"{k}={d[k]}" for k in keys if k in d)
           + (f", bad={len(d['bad'])}" if "bad" in d else "")
           + (f", mismatch_edge_rel_max={list(np.round(d['mismatch_edge_rel'], 9))}" if "mismatch_edge_rel" in d else ""),

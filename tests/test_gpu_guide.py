@@ -163,7 +163,7 @@ def test_guided_render_is_unbiased(srt, ctx):
     b = srt.SceneBuilder()
     cam = b.add_preset(srt.PRESET_CORNELL_BOX)
     scene = b.build(ctx)
-    w, h, frames = 64, 48, 1024
+    w, h, frames = 64, 48, 2048
     plain = _render(srt, ctx, scene, cam, w, h, srt.FLAG_FP64_ACCUM, frames)
     guided = _render(srt, ctx, scene, cam, w, h, srt.FLAG_FP64_ACCUM | srt.FLAG_GUIDING, frames)
     a = plain.read_accum64()
