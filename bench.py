@@ -503,10 +503,12 @@ def main(argv=None):
             rt.render(cam_u(k))
             rc.render(cam_u(k))
         s1, s2 = rt.stats(), rc.stats()
-        launches = s1["launches_trace_closest"]
+        bt, bc = rt.bounce_stats(), rc.bounce_stats()
+        tail = int(s1["tail_first"])  # bounces >= tail run in the tail kernel
+        launches = s1["launches_trace_closest"]  # closest-hit launches of bounces < tail
         ms_launch = s1["ms_trace_closest"] / launches
-        rays = s2["rays_closest"]
-        alg_bytes = rays * (32 + 16) + s2["nodes_visited"][0] * 80 + s2["tris_tested"][0] * 48
+        rays = int(bc["rays"][0][:tail].sum())
+        alg_bytes = rays * (32 + 16) + float(bc["nodes"][0][:tail].sum()) * 80 + float(bc["tris"][0][:tail].sum()) * 48
         bytes_launch = alg_bytes / launches
         achieved = bytes_launch / (ms_launch * 1e-3) / 1e9
         peak, peak_kind = _peaks()
@@ -516,18 +518,17 @@ def main(argv=None):
                 "kernel": "k_trace<closest> (trace_kernels.cu)",
                 "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                 "bytes_per_launch": round(bytes_launch), "ms_per_launch": round(ms_launch, 4),
-                "nodes_per_ray": round(s2["nodes_visited"][0] / max(1, rays), 2),
-                "tris_per_ray": round(s2["tris_tested"][0] / max(1, rays), 2),
+                "nodes_per_ray": round(float(bc["nodes"][0][:tail].sum()) / max(1, rays), 2),
+                "tris_per_ray": round(float(bc["tris"][0][:tail].sum()) / max(1, rays), 2),
                 "stage_ms_per_frame": {k: round(s1[k] / nf, 3) for k in
                                        ("ms_photon_pass", "ms_raygen", "ms_trace_closest", "ms_shade",
-                                        "ms_trace_shadow", "ms_finalize")}}
+                                        "ms_trace_shadow", "ms_tail", "ms_finalize")}}
         if traffic is not None:
             roof["traffic_note"] = tnote
-        # per bounce: rays, algorithmic GB/s of the closest-hit launch, and the
-        # share of closest-hit time spent in the launches past the first four
-        bt, bc = rt.bounce_stats(), rc.bounce_stats()
+        # per bounce: rays, algorithmic GB/s of the closest-hit launch, node
+        # visits per ray; the bounces from `tail` on run in the tail kernel
         per = []
-        for k in range(depth):
+        for k in range(min(tail, depth)):
             rays_k = float(bc["rays"][0][k]) / nf
             bytes_k = (float(bc["rays"][0][k]) * 48 + float(bc["nodes"][0][k]) * 80 + float(bc["tris"][0][k]) * 48) / nf
             ms_k = float(bt["ms"][0][k]) / nf
@@ -537,8 +538,16 @@ def main(argv=None):
                         "shadow_rays": round(float(bc["rays"][1][k]) / nf),
                         "shadow_ms": round(float(bt["ms"][1][k]) / nf, 4)})
         roof["per_bounce_closest"] = per
-        tail = sum(x["ms"] for x in per[4:])
-        roof["tail_share"] = round(tail / max(1e-9, sum(x["ms"] for x in per)), 3)
+        if tail < depth:
+            # the tail kernel: closest-hit and shadow traversal of the last bounces plus their shading
+            tb = sum(float(bc["rays"][0][k]) * 48 + float(bc["nodes"][0][k]) * 80 + float(bc["tris"][0][k]) * 48 +
+                     float(bc["rays"][1][k]) * 36 + float(bc["nodes"][1][k]) * 80 + float(bc["tris"][1][k]) * 48
+                     for k in range(tail, depth)) / nf
+            ms_t = s1["ms_tail"] / nf
+            roof["tail_kernel"] = {"first_bounce": tail, "ms": round(ms_t, 4),
+                                   "closest_rays": round(float(bc["rays"][0][tail:depth].sum()) / nf),
+                                   "shadow_rays": round(float(bc["rays"][1][tail:depth].sum()) / nf),
+                                   "traversal_gbs": round(tb / (ms_t * 1e-3) / 1e9, 1) if ms_t > 0 else None}
         rt.close()
         rc.close()
 

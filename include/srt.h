@@ -182,6 +182,9 @@ typedef struct srt_stats {
     uint64_t launches_trace_closest;
     uint64_t kernel_launches;   /* kernels launched by the library in these frames */
     double ms_guide_train;      /* SRT_FLAG_STAGE_TIMING + SRT_FLAG_GUIDING: training step times */
+    double ms_tail;             /* SRT_FLAG_STAGE_TIMING: the tail kernel (srt_renderer_set_tail) */
+    uint32_t tail_first;        /* first bounce the tail kernel runs (max_depth: none) */
+    uint32_t pad;
 } srt_stats;
 
 /* Per-bounce statistics of a renderer's frames since the last
@@ -386,6 +389,14 @@ srt_status srt_screenshot_write_async(const char* path, const uint8_t* rgba, uin
 srt_status srt_screenshot_flush(uint32_t* failed_writes);
 srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out);
 srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_stats* out);
+/* Bounces first_bounce .. max_depth - 1 of every frame run as one persistent
+ * kernel that follows each remaining path to its end (closest hit, shading,
+ * shadow ray) instead of one closest-hit, shading and shadow launch per
+ * bounce: the same arithmetic per path, so the same image, with the latency
+ * of the short last bounces paid once.  Default 5; 0 = bounce by bounce.
+ * Not used with SRT_FLAG_RAY_SORT, nor where guided bounces reach it
+ * (srt_renderer_guide_set_bounces).  No reference counterpart. */
+srt_status srt_renderer_set_tail(srt_renderer* r, uint32_t first_bounce);
 srt_status srt_renderer_reset_stats(srt_renderer* r);
 /* The photon set of the last frame in emission order (photon_emit.wgsl
  * storage): copies min(count, capacity) photons to `out` (may be NULL) and

@@ -88,7 +88,8 @@ class Stats(C.Structure):
                 ("ms_photon_pass", C.c_double), ("ms_trace_closest", C.c_double), ("ms_shade", C.c_double),
                 ("ms_trace_shadow", C.c_double), ("ms_finalize", C.c_double), ("ms_raygen", C.c_double),
                 ("launches_trace_closest", C.c_uint64), ("kernel_launches", C.c_uint64),
-                ("ms_guide_train", C.c_double)]
+                ("ms_guide_train", C.c_double), ("ms_tail", C.c_double), ("tail_first", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 
 class BounceStats(C.Structure):  # srt_bounce_stats
@@ -184,6 +185,7 @@ SIGNATURES = {
     "srt_screenshot_flush": (_I, [_P]),
     "srt_renderer_get_stats": (_I, [_P, C.POINTER(Stats)]),
     "srt_renderer_get_bounce_stats": (_I, [_P, C.POINTER(BounceStats)]),
+    "srt_renderer_set_tail": (_I, [_P, _U32]),
     "srt_renderer_reset_stats": (_I, [_P]),
     "srt_renderer_read_photons": (_I, [_P, _P, _U32, C.POINTER(_U32)]),
     "srt_trace_rays": (_I, [_P, _P, _U32, _P, _I]),
@@ -565,6 +567,10 @@ class Renderer:
         _check(lib().srt_renderer_get_bounce_stats(self.h, C.byref(s)), self.ctx.h)
         return {"rays": np.array(s.rays, np.uint64), "nodes": np.array(s.nodes, np.uint64),
                 "tris": np.array(s.tris, np.uint64), "ms": np.array(s.ms, np.float64)}
+
+    def set_tail(self, first_bounce: int) -> None:
+        """Bounces >= first_bounce in one persistent kernel per frame (0: bounce by bounce)."""
+        _check(lib().srt_renderer_set_tail(self.h, first_bounce), self.ctx.h)
 
     def reset_stats(self):
         _check(lib().srt_renderer_reset_stats(self.h), self.ctx.h)

@@ -674,6 +674,11 @@ extern "C" srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width) {
 }
 
 // ====================================================================== renderer
+// First bounce of the tail kernel by default (launch_tail): the reference's
+// Russian roulette starts after bounce 3, so from bounce 5 on few paths live.
+#ifndef SRT_TAIL_FIRST_DEFAULT
+#define SRT_TAIL_FIRST_DEFAULT 5u
+#endif
 // Frames enqueue independent stages on two branches (srt_renderer::record_overlapped).
 #ifndef SRT_FRAME_OVERLAP
 #define SRT_FRAME_OVERLAP 1
@@ -723,7 +728,8 @@ struct srt_renderer {
     int launches_per_frame = 0;
     uint32_t frame_count = 0;
     uint64_t frames = 0, launches = 0, photons_emitted = 0, trace_launches = 0;
-    double ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // photon, -, closest, shade, shadow, finalize, raygen, guide training
+    double ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // photon, -, closest, shade, shadow, finalize, raygen, guide
+                                                 // training, tail
     double ms_bounce[2][MAX_BOUNCES + 1] = {};  // closest-hit and shadow traversal per bounce
     std::vector<cudaEvent_t> ev;
     GuideArgs guide{};  // SRT_FLAG_GUIDING only
@@ -764,36 +770,60 @@ struct srt_renderer {
 
     // Enqueues one frame (after the camera upload).  stage timing: events
     // between stages (only when `timed`, which keeps every stage in order).
+    // First bounce handled by the tail kernel (launch_tail), or max_depth for
+    // none: a setting of the renderer, used where the whole remainder of a
+    // path can run in one kernel (no ray reordering, no guided vertex left).
+    uint32_t tail_first = SRT_TAIL_FIRST_DEFAULT;
+    uint32_t tail_start() const {
+        const uint32_t t = tail_first;
+        if (t == 0u || t >= p.max_depth || args.ray_sort) return p.max_depth;
+        if (args.guiding && args.guide_bounces > t) return p.max_depth;
+        return t;
+    }
+
+    // Enqueues one frame (after the camera upload).  With stage timing,
+    // events between stages (stage_of[i]: the stage and bounce of the
+    // interval that ends at event i), every stage in order.
+    std::vector<std::pair<int, int>> stage_of;
     int record(cudaStream_t st, bool timed) {
         if (!timed && SRT_FRAME_OVERLAP) return record_overlapped(st);
         int n = 0;
         size_t e = 0;
-        auto mark = [&]() {
-            if (timed) cudaEventRecord(ev[e++], st);
+        stage_of.clear();
+        auto mark = [&](int stage, int bounce) {
+            if (timed) {
+                cudaEventRecord(ev[e++], st);
+                stage_of.emplace_back(stage, bounce);
+            }
         };
         cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
-        mark();  // 0
+        mark(-1, 0);
         if (p.photons_per_frame > 0 && scene->n_lights > 0) {
             // without lights the reference emits nothing (photon_emit.wgsl:161-162); the grid stays empty
             FrameArgs& a = args;
             n += launch_photon_pass(a, st);
         }
-        mark();  // 1 (photon pass total)
+        mark(0, 0);  // photon pass
         n += launch_raygen(args, st);
-        mark();  // 2
-        for (uint32_t b = 0; b < p.max_depth; ++b) {
+        mark(6, 0);
+        const uint32_t tail = tail_start();
+        for (uint32_t b = 0; b < tail; ++b) {
             n += launch_bounce(args, b, st, 1);
-            mark();
+            mark(2, (int)b);
             n += launch_bounce(args, b, st, 2);
-            mark();
+            mark(3, (int)b);
             n += launch_bounce(args, b, st, 3);
-            mark();
+            mark(4, (int)b);
+        }
+        if (tail < p.max_depth) {
+            n += launch_tail(args, tail, st);
+            mark(8, (int)tail);
         }
         n += launch_finalize(args, st);
         n += launch_frame_stats(args, st);
-        mark();
+        mark(5, 0);
         if (args.guiding) n += launch_guide_train(args, st);
-        mark();
+        mark(7, 0);
         return n;
     }
 
@@ -834,8 +864,15 @@ struct srt_renderer {
         if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
         join();
         if (deferred) cudaStreamWaitEvent(st, tjoin_ev, 0);
+        const uint32_t tail = tail_start();
         for (uint32_t b = 0; b < p.max_depth; ++b) {
             n += launch_bounce(args, b, st, 2);
+            if (b + 1 == tail) {
+                // the tail kernel shades paths whose radiance these shadow rays add to: after them
+                n += launch_bounce(args, b, st, 3);
+                n += launch_tail(args, tail, st);
+                break;
+            }
             if (b + 1 < p.max_depth) {
                 fork();
                 n += launch_bounce(args, b, s2, 3);
@@ -1109,24 +1146,18 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
                 cudaEventElapsedTime(&t, r->ev[a], r->ev[b]);
                 return (double)t;
             };
-            r->ms[0] += el(0, 1);
-            r->ms[6] += el(1, 2);
-            for (uint32_t b = 0; b < r->p.max_depth; ++b) {
-                size_t base = 2 + 3 * b;
-                const double tc = el(base, base + 1), ts = el(base + 2, base + 3);
-                r->ms[2] += tc;
-                r->ms[3] += el(base + 1, base + 2);
-                r->ms[4] += ts;
-                r->ms_bounce[0][b] += tc;
-                r->ms_bounce[1][b] += ts;
+            for (size_t i = 1; i < r->stage_of.size(); ++i) {
+                const int stage = r->stage_of[i].first, b = r->stage_of[i].second;
+                const double t_ms = el(i - 1, i);
+                r->ms[stage] += t_ms;
+                if (stage == 2) r->ms_bounce[0][b] += t_ms;
+                if (stage == 4) r->ms_bounce[1][b] += t_ms;
             }
-            r->ms[5] += el(2 + 3 * r->p.max_depth, 3 + 3 * r->p.max_depth);
-            r->ms[7] += el(3 + 3 * r->p.max_depth, 4 + 3 * r->p.max_depth);
         }
     }
     // an overlapped guided frame leaves its training steps to the next frame
     r->train_pending = r->args.guiding && !timed && SRT_FRAME_OVERLAP;
-    r->trace_launches += r->p.max_depth;
+    r->trace_launches += r->tail_start();
     r->frames += 1;
     r->photons_emitted += r->p.photons_per_frame;
     r->frame_count += 1;  // renderer/mod.rs:204
@@ -1277,6 +1308,8 @@ extern "C" srt_status srt_renderer_get_stats(srt_renderer* r, srt_stats* out) {
     out->ms_finalize = r->ms[5];
     out->ms_raygen = r->ms[6];
     out->ms_guide_train = r->ms[7];
+    out->ms_tail = r->ms[8];
+    out->tail_first = r->tail_start();
     out->launches_trace_closest = r->trace_launches;
     out->kernel_launches = r->launches;
     return check_device_error(c, r->err);
@@ -1299,6 +1332,19 @@ extern "C" srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_
     for (int k = 0; k < 2; ++k)
         for (int b = 0; b <= MAX_BOUNCES; ++b) out->ms[k][b] = r->ms_bounce[k][b];
     return check_device_error(c, r->err);
+}
+
+extern "C" srt_status srt_renderer_set_tail(srt_renderer* r, uint32_t first_bounce) {
+    if (!r || r->batch_owned) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->tail_first = first_bounce;
+    if (r->graph) {  // the tail shapes the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return SRT_OK;
 }
 
 extern "C" srt_status srt_renderer_reset_stats(srt_renderer* r) {

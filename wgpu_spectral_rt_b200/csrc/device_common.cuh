@@ -422,33 +422,43 @@ SRT_DEV RayShear make_shear(float3 d) {
     r.sz = 1.0f / dz;
     return r;
 }
-// Returns true on a hit with tmin <= t <= tmax; u, v = weights of v1, v2.
-SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3 v1, float3 v2, float& t,
-                           float& u, float& v) {
-    float3 A = v0 - ray.o, B = v1 - ray.o, C = v2 - ray.o;
-    float Az = comp(A, sh.kz), Bz = comp(B, sh.kz), Cz = comp(C, sh.kz);
-    float Ax = comp(A, sh.kx) - sh.sx * Az, Ay = comp(A, sh.ky) - sh.sy * Az;
-    float Bx = comp(B, sh.kx) - sh.sx * Bz, By = comp(B, sh.ky) - sh.sy * Bz;
-    float Cx = comp(C, sh.kx) - sh.sx * Cz, Cy = comp(C, sh.ky) - sh.sy * Cz;
-    float U = Cx * By - Cy * Bx;
-    float V = Ax * Cy - Ay * Cx;
-    float W = Bx * Ay - By * Ax;
-    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+SRT_DEV float comp_i(float3 v, uint32_t k) { return k == 0u ? v.x : (k == 1u ? v.y : v.z); }
+// The watertight test on vertices v0, v1, v2 for a ray from o sheared by
+// (kx, ky, kz, sx, sy, sz).  Every rounding is written out (explicit fused
+// multiply-adds and products), so the test gives the same bits in every
+// translation unit whatever its contraction setting.  Returns true on a hit
+// with tmin <= t <= tmax; u, v = weights of v1, v2.
+SRT_DEV bool tri_test(float3 v0, float3 v1, float3 v2, float3 o, uint32_t kx, uint32_t ky, uint32_t kz, float sx,
+                      float sy, float sz, float tmin, float tmax, float& t, float& u, float& v) {
+    const float3 A = v0 - o, B = v1 - o, C = v2 - o;
+    const float Az = comp_i(A, kz), Bz = comp_i(B, kz), Cz = comp_i(C, kz);
+    const float Ax = fmaf(-sx, Az, comp_i(A, kx)), Ay = fmaf(-sy, Az, comp_i(A, ky));
+    const float Bx = fmaf(-sx, Bz, comp_i(B, kx)), By = fmaf(-sy, Bz, comp_i(B, ky));
+    const float Cx = fmaf(-sx, Cz, comp_i(C, kx)), Cy = fmaf(-sy, Cz, comp_i(C, ky));
+    float U = fmaf(Cx, By, -__fmul_rn(Cy, Bx));
+    float V = fmaf(Ax, Cy, -__fmul_rn(Ay, Cx));
+    float W = fmaf(Bx, Ay, -__fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {  // FP64 fallback: exact products
         U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
         V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
         W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
     }
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
-    float det = U + V + W;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
     if (det == 0.0f) return false;
-    float T = U * (sh.sz * Az) + V * (sh.sz * Bz) + W * (sh.sz * Cz);
-    float inv = 1.0f / det;
-    float tt = T * inv;
-    if (!(tt >= ray.tmin && tt <= ray.tmax)) return false;
+    const float inv = __frcp_rn(det);
+    const float T = fmaf(W, __fmul_rn(sz, Cz), fmaf(V, __fmul_rn(sz, Bz), __fmul_rn(U, __fmul_rn(sz, Az))));
+    const float tt = __fmul_rn(T, inv);
+    if (!(tt >= tmin && tt <= tmax)) return false;
     t = tt;
-    u = V * inv;
-    v = W * inv;
+    u = __fmul_rn(V, inv);
+    v = __fmul_rn(W, inv);
     return true;
+}
+SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3 v1, float3 v2, float& t, float& u,
+                           float& v) {
+    return tri_test(v0, v1, v2, ray.o, (uint32_t)sh.kx, (uint32_t)sh.ky, (uint32_t)sh.kz, sh.sx, sh.sy, sh.sz,
+                    ray.tmin, ray.tmax, t, u, v);
 }
 
 SRT_DEV uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xFFu; }
@@ -747,8 +757,6 @@ struct TravState {
     float bu, bv;
 };
 
-SRT_DEV float comp_i(float3 v, uint32_t k) { return k == 0u ? v.x : (k == 1u ? v.y : v.z); }
-
 // Returns false when the ray cannot hit anything (finished at once).
 SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, float tmin, float tmax) {
     T.best = MISS;
@@ -823,24 +831,9 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         const TriSlot* ts = S.tris + T.tg.x + (uint32_t)b;
         float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
         ++n_tris;
-        // watertight test (Woop, Benthin, Wald 2013), as intersect_tri
-        float3 A = xyz(a0) - T.o, B = xyz(a1) - T.o, C = xyz(a2) - T.o;
-        float Az = comp_i(A, kz), Bz = comp_i(B, kz), Cz = comp_i(C, kz);
-        float Ax = comp_i(A, kx) - T.sx * Az, Ay = comp_i(A, ky) - T.sy * Az;
-        float Bx = comp_i(B, kx) - T.sx * Bz, By = comp_i(B, ky) - T.sy * Bz;
-        float Cx = comp_i(C, kx) - T.sx * Cz, Cy = comp_i(C, ky) - T.sy * Cz;
-        float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
-        if (U == 0.0f || V == 0.0f || W == 0.0f) {
-            U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
-            V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
-            W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
-        }
-        if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) continue;
-        float det = U + V + W;
-        if (det == 0.0f) continue;
-        float inv = 1.0f / det;
-        float t = (U * (T.sz * Az) + V * (T.sz * Bz) + W * (T.sz * Cz)) * inv;
-        if (!(t >= T.tmin && t <= T.tbest)) continue;
+        float t, tu, tv;
+        if (!tri_test(xyz(a0), xyz(a1), xyz(a2), T.o, kx, ky, kz, T.sx, T.sy, T.sz, T.tmin, T.tbest, t, tu, tv))
+            continue;
         uint32_t id = __float_as_uint(a0.w);
         if (ANY) {
             if (PF && have) cp_async_wait_all();  // no copy into the slot outlives the ray
@@ -851,8 +844,8 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         if (t < T.tbest || id < T.best) {  // (t, id) lexicographic; t <= tbest holds here
             T.tbest = t;
             T.best = id;
-            T.bu = V * inv;
-            T.bv = W * inv;
+            T.bu = tu;
+            T.bv = tv;
         }
     }
 #if SRT_TRAV_ONE_TRI_PER_STEP

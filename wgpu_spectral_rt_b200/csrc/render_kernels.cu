@@ -359,121 +359,210 @@ SRT_DEV LightSample sample_light(const DevScene& S, float3 hp, float4 wl, uint32
     return ls;
 }
 
+// What one path's vertex produced: the continuation (written to the path
+// state when alive), a shadow ray, or a vertex deferred to the guide.
+struct VertexOut {
+    bool alive = false, shadow = false, guided = false;
+    float3 sh_o = f3(0.f, 0.f, 0.f), sh_d = f3(0.f, 0.f, 0.f);
+    float sh_tmax = 0.f;
+    float4 sh_c = splat4(0.f);
+    uint32_t key = 0u;
+    float4 g_p = splat4(0.f), g_n = splat4(0.f), g_wo = splat4(0.f), g_spec = splat4(0.f);
+};
+
 // One iteration of ray_color's bounce loop after the closest-hit query
-// (shader.wgsl:568-700).
-// GUIDE: Lambert continuations are left to k_guide_infer (guide.cu).
+// (shader.wgsl:568-700) for path `id`, whose hit is in a.pb.hit[id]: writes
+// the path's radiance and, when it continues, its next ray and state.
+// GUIDE: Lambert continuations of bounces < guide_bounces are left to
+// k_guide_infer (guide.cu); every guided renderer records the radiance a
+// training record's next vertex sees.
+template <bool GUIDE>
+SRT_DEV VertexOut shade_vertex(const FrameArgs& a, uint32_t id, uint32_t bounce) {
+    VertexOut out;
+    const DevScene& S = a.scene;
+    float4 h = a.pb.hit[id];
+    uint32_t prim = __float_as_uint(h.y);
+    if (prim == MISS) return out;
+    float4 o4 = a.pb.ray_o[id], d4 = a.pb.ray_d[id];
+    float3 o = xyz(o4), d = xyz(d4);
+    float4 thr = a.pb.thr[id], wl = a.pb.wl[id], rad = a.pb.rad[id];
+    uint4 misc = a.pb.misc[id];
+    uint32_t s = misc.x, flags = misc.y;
+    // a training record of the previous vertex: radiance before this vertex
+    if (GUIDE && misc.w != 0u) a.guide.rec.rad[misc.w - 1u] = rad;
+    Surface sf = surface_at(S, prim, h.z, h.w, d);
+    float4 color = S.materials[2 * sf.mat], extra = S.materials[2 * sf.mat + 1];
+    float3 ffn = sf.front ? sf.wn : -sf.wn;
+    uint32_t type = (uint32_t)extra.x;
+    if (type == 3u) {
+        if (!(flags & FLAG_CAUSTIC) && (sf.front || extra.y > 0.0f)) {
+            float4 em = blackbody4(wl, color.x) * color.y;
+            a.pb.rad[id] = rad + em * thr;
+        }
+        return out;
+    }
+    if (type == 0u) flags = (flags | FLAG_DIFFUSE) & ~FLAG_CAUSTIC;
+    else if (type == 2u && (flags & FLAG_DIFFUSE)) flags |= FLAG_CAUSTIC;
+    if (type == 0u) {
+        float4 spec = rgb_to_spectrum4(xyz(color), wl);
+        float3 hp = o + d * h.x;
+        if (a.gather.enabled) {
+            float4 gl = gather(a.gather, a.cam->frame_count, hp, ffn, wl);
+            rad = rad + thr * (spec / PI) * gl;
+        }
+        LightSample ls = sample_light(S, hp, wl, s);
+        if (ls.pdf > 0.0f) {
+            float ct = fmaxf(dot(ffn, ls.dir), 0.0f);
+            float bpdf = ct / PI;
+            float mis = ls.pdf / (ls.pdf + bpdf);
+            out.sh_c = thr * (spec / PI) * ls.radiance * ct * (mis / ls.pdf);
+            out.sh_o = hp;
+            out.sh_d = ls.dir;
+            out.sh_tmax = ls.dist - 0.001f;
+            out.shadow = true;
+        }
+        a.pb.rad[id] = rad;
+        if (GUIDE && bounce + 1u < a.max_depth && bounce < a.guide_bounces) {
+            out.guided = true;
+            out.g_p = f4(hp.x, hp.y, hp.z, wl.x);
+            out.g_n = f4(ffn.x, ffn.y, ffn.z, 0.f);
+            out.g_wo = f4(-d.x, -d.y, -d.z, 0.f);
+            out.g_spec = spec;
+            a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
+            return out;
+        }
+    }
+    Scatter sc = sample_bsdf(d, ffn, color, extra, sf.front, wl, thr, s);
+    if (!sc.absorbed) {
+        thr = thr * sc.att;
+        o = o + d * h.x;
+        bool alive = true;
+        if (bounce > 3u) {
+            float p = max4(thr);
+            if (rng_next(s) > p) alive = false;
+            else thr = thr / p;
+        }
+        if (bounce + 1u >= a.max_depth) alive = false;
+        if (alive) {
+            a.pb.thr[id] = thr;
+            a.pb.ray_o[id] = f4(o.x, o.y, o.z, 0.0001f);
+            a.pb.ray_d[id] = f4(sc.dir.x, sc.dir.y, sc.dir.z, 100.0f);
+            a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
+            if (a.ray_sort) out.key = ray_sort_key(o, sc.dir, S.bmin, S.binv);
+        }
+        out.alive = alive;
+    }
+    return out;
+}
+
+// One bounce of every live path: shade_vertex, then the live paths, shadow
+// rays and guided vertices go to their queues (warp-aggregated slots).
 template <bool GUIDE>
 __global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(FrameArgs a, uint32_t bounce) {
     uint32_t n = a.counters->paths[bounce];
     if (blockIdx.x * blockDim.x >= n) return;
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    const DevScene& S = a.scene;
     bool valid = q < n;
-    bool alive = false, shadow = false;
     uint32_t id = valid ? a.pb.queue[bounce & 1][q] : 0u;
-    float3 sh_o = f3(0.f, 0.f, 0.f), sh_d = f3(0.f, 0.f, 0.f);
-    uint32_t key = 0u;
-    float sh_tmax = 0.f;
-    float4 sh_c = splat4(0.f);
-    bool guided = false;  // continuation deferred to the guide
-    float4 g_p = splat4(0.f), g_n = splat4(0.f), g_wo = splat4(0.f), g_spec = splat4(0.f);
-    if (valid) {
-        float4 h = a.pb.hit[id];
-        uint32_t prim = __float_as_uint(h.y);
-        if (prim != MISS) {
-            float4 o4 = a.pb.ray_o[id], d4 = a.pb.ray_d[id];
-            float3 o = xyz(o4), d = xyz(d4);
-            float4 thr = a.pb.thr[id], wl = a.pb.wl[id], rad = a.pb.rad[id];
-            uint4 misc = a.pb.misc[id];
-            uint32_t s = misc.x, flags = misc.y;
-            // a training record of the previous vertex: radiance before this vertex
-            if (GUIDE && misc.w != 0u) a.guide.rec.rad[misc.w - 1u] = rad;
-            Surface sf = surface_at(S, prim, h.z, h.w, d);
-            float4 color = S.materials[2 * sf.mat], extra = S.materials[2 * sf.mat + 1];
-            float3 ffn = sf.front ? sf.wn : -sf.wn;
-            uint32_t type = (uint32_t)extra.x;
-            if (type == 3u) {
-                if (!(flags & FLAG_CAUSTIC) && (sf.front || extra.y > 0.0f)) {
-                    float4 em = blackbody4(wl, color.x) * color.y;
-                    a.pb.rad[id] = rad + em * thr;
-                }
-            } else {
-                if (type == 0u) flags = (flags | FLAG_DIFFUSE) & ~FLAG_CAUSTIC;
-                else if (type == 2u && (flags & FLAG_DIFFUSE)) flags |= FLAG_CAUSTIC;
-                if (type == 0u) {
-                    float4 spec = rgb_to_spectrum4(xyz(color), wl);
-                    float3 hp = o + d * h.x;
-                    if (a.gather.enabled) {
-                        float4 gl = gather(a.gather, a.cam->frame_count, hp, ffn, wl);
-                        rad = rad + thr * (spec / PI) * gl;
-                    }
-                    LightSample ls = sample_light(S, hp, wl, s);
-                    if (ls.pdf > 0.0f) {
-                        float ct = fmaxf(dot(ffn, ls.dir), 0.0f);
-                        float bpdf = ct / PI;
-                        float mis = ls.pdf / (ls.pdf + bpdf);
-                        sh_c = thr * (spec / PI) * ls.radiance * ct * (mis / ls.pdf);
-                        sh_o = hp;
-                        sh_d = ls.dir;
-                        sh_tmax = ls.dist - 0.001f;
-                        shadow = true;
-                    }
-                    a.pb.rad[id] = rad;
-                    if (GUIDE && bounce + 1u < a.max_depth && bounce < a.guide_bounces) {
-                        guided = true;
-                        g_p = f4(hp.x, hp.y, hp.z, wl.x);
-                        g_n = f4(ffn.x, ffn.y, ffn.z, 0.f);
-                        g_wo = f4(-d.x, -d.y, -d.z, 0.f);
-                        g_spec = spec;
-                        a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
-                    }
-                }
-                Scatter sc;
-                sc.absorbed = true;
-                if (!guided) sc = sample_bsdf(d, ffn, color, extra, sf.front, wl, thr, s);
-                if (!sc.absorbed) {
-                    thr = thr * sc.att;
-                    o = o + d * h.x;
-                    alive = true;
-                    if (bounce > 3u) {
-                        float p = max4(thr);
-                        if (rng_next(s) > p) alive = false;
-                        else thr = thr / p;
-                    }
-                    if (bounce + 1u >= a.max_depth) alive = false;
-                    if (alive) {
-                        a.pb.thr[id] = thr;
-                        a.pb.ray_o[id] = f4(o.x, o.y, o.z, 0.0001f);
-                        a.pb.ray_d[id] = f4(sc.dir.x, sc.dir.y, sc.dir.z, 100.0f);
-                        a.pb.misc[id] = make_uint4(s, flags, misc.z, 0u);
-                        if (a.ray_sort) key = ray_sort_key(o, sc.dir, S.bmin, S.binv);
-                    }
-                }
-            }
-        }
-    }
-    uint32_t slot = warp_push(alive, &a.counters->paths[bounce + 1]);
-    if (alive) {
+    VertexOut v;
+    if (valid) v = shade_vertex<GUIDE>(a, id, bounce);
+    uint32_t slot = warp_push(v.alive, &a.counters->paths[bounce + 1]);
+    if (v.alive) {
         a.pb.queue[(bounce + 1) & 1][slot] = id;
-        if (a.ray_sort) a.pb.sort_keys[slot] = key;
+        if (a.ray_sort) a.pb.sort_keys[slot] = v.key;
     }
-    uint32_t sslot = warp_push(shadow, &a.counters->shadow[bounce]);
-    if (shadow) {
-        a.pb.sh_o[sslot] = f4(sh_o.x, sh_o.y, sh_o.z, 0.001f);
-        a.pb.sh_d[sslot] = f4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-        a.pb.sh_c[sslot] = sh_c;
+    uint32_t sslot = warp_push(v.shadow, &a.counters->shadow[bounce]);
+    if (v.shadow) {
+        a.pb.sh_o[sslot] = f4(v.sh_o.x, v.sh_o.y, v.sh_o.z, 0.001f);
+        a.pb.sh_d[sslot] = f4(v.sh_d.x, v.sh_d.y, v.sh_d.z, v.sh_tmax);
+        a.pb.sh_c[sslot] = v.sh_c;
         a.pb.sh_id[sslot] = id;
     }
     if (GUIDE) {
-        uint32_t gslot = warp_push(guided, &a.guide.gc->verts[bounce]);
-        if (guided) {
-            a.guide.gv.p[gslot] = g_p;
-            a.guide.gv.n[gslot] = g_n;
-            a.guide.gv.wo[gslot] = g_wo;
-            a.guide.gv.spec[gslot] = g_spec;
+        uint32_t gslot = warp_push(v.guided, &a.guide.gc->verts[bounce]);
+        if (v.guided) {
+            a.guide.gv.p[gslot] = v.g_p;
+            a.guide.gv.n[gslot] = v.g_n;
+            a.guide.gv.wo[gslot] = v.g_wo;
+            a.guide.gv.spec[gslot] = v.g_spec;
             a.guide.gv.id[gslot] = id;
         }
     }
+}
+
+// Resident blocks per SM the tail kernel is compiled for (traversal and
+// shading in one kernel: 4 blocks of 128 allow 128 registers).
+#ifndef SRT_TAIL_MIN_BLOCKS
+#define SRT_TAIL_MIN_BLOCKS 4
+#endif
+
+// The last bounces of the live paths in one persistent launch: each thread
+// takes a path entering bounce `first` and follows it to its end (closest
+// hit, shade_vertex, its shadow ray), then takes the next path.  Per path
+// the operations and the order of its radiance updates are those of the
+// bounce-by-bounce wavefront (the traversal rounds alike in every kernel), so
+// the image is bit-identical; where few paths remain, one launch replaces a
+// chain of launches that each last as long as their slowest ray.
+template <bool GUIDE, bool COUNT, int STACK>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TAIL_MIN_BLOCKS) k_tail(FrameArgs a, uint32_t first) {
+    extern __shared__ uint2 stack_smem[];
+    __shared__ uint32_t n_closest[MAX_BOUNCES + 1], n_shadow[MAX_BOUNCES + 1];
+    for (uint32_t i = threadIdx.x; i <= (uint32_t)MAX_BOUNCES; i += blockDim.x) n_closest[i] = n_shadow[i] = 0u;
+    __syncthreads();
+    uint2* stack = stack_smem + threadIdx.x;
+    const uint32_t n = a.counters->paths[first];
+    uint32_t* fetch = &a.counters->fetch[TRAV_CLOSEST][first];
+    const uint32_t* queue = a.pb.queue[first & 1];
+    while (true) {
+        const uint32_t q = atomicAdd(fetch, 1u);
+        if (q >= n) break;
+        const uint32_t id = queue[q];
+        for (uint32_t b = first; b < a.max_depth; ++b) {
+            if (b > first) atomicAdd(&n_closest[b], 1u);  // paths[first] was counted by the last shading step
+            const float4 o = a.pb.ray_o[id], d = a.pb.ray_d[id];
+            float t = 0.f, u = 0.f, v = 0.f;
+            uint32_t prim;
+            TravCounters tc{&a.stats->nodes_bounce[TRAV_CLOSEST][b], &a.stats->tris_bounce[TRAV_CLOSEST][b]};
+            const bool h = traverse<false, COUNT, STACK>(a.scene, Ray{xyz(o), xyz(d), o.w, d.w}, stack, TRACE_BLOCK, t,
+                                                         prim, u, v, a.err, tc);
+            a.pb.hit[id] = h ? make_float4(t, __uint_as_float(prim), u, v) : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+            const VertexOut vo = shade_vertex<GUIDE>(a, id, b);
+            if (vo.shadow) {
+                atomicAdd(&n_shadow[b], 1u);
+                TravCounters ts{&a.stats->nodes_bounce[TRAV_SHADOW][b], &a.stats->tris_bounce[TRAV_SHADOW][b]};
+                const bool occluded = traverse<true, COUNT, STACK>(a.scene, Ray{vo.sh_o, vo.sh_d, 0.001f, vo.sh_tmax},
+                                                                   stack, TRACE_BLOCK, t, prim, u, v, a.err, ts);
+                if (!occluded) {  // as the shadow-ray kernel adds it (shader.wgsl:659-669)
+                    const float4 r = a.pb.rad[id], c = vo.sh_c;
+                    a.pb.rad[id] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z),
+                                               __fadd_rn(r.w, c.w));
+                }
+            }
+            if (!vo.alive) break;
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i <= (uint32_t)MAX_BOUNCES; i += blockDim.x) {
+        if (n_closest[i]) atomicAdd(&a.counters->paths[i], n_closest[i]);
+        if (n_shadow[i]) atomicAdd(&a.counters->shadow[i], n_shadow[i]);
+    }
+}
+
+template <bool GUIDE, bool COUNT, int STACK>
+int launch_tail_t(const FrameArgs& a, uint32_t first, cudaStream_t st) {
+    const size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
+    static int per_sm = 0;  // resident blocks per SM of this instantiation
+    if (per_sm == 0) {
+        int x = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, k_tail<GUIDE, COUNT, STACK>, TRACE_BLOCK, smem) !=
+                cudaSuccess ||
+            x < 1)
+            x = 1;
+        per_sm = x;
+    }
+    const uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * (uint32_t)per_sm;
+    k_tail<GUIDE, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a, first);
+    return 1;
 }
 
 // shader.wgsl:774-822: hero tuple -> XYZ / sum pdf -> linear sRGB ->
@@ -708,6 +797,18 @@ int launch_finalize(const FrameArgs& a, cudaStream_t st) {
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st) {
     k_frame_stats<<<1, 32, 0, st>>>(a);
     return 1;
+}
+
+int launch_tail(const FrameArgs& a, uint32_t first, cudaStream_t st) {
+    if (first >= a.max_depth) return 0;
+    const bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
+    const bool g = a.guiding != 0;
+    if (a.count_visits) {
+        if (g) return small ? launch_tail_t<true, true, TRAV_STACK_SMALL>(a, first, st) : launch_tail_t<true, true, TRAV_STACK>(a, first, st);
+        return small ? launch_tail_t<false, true, TRAV_STACK_SMALL>(a, first, st) : launch_tail_t<false, true, TRAV_STACK>(a, first, st);
+    }
+    if (g) return small ? launch_tail_t<true, false, TRAV_STACK_SMALL>(a, first, st) : launch_tail_t<true, false, TRAV_STACK>(a, first, st);
+    return small ? launch_tail_t<false, false, TRAV_STACK_SMALL>(a, first, st) : launch_tail_t<false, false, TRAV_STACK>(a, first, st);
 }
 
 int launch_gather_queries(const GatherArgs& g, uint32_t frame, const float* queries, uint32_t n_q, float4* out,

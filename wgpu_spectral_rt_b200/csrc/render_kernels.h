@@ -117,6 +117,9 @@ int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st);  
 int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue, const uint32_t* count,
                        uint32_t* fetch, uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind, int count_visits,
                        uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st);  // trace_kernels.cu
+// Bounces first .. max_depth - 1 of the paths queued for bounce `first`, in
+// one persistent launch (closest hit, shading and shadow ray per path).
+int launch_tail(const FrameArgs& a, uint32_t first, cudaStream_t st);
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
 
