@@ -2018,11 +2018,20 @@ struct srt_batch {
         for (int k = 0; k < na; ++k) n += r[act[k]]->record_raygen(cap);
         n += closest(0, cap);
         for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
+        // the tail: from the latest first tail bounce of the scenes, each
+        // scene's remaining bounces run in its own tail launch on its branch
+        uint32_t tail = 0;
+        for (int k = 0; k < na; ++k) tail = std::max(tail, r[act[k]]->tail_start());
         for (uint32_t b = 0; b < max_depth; ++b) {
             fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
             if (ng && b + 1 < guide_depth)
                 n += launch_guide_infer_multi(guide_items_dev, ng, b, fetch_dev + 2 * MAX_BOUNCES + b, c->sm_count,
                                               cap);
+            if (b + 1 == tail) {
+                n += shadow(b, cap);
+                fork_join([tail](srt_renderer* x, cudaStream_t s) { return launch_tail(x->args, tail, s); });
+                break;
+            }
             if (b + 1 < max_depth) {
                 // independent: the shadow rays add to the radiance, the closest hits read rays and queues
                 cudaEventRecord(ovl_fork, cap);
