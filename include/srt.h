@@ -532,6 +532,14 @@ srt_status srt_guide_test_forward_tc(srt_ctx* ctx, const float* params, const fl
 #define SRT_GUIDE_INFER_MMA_SYNC 0
 #define SRT_GUIDE_INFER_TCGEN05  1
 srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind);
+/* Training step kernels of a guiding renderer: mma.sync forward/backward
+ * with a split-K weight-gradient product, or one fused tcgen05 kernel per
+ * step (forward, loss gradient, backward and weight gradients of 128-record
+ * tiles, the weight gradients accumulated in tensor memory).  The batched
+ * renderer's grouped training uses the mma.sync kernels. */
+#define SRT_GUIDE_TRAIN_MMA_SYNC 0
+#define SRT_GUIDE_TRAIN_TCGEN05  1
+srt_status srt_renderer_guide_set_training(srt_renderer* r, int kind);
 srt_status srt_guide_test_mixture(srt_ctx* ctx, const float* raw, const float* omega, const float* u, uint32_t n,
                                   float* out);
 /* The same for the mixture functions of the tcgen05 inference kernel (fast
@@ -542,6 +550,11 @@ srt_status srt_guide_test_train(srt_ctx* ctx, const float* params, const float* 
                                 uint32_t adam_step, float lr, const float* x, const float* omega,
                                 const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
                                 float* params_out, float* m_out, float* v_out);
+/* The same on the fused tcgen05 training kernel. */
+srt_status srt_guide_test_train_tc(srt_ctx* ctx, const float* params, const float* adam_m, const float* adam_v,
+                                   uint32_t adam_step, float lr, const float* x, const float* omega,
+                                   const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
+                                   float* params_out, float* m_out, float* v_out);
 
 /* ------------------------------------------------------------------------ */
 /* Headless presentation: the reference's raster steps as CUDA kernels.       */

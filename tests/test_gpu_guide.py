@@ -99,12 +99,13 @@ def test_mixture_sampling_statistics(srt, ctx, tc):
     assert mean_cos == pytest.approx(1 / math.tanh(kappa) - 1 / kappa, abs=2e-3)
 
 
+@pytest.mark.parametrize("tc", [False, True], ids=["mma_sync", "tcgen05"])
 @pytest.mark.parametrize("n,out_scale", [(16, 1.0), (1000, 4.0), (65_536, 1.0)])
-def test_gradients_match_oracle(srt, ctx, n, out_scale):
+def test_gradients_match_oracle(srt, ctx, n, out_scale, tc):
     rng = np.random.default_rng(100 + n)
     w = _weights(srt, 3 + n, out_scale)
     x, om, pb, wt = _batch(rng, n)
-    grad = srt.guide_train_step(ctx, w, x, om, pb, wt, adam=False)
+    grad = srt.guide_train_step(ctx, w, x, om, pb, wt, adam=False, tcgen05=tc)
     params = go.unpack(w)
     raw16, ins = go.forward_bf16(params, x.astype(np.float64))
     _, gout16 = go.loss_and_output_grad(raw16, om.astype(np.float64), wt.astype(np.float64), pb.astype(np.float64))
@@ -121,6 +122,48 @@ def test_gradients_match_oracle(srt, ctx, n, out_scale):
             assert err < 2e-2, (li, part, err)
     cosine = grad @ ref / (np.linalg.norm(grad) * np.linalg.norm(ref))
     assert cosine > 0.99
+
+
+def test_tcgen05_training_matches_mma_sync(srt, ctx):
+    """The fused tcgen05 training step against the mma.sync kernels on the
+    same records: the same bf16 products with FP32 accumulation in another
+    summation order, so the gradients agree closely (relative Frobenius error
+    per layer), and a renderer trained with it moves its weights like the
+    mma.sync renderer does."""
+    rng = np.random.default_rng(77)
+    n = 40_000
+    w = _weights(srt, 77)
+    x, om, pb, wt = _batch(rng, n)
+    g0 = srt.guide_train_step(ctx, w, x, om, pb, wt, adam=False)
+    g1 = srt.guide_train_step(ctx, w, x, om, pb, wt, adam=False, tcgen05=True)
+    o = 0
+    for li, (fi, fo) in enumerate(go.DIMS):
+        for part, size in (("W", fi * fo), ("b", fo)):
+            a, b = g1[o:o + size].astype(np.float64), g0[o:o + size].astype(np.float64)
+            o += size
+            err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+            print(f"[parity] tcgen05 vs mma.sync gradient layer {li} {part}: {err:.2e}", flush=True)
+            assert err < 1e-2, (li, part, err)
+    # renderers: two frames of training each
+    b_ = srt.SceneBuilder()
+    cam = b_.add_preset(srt.PRESET_CORNELL_BOX)
+    scene = b_.build(ctx)
+    ctl = srt.CameraController(*cam)
+    ws = []
+    for kind in (srt.GUIDE_TRAIN_MMA_SYNC, srt.GUIDE_TRAIN_TCGEN05):
+        r = srt.Renderer(ctx, scene, 64, 48, srt.default_params(photons_per_frame=1 << 14, flags=srt.FLAG_GUIDING))
+        r.set_guide_training(kind)
+        w0 = r.guide_weights()
+        for f in range(2):
+            r.render(ctl.build_uniform(64 / 48, f))
+        ws.append(r.guide_weights() - w0)
+        assert r.guide_info()["adam_steps"] == 2
+        r.close()
+    moved = np.abs(ws[0]) > 1e-6
+    assert moved.mean() > 0.5
+    close = np.abs(ws[1] - ws[0]) <= 0.02 * 1e-3 + 0.05 * np.abs(ws[0])
+    assert close[moved].mean() > 0.95, close[moved].mean()
+    scene.close()
 
 
 def test_adam_step_matches_oracle(srt, ctx):

@@ -131,6 +131,8 @@ BVH_LBVH = 1
 
 GUIDE_INFER_MMA_SYNC = 0
 GUIDE_INFER_TCGEN05 = 1
+GUIDE_TRAIN_MMA_SYNC = 0
+GUIDE_TRAIN_TCGEN05 = 1
 
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "DEVICE_ASSERT", 6: "NO_DEVICE",
           7: "UNSUPPORTED", 8: "CAPACITY"}
@@ -221,6 +223,7 @@ SIGNATURES = {
     "srt_guide_test_forward": (_I, [_P, _P, _P, _U32, _P]),
     "srt_guide_test_forward_tc": (_I, [_P, _P, _P, _U32, _P]),
     "srt_renderer_guide_set_inference": (_I, [_P, _I]),
+    "srt_renderer_guide_set_training": (_I, [_P, _I]),
     "srt_guide_test_mixture": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_guide_test_mixture_tc": (_I, [_P, _P, _P, _P, _U32, _P]),
     "srt_renderer_guide_set_steps": (_I, [_P, _U32]),
@@ -230,6 +233,7 @@ SIGNATURES = {
     "srt_write_accum_f64": (_I, [_P, _P]),
     "srt_test_wait_timeout": (_I, [_P, _U32]),
     "srt_guide_test_train": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
+    "srt_guide_test_train_tc": (_I, [_P, _P, _P, _P, _U32, _F, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -621,6 +625,10 @@ class Renderer:
         """GUIDE_INFER_MMA_SYNC or GUIDE_INFER_TCGEN05."""
         _check(lib().srt_renderer_guide_set_inference(self.h, kind), self.ctx.h)
 
+    def set_guide_training(self, kind: int) -> None:
+        """GUIDE_TRAIN_MMA_SYNC or GUIDE_TRAIN_TCGEN05."""
+        _check(lib().srt_renderer_guide_set_training(self.h, kind), self.ctx.h)
+
     def set_guide_weights(self, w: np.ndarray) -> None:
         a = np.ascontiguousarray(w, np.float32)
         _check(lib().srt_renderer_guide_set_weights(self.h, ptr(a), len(a)), self.ctx.h)
@@ -750,9 +758,10 @@ def guide_mixture(ctx: Context, raw: np.ndarray, omega: np.ndarray, u: np.ndarra
 
 
 def guide_train_step(ctx: Context, params, x, omega, pdf_bsdf, weight, adam_m=None, adam_v=None, adam_step=0,
-                     lr=1e-3, adam=True):
+                     lr=1e-3, adam=True, tcgen05=False):
     """Loss gradients (summed over the samples) and, with adam, the parameters
-    and Adam moments after one step (srt_guide_test_train)."""
+    and Adam moments after one step (srt_guide_test_train; tcgen05: the fused
+    tensor-core training kernel, srt_guide_test_train_tc)."""
     n = len(x)
     w = np.ascontiguousarray(params, np.float32)
     m = None if adam_m is None else np.ascontiguousarray(adam_m, np.float32)
@@ -763,7 +772,8 @@ def guide_train_step(ctx: Context, params, x, omega, pdf_bsdf, weight, adam_m=No
     wt = np.ascontiguousarray(weight, np.float32).reshape(-1)
     grad = np.zeros_like(w)
     outs = [np.zeros_like(w) for _ in range(3)] if adam else [None, None, None]
-    _check(lib().srt_guide_test_train(ctx.h, ptr(w), ptr(m) if m is not None else None,
+    fn = lib().srt_guide_test_train_tc if tcgen05 else lib().srt_guide_test_train
+    _check(fn(ctx.h, ptr(w), ptr(m) if m is not None else None,
                                       ptr(v) if v is not None else None, adam_step, lr, ptr(xs), ptr(om), ptr(pb),
                                       ptr(wt), n, ptr(grad), *(ptr(o) if o is not None else None for o in outs)),
            ctx.h)

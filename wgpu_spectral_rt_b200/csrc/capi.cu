@@ -1080,6 +1080,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
         guide_default_params(1, w.data());
         CUDA_TRY(c, guide_upload(r->guide, w.data(), nullptr, nullptr, 0));
         r->guide.train = (p.flags & SRT_FLAG_GUIDE_FROZEN) ? 0 : 1;
+        r->guide.err = r->err;
         a.guiding = 1;
         a.guide_bounces = MAX_BOUNCES + 1;  // every bounce
         a.guide = r->guide;
@@ -1698,6 +1699,22 @@ extern "C" srt_status srt_guide_test_forward_tc(srt_ctx* c, const float* params,
     return guide_test_forward(c, params, x, n, out, 1);
 }
 
+extern "C" srt_status srt_renderer_guide_set_training(srt_renderer* r, int kind) {
+    if (!r || (kind != SRT_GUIDE_TRAIN_MMA_SYNC && kind != SRT_GUIDE_TRAIN_TCGEN05)) return SRT_ERR_INVALID_ARG;
+    srt_ctx* c = r->ctx;
+    if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
+    if (srt_status fs = guide_flush(r)) return fs;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    r->guide.tc_train = kind == SRT_GUIDE_TRAIN_TCGEN05 ? 1 : 0;
+    r->args.guide = r->guide;
+    r->args_gen += 1;
+    if (r->graph) {  // the choice is baked into the captured frame
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    return SRT_OK;
+}
+
 extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind) {
     if (!r || (kind != SRT_GUIDE_INFER_MMA_SYNC && kind != SRT_GUIDE_INFER_TCGEN05)) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
@@ -1748,10 +1765,11 @@ extern "C" srt_status srt_guide_test_mixture_tc(srt_ctx* c, const float* raw, co
     return guide_test_mixture(c, raw, omega, u, n, out, 1);
 }
 
-extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, const float* adam_m, const float* adam_v,
-                                           uint32_t adam_step, float lr, const float* x, const float* omega,
-                                           const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
-                                           float* params_out, float* m_out, float* v_out) {
+namespace {
+srt_status guide_test_train(srt_ctx* c, const float* params, const float* adam_m, const float* adam_v,
+                            uint32_t adam_step, float lr, const float* x, const float* omega, const float* pdf_bsdf,
+                            const float* weight, uint32_t n, float* grad_out, float* params_out, float* m_out,
+                            float* v_out, int tc) {
     if (!c || !params || !x || !omega || !pdf_bsdf || !weight || !grad_out || n == 0 || n > G_REC_CAP)
         return SRT_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
@@ -1761,6 +1779,8 @@ extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, cons
     CUDA_TRY(c, guide_upload(s.g, params, adam_m, adam_v, adam_step));
     s.g.lr = lr;
     s.g.batch = n;
+    s.g.tc_train = tc;
+    s.g.err = c->d_err;
     std::vector<float4> x0(n), x1(n), x2(n), w(n), b(n);
     for (uint32_t i = 0; i < n; ++i) {
         const float* xi = x + (size_t)i * G_IN;
@@ -1794,7 +1814,25 @@ extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, cons
         if (v_out) CUDA_TRY(c, cudaMemcpyAsync(v_out, s.g.net.adam_v, G_NPARAMS * 4, cudaMemcpyDeviceToHost, c->stream));
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    return SRT_OK;
+    return check_device_error(c, c->d_err);
+}
+}  // namespace
+
+extern "C" srt_status srt_guide_test_train(srt_ctx* c, const float* params, const float* adam_m, const float* adam_v,
+                                           uint32_t adam_step, float lr, const float* x, const float* omega,
+                                           const float* pdf_bsdf, const float* weight, uint32_t n, float* grad_out,
+                                           float* params_out, float* m_out, float* v_out) {
+    return guide_test_train(c, params, adam_m, adam_v, adam_step, lr, x, omega, pdf_bsdf, weight, n, grad_out,
+                            params_out, m_out, v_out, 0);
+}
+
+extern "C" srt_status srt_guide_test_train_tc(srt_ctx* c, const float* params, const float* adam_m,
+                                              const float* adam_v, uint32_t adam_step, float lr, const float* x,
+                                              const float* omega, const float* pdf_bsdf, const float* weight,
+                                              uint32_t n, float* grad_out, float* params_out, float* m_out,
+                                              float* v_out) {
+    return guide_test_train(c, params, adam_m, adam_v, adam_step, lr, x, omega, pdf_bsdf, weight, n, grad_out,
+                            params_out, m_out, v_out, 1);
 }
 
 // ------------------------------------------------------------------ headless presentation

@@ -620,6 +620,39 @@ __global__ void k_guide_targets(FrameArgs a) { guide_targets(a); }
 // many renderers: blockIdx.y = item
 __global__ void k_guide_targets_multi(const FrameArgs* __restrict__ items) { guide_targets(items[blockIdx.y]); }
 
+// Gradient of the loss of one record with respect to the 48 raw outputs
+// (gr[41..47] are untouched): -w log q(omega) for the lobes and
+// -w log(sel q + (1 - sel) p_bsdf) for the selection output with q held
+// fixed.  w4 = sampled direction, b4.x = BSDF pdf, wt = normalised weight.
+SRT_DEV void loss_grad(const float* raw, float4 w4, float4 b4, float wt, float* gr) {
+    Mix m;
+    mixture_fast(raw, m);
+    float3 om = xyz(w4);
+    float vm[G_LOBES], q = 0.f;
+    for (int j = 0; j < G_LOBES; ++j) {
+        vm[j] = m.c[j] * __expf(m.kappa[j] * (dot(m.mu[j], om) - 1.0f));
+        q += m.pi[j] * vm[j];
+    }
+    q = fmaxf(q, 1e-30f);
+    const float iq = 1.0f / q;
+    for (int j = 0; j < G_LOBES; ++j) {
+        float gam = m.pi[j] * vm[j] * iq;
+        gr[5 * j + 4] = wt * (m.pi[j] - gam);
+        float k = m.kappa[j];
+        float mw = dot(m.mu[j], om);
+        float dl = 1.0f / k - 2.0f / expm1f(2.0f * k) + mw - 1.0f;
+        bool inside = m.lk[j] > G_KAPPA_LO && m.lk[j] < G_KAPPA_HI;
+        gr[5 * j + 3] = inside ? -wt * gam * dl * k : 0.f;
+        float3 gd = (om - m.mu[j] * mw) * __fdividef(-wt * gam * k, m.norm[j]);
+        gr[5 * j] = gd.x;
+        gr[5 * j + 1] = gd.y;
+        gr[5 * j + 2] = gd.z;
+    }
+    float pb = b4.x;
+    float pmix = fmaxf(m.sel * q + (1.0f - m.sel) * pb, 1e-30f);
+    gr[40] = __fdividef(-wt * (q - pb), pmix) * G_SEL_SPAN * m.sel_sig * (1.0f - m.sel_sig);
+}
+
 // Forward + backward of 16 records per warp: stores the encoded inputs,
 // post-ReLU activations and per-layer deltas (bf16) for the weight-gradient
 // product.  Loss per sample (weight w normalised by the batch mean):
@@ -665,37 +698,7 @@ SRT_DEV void guide_fwdbwd(const GuideArgs& G, int step) {
             const uint32_t j = base + lane, r = rec_at(sr, j);
             float gr[G_OUT];
             for (int i = 0; i < G_OUT; ++i) gr[i] = 0.f;
-            if (j < n) {
-                const float* raw = out + lane * 52;
-                Mix m;
-                mixture_fast(raw, m);
-                float4 w4 = G.rec.w[r], b4 = G.rec.b[r];
-                float3 om = xyz(w4);
-                float wt = G.rec.weight[r] * inv_mean;
-                float vm[G_LOBES], q = 0.f;
-                for (int j = 0; j < G_LOBES; ++j) {
-                    vm[j] = m.c[j] * __expf(m.kappa[j] * (dot(m.mu[j], om) - 1.0f));
-                    q += m.pi[j] * vm[j];
-                }
-                q = fmaxf(q, 1e-30f);
-                const float iq = 1.0f / q;
-                for (int j = 0; j < G_LOBES; ++j) {
-                    float gam = m.pi[j] * vm[j] * iq;
-                    gr[5 * j + 4] = wt * (m.pi[j] - gam);
-                    float k = m.kappa[j];
-                    float mw = dot(m.mu[j], om);
-                    float dl = 1.0f / k - 2.0f / expm1f(2.0f * k) + mw - 1.0f;
-                    bool inside = m.lk[j] > G_KAPPA_LO && m.lk[j] < G_KAPPA_HI;
-                    gr[5 * j + 3] = inside ? -wt * gam * dl * k : 0.f;
-                    float3 gd = (om - m.mu[j] * mw) * __fdividef(-wt * gam * k, m.norm[j]);
-                    gr[5 * j] = gd.x;
-                    gr[5 * j + 1] = gd.y;
-                    gr[5 * j + 2] = gd.z;
-                }
-                float pb = b4.x;
-                float pmix = fmaxf(m.sel * q + (1.0f - m.sel) * pb, 1e-30f);
-                gr[40] = __fdividef(-wt * (q - pb), pmix) * G_SEL_SPAN * m.sel_sig * (1.0f - m.sel_sig);
-            }
+            if (j < n) loss_grad(out + lane * 52, G.rec.w[r], G.rec.b[r], G.rec.weight[r] * inv_mean, gr);
             for (int i = 0; i < G_OUT; i += 2)
                 *reinterpret_cast<uint32_t*>(d4 + lane * g_pad(G_OUT) + i) = pack2(gr[i], gr[i + 1]);
         }
@@ -1399,6 +1402,243 @@ __global__ void __launch_bounds__(TC_ROWS * TC_GROUPS, 2) k_guide_test_forward_t
     tc_teardown(grp, ok, phase, err);
 }
 
+// ---------------------------------------------------------------- training on tcgen05
+// One training step of the network on the fifth-generation tensor cores,
+// fused: a block (128 threads, thread r = record row r of a 128-record
+// tile) runs, per tile, the five forward layers (D = A W^T into tensor
+// memory, bias + ReLU by the epilogue into the next A operand), the loss
+// gradient, and the backward pass: per layer one product
+// delta_{l-1} = (delta_l W_l) * relu'(a_{l-1}) and the weight-gradient
+// product dW_l += delta_l^T a_{l-1}, both issued together.  The weight
+// gradients accumulate in tensor memory over all of the block's tiles and
+// reach the global gradient once, at the end; activations and deltas never
+// leave shared memory.
+//
+// Operands: the K-major core-matrix layout of umma.cuh (the forward A, the
+// weights, and the deltas as A of the backward product).  The same bytes
+// read with the MN-major descriptor form serve the transposed products: the
+// weights as B of the backward product (n = input, k = output) and the
+// deltas and activations as the A and B of the weight gradient (k = record).
+// In the MN-major no-swizzle form a core matrix is 8 (k) rows of 16 bytes
+// holding 8 consecutive (mn) elements, adjacent core matrices along MN are
+// 128 bytes apart (the stride byte offset) and along K `lbo` bytes apart
+// (the leading byte offset): for a K-major buffer of K columns this is the
+// buffer's row-block stride K / 8 * 128.
+constexpr uint32_t TT_X_OFF = 47104u;                     // encoded inputs, 128 x 128
+constexpr uint32_t TT_H_OFF = TT_X_OFF + 32768u;          // a0..a3, 4 x (128 x 64)
+constexpr uint32_t TT_D_OFF = TT_H_OFF + 4u * 16384u;     // deltas, 2 x (128 x 64), ping-pong
+// The weight-gradient product reads its A (out x 128 records) with M = 128
+// rows; rows beyond the layer's outputs are other bytes of the buffers (their
+// products are never read), so 2 KB of slack follow the second delta buffer.
+constexpr uint32_t TT_B_OFF = TT_D_OFF + 2u * 16384u + 2048u;
+constexpr uint32_t TT_BAR_OFF = TT_B_OFF + SB_ELEMS * 4;  // mbarrier, then the TMEM base
+constexpr uint32_t TT_SMEM = TT_BAR_OFF + 16u;
+constexpr uint32_t TT_TMEM_COLS = 512;
+// tensor-memory columns: [0, 64) the layer products, then dW_0 .. dW_4
+__host__ __device__ constexpr uint32_t tt_dw_col(int l) { return l == 0 ? 64u : 192u + 64u * (uint32_t)(l - 1); }
+static_assert(tt_dw_col(4) + 64u <= TT_TMEM_COLS && TT_SMEM + 1024 <= 227 * 1024, "training kernel resources");
+static_assert(TT_B_OFF % 16 == 0 && TT_BAR_OFF % 8 == 0, "training kernel alignment");
+
+SRT_DEV uint32_t tt_idesc(uint32_t N, uint32_t a_mn, uint32_t b_mn) {
+    return umma_idesc_bf16(128u, N) | (a_mn << 15) | (b_mn << 16);
+}
+
+// Bounded wait of the block on the MMAs committed to `mbar`; false for the
+// whole block if they did not complete.
+SRT_DEV bool tt_wait(uint64_t* mbar, uint32_t& phase) {
+    const bool ok = __syncthreads_and(mbar_wait(mbar, phase, TC_WAIT_POLLS)) != 0;
+    if (ok) phase ^= 1u;
+    tc_fence_after();
+    return ok;
+}
+
+__global__ void __launch_bounds__(128, 1) k_guide_train_tc(GuideArgs G, int step) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const StepRecs sr = step_recs(G, step);
+    const uint32_t n = sr.count;
+    const uint32_t n_tiles = (n + 127u) / 128u;
+    if (blockIdx.x >= n_tiles) return;
+    float* sb = reinterpret_cast<float*>(smem + TT_B_OFF);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + TT_BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TT_BAR_OFF + 8);
+    if ((threadIdx.x >> 5) == 0) {
+        tmem_alloc(tslot, TT_TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) mbar_init(mbar, 1);
+    load_weights_tc(G.net, smem, sb);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t r = threadIdx.x;
+    const uint32_t trow = tmem + (((r >> 5) * 32u) << 16);  // this thread's lane
+    unsigned char* X = smem + TT_X_OFF;
+    const uint32_t w_addr = smem_u32(smem), x_addr = smem_u32(X);
+    const uint32_t n_all = min(G.gc->records, G.batch);
+    const float inv_mean = G.gc->weight_sum > 0.f ? (float)n_all / G.gc->weight_sum : 0.f;
+    uint32_t phase = 0;
+    bool ok = true, first = true;
+    float db[G_LAYERS] = {0.f, 0.f, 0.f, 0.f, 0.f};  // bias gradient of output r of each layer
+    for (uint32_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const uint32_t j = tile * 128u + r;
+        const bool valid = j < n;
+        const uint32_t rec = rec_at(sr, valid ? j : 0u);
+        float x[G_IN];
+        if (valid) {
+            const float4 x0 = G.rec.x0[rec], x1 = G.rec.x1[rec], x2 = G.rec.x2[rec];
+            x[0] = x0.x; x[1] = x0.y; x[2] = x0.z; x[3] = x0.w;
+            x[4] = x1.x; x[5] = x1.y; x[6] = x1.z; x[7] = x1.w;
+            x[8] = x2.x; x[9] = x2.y;
+        } else {
+            for (int i = 0; i < G_IN; ++i) x[i] = 0.f;
+        }
+        encode_row_tc(x, X, r);
+        fence_async_smem();
+        __syncthreads();
+        // ---- forward: a_l = relu(a_{l-1} W_l^T + b_l), raw = a_3 W_4^T + b_4
+        uint32_t mask[4][2];  // ReLU derivative bits of a_0 .. a_3
+        float raw[G_OUT];
+        for (int l = 0; l < G_LAYERS && ok; ++l) {
+            const uint32_t K = (uint32_t)g_in(l), N = (uint32_t)g_out(l), SBO = K / 8u * 128u;
+            const uint32_t a_addr = l == 0 ? x_addr : smem_u32(smem + TT_H_OFF + 16384u * (uint32_t)(l - 1));
+            if (r == 0) {
+                tc_fence_after();
+                for (uint32_t k = 0; k < K / 16u; ++k)
+                    umma_bf16(tmem, umma_desc(a_addr + 256u * k, 128u, SBO),
+                              umma_desc(w_addr + tc_woff(l) + 256u * k, 128u, SBO), tt_idesc(N, 0, 0), k);
+                umma_commit(mbar);
+            }
+            ok = tt_wait(mbar, phase);
+            if (!ok) break;
+            const float* bias = sb + G_HID * l;
+            uint32_t v[4][16];
+            for (uint32_t c = 0; c < N / 16u; ++c) tmem_ld16(trow + 16u * c, v[c]);
+            for (uint32_t c = 0; c < N / 16u; ++c) tmem_wait16(v[c]);
+            if (l < G_LAYERS - 1) {
+                unsigned char* H = smem + TT_H_OFF + 16384u * (uint32_t)l;
+                mask[l][0] = mask[l][1] = 0u;
+                for (int ch = 0; ch < G_HID / 8; ++ch) {
+                    uint32_t pk[4];
+                    for (int i = 0; i < 4; ++i) {
+                        const int col = 8 * ch + 2 * i;
+                        const float z0 = __uint_as_float(v[col >> 4][col & 15]) + bias[col];
+                        const float z1 = __uint_as_float(v[(col + 1) >> 4][(col + 1) & 15]) + bias[col + 1];
+                        pk[i] = pack2_relu(z0, z1);
+                        // a ReLU derivative of 1 where the stored activation is nonzero
+                        if (pk[i] & 0xFFFFu) mask[l][col >> 5] |= 1u << (col & 31);
+                        if (pk[i] >> 16) mask[l][(col + 1) >> 5] |= 1u << ((col + 1) & 31);
+                    }
+                    *reinterpret_cast<uint4*>(H + umma_offset(r, 8u * (uint32_t)ch, G_HID)) =
+                        make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                }
+                fence_async_smem();
+            } else {
+                for (int i = 0; i < G_OUT; ++i) raw[i] = __uint_as_float(v[i >> 4][i & 15]) + bias[i];
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (!ok) break;
+        // ---- the output delta (0 for rows past the step's records)
+        {
+            float gr[G_OUT];
+            for (int i = 0; i < G_OUT; ++i) gr[i] = 0.f;
+            if (valid) loss_grad(raw, G.rec.w[rec], G.rec.b[rec], G.rec.weight[rec] * inv_mean, gr);
+            unsigned char* D = smem + TT_D_OFF;
+            for (int ch = 0; ch < G_OUT / 8; ++ch)
+                *reinterpret_cast<uint4*>(D + umma_offset(r, 8u * (uint32_t)ch, G_OUT)) =
+                    make_uint4(pack2(gr[8 * ch], gr[8 * ch + 1]), pack2(gr[8 * ch + 2], gr[8 * ch + 3]),
+                               pack2(gr[8 * ch + 4], gr[8 * ch + 5]), pack2(gr[8 * ch + 6], gr[8 * ch + 7]));
+            fence_async_smem();
+        }
+        __syncthreads();
+        // ---- backward
+        uint32_t cur = 0;
+        for (int l = G_LAYERS - 1; l >= 0 && ok; --l) {
+            const uint32_t out_l = (uint32_t)g_out(l), in_l = (uint32_t)g_in(l);
+            unsigned char* Dc = smem + TT_D_OFF + 16384u * cur;
+            // bias gradient: the sum of this layer's delta over the tile (bf16 as stored)
+            if (r < out_l) {
+                float acc = 0.f;
+                for (uint32_t row = 0; row < 128u; ++row)
+                    acc += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(Dc + umma_offset(row, r, out_l)));
+                db[l] += acc;
+            }
+            const uint32_t d_addr = smem_u32(Dc);
+            const uint32_t in_addr = l == 0 ? x_addr : smem_u32(smem + TT_H_OFF + 16384u * (uint32_t)(l - 1));
+            const uint32_t d_lbo = out_l / 8u * 128u, in_lbo = in_l / 8u * 128u;
+            if (r == 0) {
+                tc_fence_after();
+                if (l > 0) {
+                    // delta_l W_l: A = delta_l (K-major, k = output), B = W_l read MN-major (n = input)
+                    for (uint32_t k = 0; k < out_l / 16u; ++k)
+                        umma_bf16(tmem, umma_desc(d_addr + 256u * k, 128u, d_lbo),
+                                  umma_desc(w_addr + tc_woff(l) + 2u * in_lbo * k, in_lbo, 128u), tt_idesc(in_l, 0, 1),
+                                  k);
+                }
+                // dW_l += delta_l^T a_{l-1}: both read MN-major, k = record
+                for (uint32_t k = 0; k < 8u; ++k)
+                    umma_bf16(tmem + tt_dw_col(l), umma_desc(d_addr + 2u * d_lbo * k, d_lbo, 128u),
+                              umma_desc(in_addr + 2u * in_lbo * k, in_lbo, 128u), tt_idesc(in_l, 1, 1),
+                              (first && k == 0) ? 0u : 1u);
+                umma_commit(mbar);
+            }
+            ok = tt_wait(mbar, phase);
+            if (!ok || l == 0) break;
+            // delta_{l-1} = (delta_l W_l) * relu'(a_{l-1}) into the other buffer
+            uint32_t v[4][16];
+            for (uint32_t c = 0; c < 4u; ++c) tmem_ld16(trow + 16u * c, v[c]);
+            for (uint32_t c = 0; c < 4u; ++c) tmem_wait16(v[c]);
+            unsigned char* Dn = smem + TT_D_OFF + 16384u * (cur ^ 1u);
+            for (int ch = 0; ch < G_HID / 8; ++ch) {
+                uint32_t pk[4];
+                for (int i = 0; i < 4; ++i) {
+                    const int col = 8 * ch + 2 * i;
+                    const float g0 = (mask[l - 1][col >> 5] >> (col & 31)) & 1u ? __uint_as_float(v[col >> 4][col & 15]) : 0.f;
+                    const float g1 = (mask[l - 1][(col + 1) >> 5] >> ((col + 1) & 31)) & 1u
+                                         ? __uint_as_float(v[(col + 1) >> 4][(col + 1) & 15])
+                                         : 0.f;
+                    pk[i] = pack2(g0, g1);
+                }
+                *reinterpret_cast<uint4*>(Dn + umma_offset(r, 8u * (uint32_t)ch, G_HID)) =
+                    make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            }
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            cur ^= 1u;
+        }
+        if (!ok) break;
+        first = false;
+        tc_fence_before();
+        __syncthreads();  // the next tile overwrites the operands of this tile's last products
+    }
+    if (ok && !first) {
+        // the block's weight gradients: TMEM lane r holds output row r of each dW_l
+        for (int l = 0; l < G_LAYERS; ++l) {
+            const uint32_t out_l = (uint32_t)g_out(l), in_l = (uint32_t)g_in(l);
+            float* gw = G.net.grad + g_woff(l);
+            for (uint32_t c0 = 0; c0 < in_l; c0 += 16u) {
+                uint32_t v[16];
+                tmem_ld16(trow + tt_dw_col(l) + c0, v);
+                tmem_wait16(v);
+                if (r < out_l)
+                    for (int i = 0; i < 16; ++i) atomicAdd(gw + r * in_l + c0 + (uint32_t)i, __uint_as_float(v[i]));
+            }
+            if (r < out_l && db[l] != 0.f) atomicAdd(G.net.grad + g_boff(l) + r, db[l]);
+        }
+    }
+    if (!ok) {
+        if (r == 0 && G.err) atomicOr(G.err, ERR_MMA_TIMEOUT);
+        mbar_wait(mbar, phase, TC_WAIT_POLLS);  // MMAs still in flight: one more bounded wait
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 0) tmem_dealloc(tmem, TT_TMEM_COLS);
+}
+
 // ---------------------------------------------------------------- launchers
 size_t guide_infer_smem() {
     return SW_ELEMS * 2 + SB_ELEMS * 4 + GWI * IN_BYTES;
@@ -1425,6 +1665,8 @@ cudaError_t guide_configure() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_guide_fwdbwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)guide_train_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM);
     return e;
 }
 
@@ -1439,10 +1681,15 @@ namespace {
 int launch_train_steps(const GuideArgs& g, int sm, int adam, cudaStream_t st) {
     int n = 0;
     for (int k = 0; k < (int)std::max(g.steps, 1u); ++k) {
-        k_guide_fwdbwd<<<sm, GWT * 32, guide_train_smem(), st>>>(g, k);
-        dim3 wg(WGRAD_BLOCKS, 6);
-        k_guide_wgrad<<<wg, 256, 0, st>>>(g, k);
-        n += 2;
+        if (g.tc_train) {
+            k_guide_train_tc<<<sm, 128, TT_SMEM, st>>>(g, k);
+            n += 1;
+        } else {
+            k_guide_fwdbwd<<<sm, GWT * 32, guide_train_smem(), st>>>(g, k);
+            dim3 wg(WGRAD_BLOCKS, 6);
+            k_guide_wgrad<<<wg, 256, 0, st>>>(g, k);
+            n += 2;
+        }
         if (!adam) continue;
         k_guide_adam<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g, k);
         ++n;

@@ -101,6 +101,8 @@ struct GuideArgs {
     uint32_t batch;          // training samples recorded per frame (<= G_REC_CAP)
     uint32_t steps;          // Adam steps per frame, each on a consecutive 1/steps of the records
     int tc;                  // inference on tcgen05 / tensor memory (else mma.sync)
+    int tc_train;            // training step on tcgen05 (k_guide_train_tc; else mma.sync + split-K)
+    uint32_t* err;           // device error word (an MMA wait that gave up), may be null
 };
 static_assert(G_NPARAMS % 8 == 0 && g_woff(1) % 8 == 0 && g_woff(2) % 8 == 0 && g_woff(3) % 8 == 0 &&
                   g_woff(4) % 8 == 0,
