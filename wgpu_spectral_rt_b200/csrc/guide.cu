@@ -1429,8 +1429,11 @@ constexpr uint32_t TT_H_OFF = TT_X_OFF + 32768u;          // a0..a3, 4 x (128 x 
 constexpr uint32_t TT_D_OFF = TT_H_OFF + 4u * 16384u;     // deltas, 2 x (128 x 64), ping-pong
 // The weight-gradient product reads its A (out x 128 records) with M = 128
 // rows; rows beyond the layer's outputs are other bytes of the buffers (their
-// products are never read), so 2 KB of slack follow the second delta buffer.
-constexpr uint32_t TT_B_OFF = TT_D_OFF + 2u * 16384u + 2048u;
+// products are never read).  The slack after the second delta buffer keeps
+// every operand read of the MN-major products inside the block's shared
+// memory even if the two stride fields were taken the other way round
+// (MN stride = the K-block stride): 30 KB.
+constexpr uint32_t TT_B_OFF = TT_D_OFF + 2u * 16384u + 30720u;
 constexpr uint32_t TT_BAR_OFF = TT_B_OFF + SB_ELEMS * 4;  // mbarrier, then the TMEM base
 constexpr uint32_t TT_SMEM = TT_BAR_OFF + 16u;
 constexpr uint32_t TT_TMEM_COLS = 512;
