@@ -89,7 +89,10 @@ MISS = 0xFFFFFFFF
 #          magnitude of the FP32 coordinates involved; cos = cosine between
 #          the ray and the triangle's normal: a plane position uncertain by d
 #          moves the hit point d / |cos| along a grazing ray)
-#   range  the oracle's hit lies within RANGE_REL * scale of tmin or tmax
+#   range  the oracle's or the GPU's triangle is met within
+#          RANGE_REL * scale * (1 + 1 / |cos|) of tmin or tmax (a ray leaving
+#          a surface nearly tangentially meets its own triangle at
+#          t = offset / |cos|, which FP32 rounding puts on either side of tmin)
 # Hit distances of agreeing ids: |dt| <= 1e-5 t + EDGE_REL * scale / |cos|.
 EDGE_REL = 2.0 ** -19
 RANGE_REL = 2.0 ** -19
@@ -110,13 +113,17 @@ def closest_hit_parity(scene, oracle, rays, brute=True, hits=None):
     scale = np.maximum(1.0, np.maximum(np.abs(o).max(1), np.abs(x).max(1)))
     with np.errstate(invalid="ignore"):
         tie = hit_o & (np.abs(t2 - t) < 1e-6)
-    _, e_o, c_o = oracle.tri_probe(rays, prim, with_cos=True)
-    _, e_g, c_g = oracle.tri_probe(rays, pg, with_cos=True)
+    tp_o, e_o, c_o = oracle.tri_probe(rays, prim, with_cos=True)
+    tp_g, e_g, c_g = oracle.tri_probe(rays, pg, with_cos=True)
     with np.errstate(divide="ignore"):
         slack_o = EDGE_REL * scale * (1.0 + 1.0 / np.maximum(c_o, 1e-12))
         slack_g = EDGE_REL * scale * (1.0 + 1.0 / np.maximum(c_g, 1e-12))
     edge = (np.abs(e_o) < slack_o) | (np.abs(e_g) < slack_g)
-    rng_ = hit_o & ((np.abs(t - rays[:, 3]) < RANGE_REL * scale) | (np.abs(t - rays[:, 7]) < RANGE_REL * scale))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r_o = RANGE_REL * scale * (1.0 + 1.0 / np.maximum(c_o, 1e-12))
+        r_g = RANGE_REL * scale * (1.0 + 1.0 / np.maximum(c_g, 1e-12))
+        rng_ = ((np.abs(tp_o - rays[:, 3]) < r_o) | (np.abs(tp_o - rays[:, 7]) < r_o) |
+                (np.abs(tp_g - rays[:, 3]) < r_g) | (np.abs(tp_g - rays[:, 7]) < r_g))
     excluded = tie | edge | rng_
     mismatch = pg != prim
     both = hit_o & hit_g & (pg == prim)
