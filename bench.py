@@ -335,6 +335,7 @@ def batched_section(srt, ctx, stream, n_scenes=32, seed=12345):
         batch.render(cams(0), active=[k * 32 <= x for x in spp])
     for r in batch.renderers:
         r.reset_accumulation()
+        r.reset_stats()
 
     def run():
         for f in range(iters):
@@ -374,7 +375,7 @@ def guided_section(seconds=15.0, ref_spp=8192):
             "time_fraction_ref_noise_subtracted": (round(d["time_fraction_ref_noise_subtracted"], 3)
                                                    if d["time_fraction_ref_noise_subtracted"] else None),
             "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"],
-            "guided_bounces": d["guide_bounces"] or "all"}
+            "guided_bounces": d["guide_bounces"] or "0..4 (the library default)"}
 
 
 def batched_guided_section(seconds=2.0, ref_spp=256):

@@ -514,10 +514,12 @@ srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batc
  * split into `steps` consecutive sub-batches, one forward/backward, gradient
  * and Adam step each. */
 srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t steps);
-/* Guided bounces (>= 1, default all): the guide samples the Lambert
+/* Guided bounces (>= 1, default 5): the guide samples the Lambert
  * continuations of bounces < `bounces` (and trains on them); later Lambert
- * vertices sample the cosine lobe as the reference does.  The estimator stays
- * unbiased either way; fewer guided bounces trade variance for time. */
+ * vertices sample the cosine lobe as the reference does, and from the tail
+ * kernel's first bounce on (srt_renderer_set_tail) the tail kernel runs them.
+ * The estimator stays unbiased either way; fewer guided bounces trade
+ * variance for time. */
 srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces);
 /* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
  * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),
