@@ -357,7 +357,7 @@ def batched_section(srt, ctx, stream, n_scenes=32, seed=12345):
                          "a speed knob of the compatible renderer"}
 
 
-def guided_section(seconds=15.0, ref_spp=8192):
+def guided_section(seconds=30.0, ref_spp=8192):
     """C4 at full size (1920x1080, depth 16): equal-time relMSE of guided vs
     plain against an FP64 reference of ref_spp frames rendered in two halves
     (their difference measures the reference's own noise, reported and
@@ -375,7 +375,8 @@ def guided_section(seconds=15.0, ref_spp=8192):
             "time_fraction_ref_noise_subtracted": (round(d["time_fraction_ref_noise_subtracted"], 3)
                                                    if d["time_fraction_ref_noise_subtracted"] else None),
             "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"],
-            "guided_bounces": d["guide_bounces"] or "0..4 (the library default)"}
+            "tail_first_plain": d["plain"]["tail_first"], "tail_first_guided": d["guided"]["tail_first"],
+            "guided_bounces": d["guide_bounces"] or "every bounce before the tail kernel (the library default)"}
 
 
 def batched_guided_section(seconds=2.0, ref_spp=256):
@@ -452,6 +453,10 @@ def main(argv=None):
 
     for k in range(args.warmup):
         r.render(cam_u(k))
+        if k == 0:
+            # the renderer picks its tail start from the first frame's path
+            # counts; they are back before the second warm-up frame
+            ctx.synchronize()
     ctx.synchronize()
     r.reset_stats()
     start = torch.cuda.Event(enable_timing=True)
@@ -505,10 +510,16 @@ def main(argv=None):
                                                                flags=srt.FLAG_STAGE_TIMING))
         rc = srt.Renderer(ctx, scene, w, h, srt.default_params(max_depth=depth, photons_per_frame=photons,
                                                                flags=srt.FLAG_COUNT_VISITS))
+        # one frame first: the renderers choose their tail start from its path counts
+        rt.render(cam_u(0))
+        rc.render(cam_u(0))
+        ctx.synchronize()
+        rt.reset_stats()
+        rc.reset_stats()
         nf = 4
         for k in range(nf):
-            rt.render(cam_u(k))
-            rc.render(cam_u(k))
+            rt.render(cam_u(1 + k))
+            rc.render(cam_u(1 + k))
         s1, s2 = rt.stats(), rc.stats()
         bt, bc = rt.bounce_stats(), rc.bounce_stats()
         tail = int(s1["tail_first"])  # bounces >= tail run in the tail kernel

@@ -393,9 +393,18 @@ srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_stats* out)
  * kernel that follows each remaining path to its end (closest hit, shading,
  * shadow ray) instead of one closest-hit, shading and shadow launch per
  * bounce: the same arithmetic per path, so the same image, with the latency
- * of the short last bounces paid once.  Default 5; 0 = bounce by bounce.
- * Not used with SRT_FLAG_RAY_SORT, nor where guided bounces reach it
- * (srt_renderer_guide_set_bounces).  No reference counterpart. */
+ * of the short last bounces paid once.  It runs one path per thread at a
+ * time, so it pays once the live paths fit in about one wave of it.
+ * SRT_TAIL_AUTO (the default): the renderer reads back the path counts of
+ * its first frame without waiting for them and, once they are there, starts
+ * the tail at the first bounce >= 1 whose live paths fit in one wave of the
+ * tail kernel's resident threads (a batch: the scenes' paths summed), for a
+ * guiding renderer not before bounce 5; frames before that run bounce by
+ * bounce.  0 = bounce by bounce.  Not used with
+ * SRT_FLAG_RAY_SORT, nor where a set number of guided bounces reaches it
+ * (srt_renderer_guide_set_bounces).  srt_stats.tail_first reports the bounce
+ * in use.  No reference counterpart. */
+#define SRT_TAIL_AUTO 0xFFFFFFFFu
 srt_status srt_renderer_set_tail(srt_renderer* r, uint32_t first_bounce);
 srt_status srt_renderer_reset_stats(srt_renderer* r);
 /* The photon set of the last frame in emission order (photon_emit.wgsl
@@ -514,12 +523,14 @@ srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batc
  * split into `steps` consecutive sub-batches, one forward/backward, gradient
  * and Adam step each. */
 srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t steps);
-/* Guided bounces (>= 1, default 5): the guide samples the Lambert
- * continuations of bounces < `bounces` (and trains on them); later Lambert
- * vertices sample the cosine lobe as the reference does, and from the tail
- * kernel's first bounce on (srt_renderer_set_tail) the tail kernel runs them.
- * The estimator stays unbiased either way; fewer guided bounces trade
- * variance for time. */
+/* Guided bounces: the guide samples the Lambert continuations of bounces <
+ * `bounces` (and trains on them); later Lambert vertices sample the cosine
+ * lobe as the reference does.  SRT_GUIDE_BOUNCES_AUTO (0, the default): every
+ * bounce before the tail kernel's first one (srt_renderer_set_tail), which
+ * runs the rest unguided; a set number >= 1 keeps the tail from starting
+ * before it.  The estimator stays unbiased either way; fewer guided bounces
+ * trade variance for time. */
+#define SRT_GUIDE_BOUNCES_AUTO 0u
 srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces);
 /* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
  * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),

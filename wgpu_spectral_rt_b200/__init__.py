@@ -131,6 +131,8 @@ BVH_LBVH = 1
 
 GUIDE_INFER_MMA_SYNC = 0
 GUIDE_INFER_TCGEN05 = 1
+TAIL_AUTO = 0xFFFFFFFF  # srt_renderer_set_tail: chosen from the first frame's path counts
+GUIDE_BOUNCES_AUTO = 0  # srt_renderer_guide_set_bounces: every bounce before the tail
 GUIDE_TRAIN_MMA_SYNC = 0
 GUIDE_TRAIN_TCGEN05 = 1
 
@@ -573,7 +575,8 @@ class Renderer:
                 "tris": np.array(s.tris, np.uint64), "ms": np.array(s.ms, np.float64)}
 
     def set_tail(self, first_bounce: int) -> None:
-        """Bounces >= first_bounce in one persistent kernel per frame (0: bounce by bounce)."""
+        """Bounces >= first_bounce in one persistent kernel per frame (0: bounce by bounce; TAIL_AUTO, the
+        default: chosen from the first frame's path counts)."""
         _check(lib().srt_renderer_set_tail(self.h, first_bounce), self.ctx.h)
 
     def reset_stats(self):
@@ -643,7 +646,8 @@ class Renderer:
         _check(lib().srt_renderer_guide_set_steps(self.h, steps), self.ctx.h)
 
     def set_guide_bounces(self, bounces: int) -> None:
-        """Guide the Lambert continuations of bounces < `bounces` only (later ones sample the cosine lobe)."""
+        """Guide the Lambert continuations of bounces < `bounces` only (later ones sample the cosine lobe);
+        GUIDE_BOUNCES_AUTO (0, the default): every bounce before the tail kernel's first."""
         _check(lib().srt_renderer_guide_set_bounces(self.h, bounces), self.ctx.h)
 
     def configure_guide(self, lr: float | None = None, batch: int | None = None) -> None:

@@ -674,17 +674,23 @@ extern "C" srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width) {
 }
 
 // ====================================================================== renderer
-// First bounce of the tail kernel by default (launch_tail): the reference's
-// Russian roulette starts after bounce 3, so from bounce 5 on few paths live.
-#ifndef SRT_TAIL_FIRST_DEFAULT
-#define SRT_TAIL_FIRST_DEFAULT 5u
+// The tail kernel (launch_tail) follows each remaining path through its
+// last bounces in one launch, one thread per path at a time: it pays once
+// the live paths fit in about one wave of it, and costs where many long paths
+// remain (1080p: config 2 from bounce 5, 118k paths, 10.76 vs 11.04 ms per
+// frame; the caustic-slab scene from bounce 5, 202k paths, 7.05 vs 5.93 ms,
+// from bounce 7, 69k paths, 5.92 ms).  SRT_TAIL_AUTO (the default) starts it
+// at the first bounce whose live paths in the renderer's first frame number
+// at most SRT_TAIL_WAVES waves of the tail kernel's resident threads.
+#ifndef SRT_TAIL_WAVES
+#define SRT_TAIL_WAVES 1.0
 #endif
-// Guided bounces by default: the first five, so that a guiding renderer's
-// remaining bounces run in the tail kernel like a plain renderer's (C4 at
-// 960x540, 8-s arms: time to the plain error 0.63 of the plain time with
-// bounces 0..4 guided, 0.65 with 0..2, 0.72 with all).
-#ifndef SRT_GUIDE_BOUNCES_DEFAULT
-#define SRT_GUIDE_BOUNCES_DEFAULT 5u
+// A guiding renderer's automatic tail starts no earlier than this bounce:
+// its guided bounces end where the tail starts, and the guide's gain is in
+// the first bounces (the caustic-slab scene at 1080p: relMSE at equal time
+// 0.0500 with bounces 0..4 guided, 0.0497 with all, 0.0487 with 0..7).
+#ifndef SRT_GUIDE_TAIL_MIN
+#define SRT_GUIDE_TAIL_MIN 5u
 #endif
 // Frames enqueue independent stages on two branches (srt_renderer::record_overlapped).
 #ifndef SRT_FRAME_OVERLAP
@@ -747,6 +753,8 @@ struct srt_renderer {
 
     ~srt_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (counts_ev) cudaEventDestroy(counts_ev);
+        if (counts_host) cudaFreeHost(counts_host);
         if (cap_stream) cudaStreamDestroy(cap_stream);
         if (side_stream) cudaStreamDestroy(side_stream);
         if (fork_ev) cudaEventDestroy(fork_ev);
@@ -777,15 +785,73 @@ struct srt_renderer {
 
     // Enqueues one frame (after the camera upload).  stage timing: events
     // between stages (only when `timed`, which keeps every stage in order).
-    // First bounce handled by the tail kernel (launch_tail), or max_depth for
-    // none: a setting of the renderer, used where the whole remainder of a
-    // path can run in one kernel (no ray reordering, no guided vertex left).
-    uint32_t tail_first = SRT_TAIL_FIRST_DEFAULT;
+    // First bounce handled by the tail kernel (launch_tail): SRT_TAIL_AUTO,
+    // 0 (none) or a bounce; used where the whole remainder of a path can run
+    // in one kernel (no ray reordering, no guided vertex left).  tail_auto is
+    // the automatic choice, 0 until the first frame's path counts are back.
+    uint32_t tail_first = SRT_TAIL_AUTO;
+    uint32_t tail_auto = 0;
+    uint32_t* counts_host = nullptr;  // pinned: paths entering each bounce of one frame
+    cudaEvent_t counts_ev = nullptr;
+    int counts_state = 0;             // 0: not requested, 1: copy in flight, 2: read
+    // guided bounces follow the tail: every bounce before it (the tail samples
+    // cosine lobes), unless srt_renderer_guide_set_bounces set a number
+    bool guide_bounces_auto = true;
     uint32_t tail_start() const {
-        const uint32_t t = tail_first;
+        const uint32_t t = tail_first == SRT_TAIL_AUTO ? tail_auto : tail_first;
         if (t == 0u || t >= p.max_depth || args.ray_sort) return p.max_depth;
-        if (args.guiding && args.guide_bounces > t) return p.max_depth;
+        if (args.guiding && !guide_bounces_auto && args.guide_bounces > t) return p.max_depth;
         return t;
+    }
+    // The automatic tail start from one frame's path counts (paths[b] = paths
+    // entering bounce b): the first bounce >= 1 whose paths fit in
+    // SRT_TAIL_WAVES waves of the tail kernel, 0 if none.
+    static uint32_t choose_tail(const uint32_t* paths, uint32_t max_depth, double capacity) {
+        for (uint32_t b = 1; b < max_depth; ++b)
+            if ((double)paths[b] <= SRT_TAIL_WAVES * capacity) return b;
+        return 0u;
+    }
+    // The automatic choice t for this renderer (guiding: not before SRT_GUIDE_TAIL_MIN).
+    uint32_t auto_tail_for(uint32_t t) const {
+        return (args.guiding && t != 0u) ? std::max<uint32_t>(t, SRT_GUIDE_TAIL_MIN) : t;
+    }
+    // Drops the captured frame (its shape changed).
+    void drop_graph() {
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+    }
+    // The guided bounces when they follow the tail.
+    void sync_guide_bounces() {
+        if (!args.guiding || !guide_bounces_auto) return;
+        const uint32_t gb = std::min<uint32_t>(tail_start(), MAX_BOUNCES + 1);
+        if (args.guide_bounces != gb) {
+            args.guide_bounces = gb;
+            args_gen += 1;
+            drop_graph();
+        }
+    }
+    // SRT_TAIL_AUTO: after the first frame, read its path counts back without
+    // waiting and, once they are there, choose the tail (the next frame is
+    // captured with it; the image does not change).
+    void auto_tail_before_frame() {
+        if (tail_first != SRT_TAIL_AUTO || counts_state != 1) return;
+        if (cudaEventQuery(counts_ev) != cudaSuccess) return;
+        counts_state = 2;
+        const uint32_t t = auto_tail_for(choose_tail(counts_host, p.max_depth, (double)tail_threads(args)));
+        if (t != tail_auto) {
+            tail_auto = t;
+            drop_graph();
+            sync_guide_bounces();
+        }
+    }
+    void auto_tail_after_frame(cudaStream_t st) {
+        if (tail_first != SRT_TAIL_AUTO || counts_state != 0) return;
+        if (cudaMemcpyAsync(counts_host, counters->paths, sizeof(uint32_t) * (MAX_BOUNCES + 1), cudaMemcpyDeviceToHost,
+                            st) == cudaSuccess &&
+            cudaEventRecord(counts_ev, st) == cudaSuccess)
+            counts_state = 1;
     }
 
     // Enqueues one frame (after the camera upload).  With stage timing,
@@ -1089,7 +1155,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
         r->guide.train = (p.flags & SRT_FLAG_GUIDE_FROZEN) ? 0 : 1;
         r->guide.err = r->err;
         a.guiding = 1;
-        a.guide_bounces = SRT_GUIDE_BOUNCES_DEFAULT;
+        a.guide_bounces = std::min<uint32_t>(p.max_depth, MAX_BOUNCES + 1);  // every bounce until a tail is chosen
         a.guide = r->guide;
     }
     size_t n_events = 5 + 3 * (size_t)p.max_depth;
@@ -1102,6 +1168,8 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     CUDA_TRY(c, cudaStreamCreateWithFlags(&r->train_stream, cudaStreamNonBlocking));
     CUDA_TRY(c, cudaEventCreateWithFlags(&r->tfork_ev, cudaEventDisableTiming));
     CUDA_TRY(c, cudaEventCreateWithFlags(&r->tjoin_ev, cudaEventDisableTiming));
+    CUDA_TRY(c, cudaMallocHost(&r->counts_host, sizeof(uint32_t) * (MAX_BOUNCES + 1)));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&r->counts_ev, cudaEventDisableTiming));
     if (env_fault("launch")) return fail(c, SRT_ERR_CUDA, "injected launch failure");
     ctx_retain(c);
     *out = r.release();
@@ -1123,6 +1191,7 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
     srt_ctx* c = r->ctx;
     cudaSetDevice(c->device);
     r->refresh_scene();
+    r->auto_tail_before_frame();
     cudaStream_t st = c->stream;
     int slot = r->ring_i++ & 3;
     CUDA_TRY(c, cudaEventSynchronize(r->ring_ev[slot]));
@@ -1164,6 +1233,7 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
             }
         }
     }
+    r->auto_tail_after_frame(st);
     // an overlapped guided frame leaves its training steps to the next frame
     r->train_pending = r->args.guiding && !timed && SRT_FRAME_OVERLAP;
     r->trace_launches += r->tail_start();
@@ -1349,10 +1419,9 @@ extern "C" srt_status srt_renderer_set_tail(srt_renderer* r, uint32_t first_boun
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     r->tail_first = first_bounce;
-    if (r->graph) {  // the tail shapes the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // the tail shapes the captured frame
+    r->args_gen += 1;
+    r->sync_guide_bounces();
     return SRT_OK;
 }
 
@@ -1648,18 +1717,17 @@ extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t ste
 }
 
 extern "C" srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces) {
-    if (!r || bounces < 1) return SRT_ERR_INVALID_ARG;
+    if (!r) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
     if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
+    r->guide_bounces_auto = bounces == SRT_GUIDE_BOUNCES_AUTO;
+    if (!r->guide_bounces_auto) r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
     r->args_gen += 1;
-    if (r->graph) {  // the guided bounces shape the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // the guided bounces shape the captured frame
+    r->sync_guide_bounces();
     return SRT_OK;
 }
 
@@ -1944,6 +2012,12 @@ extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_came
 // and shadow rays of all scenes are traced in one launch per bounce
 // (k_trace_multi).  The graph is re-captured when the set of active scenes
 // or the tuning changes.
+// The batch shades all its scenes' vertices of a bounce in one launch
+// (k_shade_multi); 0: one shading launch per scene on its graph branch.
+#ifndef SRT_BATCH_SHADE_MULTI
+#define SRT_BATCH_SHADE_MULTI 1
+#endif
+
 struct srt_batch {
     srt_ctx* ctx = nullptr;
     std::vector<srt_renderer*> r;
@@ -1952,8 +2026,9 @@ struct srt_batch {
     cudaEvent_t up_ev[2] = {};
     int up_i = 0;
     MultiTraceItem* items_dev = nullptr;  // [2 kinds][MAX_BOUNCES][MAX_BATCH]
-    uint32_t* fetch_dev = nullptr;        // [3][MAX_BOUNCES]: closest-hit, shadow, guide chunk counters
+    uint32_t* fetch_dev = nullptr;        // [4][MAX_BOUNCES]: closest-hit, shadow, guide, shading chunk counters
     FrameArgs* guide_items_dev = nullptr; // [MAX_BATCH] frame arguments of the guided renderers
+    FrameArgs* shade_items_dev = nullptr; // [MAX_BATCH] frame arguments of the active renderers
     std::vector<uint32_t> graph_gen;      // the renderers' args_gen at capture
     std::vector<cudaStream_t> side;
     cudaStream_t cap = nullptr;
@@ -1967,6 +2042,13 @@ struct srt_batch {
     srt_batch_tuning tune{8, 32, 0.0f, 0, 8};
     uint32_t max_depth = 0;
     bool small_stack = true;
+    // SRT_TAIL_AUTO for the batch: the first iteration's path counts of every
+    // active scene (each renderer's counts_host), summed, choose one tail
+    // start for the scenes whose renderers leave it automatic
+    int counts_state = 0;  // 0: not requested, 1: copies in flight, 2: read
+    cudaEvent_t counts_ev = nullptr;
+    std::vector<uint8_t> counts_active;
+    bool recapture = false;
 
     ~srt_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1977,6 +2059,7 @@ struct srt_batch {
         if (ovl) cudaStreamDestroy(ovl);
         if (ovl_fork) cudaEventDestroy(ovl_fork);
         if (ovl_join) cudaEventDestroy(ovl_join);
+        if (counts_ev) cudaEventDestroy(counts_ev);
         for (auto e : join_ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : up_ev)
@@ -1986,6 +2069,7 @@ struct srt_batch {
         cudaFree(items_dev);
         cudaFree(fetch_dev);
         cudaFree(guide_items_dev);
+        cudaFree(shade_items_dev);
         for (srt_renderer* x : r) {
             if (x) {
                 x->batch_owned = false;
@@ -2042,7 +2126,7 @@ struct srt_batch {
             }
             for (int k = 0; k < na; ++k) cudaStreamWaitEvent(cap, join_ev[k], 0);
         };
-        cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 3 * MAX_BOUNCES, cap);
+        cudaMemsetAsync(fetch_dev, 0, sizeof(uint32_t) * 4 * MAX_BOUNCES, cap);
         for (int k = 0; k < na; ++k) r[act[k]]->record_clear(cap);
         auto closest = [&](uint32_t b, cudaStream_t s) {
             return launch_trace_multi(items_dev + (size_t)b * MAX_BATCH, na, 0, small_stack, fetch_dev + b,
@@ -2069,7 +2153,10 @@ struct srt_batch {
         uint32_t tail = 0;
         for (int k = 0; k < na; ++k) tail = std::max(tail, r[act[k]]->tail_start());
         for (uint32_t b = 0; b < max_depth; ++b) {
-            fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
+            if (SRT_BATCH_SHADE_MULTI)
+                n += launch_shade_multi(shade_items_dev, na, b, fetch_dev + 3 * MAX_BOUNCES + b, c->sm_count, cap);
+            else
+                fork_join([b](srt_renderer* x, cudaStream_t s) { return x->record_shade(b, s, false); });
             if (ng && b + 1 < guide_depth)
                 n += launch_guide_infer_multi(guide_items_dev, ng, b, fetch_dev + 2 * MAX_BOUNCES + b, c->sm_count,
                                               cap);
@@ -2094,6 +2181,13 @@ struct srt_batch {
         if (ng) n += launch_guide_train_multi(guide_items_dev, ng, guide_steps, c->sm_count, cap);
         cudaError_t e = cudaStreamEndCapture(cap, &g);
         CUDA_TRY(c, e);
+        {
+            std::vector<FrameArgs> sargs;
+            for (int k = 0; k < na; ++k) sargs.push_back(r[act[k]]->args);
+            e = cudaMemcpy(shade_items_dev, sargs.data(), na * sizeof(FrameArgs), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) cudaGraphDestroy(g);
+            CUDA_TRY(c, e);
+        }
         if (ng) {
             std::vector<FrameArgs> gargs;
             for (srt_renderer* x : guided) gargs.push_back(x->args);
@@ -2108,6 +2202,7 @@ struct srt_batch {
         graph_gen.clear();
         for (srt_renderer* x : r) graph_gen.push_back(x->args_gen);
         graph_launches = n;
+        recapture = false;
         return SRT_OK;
     }
 
@@ -2122,7 +2217,8 @@ struct srt_batch {
         for (uint8_t a : active) any = any || a;
         if (!any) return SRT_OK;
         for (srt_renderer* x : r) x->refresh_scene();  // trees rebuilt since the capture
-        bool stale = graph_gen.size() != n;
+        auto_tail_before();
+        bool stale = recapture || graph_gen.size() != n;
         for (size_t i = 0; i < n && !stale; ++i) stale = graph_gen[i] != r[i]->args_gen;
         if (!graph || active != graph_active || stale) {
             srt_status s = capture(active);
@@ -2143,7 +2239,44 @@ struct srt_batch {
             x->frame_count += 1;
         }
         if (!r.empty()) r[0]->launches += (uint64_t)graph_launches;
+        auto_tail_after(active);
         return SRT_OK;
+    }
+
+    void auto_tail_after(const std::vector<uint8_t>& active) {
+        if (counts_state != 0) return;
+        bool any_auto = false;
+        for (srt_renderer* x : r) any_auto = any_auto || x->tail_first == SRT_TAIL_AUTO;
+        if (!any_auto) return;
+        for (size_t i = 0; i < r.size(); ++i)
+            if (active[i] && cudaMemcpyAsync(r[i]->counts_host, r[i]->counters->paths,
+                                             sizeof(uint32_t) * (MAX_BOUNCES + 1), cudaMemcpyDeviceToHost,
+                                             ctx->stream) != cudaSuccess)
+                return;
+        if (cudaEventRecord(counts_ev, ctx->stream) != cudaSuccess) return;
+        counts_active = active;
+        counts_state = 1;
+    }
+    void auto_tail_before() {
+        if (counts_state != 1 || cudaEventQuery(counts_ev) != cudaSuccess) return;
+        counts_state = 2;
+        std::vector<uint32_t> sum(MAX_BOUNCES + 1, 0u);
+        uint32_t depth = 0;
+        int first = -1;
+        for (size_t i = 0; i < r.size(); ++i) {
+            if (!counts_active[i]) continue;
+            if (first < 0) first = (int)i;
+            depth = std::max(depth, r[i]->p.max_depth);
+            for (int b = 0; b <= MAX_BOUNCES; ++b) sum[b] += r[i]->counts_host[b];
+        }
+        if (first < 0) return;
+        const uint32_t t = srt_renderer::choose_tail(sum.data(), depth, (double)tail_threads(r[first]->args));
+        for (srt_renderer* x : r) {
+            if (x->tail_first != SRT_TAIL_AUTO || x->tail_auto == x->auto_tail_for(t)) continue;
+            x->tail_auto = x->auto_tail_for(t);
+            x->sync_guide_bounces();
+            recapture = true;
+        }
     }
 };
 
@@ -2161,8 +2294,10 @@ extern "C" srt_status srt_batch_create(srt_ctx* c, uint32_t n, srt_scene* const*
     CUDA_TRY(c, cudaMemset(B->cams_dev, 0, n * sizeof(srt_camera_uniform)));
     for (auto& e : B->up_ev) CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CUDA_TRY(c, dev_alloc(&B->items_dev, (size_t)2 * MAX_BOUNCES * MAX_BATCH));
-    CUDA_TRY(c, dev_alloc(&B->fetch_dev, (size_t)3 * MAX_BOUNCES));
+    CUDA_TRY(c, dev_alloc(&B->fetch_dev, (size_t)4 * MAX_BOUNCES));
     CUDA_TRY(c, dev_alloc(&B->guide_items_dev, (size_t)MAX_BATCH));
+    CUDA_TRY(c, dev_alloc(&B->shade_items_dev, (size_t)MAX_BATCH));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&B->counts_ev, cudaEventDisableTiming));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
     CUDA_TRY(c, cudaEventCreateWithFlags(&B->fork_ev, cudaEventDisableTiming));
     CUDA_TRY(c, cudaStreamCreateWithFlags(&B->ovl, cudaStreamNonBlocking));

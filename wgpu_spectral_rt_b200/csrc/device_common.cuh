@@ -493,9 +493,11 @@ SRT_DEV float2 fma2(float2 a, float2 b, float2 c) {
 }
 
 // Child bookkeeping of a node visit in one pass after the slab tests
-// (SRT_TRAV_LEAN) instead of per child.
+// (SRT_TRAV_LEAN, the default: a hit mask from the child loop, then the octant
+// order of the internal children and the leaves' triangle bits once per node)
+// instead of per child (config-2 closest-hit 3.35 vs 3.43 ms per frame).
 #ifndef SRT_TRAV_LEAN
-#define SRT_TRAV_LEAN 0
+#define SRT_TRAV_LEAN 1
 #endif
 
 struct TravCounters {

@@ -457,11 +457,10 @@ SRT_DEV VertexOut shade_vertex(const FrameArgs& a, uint32_t id, uint32_t bounce)
 
 // One bounce of every live path: shade_vertex, then the live paths, shadow
 // rays and guided vertices go to their queues (warp-aggregated slots).
+// shade_slot is one thread's vertex: queue position q of `bounce` (q >= n:
+// no vertex; the thread still takes part in the warp's queue pushes).
 template <bool GUIDE>
-__global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(FrameArgs a, uint32_t bounce) {
-    uint32_t n = a.counters->paths[bounce];
-    if (blockIdx.x * blockDim.x >= n) return;
-    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+SRT_DEV void shade_slot(const FrameArgs& a, uint32_t bounce, uint32_t q, uint32_t n) {
     bool valid = q < n;
     uint32_t id = valid ? a.pb.queue[bounce & 1][q] : 0u;
     VertexOut v;
@@ -487,6 +486,57 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(Fra
             a.guide.gv.spec[gslot] = v.g_spec;
             a.guide.gv.id[gslot] = id;
         }
+    }
+}
+
+template <bool GUIDE>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_shade(FrameArgs a, uint32_t bounce) {
+    uint32_t n = a.counters->paths[bounce];
+    if (blockIdx.x * blockDim.x >= n) return;
+    shade_slot<GUIDE>(a, bounce, blockIdx.x * blockDim.x + threadIdx.x, n);
+}
+
+// The shading of many scenes in one launch (the batched renderer): a virtual
+// queue concatenates the scenes' path queues of this bounce, each padded to
+// whole blocks, so a block's chunk belongs to one scene; blocks draw chunks
+// from *fetch and copy that scene's frame arguments into shared memory when
+// the scene changes.  Per vertex the work is k_shade's (guided scenes write
+// their Lambert vertices for the grouped guide inference).
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS)
+    k_shade_multi(const FrameArgs* __restrict__ items, int n_items, uint32_t bounce, uint32_t* __restrict__ fetch) {
+    __shared__ FrameArgs sa;
+    __shared__ uint32_t pre[MAX_BATCH + 1];
+    __shared__ uint32_t chunk;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < n_items; ++i) {
+            pre[i] = acc;
+            acc += (items[i].counters->paths[bounce] + TRACE_BLOCK - 1u) / TRACE_BLOCK;
+        }
+        pre[n_items] = acc;
+    }
+    int cur = -1;
+    constexpr int kWords = (int)(sizeof(FrameArgs) / sizeof(uint32_t));
+    static_assert(sizeof(FrameArgs) % sizeof(uint32_t) == 0, "FrameArgs is copied as words");
+    while (true) {
+        __syncthreads();  // the previous chunk is done with `chunk` and `sa`
+        if (threadIdx.x == 0) chunk = atomicAdd(fetch, 1u);
+        __syncthreads();
+        const uint32_t c = chunk;
+        if (c >= pre[n_items]) break;
+        int sc = 0;
+        while (sc + 1 < n_items && pre[sc + 1] <= c) ++sc;
+        if (sc != cur) {  // block-uniform
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(items + sc);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+            for (int k = (int)threadIdx.x; k < kWords; k += TRACE_BLOCK) dst[k] = src[k];
+            cur = sc;
+            __syncthreads();
+        }
+        const uint32_t n = sa.counters->paths[bounce];
+        const uint32_t q = (c - pre[sc]) * TRACE_BLOCK + threadIdx.x;
+        if (sa.guiding) shade_slot<true>(sa, bounce, q, n);
+        else shade_slot<false>(sa, bounce, q, n);
     }
 }
 
@@ -548,19 +598,25 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TAIL_MIN_BLOCKS) k_tail(Frame
     }
 }
 
+// Resident blocks per SM of one k_tail instantiation (its grid is one wave).
 template <bool GUIDE, bool COUNT, int STACK>
-int launch_tail_t(const FrameArgs& a, uint32_t first, cudaStream_t st) {
-    const size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
-    static int per_sm = 0;  // resident blocks per SM of this instantiation
+int tail_per_sm() {
+    static int per_sm = 0;
     if (per_sm == 0) {
         int x = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, k_tail<GUIDE, COUNT, STACK>, TRACE_BLOCK, smem) !=
-                cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, k_tail<GUIDE, COUNT, STACK>, TRACE_BLOCK,
+                                                          sizeof(uint2) * STACK * TRACE_BLOCK) != cudaSuccess ||
             x < 1)
             x = 1;
         per_sm = x;
     }
-    const uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * (uint32_t)per_sm;
+    return per_sm;
+}
+
+template <bool GUIDE, bool COUNT, int STACK>
+int launch_tail_t(const FrameArgs& a, uint32_t first, cudaStream_t st) {
+    const size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
+    const uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * (uint32_t)tail_per_sm<GUIDE, COUNT, STACK>();
     k_tail<GUIDE, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a, first);
     return 1;
 }
@@ -789,6 +845,14 @@ int launch_bounce(const FrameArgs& a, uint32_t bounce, cudaStream_t st, int stag
     return launches;
 }
 
+int launch_shade_multi(const FrameArgs* items, int n_items, uint32_t bounce, uint32_t* fetch, int sm_count,
+                       cudaStream_t st) {
+    if (n_items <= 0) return 0;
+    const uint32_t grid = (uint32_t)(sm_count > 0 ? sm_count : 148) * SRT_SHADE_MIN_BLOCKS;
+    k_shade_multi<<<grid, TRACE_BLOCK, 0, st>>>(items, n_items, bounce, fetch);
+    return 1;
+}
+
 int launch_finalize(const FrameArgs& a, cudaStream_t st) {
     k_finalize<<<blocks_for((uint64_t)a.width * a.height, 256), 256, 0, st>>>(a);
     return 1;
@@ -797,6 +861,17 @@ int launch_finalize(const FrameArgs& a, cudaStream_t st) {
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st) {
     k_frame_stats<<<1, 32, 0, st>>>(a);
     return 1;
+}
+
+uint32_t tail_threads(const FrameArgs& a) {
+    const bool small = a.scene.depth <= (uint32_t)TRAV_STACK_SMALL;
+    const bool g = a.guiding != 0, c = a.count_visits != 0;
+    int per_sm;
+    if (c) per_sm = g ? (small ? tail_per_sm<true, true, TRAV_STACK_SMALL>() : tail_per_sm<true, true, TRAV_STACK>())
+                      : (small ? tail_per_sm<false, true, TRAV_STACK_SMALL>() : tail_per_sm<false, true, TRAV_STACK>());
+    else per_sm = g ? (small ? tail_per_sm<true, false, TRAV_STACK_SMALL>() : tail_per_sm<true, false, TRAV_STACK>())
+                    : (small ? tail_per_sm<false, false, TRAV_STACK_SMALL>() : tail_per_sm<false, false, TRAV_STACK>());
+    return (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * (uint32_t)per_sm * TRACE_BLOCK;
 }
 
 int launch_tail(const FrameArgs& a, uint32_t first, cudaStream_t st) {

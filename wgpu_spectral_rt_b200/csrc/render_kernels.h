@@ -120,6 +120,12 @@ int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue
 // Bounces first .. max_depth - 1 of the paths queued for bounce `first`, in
 // one persistent launch (closest hit, shading and shadow ray per path).
 int launch_tail(const FrameArgs& a, uint32_t first, cudaStream_t st);
+// Threads of one launch_tail wave for these frame arguments (one path each at once).
+uint32_t tail_threads(const FrameArgs& a);
+// The shading of bounce `bounce` of n_items scenes (device table of their
+// frame arguments) in one persistent launch; *fetch starts at 0.
+int launch_shade_multi(const FrameArgs* items, int n_items, uint32_t bounce, uint32_t* fetch, int sm_count,
+                       cudaStream_t st);
 int launch_finalize(const FrameArgs& a, cudaStream_t st);
 int launch_frame_stats(const FrameArgs& a, cudaStream_t st);
 

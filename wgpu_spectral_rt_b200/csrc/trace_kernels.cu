@@ -28,9 +28,12 @@
 #ifndef SRT_TRACE_PERSISTENT
 #define SRT_TRACE_PERSISTENT 1
 #endif
-// first bounce whose shadow rays use persistent warps (0: none)
+// first bounce whose shadow rays use persistent warps (0: none).  Bounce-0
+// shadow rays leave the camera rays' hit points in pixel order, coherent
+// enough for one ray per thread; later ones are not, and refilling idle lanes
+// pays (config-2 shadow rays 2.38 vs 2.61 ms per frame).
 #ifndef SRT_SHADOW_PERSISTENT_FROM
-#define SRT_SHADOW_PERSISTENT_FROM 0
+#define SRT_SHADOW_PERSISTENT_FROM 1
 #endif
 
 // Fetch the next node with cp.async into shared memory while the pending
@@ -289,8 +292,8 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
 }
 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    // one ray per thread: the shadow queue is in pixel order and coherent, and
-    // refilling lanes from a shared counter scatters it (measured +28 %)
+    // bounce 0: one ray per thread (the queue is in pixel order and coherent);
+    // later bounces: persistent warps with refill (SRT_SHADOW_PERSISTENT_FROM)
     TraceLaunch L{a.scene, nullptr, &a.counters->shadow[bounce],
                   (SRT_SHADOW_PERSISTENT_FROM > 0 && bounce >= (uint32_t)SRT_SHADOW_PERSISTENT_FROM)
                       ? &a.counters->fetch[TRAV_SHADOW][bounce]

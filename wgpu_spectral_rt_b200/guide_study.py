@@ -138,7 +138,7 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
                 r.set_guide_bounces(guide_bounces)
         frames, el, curve = _arm(ctx, r, ctl, aspect, seconds, ref)
         out[name] = {"frames": frames, "seconds": round(el, 3), "ms_per_frame": round(1e3 * el / frames, 4),
-                     "relmse": curve[-1][2], "curve": curve}
+                     "relmse": curve[-1][2], "curve": curve, "tail_first": r.stats()["tail_first"]}
         if flags:
             out[name]["guide"] = r.guide_info()
         r.close()
