@@ -376,7 +376,7 @@ def guided_section(seconds=30.0, ref_spp=8192):
                                                    if d["time_fraction_ref_noise_subtracted"] else None),
             "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"],
             "tail_first_plain": d["plain"]["tail_first"], "tail_first_guided": d["guided"]["tail_first"],
-            "guided_bounces": d["guide_bounces"] or "every bounce before the tail kernel (the library default)"}
+            "guided_bounces": d["guide_bounces"] or "0..7 (the library default)"}
 
 
 def batched_guided_section(seconds=2.0, ref_spp=256):

@@ -399,8 +399,8 @@ srt_status srt_renderer_get_bounce_stats(srt_renderer* r, srt_bounce_stats* out)
  * its first frame without waiting for them and, once they are there, starts
  * the tail at the first bounce >= 1 whose live paths fit in one wave of the
  * tail kernel's resident threads (a batch: the scenes' paths summed), for a
- * guiding renderer not before bounce 5; frames before that run bounce by
- * bounce.  0 = bounce by bounce.  Not used with
+ * guiding renderer not before the end of its guided bounces; frames before
+ * that run bounce by bounce.  0 = bounce by bounce.  Not used with
  * SRT_FLAG_RAY_SORT, nor where a set number of guided bounces reaches it
  * (srt_renderer_guide_set_bounces).  srt_stats.tail_first reports the bounce
  * in use.  No reference counterpart. */
@@ -523,14 +523,12 @@ srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, uint32_t batc
  * split into `steps` consecutive sub-batches, one forward/backward, gradient
  * and Adam step each. */
 srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t steps);
-/* Guided bounces: the guide samples the Lambert continuations of bounces <
- * `bounces` (and trains on them); later Lambert vertices sample the cosine
- * lobe as the reference does.  SRT_GUIDE_BOUNCES_AUTO (0, the default): every
- * bounce before the tail kernel's first one (srt_renderer_set_tail), which
- * runs the rest unguided; a set number >= 1 keeps the tail from starting
- * before it.  The estimator stays unbiased either way; fewer guided bounces
- * trade variance for time. */
-#define SRT_GUIDE_BOUNCES_AUTO 0u
+/* Guided bounces (>= 1, default 8): the guide samples the Lambert
+ * continuations of bounces < `bounces` (and trains on them); later Lambert
+ * vertices sample the cosine lobe as the reference does.  The automatic tail
+ * (srt_renderer_set_tail) starts after the guided bounces; a set tail that
+ * would start before their end is not used.  The estimator stays unbiased
+ * either way; fewer guided bounces trade variance for time. */
 srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces);
 /* Test entry points (host buffers).  forward: x [n][10] -> raw outputs [n][48].
  * mixture: raw [n][48], omega [n][3], u [n][3] -> [n][4] = (pdf(omega),

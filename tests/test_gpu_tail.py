@@ -63,3 +63,46 @@ def test_guided_tail_after_the_guided_bounces(srt, ctx):
     # guided bounces reaching the tail's first bounce: bounce by bounce
     _, st2 = _frames(srt, ctx, 4, 40, 24, p, 3, guide_bounces=4)
     assert st2["tail_first"] == 16
+
+
+def test_automatic_tail_start(srt, ctx):
+    """SRT_TAIL_AUTO (the default): after the first frame's path counts are
+    back, the renderer starts the tail at the first bounce whose live paths
+    fit in one wave of the tail kernel; a small image fits from bounce 1.  The
+    image is that of the bounce-by-bounce frames, whenever the choice lands."""
+    p = srt.default_params(photons_per_frame=1 << 15, max_depth=12)
+    ref, _ = _frames(srt, ctx, 3, 48, 32, p, 0, frames=4)
+    b = srt.SceneBuilder()
+    cam = b.add_preset(3)
+    scene = b.build(ctx)
+    r = srt.Renderer(ctx, scene, 48, 32, p)
+    ctl = srt.CameraController(*cam)
+    r.render(ctl.build_uniform(1.5, 0))
+    assert r.stats()["tail_first"] == 12  # bounce by bounce until the counts are read
+    ctx.synchronize()
+    for f in range(1, 4):
+        r.render(ctl.build_uniform(1.5, f))
+    assert r.stats()["tail_first"] == 1
+    np.testing.assert_array_equal(r.read_accum(), ref)
+    r.close()
+    scene.close()
+
+
+def test_automatic_tail_starts_after_the_guided_bounces(srt, ctx):
+    """A guiding renderer's automatic tail starts after its guided bounces
+    (default 8), and its frames equal the bounce-by-bounce ones (frozen guide)."""
+    p = srt.default_params(photons_per_frame=1 << 14, max_depth=16, flags=srt.FLAG_GUIDING | srt.FLAG_GUIDE_FROZEN)
+    ref, _ = _frames(srt, ctx, 4, 40, 24, p, 0, frames=4)
+    b = srt.SceneBuilder()
+    cam = b.add_preset(4)
+    scene = b.build(ctx)
+    r = srt.Renderer(ctx, scene, 40, 24, p)
+    ctl = srt.CameraController(*cam)
+    r.render(ctl.build_uniform(40 / 24, 0))
+    ctx.synchronize()
+    for f in range(1, 4):
+        r.render(ctl.build_uniform(40 / 24, f))
+    assert r.stats()["tail_first"] == 8
+    np.testing.assert_array_equal(r.read_accum(), ref)
+    r.close()
+    scene.close()

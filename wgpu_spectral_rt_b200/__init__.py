@@ -132,7 +132,6 @@ BVH_LBVH = 1
 GUIDE_INFER_MMA_SYNC = 0
 GUIDE_INFER_TCGEN05 = 1
 TAIL_AUTO = 0xFFFFFFFF  # srt_renderer_set_tail: chosen from the first frame's path counts
-GUIDE_BOUNCES_AUTO = 0  # srt_renderer_guide_set_bounces: every bounce before the tail
 GUIDE_TRAIN_MMA_SYNC = 0
 GUIDE_TRAIN_TCGEN05 = 1
 
@@ -646,8 +645,8 @@ class Renderer:
         _check(lib().srt_renderer_guide_set_steps(self.h, steps), self.ctx.h)
 
     def set_guide_bounces(self, bounces: int) -> None:
-        """Guide the Lambert continuations of bounces < `bounces` only (later ones sample the cosine lobe);
-        GUIDE_BOUNCES_AUTO (0, the default): every bounce before the tail kernel's first."""
+        """Guide the Lambert continuations of bounces < `bounces` only (default 8; later ones sample the
+        cosine lobe)."""
         _check(lib().srt_renderer_guide_set_bounces(self.h, bounces), self.ctx.h)
 
     def configure_guide(self, lr: float | None = None, batch: int | None = None) -> None:

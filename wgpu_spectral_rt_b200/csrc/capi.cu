@@ -685,12 +685,15 @@ extern "C" srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width) {
 #ifndef SRT_TAIL_WAVES
 #define SRT_TAIL_WAVES 1.0
 #endif
-// A guiding renderer's automatic tail starts no earlier than this bounce:
-// its guided bounces end where the tail starts, and the guide's gain is in
-// the first bounces (the caustic-slab scene at 1080p: relMSE at equal time
-// 0.0500 with bounces 0..4 guided, 0.0497 with all, 0.0487 with 0..7).
-#ifndef SRT_GUIDE_TAIL_MIN
-#define SRT_GUIDE_TAIL_MIN 5u
+// Guided bounces by default: the first eight.  A guiding renderer's
+// automatic tail starts after them (the tail kernel samples cosine lobes).
+// The caustic-slab scene at 1080p: relMSE at equal time 0.0500 with bounces
+// 0..4 guided, 0.0487 with 0..7, 0.0497 with all; frame 6.59 ms with 0..7
+// and the tail from bounce 8, 6.80 ms with all bounces guided.  The number
+// is fixed rather than taken from the automatic tail because it changes the
+// estimator: a frame's image must not depend on when a read-back landed.
+#ifndef SRT_GUIDE_BOUNCES_DEFAULT
+#define SRT_GUIDE_BOUNCES_DEFAULT 8u
 #endif
 // Frames enqueue independent stages on two branches (srt_renderer::record_overlapped).
 #ifndef SRT_FRAME_OVERLAP
@@ -794,13 +797,13 @@ struct srt_renderer {
     uint32_t* counts_host = nullptr;  // pinned: paths entering each bounce of one frame
     cudaEvent_t counts_ev = nullptr;
     int counts_state = 0;             // 0: not requested, 1: copy in flight, 2: read
-    // guided bounces follow the tail: every bounce before it (the tail samples
-    // cosine lobes), unless srt_renderer_guide_set_bounces set a number
-    bool guide_bounces_auto = true;
+    // A guiding renderer's tail starts after its guided bounces: the
+    // automatic one right after them, a set one not at all if it would start
+    // before their end.
     uint32_t tail_start() const {
-        const uint32_t t = tail_first == SRT_TAIL_AUTO ? tail_auto : tail_first;
+        uint32_t t = tail_first == SRT_TAIL_AUTO ? tail_auto : tail_first;
+        if (t != 0u && args.guiding && args.guide_bounces > t) t = tail_first == SRT_TAIL_AUTO ? args.guide_bounces : 0u;
         if (t == 0u || t >= p.max_depth || args.ray_sort) return p.max_depth;
-        if (args.guiding && !guide_bounces_auto && args.guide_bounces > t) return p.max_depth;
         return t;
     }
     // The automatic tail start from one frame's path counts (paths[b] = paths
@@ -811,25 +814,11 @@ struct srt_renderer {
             if ((double)paths[b] <= SRT_TAIL_WAVES * capacity) return b;
         return 0u;
     }
-    // The automatic choice t for this renderer (guiding: not before SRT_GUIDE_TAIL_MIN).
-    uint32_t auto_tail_for(uint32_t t) const {
-        return (args.guiding && t != 0u) ? std::max<uint32_t>(t, SRT_GUIDE_TAIL_MIN) : t;
-    }
     // Drops the captured frame (its shape changed).
     void drop_graph() {
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
-        }
-    }
-    // The guided bounces when they follow the tail.
-    void sync_guide_bounces() {
-        if (!args.guiding || !guide_bounces_auto) return;
-        const uint32_t gb = std::min<uint32_t>(tail_start(), MAX_BOUNCES + 1);
-        if (args.guide_bounces != gb) {
-            args.guide_bounces = gb;
-            args_gen += 1;
-            drop_graph();
         }
     }
     // SRT_TAIL_AUTO: after the first frame, read its path counts back without
@@ -839,11 +828,10 @@ struct srt_renderer {
         if (tail_first != SRT_TAIL_AUTO || counts_state != 1) return;
         if (cudaEventQuery(counts_ev) != cudaSuccess) return;
         counts_state = 2;
-        const uint32_t t = auto_tail_for(choose_tail(counts_host, p.max_depth, (double)tail_threads(args)));
+        const uint32_t t = choose_tail(counts_host, p.max_depth, (double)tail_threads(args));
         if (t != tail_auto) {
             tail_auto = t;
             drop_graph();
-            sync_guide_bounces();
         }
     }
     void auto_tail_after_frame(cudaStream_t st) {
@@ -1155,7 +1143,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
         r->guide.train = (p.flags & SRT_FLAG_GUIDE_FROZEN) ? 0 : 1;
         r->guide.err = r->err;
         a.guiding = 1;
-        a.guide_bounces = std::min<uint32_t>(p.max_depth, MAX_BOUNCES + 1);  // every bounce until a tail is chosen
+        a.guide_bounces = SRT_GUIDE_BOUNCES_DEFAULT;
         a.guide = r->guide;
     }
     size_t n_events = 5 + 3 * (size_t)p.max_depth;
@@ -1421,7 +1409,6 @@ extern "C" srt_status srt_renderer_set_tail(srt_renderer* r, uint32_t first_boun
     r->tail_first = first_bounce;
     r->drop_graph();  // the tail shapes the captured frame
     r->args_gen += 1;
-    r->sync_guide_bounces();
     return SRT_OK;
 }
 
@@ -1717,17 +1704,15 @@ extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t ste
 }
 
 extern "C" srt_status srt_renderer_guide_set_bounces(srt_renderer* r, uint32_t bounces) {
-    if (!r) return SRT_ERR_INVALID_ARG;
+    if (!r || bounces < 1) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     if (!r->args.guiding) return fail(c, SRT_ERR_INVALID_ARG, "renderer was created without SRT_FLAG_GUIDING");
     if (srt_status fs = guide_flush(r)) return fs;
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    r->guide_bounces_auto = bounces == SRT_GUIDE_BOUNCES_AUTO;
-    if (!r->guide_bounces_auto) r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
+    r->args.guide_bounces = std::min<uint32_t>(bounces, MAX_BOUNCES + 1);
     r->args_gen += 1;
     r->drop_graph();  // the guided bounces shape the captured frame
-    r->sync_guide_bounces();
     return SRT_OK;
 }
 
@@ -2012,10 +1997,14 @@ extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_came
 // and shadow rays of all scenes are traced in one launch per bounce
 // (k_trace_multi).  The graph is re-captured when the set of active scenes
 // or the tuning changes.
-// The batch shades all its scenes' vertices of a bounce in one launch
-// (k_shade_multi); 0: one shading launch per scene on its graph branch.
+// 1: the batch shades all its scenes' vertices of a bounce in one launch
+// (k_shade_multi); 0 (the default): one shading launch per scene on its
+// graph branch, the branches running at once.  Measured on the 32-scene
+// batch (256^2..1024^2 viewports, all scenes active): 120.2 ms per iteration
+// with the branches, 123.5 ms with the single launch (it reads the frame
+// arguments from shared memory and spills more registers).
 #ifndef SRT_BATCH_SHADE_MULTI
-#define SRT_BATCH_SHADE_MULTI 1
+#define SRT_BATCH_SHADE_MULTI 0
 #endif
 
 struct srt_batch {
@@ -2272,9 +2261,8 @@ struct srt_batch {
         if (first < 0) return;
         const uint32_t t = srt_renderer::choose_tail(sum.data(), depth, (double)tail_threads(r[first]->args));
         for (srt_renderer* x : r) {
-            if (x->tail_first != SRT_TAIL_AUTO || x->tail_auto == x->auto_tail_for(t)) continue;
-            x->tail_auto = x->auto_tail_for(t);
-            x->sync_guide_bounces();
+            if (x->tail_first != SRT_TAIL_AUTO || x->tail_auto == t) continue;
+            x->tail_auto = t;
             recapture = true;
         }
     }

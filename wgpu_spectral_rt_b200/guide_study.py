@@ -94,7 +94,7 @@ def _time_to_reach(curve, target):
 
 
 def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16, photons=1 << 20, ref_spp=65536,
-          seconds=20.0, lr=None, batch=None, guide_bounces=None):
+          seconds=20.0, lr=None, batch=None, guide_bounces=None, training=None):
     """Runs the study.  The reference is rendered as two halves on decorrelated
     streams; their difference estimates the reference's own noise, which every
     measured relMSE contains as a constant floor (E (x - ref)^2 = E (x - mu)^2
@@ -136,6 +136,8 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
             r.configure_guide(lr, batch)
             if guide_bounces:
                 r.set_guide_bounces(guide_bounces)
+            if training is not None:
+                r.set_guide_training(training)
         frames, el, curve = _arm(ctx, r, ctl, aspect, seconds, ref)
         out[name] = {"frames": frames, "seconds": round(el, 3), "ms_per_frame": round(1e3 * el / frames, 4),
                      "relmse": curve[-1][2], "curve": curve, "tail_first": r.stats()["tail_first"]}
@@ -170,10 +172,13 @@ def main():
     ap.add_argument("--seconds", type=float, default=20.0)
     ap.add_argument("--lr", type=float, default=None)
     ap.add_argument("--batch", type=int, default=None, help="training samples per frame")
-    ap.add_argument("--guide-bounces", type=int, default=None, help="guide bounces < N only (default all)")
+    ap.add_argument("--guide-bounces", type=int, default=None, help="guide bounces < N only (default 8)")
+    ap.add_argument("--training", choices=("mma-sync", "tcgen05"), default=None,
+                    help="training kernel (default: the library's)")
     a = ap.parse_args()
+    training = {None: None, "mma-sync": srt.GUIDE_TRAIN_MMA_SYNC, "tcgen05": srt.GUIDE_TRAIN_TCGEN05}[a.training]
     print(json.dumps(study(a.preset, a.width, a.height, a.max_depth, a.photons, a.ref_spp, a.seconds, a.lr,
-                           a.batch, a.guide_bounces)))
+                           a.batch, a.guide_bounces, training)))
 
 
 if __name__ == "__main__":
