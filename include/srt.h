@@ -546,8 +546,8 @@ srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind);
 /* Training step kernels of a guiding renderer: mma.sync forward/backward
  * with a split-K weight-gradient product, or one fused tcgen05 kernel per
  * step (forward, loss gradient, backward and weight gradients of 128-record
- * tiles, the weight gradients accumulated in tensor memory).  The batched
- * renderer's grouped training uses the mma.sync kernels. */
+ * tiles, the weight gradients accumulated in tensor memory; the default).
+ * The batched renderer's grouped training uses the mma.sync kernels. */
 #define SRT_GUIDE_TRAIN_MMA_SYNC 0
 #define SRT_GUIDE_TRAIN_TCGEN05  1
 srt_status srt_renderer_guide_set_training(srt_renderer* r, int kind);

@@ -747,6 +747,12 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
 #ifndef SRT_TRAV_ONE_TRI_PER_STEP
 #define SRT_TRAV_ONE_TRI_PER_STEP 0
 #endif
+// The lanes of a warp that entered a step wait for each other before the
+// node visit (__syncwarp), so that it runs with all of them at once instead
+// of in the groups in which they left the triangle loop and the stack pop.
+#ifndef SRT_TRAV_WARPSYNC
+#define SRT_TRAV_WARPSYNC 0
+#endif
 
 struct TravState {
     float3 o, idir;
@@ -784,11 +790,117 @@ SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, floa
     return true;
 }
 
+// Pooled triangle tests (SRT_TRAV_POOL), called by all 32 lanes of a warp
+// at once: the triangles pending at the lanes' last node visits (T.tg of the
+// lanes with `live` set) are numbered across the warp by a prefix sum and
+// dealt out one per lane per round, so a round tests up to 32 triangles
+// whatever lanes they belong to (idle lanes work too), instead of each lane
+// looping over its own with the others waiting.  A lane fetches its task's
+// ray from the owning lane (shuffles), tests it with the same tri_test, and
+// a segmented minimum over the lanes of one owner (tasks of a lane are
+// consecutive) gives the owner the lexicographic minimum of (t, id) and its
+// (u, v); the owner keeps it if it beats its best.  The closest hit does not
+// depend on the order of the tests, so results are unchanged; any-hit rays
+// stop at their first hit (T.best != MISS afterwards).  Leaves T.tg empty.
+#ifndef SRT_TRAV_POOL
+#define SRT_TRAV_POOL 0
+#endif
+template <bool ANY>
+SRT_DEV void pool_tris(const DevScene& S, TravState& T, bool live, uint32_t& n_tris) {
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t cnt = live ? (uint32_t)__popc(T.tg.y) : 0u;
+    uint32_t incl = cnt;
+#pragma unroll
+    for (uint32_t d = 1; d < 32u; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    if (total == 0u) return;
+    const uint32_t excl = incl - cnt;
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t task = base + lane;
+        const bool have = task < total;
+        // owner = the number of lanes whose tasks end at or before this one
+        uint32_t o = 0;
+#pragma unroll
+        for (uint32_t step = 16; step >= 1u; step >>= 1) {
+            const uint32_t v = __shfl_sync(FULL, incl, (int)(o + step - 1u));
+            if (v <= task) o += step;
+        }
+        o = have ? o : 31u;
+        const uint32_t o_excl = __shfl_sync(FULL, excl, (int)o);
+        const uint32_t gx = __shfl_sync(FULL, T.tg.x, (int)o), gy = __shfl_sync(FULL, T.tg.y, (int)o);
+        const float ox = __shfl_sync(FULL, T.o.x, (int)o), oy = __shfl_sync(FULL, T.o.y, (int)o),
+                    oz = __shfl_sync(FULL, T.o.z, (int)o);
+        const float sx = __shfl_sync(FULL, T.sx, (int)o), sy = __shfl_sync(FULL, T.sy, (int)o),
+                    sz = __shfl_sync(FULL, T.sz, (int)o);
+        const float tmin = __shfl_sync(FULL, T.tmin, (int)o), tmax = __shfl_sync(FULL, T.tbest, (int)o);
+        const uint32_t axes = __shfl_sync(FULL, T.axes, (int)o);
+        uint32_t klo = 0xFFFFFFFFu, khi = 0xFFFFFFFFu;  // (t bits, id) of a hit, else all ones
+        float hu = 0.f, hv = 0.f;
+        if (have) {
+            const uint32_t bit = __fns(gy, 0u, (int)(task - o_excl + 1u)) & 31u;  // always found: task < incl[o]
+            const TriSlot* ts = S.tris + gx + bit;
+            const float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
+            ++n_tris;
+            float t, u, v;
+            if (tri_test(xyz(a0), xyz(a1), xyz(a2), f3(ox, oy, oz), axes & 3u, (axes >> 2) & 3u, (axes >> 4) & 3u, sx,
+                         sy, sz, tmin, tmax, t, u, v)) {
+                khi = __float_as_uint(t);  // t >= tmin > 0: the bits order like the values
+                klo = __float_as_uint(a0.w);
+                hu = u;
+                hv = v;
+            }
+        }
+        // segmented minimum over the lanes of one owner (consecutive lanes)
+        const uint32_t own = have ? o : 32u;
+#pragma unroll
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            const uint32_t olo = __shfl_down_sync(FULL, klo, d), ohi = __shfl_down_sync(FULL, khi, d);
+            const float ou = __shfl_down_sync(FULL, hu, d), ov = __shfl_down_sync(FULL, hv, d);
+            const uint32_t oo = __shfl_down_sync(FULL, own, d);
+            if (lane + d < 32u && oo == own && (ohi < khi || (ohi == khi && olo < klo))) {
+                khi = ohi;
+                klo = olo;
+                hu = ou;
+                hv = ov;
+            }
+        }
+        // each owner reads the minimum at the first lane of its segment
+        const bool mine = cnt > 0u && incl > base && excl < base + 32u;
+        const uint32_t first = mine ? (excl > base ? excl - base : 0u) : lane;
+        const uint32_t rlo = __shfl_sync(FULL, klo, (int)first), rhi = __shfl_sync(FULL, khi, (int)first);
+        const float ru = __shfl_sync(FULL, hu, (int)first), rv = __shfl_sync(FULL, hv, (int)first);
+        if (mine && rhi != 0xFFFFFFFFu) {
+            if (ANY) {
+                if (T.best == MISS) {
+                    T.best = rlo;
+                    T.tbest = __uint_as_float(rhi);
+                }
+            } else {
+                const uint32_t chi = __float_as_uint(T.tbest);
+                if (rhi < chi || (rhi == chi && rlo < T.best)) {
+                    T.tbest = __uint_as_float(rhi);
+                    T.best = rlo;
+                    T.bu = ru;
+                    T.bv = rv;
+                }
+            }
+        }
+    }
+    if (live) T.tg.y = 0u;
+}
+
 // Returns true when the ray is finished (for ANY: T.best != MISS on a hit).
 template <bool ANY, int STACK, bool PF = false>
 SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
                        uint32_t& n_tris, uint4* nbuf = nullptr) {
     const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
+    constexpr bool kSync = SRT_TRAV_WARPSYNC && !PF && !SRT_TRAV_ONE_TRI_PER_STEP;
+    const uint32_t entered = kSync ? __activemask() : 0u;
+    bool any_hit = false;
     bool have = true;
     if (PF) {
         // pick the next node and start fetching it; the triangle tests below
@@ -841,7 +953,9 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
             if (PF && have) cp_async_wait_all();  // no copy into the slot outlives the ray
             T.best = id;
             T.tbest = t;
-            return true;
+            if (!kSync) return true;
+            any_hit = true;
+            break;
         }
         if (t < T.tbest || id < T.best) {  // (t, id) lexicographic; t <= tbest holds here
             T.tbest = t;
@@ -850,6 +964,7 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
             T.bv = tv;
         }
     }
+
 #if SRT_TRAV_ONE_TRI_PER_STEP
     if (tri_step) return false;
 #endif
@@ -859,6 +974,47 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         ++n_nodes;
         node_children(nbuf[0], nbuf[stride], nbuf[2 * stride], nbuf[3 * stride], nbuf[4 * stride], T.o, T.idir, oct,
                       T.tmin, T.tbest, T.g, T.tg);
+        return false;
+    }
+    if constexpr (kSync) {
+        // the same steps with every exit (an any-hit, the end of the tree, an
+        // error) deferred past one __syncwarp, which every lane that entered
+        // the step reaches (nothing above returns), so that the node fetch and
+        // slab tests run with all lanes still tracing at once
+        bool fin = ANY && any_hit;
+        uint32_t idx = 0u;
+        if (!fin && (T.g.y & 0xFF000000u) == 0u) {
+            if (T.sp == 0) fin = true;
+            else {
+                --T.sp;
+                T.g = stack[T.sp * stride];
+            }
+        }
+        if (!fin) {
+            const int bit = 31 - __clz(T.g.y & 0xFF000000u);
+            T.g.y &= ~(1u << bit);
+            const uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
+            idx = T.g.x + __popc(T.g.y & ((1u << slot) - 1u) & 0xFFu);
+            if (T.g.y & 0xFF000000u) {
+                if (T.sp >= STACK) {
+                    atomicOr(err, ERR_STACK_OVERFLOW);
+                    fin = true;
+                } else {
+                    stack[T.sp * stride] = T.g;
+                    ++T.sp;
+                }
+            }
+            if (!fin && idx >= S.n_nodes) {
+                atomicOr(err, ERR_BAD_INDEX);
+                fin = true;
+            }
+        }
+        __syncwarp(entered);
+        if (fin) return true;
+        const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
+        uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+        ++n_nodes;
+        node_children(w0, w1, w2, w3, w4, T.o, T.idir, oct, T.tmin, T.tbest, T.g, T.tg);
         return false;
     }
     if ((T.g.y & 0xFF000000u) == 0u) {

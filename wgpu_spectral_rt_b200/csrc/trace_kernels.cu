@@ -47,6 +47,7 @@ namespace srt {
 namespace {
 
 constexpr bool kPrefetch = SRT_TRAV_PREFETCH != 0;
+constexpr bool kPool = SRT_TRAV_POOL != 0 && !kPrefetch;
 
 // Dynamic shared memory of a traversal block: the stacks, then (prefetch)
 // 5 x uint4 node slots per thread.
@@ -136,6 +137,11 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
         if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
             if (exhausted) break;
             continue;
+        }
+        if (kPool) {
+            // the triangles of the lanes' last node visits, dealt out over the warp
+            pool_tris<ANY>(S, T, active, n_tris);
+            if (ANY && active && T.best != MISS) active = false;  // occluded: nothing to add
         }
         if (active && trav_step<ANY, STACK, kPrefetch>(S, T, stack, TRACE_BLOCK, err, n_nodes, n_tris,
                                                        kPrefetch ? node_slots<STACK>(stack_smem) : nullptr)) {
