@@ -747,11 +747,15 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
 #ifndef SRT_TRAV_ONE_TRI_PER_STEP
 #define SRT_TRAV_ONE_TRI_PER_STEP 0
 #endif
-// The lanes of a warp that entered a step wait for each other before the
-// node visit (__syncwarp), so that it runs with all of them at once instead
-// of in the groups in which they left the triangle loop and the stack pop.
+// Closest-hit steps: the lanes of a warp that entered a step wait for each
+// other before the node visit (__syncwarp), so that it runs with all of them
+// at once instead of in the groups in which they left the triangle loop and
+// the stack pop (measured on bounce 1 of config 2: 0.75M warp node visits
+// with 21.8 lanes each instead of 1.09M with 15.0; closest-hit 3.29 vs
+// 3.37 ms per frame).  Any-hit steps use pooled triangle tests instead
+// (pool_tris); the two together measured slower than either alone.
 #ifndef SRT_TRAV_WARPSYNC
-#define SRT_TRAV_WARPSYNC 0
+#define SRT_TRAV_WARPSYNC 1
 #endif
 
 struct TravState {
@@ -802,8 +806,12 @@ SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, floa
 // (u, v); the owner keeps it if it beats its best.  The closest hit does not
 // depend on the order of the tests, so results are unchanged; any-hit rays
 // stop at their first hit (T.best != MISS afterwards).  Leaves T.tg empty.
+// Used by the persistent any-hit kernel (SRT_TRAV_POOL): the triangle loop of
+// bounce-1 closest-hit steps ran 2.15M warp iterations per config-2 frame
+// with 4.45 of 32 lanes busy; pooled, the shadow rays of bounces 1-4 take
+// 1.57 instead of 1.94 ms per frame.  Closest-hit steps measured no gain.
 #ifndef SRT_TRAV_POOL
-#define SRT_TRAV_POOL 0
+#define SRT_TRAV_POOL 1
 #endif
 template <bool ANY>
 SRT_DEV void pool_tris(const DevScene& S, TravState& T, bool live, uint32_t& n_tris) {
@@ -898,7 +906,7 @@ template <bool ANY, int STACK, bool PF = false>
 SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
                        uint32_t& n_tris, uint4* nbuf = nullptr) {
     const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
-    constexpr bool kSync = SRT_TRAV_WARPSYNC && !PF && !SRT_TRAV_ONE_TRI_PER_STEP;
+    constexpr bool kSync = SRT_TRAV_WARPSYNC && !ANY && !PF && !SRT_TRAV_ONE_TRI_PER_STEP;
     const uint32_t entered = kSync ? __activemask() : 0u;
     bool any_hit = false;
     bool have = true;

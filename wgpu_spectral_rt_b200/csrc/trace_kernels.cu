@@ -28,12 +28,21 @@
 #ifndef SRT_TRACE_PERSISTENT
 #define SRT_TRACE_PERSISTENT 1
 #endif
-// first bounce whose shadow rays use persistent warps (0: none).  Bounce-0
-// shadow rays leave the camera rays' hit points in pixel order, coherent
-// enough for one ray per thread; later ones are not, and refilling idle lanes
-// pays (config-2 shadow rays 2.38 vs 2.61 ms per frame).
+// first bounce whose shadow rays use persistent warps (> 31: none).  Shadow
+// rays of bounces >= 1 are incoherent, and refilling idle lanes pays
+// (config-2 shadow rays 2.38 vs 2.61 ms per frame); with the pooled triangle
+// tests bounce 0's do too (0.41 vs 0.45 ms).
 #ifndef SRT_SHADOW_PERSISTENT_FROM
-#define SRT_SHADOW_PERSISTENT_FROM 1
+#define SRT_SHADOW_PERSISTENT_FROM 0
+#endif
+
+// camera rays of bounce 0 in persistent warps (k_trace_pt) instead of one per thread
+#ifndef SRT_PRIMARY_PERSISTENT
+#define SRT_PRIMARY_PERSISTENT 0
+#endif
+// photon rays in persistent warps (k_trace_pt) instead of one per thread
+#ifndef SRT_PHOTON_PERSISTENT
+#define SRT_PHOTON_PERSISTENT 0
 #endif
 
 // Fetch the next node with cp.async into shared memory while the pending
@@ -138,7 +147,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
             if (exhausted) break;
             continue;
         }
-        if (kPool) {
+        if (kPool && ANY) {
             // the triangles of the lanes' last node visits, dealt out over the warp
             pool_tris<ANY>(S, T, active, n_tris);
             if (ANY && active && T.best != MISS) active = false;  // occluded: nothing to add
@@ -290,7 +299,7 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
     // primary rays (bounce 0) are pixel-ordered and coherent: one ray per
     // thread; later bounces are incoherent: persistent warps with refill
     TraceLaunch L{a.scene, a.pb.queue[bounce & 1], &a.counters->paths[bounce],
-                  bounce == 0 ? nullptr : &a.counters->fetch[TRAV_CLOSEST][bounce],
+                  (bounce == 0 && !SRT_PRIMARY_PERSISTENT) ? nullptr : &a.counters->fetch[TRAV_CLOSEST][bounce],
                   a.width * a.height, a.pb.ray_o, a.pb.ray_d, a.pb.hit, nullptr, nullptr, nullptr, a.err, a.stats,
                   TRAV_CLOSEST, a.sm_count, (int)bounce};
     launch_kind<false>(L, a.count_visits, st);
@@ -298,10 +307,9 @@ int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
 }
 
 int launch_trace_shadow(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    // bounce 0: one ray per thread (the queue is in pixel order and coherent);
-    // later bounces: persistent warps with refill (SRT_SHADOW_PERSISTENT_FROM)
+    // persistent warps with refill and pooled triangle tests (SRT_SHADOW_PERSISTENT_FROM)
     TraceLaunch L{a.scene, nullptr, &a.counters->shadow[bounce],
-                  (SRT_SHADOW_PERSISTENT_FROM > 0 && bounce >= (uint32_t)SRT_SHADOW_PERSISTENT_FROM)
+                  bounce >= (uint32_t)SRT_SHADOW_PERSISTENT_FROM
                       ? &a.counters->fetch[TRAV_SHADOW][bounce]
                       : nullptr,
                   a.width * a.height, a.pb.sh_o, a.pb.sh_d, nullptr, a.pb.sh_id, a.pb.sh_c, a.pb.rad, a.err, a.stats,
@@ -316,9 +324,8 @@ int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue
     if (max_n == 0) return 0;
     // photon rays arrive direction-sorted: one ray per thread keeps that order
     // (persistent refill measured slower, 3.35 vs 3.15 ms per photon pass)
-    (void)fetch;
-    TraceLaunch L{s, queue, count, nullptr, max_n, ro, rd, hit, nullptr, nullptr, nullptr, err, stats, kind, sm_count,
-                  (int)bounce};
+    TraceLaunch L{s, queue, count, SRT_PHOTON_PERSISTENT ? fetch : nullptr, max_n, ro, rd, hit, nullptr, nullptr,
+                  nullptr, err, stats, kind, sm_count, (int)bounce};
     launch_kind<false>(L, count_visits, st);
     return 1;
 }
