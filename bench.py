@@ -533,7 +533,8 @@ def main(argv=None):
         traffic, tnote = _traffic_from_profile(f"trace_closest_{args.config}", rays / launches)
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "k_trace<closest> (trace_kernels.cu)",
+                "kernel": "camera closest-hit traversal: k_trace (bounce 0) and k_trace_pt (bounces 1..tail-1), "
+                          "trace_kernels.cu",
                 "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                 "bytes_per_launch": round(bytes_launch), "ms_per_launch": round(ms_launch, 4),
                 "nodes_per_ray": round(float(bc["nodes"][0][:tail].sum()) / max(1, rays), 2),

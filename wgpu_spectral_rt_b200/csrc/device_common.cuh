@@ -809,7 +809,8 @@ SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, floa
 // Used by the persistent any-hit kernel (SRT_TRAV_POOL): the triangle loop of
 // bounce-1 closest-hit steps ran 2.15M warp iterations per config-2 frame
 // with 4.45 of 32 lanes busy; pooled, the shadow rays of bounces 1-4 take
-// 1.57 instead of 1.94 ms per frame.  Closest-hit steps measured no gain.
+// 1.57 instead of 1.94 ms per frame.  Closest-hit steps measured no gain
+// (SRT_TRAV_POOL=2 pools them too).
 #ifndef SRT_TRAV_POOL
 #define SRT_TRAV_POOL 1
 #endif

@@ -36,13 +36,17 @@
 #define SRT_SHADOW_PERSISTENT_FROM 0
 #endif
 
-// camera rays of bounce 0 in persistent warps (k_trace_pt) instead of one per thread
+// camera rays of bounce 0 in persistent warps (k_trace_pt) instead of one
+// per thread: measured slower (0.44 vs 0.42 ms per config-2 frame), the
+// pixel-ordered rays are coherent and end together
 #ifndef SRT_PRIMARY_PERSISTENT
 #define SRT_PRIMARY_PERSISTENT 0
 #endif
-// photon rays in persistent warps (k_trace_pt) instead of one per thread
+// photon rays in persistent warps (k_trace_pt) instead of one per thread:
+// with the warp-synchronous node visits the refill pays (photon pass 2.53 vs
+// 2.62 ms per config-2 frame; before it, 3.35 vs 3.15)
 #ifndef SRT_PHOTON_PERSISTENT
-#define SRT_PHOTON_PERSISTENT 0
+#define SRT_PHOTON_PERSISTENT 1
 #endif
 
 // Fetch the next node with cp.async into shared memory while the pending
@@ -147,7 +151,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
             if (exhausted) break;
             continue;
         }
-        if (kPool && ANY) {
+        if (kPool && (ANY || SRT_TRAV_POOL >= 2)) {
             // the triangles of the lanes' last node visits, dealt out over the warp
             pool_tris<ANY>(S, T, active, n_tris);
             if (ANY && active && T.best != MISS) active = false;  // occluded: nothing to add
@@ -322,8 +326,8 @@ int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue
                        uint32_t* fetch, uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind,
                        int count_visits, uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st) {
     if (max_n == 0) return 0;
-    // photon rays arrive direction-sorted: one ray per thread keeps that order
-    // (persistent refill measured slower, 3.35 vs 3.15 ms per photon pass)
+    // photon rays arrive direction-sorted; persistent warps take them in that
+    // order (SRT_PHOTON_PERSISTENT)
     TraceLaunch L{s, queue, count, SRT_PHOTON_PERSISTENT ? fetch : nullptr, max_n, ro, rd, hit, nullptr, nullptr,
                   nullptr, err, stats, kind, sm_count, (int)bounce};
     launch_kind<false>(L, count_visits, st);
