@@ -758,16 +758,62 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
 #define SRT_TRAV_WARPSYNC 1
 #endif
 
+// The top entry of the traversal stack in registers (SRT_TRAV_REG_TOP): a
+// push keeps the new group in `top` and moves the previous top to shared
+// memory; a pop takes `top` if there is one.  A group pushed at a node visit
+// and popped when that node's subtree is done never touches shared memory.
+#ifndef SRT_TRAV_REG_TOP
+#define SRT_TRAV_REG_TOP 0
+#endif
+constexpr uint32_t AXES_HAS_TOP = 1u << 16;  // TravState.axes: `top` holds an entry
+
 struct TravState {
     float3 o, idir;
     float tmin, tbest;
     float sx, sy, sz;
-    uint32_t axes;  // kx | ky << 2 | kz << 4 | oct << 8
+    uint32_t axes;  // kx | ky << 2 | kz << 4 | oct << 8 (| AXES_HAS_TOP)
     uint2 g, tg;
     int sp;
     uint32_t best;
     float bu, bv;
+#if SRT_TRAV_REG_TOP
+    uint2 top;
+#endif
 };
+
+// Pops the next node group into T.g; false when the stack is empty.
+SRT_DEV bool trav_pop(TravState& T, const uint2* stack, int stride) {
+#if SRT_TRAV_REG_TOP
+    if (T.axes & AXES_HAS_TOP) {
+        T.g = T.top;
+        T.axes &= ~AXES_HAS_TOP;
+        return true;
+    }
+#endif
+    if (T.sp == 0) return false;
+    --T.sp;
+    T.g = stack[T.sp * stride];
+    return true;
+}
+// Pushes T.g; false when STACK shared-memory entries are in use (overflow).
+template <int STACK>
+SRT_DEV bool trav_push(TravState& T, uint2* stack, int stride) {
+#if SRT_TRAV_REG_TOP
+    if (T.axes & AXES_HAS_TOP) {
+        if (T.sp >= STACK) return false;
+        stack[T.sp * stride] = T.top;
+        ++T.sp;
+    }
+    T.top = T.g;
+    T.axes |= AXES_HAS_TOP;
+    return true;
+#else
+    if (T.sp >= STACK) return false;
+    stack[T.sp * stride] = T.g;
+    ++T.sp;
+    return true;
+#endif
+}
 
 // Returns false when the ray cannot hit anything (finished at once).
 SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, float tmin, float tmax) {
@@ -906,7 +952,7 @@ SRT_DEV void pool_tris(const DevScene& S, TravState& T, bool live, uint32_t& n_t
 template <bool ANY, int STACK, bool PF = false>
 SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride, uint32_t* err, uint32_t& n_nodes,
                        uint32_t& n_tris, uint4* nbuf = nullptr) {
-    const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = T.axes >> 8;
+    const uint32_t kx = T.axes & 3u, ky = (T.axes >> 2) & 3u, kz = (T.axes >> 4) & 3u, oct = (T.axes >> 8) & 7u;
     constexpr bool kSync = SRT_TRAV_WARPSYNC && !ANY && !PF && !SRT_TRAV_ONE_TRI_PER_STEP;
     const uint32_t entered = kSync ? __activemask() : 0u;
     bool any_hit = false;
@@ -992,26 +1038,15 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         // slab tests run with all lanes still tracing at once
         bool fin = ANY && any_hit;
         uint32_t idx = 0u;
-        if (!fin && (T.g.y & 0xFF000000u) == 0u) {
-            if (T.sp == 0) fin = true;
-            else {
-                --T.sp;
-                T.g = stack[T.sp * stride];
-            }
-        }
+        if (!fin && (T.g.y & 0xFF000000u) == 0u) fin = !trav_pop(T, stack, stride);
         if (!fin) {
             const int bit = 31 - __clz(T.g.y & 0xFF000000u);
             T.g.y &= ~(1u << bit);
             const uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
             idx = T.g.x + __popc(T.g.y & ((1u << slot) - 1u) & 0xFFu);
-            if (T.g.y & 0xFF000000u) {
-                if (T.sp >= STACK) {
-                    atomicOr(err, ERR_STACK_OVERFLOW);
-                    fin = true;
-                } else {
-                    stack[T.sp * stride] = T.g;
-                    ++T.sp;
-                }
+            if ((T.g.y & 0xFF000000u) && !trav_push<STACK>(T, stack, stride)) {
+                atomicOr(err, ERR_STACK_OVERFLOW);
+                fin = true;
             }
             if (!fin && idx >= S.n_nodes) {
                 atomicOr(err, ERR_BAD_INDEX);
@@ -1026,22 +1061,14 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
         node_children(w0, w1, w2, w3, w4, T.o, T.idir, oct, T.tmin, T.tbest, T.g, T.tg);
         return false;
     }
-    if ((T.g.y & 0xFF000000u) == 0u) {
-        if (T.sp == 0) return true;
-        --T.sp;
-        T.g = stack[T.sp * stride];
-    }
+    if ((T.g.y & 0xFF000000u) == 0u && !trav_pop(T, stack, stride)) return true;
     int bit = 31 - __clz(T.g.y & 0xFF000000u);
     T.g.y &= ~(1u << bit);
     uint32_t slot = (uint32_t)(bit - 24) ^ (oct ^ 7u);
     uint32_t idx = T.g.x + __popc(T.g.y & ((1u << slot) - 1u) & 0xFFu);
-    if (T.g.y & 0xFF000000u) {
-        if (T.sp >= STACK) {
-            atomicOr(err, ERR_STACK_OVERFLOW);
-            return true;
-        }
-        stack[T.sp * stride] = T.g;
-        ++T.sp;
+    if ((T.g.y & 0xFF000000u) && !trav_push<STACK>(T, stack, stride)) {
+        atomicOr(err, ERR_STACK_OVERFLOW);
+        return true;
     }
     if (idx >= S.n_nodes) {
         atomicOr(err, ERR_BAD_INDEX);
