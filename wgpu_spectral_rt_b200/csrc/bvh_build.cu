@@ -701,10 +701,6 @@ __global__ void k_expand_lights(const LightInst* __restrict__ li, const uint8_t*
     }
 }
 
-#ifndef SRT_BVH_OPEN_BIG_FIRST
-#define SRT_BVH_OPEN_BIG_FIRST 0
-#endif
-
 // One thread per 8-wide node of this level: queue entries (bvh2 ref, node).
 __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in, uint2* __restrict__ qout,
                            uint32_t* __restrict__ n_out, Node8* __restrict__ nodes, uint32_t* __restrict__ node_alloc,
@@ -728,22 +724,15 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
     while (nc < width) {
         int best = -1;
         float best_area = -1.0f;
-        bool best_big = false;
         for (int c = 0; c < nc; ++c) {
             if (refs[c] & LEAF) continue;
             float3 lo, hi;
             ref_box(b, refs[c], lo, hi);
             float3 ext = hi - lo;
             float area = ext.x * ext.y + ext.y * ext.z + ext.z * ext.x;
-            // SRT_BVH_OPEN_BIG_FIRST: open the children that would become
-            // nodes (> 3 triangles) before those that would become leaves
-            uint32_t f0, cnt;
-            ref_range(b, refs[c], f0, cnt);
-            const bool big = SRT_BVH_OPEN_BIG_FIRST && cnt > 3u;
-            if ((big && !best_big) || (big == best_big && area > best_area)) {
+            if (area > best_area) {
                 best_area = area;
                 best = c;
-                best_big = big;
             }
         }
         if (best < 0) break;
