@@ -375,6 +375,10 @@ def guided_section(seconds=30.0, ref_spp=8192):
             "time_fraction_ref_noise_subtracted": (round(d["time_fraction_ref_noise_subtracted"], 3)
                                                    if d["time_fraction_ref_noise_subtracted"] else None),
             "ms_per_frame_plain": d["plain"]["ms_per_frame"], "ms_per_frame_guided": d["guided"]["ms_per_frame"],
+            "cost_ratio_guided_over_plain": round(d["cost_ratio_guided_over_plain"], 3),
+            "variance_ratio_per_sample_ref_noise_subtracted": (
+                round(d["variance_ratio_per_sample_ref_noise_subtracted"], 3)
+                if d.get("variance_ratio_per_sample_ref_noise_subtracted") else None),
             "tail_first_plain": d["plain"]["tail_first"], "tail_first_guided": d["guided"]["tail_first"],
             "guided_bounces": d["guide_bounces"] or "0..7 (the library default)"}
 

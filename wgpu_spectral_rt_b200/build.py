@@ -4,7 +4,9 @@ Compiles every CUDA source with nvcc for sm_100a (`-gencode
 arch=compute_100a,code=sm_100a -lineinfo`), the host C++ sources with g++,
 and links them into wgpu_spectral_rt_b200/libsrt_b200.so.  Objects go to
 wgpu_spectral_rt_b200/_build/.  Rebuilds only what changed (by mtime,
-headers included).
+headers included).  Then builds the headless driver
+wgpu_spectral_rt_b200/srt_render (driver/srt_render.cpp), a C++ caller of
+the C ABI linked against the library.
 
 Usage:  python -m wgpu_spectral_rt_b200.build [-v] [--force]
 """
@@ -23,6 +25,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "libsrt_b200.so"
+DRIVER_SRC = PKG / "driver" / "srt_render.cpp"
+DRIVER = PKG / "srt_render"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -94,6 +98,15 @@ def build(verbose: bool = False, force: bool = False, out: Path | None = None, b
         tmp = lib.with_suffix(".so.tmp")
         run([_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
         os.replace(tmp, lib)
+    if out is None:
+        # the headless driver: a native caller of the C ABI, beside the library
+        src = DRIVER_SRC
+        if force or not DRIVER.exists() or any(x.stat().st_mtime > DRIVER.stat().st_mtime
+                                              for x in (src, lib, INCLUDE / "srt.h")):
+            tmp = DRIVER.with_suffix(".tmp")
+            run([_cxx(), "-O2", "-std=c++17", "-Wall", "-Wextra", f"-I{INCLUDE}", str(src), f"-L{PKG}",
+                 "-lsrt_b200", "-Wl,-rpath,$ORIGIN", "-o", str(tmp)])
+            os.replace(tmp, DRIVER)
     return lib
 
 

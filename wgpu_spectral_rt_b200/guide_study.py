@@ -155,6 +155,12 @@ def study(preset=srt.PRESET_CAUSTIC_SLAB, width=1920, height=1080, max_depth=16,
     out["time_fraction_ref_noise_subtracted"] = (t_s / out["plain"]["seconds"]) if t_s is not None else None
     out["relmse_ratio_ref_noise_subtracted"] = ((target - floor) / max(out["guided"]["relmse"] - floor, 1e-30)
                                                 if target > floor else None)
+    # per sample: relMSE x frames (noise floor out), guided over plain; the
+    # time fraction is about this times the cost ratio of a guided frame
+    if target > floor and out["guided"]["relmse"] > floor:
+        out["variance_ratio_per_sample_ref_noise_subtracted"] = (
+            (out["guided"]["relmse"] - floor) * out["guided"]["frames"] / ((target - floor) * out["plain"]["frames"]))
+    out["cost_ratio_guided_over_plain"] = out["guided"]["ms_per_frame"] / out["plain"]["ms_per_frame"]
     out["guide_bounces"] = guide_bounces
     scene.close()
     ctx.close()
