@@ -383,7 +383,7 @@ def guided_section(seconds=30.0, ref_spp=8192):
             "guided_bounces": d["guide_bounces"] or "0..7 (the library default)"}
 
 
-def batched_guided_section(seconds=2.0, ref_spp=256):
+def batched_guided_section(seconds=4.0, ref_spp=256):
     """C5 reduced (full-size study: wgpu_spectral_rt_b200.batch_guide_study): 16 seeded scenes, each
     with its own online-trained network, in one batched renderer (grouped guide launches) vs the
     plain batched renderer at equal time, per-scene relMSE against FP64 plain references."""
