@@ -357,6 +357,48 @@ def batched_section(srt, ctx, stream, n_scenes=32, seed=12345):
                          "a speed knob of the compatible renderer"}
 
 
+def config1_section(srt, ctx, stream, cpu=True):
+    """C1 as a whole (Cornell walls + 2-triangle light + dispersive UV sphere,
+    256x256, 16 spp, depth 8, 2^18 photons per frame): the GPU renderer timed
+    with CUDA events after warm-up, and the CPU oracle port on the same 16
+    frames (all host threads)."""
+    import torch
+
+    preset, w, h, depth, photons = CONFIGS["config1"]
+    _, scene, cam = build_scene(srt, ctx, preset)
+    pos, yaw, pitch = cam
+    r = srt.Renderer(ctx, scene, w, h, srt.default_params(max_depth=depth, photons_per_frame=photons))
+    spp = 16
+    r.render(srt.camera_uniform(pos, yaw, pitch, w / h, 0))
+    ctx.synchronize()
+    for k in range(1, 4):
+        r.render(srt.camera_uniform(pos, yaw, pitch, w / h, k))
+    ctx.synchronize()
+    r.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(spp):
+        r.render(srt.camera_uniform(pos, yaw, pitch, w / h, k))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = r.stats()
+    rays = st["rays_closest"] + st["rays_shadow"] + st["rays_photon"]
+    out = {"workload": f"C1: {scene.info()['triangles']} triangles, {w}x{h}, {spp} spp, depth {depth}, {photons} "
+                       f"photons/frame",
+           "gpu": {"ms_total": round(ms, 3), "mpaths_per_s": round(w * h * spp / ms / 1e3, 2),
+                   "mphotons_per_s": round(photons * spp / ms / 1e3, 2), "mrays_per_s": round(rays / ms / 1e3, 2)}}
+    r.close()
+    scene.close()
+    if cpu:
+        c = cpu_baseline(CONFIGS["config1"], frames=spp)
+        out["cpu"] = {"mpaths_per_s": c["value"], "cores": c["cores"], "seconds": c["seconds"],
+                      "mphotons_per_s": round(photons * spp / c["seconds"] / 1e6, 3),
+                      "mrays_per_s": round((c["rays_closest"] + c["rays_shadow"]) / c["seconds"] / 1e6, 3),
+                      "kind": "port"}
+    return out
+
+
 def guided_section(seconds=30.0, ref_spp=8192):
     """C4 at full size (1920x1080, depth 16): equal-time relMSE of guided vs
     plain against an FP64 reference of ref_spp frames rendered in two halves
@@ -412,6 +454,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--no-config1", action="store_true", help="skip the C1 section (GPU and CPU)")
     ap.add_argument("--no-batched", action="store_true", help="skip the C3 batched-renderer section")
     ap.add_argument("--no-guided", action="store_true", help="skip the C4 guided-vs-plain section")
     ap.add_argument("--no-batched-guided", action="store_true", help="skip the C5 batched-guiding section")
@@ -574,6 +617,9 @@ def main(argv=None):
         rt.close()
         rc.close()
 
+    config1 = None
+    if rank == 0 and world == 1 and not args.no_config1:
+        config1 = config1_section(srt, ctx, stream, cpu=not args.no_cpu_baseline)
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_section(srt, ctx, stream)
@@ -606,6 +652,7 @@ def main(argv=None):
                     "d2h_bytes_per_step": w * h * 4, "steps": e2e_steps} if e2e_steps else None,
             "gpu_launches": int(st["kernel_launches"]),
             "roofline": roof,
+            "config1": config1,
             "batched": batched,
             "guided": guided,
             "batched_guided": batched_guided,
