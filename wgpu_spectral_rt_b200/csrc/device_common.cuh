@@ -455,98 +455,6 @@ SRT_DEV bool tri_test(float3 v0, float3 v1, float3 v2, float3 o, uint32_t kx, ui
     v = __fmul_rn(W, inv);
     return true;
 }
-// Packed pairs of FP32 values (element 0 in the low word) and their
-// operations: add / sub / mul / fma .rn.f32x2 round each element exactly like
-// the scalar .rn operation.
-SRT_DEV uint64_t pk2(float a, float b) {
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-SRT_DEV float2 upk2(uint64_t x) {
-    float2 o;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(x));
-    return o;
-}
-SRT_DEV uint64_t sub2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-SRT_DEV uint64_t add2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-SRT_DEV uint64_t mul2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-SRT_DEV uint64_t fma2u(uint64_t a, uint64_t b, uint64_t c) {
-    uint64_t r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-SRT_DEV uint64_t neg2(uint64_t a) { return a ^ 0x8000000080000000ull; }
-SRT_DEV uint64_t sel3(uint64_t x, uint64_t y, uint64_t z, uint32_t k) { return k == 0u ? x : (k == 1u ? y : z); }
-
-// Two triangles P (p0, p1, p2) and Q (q0, q1, q2) against one ray: tri_test
-// on each, with the element-wise identical packed operations (bit 0: P hit,
-// bit 1: Q hit; t, u, v per element).  Where an edge function of a triangle
-// is exactly zero its three edge functions are redone in FP64, as in
-// tri_test, and the packed values are rebuilt from them.
-SRT_DEV uint32_t tri_test2(float3 p0, float3 p1, float3 p2, float3 q0, float3 q1, float3 q2, float3 o, uint32_t kx,
-                           uint32_t ky, uint32_t kz, float sx, float sy, float sz, float tmin, float tmax, float2& t,
-                           float2& u, float2& v) {
-    const uint64_t ox = pk2(o.x, o.x), oy = pk2(o.y, o.y), oz = pk2(o.z, o.z);
-    const uint64_t A0 = sub2(pk2(p0.x, q0.x), ox), A1 = sub2(pk2(p0.y, q0.y), oy), A2 = sub2(pk2(p0.z, q0.z), oz);
-    const uint64_t B0 = sub2(pk2(p1.x, q1.x), ox), B1 = sub2(pk2(p1.y, q1.y), oy), B2 = sub2(pk2(p1.z, q1.z), oz);
-    const uint64_t C0 = sub2(pk2(p2.x, q2.x), ox), C1 = sub2(pk2(p2.y, q2.y), oy), C2 = sub2(pk2(p2.z, q2.z), oz);
-    const uint64_t Az = sel3(A0, A1, A2, kz), Bz = sel3(B0, B1, B2, kz), Cz = sel3(C0, C1, C2, kz);
-    const uint64_t nsx = pk2(-sx, -sx), nsy = pk2(-sy, -sy);
-    const uint64_t Ax = fma2u(nsx, Az, sel3(A0, A1, A2, kx)), Ay = fma2u(nsy, Az, sel3(A0, A1, A2, ky));
-    const uint64_t Bx = fma2u(nsx, Bz, sel3(B0, B1, B2, kx)), By = fma2u(nsy, Bz, sel3(B0, B1, B2, ky));
-    const uint64_t Cx = fma2u(nsx, Cz, sel3(C0, C1, C2, kx)), Cy = fma2u(nsy, Cz, sel3(C0, C1, C2, ky));
-    uint64_t U = fma2u(Cx, By, neg2(mul2(Cy, Bx)));
-    uint64_t V = fma2u(Ax, Cy, neg2(mul2(Ay, Cx)));
-    uint64_t W = fma2u(Bx, Ay, neg2(mul2(By, Ax)));
-    float2 u2 = upk2(U), v2 = upk2(V), w2 = upk2(W);
-    const bool zp = u2.x == 0.0f || v2.x == 0.0f || w2.x == 0.0f, zq = u2.y == 0.0f || v2.y == 0.0f || w2.y == 0.0f;
-    if (zp || zq) {  // FP64 fallback: exact products (tri_test's)
-        const float2 ax = upk2(Ax), ay = upk2(Ay), bx = upk2(Bx), by = upk2(By), cx = upk2(Cx), cy = upk2(Cy);
-        if (zp) {
-            u2.x = (float)((double)cx.x * (double)by.x - (double)cy.x * (double)bx.x);
-            v2.x = (float)((double)ax.x * (double)cy.x - (double)ay.x * (double)cx.x);
-            w2.x = (float)((double)bx.x * (double)ay.x - (double)by.x * (double)ax.x);
-        }
-        if (zq) {
-            u2.y = (float)((double)cx.y * (double)by.y - (double)cy.y * (double)bx.y);
-            v2.y = (float)((double)ax.y * (double)cy.y - (double)ay.y * (double)cx.y);
-            w2.y = (float)((double)bx.y * (double)ay.y - (double)by.y * (double)ax.y);
-        }
-        U = pk2(u2.x, u2.y);
-        V = pk2(v2.x, v2.y);
-        W = pk2(w2.x, w2.y);
-    }
-    const bool sp = (u2.x < 0.0f || v2.x < 0.0f || w2.x < 0.0f) && (u2.x > 0.0f || v2.x > 0.0f || w2.x > 0.0f);
-    const bool sq = (u2.y < 0.0f || v2.y < 0.0f || w2.y < 0.0f) && (u2.y > 0.0f || v2.y > 0.0f || w2.y > 0.0f);
-    if (sp && sq) return 0u;
-    const float2 det = upk2(add2(add2(U, V), W));
-    const bool okp = !sp && det.x != 0.0f, okq = !sq && det.y != 0.0f;
-    if (!okp && !okq) return 0u;
-    const float ip = okp ? __frcp_rn(det.x) : 0.0f, iq = okq ? __frcp_rn(det.y) : 0.0f;
-    const uint64_t inv = pk2(ip, iq), sz2 = pk2(sz, sz);
-    const uint64_t T = fma2u(W, mul2(sz2, Cz), fma2u(V, mul2(sz2, Bz), mul2(U, mul2(sz2, Az))));
-    t = upk2(mul2(T, inv));
-    u = upk2(mul2(V, inv));
-    v = upk2(mul2(W, inv));
-    uint32_t hits = 0u;
-    if (okp && t.x >= tmin && t.x <= tmax) hits |= 1u;
-    if (okq && t.y >= tmin && t.y <= tmax) hits |= 2u;
-    return hits;
-}
-
 SRT_DEV bool intersect_tri(const Ray& ray, const RayShear& sh, float3 v0, float3 v1, float3 v2, float& t, float& u,
                            float& v) {
     return tri_test(v0, v1, v2, ray.o, (uint32_t)sh.kx, (uint32_t)sh.ky, (uint32_t)sh.kz, sh.sx, sh.sy, sh.sz,
@@ -590,12 +498,6 @@ SRT_DEV float2 fma2(float2 a, float2 b, float2 c) {
 // instead of per child (config-2 closest-hit 3.35 vs 3.43 ms per frame).
 #ifndef SRT_TRAV_LEAN
 #define SRT_TRAV_LEAN 1
-#endif
-
-// Closest-hit steps test the pending triangles two at a time (tri_test2,
-// packed FP32x2 arithmetic that rounds like tri_test).
-#ifndef SRT_TRAV_TRI_PAIRS
-#define SRT_TRAV_TRI_PAIRS 0
 #endif
 
 // Closest-hit steps of the one-ray-per-thread loop (traverse<>): the lanes
@@ -1106,7 +1008,6 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
     // well formed.  Syncing the ballot of all lanes that take the step instead
     // (a stronger wait) measured slower: closest-hit 3.40 vs 3.30 ms per frame.
     constexpr bool kSync = SRT_TRAV_WARPSYNC && !ANY && !PF && !SRT_TRAV_ONE_TRI_PER_STEP;
-    constexpr bool kPairs = SRT_TRAV_TRI_PAIRS && !ANY && !SRT_TRAV_ONE_TRI_PER_STEP;
     const uint32_t entered = kSync ? __activemask() : 0u;
     bool any_hit = false;
     bool have = true;
@@ -1150,40 +1051,6 @@ SRT_DEV bool trav_step(const DevScene& S, TravState& T, uint2* stack, int stride
 #endif
         int b = __ffs(T.tg.y) - 1;
         T.tg.y &= T.tg.y - 1u;
-        if constexpr (kPairs) {
-            if (T.tg.y != 0u) {  // two triangles at once (tri_test2)
-                const int b2 = __ffs(T.tg.y) - 1;
-                T.tg.y &= T.tg.y - 1u;
-                const TriSlot* tp = S.tris + T.tg.x + (uint32_t)b;
-                const TriSlot* tq = S.tris + T.tg.x + (uint32_t)b2;
-                const float4 p0 = __ldg(&tp->v0), p1 = __ldg(&tp->v1), p2 = __ldg(&tp->v2);
-                const float4 q0 = __ldg(&tq->v0), q1 = __ldg(&tq->v1), q2 = __ldg(&tq->v2);
-                n_tris += 2;
-                float2 t2, u2, v2;
-                const uint32_t h = tri_test2(xyz(p0), xyz(p1), xyz(p2), xyz(q0), xyz(q1), xyz(q2), T.o, kx, ky, kz,
-                                             T.sx, T.sy, T.sz, T.tmin, T.tbest, t2, u2, v2);
-                // (t, id) lexicographic in full: Q was tested against the t_max before P's hit
-                if (h & 1u) {
-                    const uint32_t id = __float_as_uint(p0.w);
-                    if (t2.x < T.tbest || (t2.x == T.tbest && id < T.best)) {
-                        T.tbest = t2.x;
-                        T.best = id;
-                        T.bu = u2.x;
-                        T.bv = v2.x;
-                    }
-                }
-                if (h & 2u) {
-                    const uint32_t id = __float_as_uint(q0.w);
-                    if (t2.y < T.tbest || (t2.y == T.tbest && id < T.best)) {
-                        T.tbest = t2.y;
-                        T.best = id;
-                        T.bu = u2.y;
-                        T.bv = v2.y;
-                    }
-                }
-                continue;
-            }
-        }
         const TriSlot* ts = S.tris + T.tg.x + (uint32_t)b;
         float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
         ++n_tris;

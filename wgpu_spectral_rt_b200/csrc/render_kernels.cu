@@ -598,122 +598,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TAIL_MIN_BLOCKS) k_tail(Frame
     }
 }
 
-// The tail with warp-synchronous stages (SRT_TAIL_WARP_STAGES): the lanes of
-// a warp each hold a path and take their stages together — every lane's
-// closest hit (resumable traversal steps until the warp's last ray is done),
-// then every lane's shading, then every lane's shadow ray (pooled triangle
-// tests) — and a lane whose path ends takes a new one from the queue at the
-// next round.  Per path the operations and their order are k_tail's, so the
-// image and the counts are the same.
-#ifndef SRT_TAIL_WARP_STAGES
-#define SRT_TAIL_WARP_STAGES 0
-#endif
-template <bool GUIDE, bool COUNT, int STACK>
-__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TAIL_MIN_BLOCKS) k_tail_ws(FrameArgs a, uint32_t first) {
-    extern __shared__ uint2 stack_smem[];
-    __shared__ uint32_t n_closest[MAX_BOUNCES + 1], n_shadow[MAX_BOUNCES + 1];
-    for (uint32_t i = threadIdx.x; i <= (uint32_t)MAX_BOUNCES; i += blockDim.x) n_closest[i] = n_shadow[i] = 0u;
-    __syncthreads();
-    constexpr uint32_t FULL = 0xFFFFFFFFu;
-    uint2* stack = stack_smem + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t n = a.counters->paths[first];
-    uint32_t* fetch = &a.counters->fetch[TRAV_CLOSEST][first];
-    const uint32_t* queue = a.pb.queue[first & 1];
-    const DevScene& S = a.scene;
-    bool has = false, exhausted = false;
-    uint32_t id = 0, b = first;
-    while (true) {
-        // lanes without a path take the next ones (one atomic per warp)
-        const uint32_t need = __ballot_sync(FULL, !has);
-        if (need != 0u && !exhausted) {
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(need));
-            base = __shfl_sync(FULL, base, 0);
-            if (base + (uint32_t)__popc(need) >= n) exhausted = true;
-            if (!has) {
-                const uint32_t my = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                if (my < n) {
-                    id = queue[my];
-                    b = first;
-                    has = true;
-                }
-            }
-        }
-        if (__ballot_sync(FULL, has) == 0u) {
-            if (exhausted) break;
-            continue;
-        }
-        if (has && b > first) atomicAdd(&n_closest[b], 1u);  // paths[first] was counted by the last shading step
-        // closest hit of every lane's ray
-        TravState T;
-        bool tracing = false;
-        if (has) {
-            const float4 o = a.pb.ray_o[id], d = a.pb.ray_d[id];
-            tracing = trav_init(T, S, xyz(o), xyz(d), o.w, d.w);
-            if (!tracing) T.best = MISS;
-        }
-        uint32_t nn = 0, nt = 0;
-        while (__ballot_sync(FULL, tracing) != 0u) {
-            if (tracing && trav_step<false, STACK>(S, T, stack, TRACE_BLOCK, a.err, nn, nt)) tracing = false;
-        }
-        VertexOut vo;
-        if (has) {
-            if (COUNT) {
-                atomicAdd(&a.stats->nodes_bounce[TRAV_CLOSEST][b], (unsigned long long)nn);
-                atomicAdd(&a.stats->tris_bounce[TRAV_CLOSEST][b], (unsigned long long)nt);
-            }
-            a.pb.hit[id] = T.best != MISS ? make_float4(T.tbest, __uint_as_float(T.best), T.bu, T.bv)
-                                          : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
-            vo = shade_vertex<GUIDE>(a, id, b);
-        }
-        // shadow ray of every lane that has one
-        const bool sh = has && vo.shadow;
-        if (sh) atomicAdd(&n_shadow[b], 1u);
-        TravState U;
-        bool stracing = false;
-        if (sh) {
-            stracing = trav_init(U, S, vo.sh_o, vo.sh_d, 0.001f, vo.sh_tmax);
-            if (!stracing) U.best = MISS;
-        }
-        uint32_t sn = 0, st = 0;
-        while (__ballot_sync(FULL, stracing) != 0u) {
-            pool_tris<true>(S, U, stracing, st);
-            if (stracing && U.best != MISS) stracing = false;  // occluded
-            if (stracing && trav_step<true, STACK>(S, U, stack, TRACE_BLOCK, a.err, sn, st)) stracing = false;
-        }
-        if (sh) {
-            if (COUNT) {
-                atomicAdd(&a.stats->nodes_bounce[TRAV_SHADOW][b], (unsigned long long)sn);
-                atomicAdd(&a.stats->tris_bounce[TRAV_SHADOW][b], (unsigned long long)st);
-            }
-            if (U.best == MISS) {  // as the shadow-ray kernel adds it (shader.wgsl:659-669)
-                const float4 r = a.pb.rad[id], c = vo.sh_c;
-                a.pb.rad[id] =
-                    make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z), __fadd_rn(r.w, c.w));
-            }
-        }
-        if (has) {
-            if (vo.alive) ++b;
-            else has = false;
-        }
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i <= (uint32_t)MAX_BOUNCES; i += blockDim.x) {
-        if (n_closest[i]) atomicAdd(&a.counters->paths[i], n_closest[i]);
-        if (n_shadow[i]) atomicAdd(&a.counters->shadow[i], n_shadow[i]);
-    }
-}
-
 // Resident blocks per SM of one k_tail instantiation (its grid is one wave).
 template <bool GUIDE, bool COUNT, int STACK>
 int tail_per_sm() {
     static int per_sm = 0;
     if (per_sm == 0) {
         int x = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, SRT_TAIL_WARP_STAGES ? k_tail_ws<GUIDE, COUNT, STACK>
-                                                                                : k_tail<GUIDE, COUNT, STACK>,
-                                                          TRACE_BLOCK,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, k_tail<GUIDE, COUNT, STACK>, TRACE_BLOCK,
                                                           sizeof(uint2) * STACK * TRACE_BLOCK) != cudaSuccess ||
             x < 1)
             x = 1;
@@ -726,8 +617,7 @@ template <bool GUIDE, bool COUNT, int STACK>
 int launch_tail_t(const FrameArgs& a, uint32_t first, cudaStream_t st) {
     const size_t smem = sizeof(uint2) * STACK * TRACE_BLOCK;
     const uint32_t grid = (uint32_t)(a.sm_count > 0 ? a.sm_count : 148) * (uint32_t)tail_per_sm<GUIDE, COUNT, STACK>();
-    if (SRT_TAIL_WARP_STAGES) k_tail_ws<GUIDE, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a, first);
-    else k_tail<GUIDE, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a, first);
+    k_tail<GUIDE, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(a, first);
     return 1;
 }
 
