@@ -500,13 +500,6 @@ SRT_DEV float2 fma2(float2 a, float2 b, float2 c) {
 #define SRT_TRAV_LEAN 1
 #endif
 
-// Closest-hit steps of the one-ray-per-thread loop (traverse<>): the lanes
-// converged at an iteration's start wait for each other before its node
-// visit (__syncwarp; trav_step does the same for the persistent kernels).
-#ifndef SRT_TRAV_WARPSYNC_LOOP
-#define SRT_TRAV_WARPSYNC_LOOP 0
-#endif
-
 struct TravCounters {
     unsigned long long* nodes;
     unsigned long long* tris;
@@ -635,12 +628,7 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
     // virtual group holding the root as child slot 0
     uint2 g = make_uint2(0u, (1u << (24 + (0u ^ (oct ^ 7u)))) | 1u);
     uint2 tg = make_uint2(0u, 0u);
-    // closest hit without prefetch: the lanes converged at an iteration's
-    // start wait for each other before its node visit, every exit deferred
-    // past the __syncwarp (as in trav_step)
-    constexpr bool kLoopSync = SRT_TRAV_WARPSYNC_LOOP && !ANY && !PF;
     while (true) {
-        const uint32_t entered = kLoopSync ? __activemask() : 0u;
         // ---- with PF: pick the next node and start fetching it before the
         // triangle tests of the last node (the same visiting order)
         bool have = true;
@@ -713,43 +701,6 @@ SRT_DEV bool traverse(const DevScene& S, Ray ray, uint2* stack, int stride, floa
             continue;
         }
         // ---- next node
-        if constexpr (kLoopSync) {
-            bool fin = false;
-            uint32_t nidx = 0u;
-            if ((g.y & 0xFF000000u) == 0u) {
-                if (sp == 0) fin = true;
-                else {
-                    --sp;
-                    g = stack[sp * stride];
-                }
-            }
-            if (!fin) {
-                const int b2 = 31 - __clz(g.y & 0xFF000000u);
-                g.y &= ~(1u << b2);
-                const uint32_t sl = (uint32_t)(b2 - 24) ^ (oct ^ 7u);
-                nidx = g.x + __popc(g.y & ((1u << sl) - 1u) & 0xFFu);
-                if (g.y & 0xFF000000u) {
-                    if (sp >= STACK) {
-                        atomicOr(err, ERR_STACK_OVERFLOW);
-                        fin = true;
-                    } else {
-                        stack[sp * stride] = g;
-                        ++sp;
-                    }
-                }
-                if (!fin && nidx >= S.n_nodes) {
-                    atomicOr(err, ERR_BAD_INDEX);
-                    fin = true;
-                }
-            }
-            __syncwarp(entered);
-            if (fin) break;
-            const uint4* np = reinterpret_cast<const uint4*>(S.nodes + nidx);
-            uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-            if (COUNT) ++n_nodes;
-            node_children(w0, w1, w2, w3, w4, ray.o, idir, oct, ray.tmin, tbest, g, tg);
-            continue;
-        }
         if ((g.y & 0xFF000000u) == 0u) {
             if (sp == 0) break;
             --sp;
