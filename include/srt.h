@@ -335,7 +335,11 @@ srt_status srt_renderer_destroy(srt_renderer* r);
 /* One frame = one sample per pixel: photon emit -> grid build -> camera
  * paths -> accumulate + tonemap (renderer/mod.rs:168-207).  cam->frame_count
  * seeds the RNG and resets the accumulation when 0 (engine.rs:154-166,
- * shader.wgsl:803-805).  Asynchronous on the context's stream. */
+ * shader.wgsl:803-805).  Asynchronous on the context's stream.  A frame also
+ * builds, beside its camera paths, the photon map of frame count
+ * cam->frame_count + 1 for the next call; a call with another count, or after
+ * the scene changed, builds its own map first.  The images are those of
+ * building each frame's map inside the frame. */
 srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform* cam);
 /* Renderer.frame_count (renderer/mod.rs:30, incremented at :204). */
 uint32_t srt_renderer_frame_count(const srt_renderer* r);

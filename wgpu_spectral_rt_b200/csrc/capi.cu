@@ -321,6 +321,9 @@ struct srt_scene {
     uint32_t* refit_err = nullptr;
     // tree rebuilds: renderers compare gen with the one they captured
     uint32_t gen = 0;
+    // any change of the geometry (instance updates, rebuilds): a photon map
+    // built ahead of a frame is stale after it
+    uint32_t version = 0;
     int builder = BVH_BUILDER_SAH;
     int width = 8;
     uint32_t n_inst = 0;
@@ -537,6 +540,7 @@ extern "C" srt_status srt_scene_update_instances(srt_scene* s, const uint32_t* i
     cudaStream_t st = c->stream;
     const uint32_t ni = (uint32_t)s->h_inst.size();
     if (n == 0 || ni == 0) return SRT_OK;
+    s->version += 1;
     std::vector<InstDev> nd(n);
     std::vector<InstFwd> nf(n);
     for (uint32_t k = 0; k < n; ++k) {
@@ -664,6 +668,7 @@ extern "C" srt_status srt_scene_rebuild_bvh(srt_scene* s, uint32_t width) {
     d.n_nodes = s->bvh.n_nodes;
     d.depth = s->bvh.depth;
     s->gen += 1;
+    s->version += 1;
     return SRT_OK;
 }
 
@@ -699,6 +704,11 @@ extern "C" srt_status srt_scene_bvh_width(const srt_scene* s, uint32_t* width) {
 #ifndef SRT_FRAME_OVERLAP
 #define SRT_FRAME_OVERLAP 1
 #endif
+// A frame builds the next frame's photon map beside its own camera paths
+// (srt_renderer::record_overlapped with a photon set).
+#ifndef SRT_PHOTON_PIPELINE
+#define SRT_PHOTON_PIPELINE 1
+#endif
 
 struct srt_renderer {
     srt_ctx* ctx = nullptr;
@@ -711,10 +721,7 @@ struct srt_renderer {
         scene_gen = scene->gen;
         args.scene = scene->dev;
         args_gen += 1;
-        if (graph) {
-            cudaGraphExecDestroy(graph);
-            graph = nullptr;
-        }
+        drop_graph();
     }
     uint32_t w = 0, h = 0;
     srt_params p{};
@@ -754,8 +761,108 @@ struct srt_renderer {
     cudaEvent_t ldr_ev[2] = {nullptr, nullptr};
     uint32_t ldr_calls = 0;
 
+    // Photon-pass pipelining (SRT_PHOTON_PIPELINE): frame F's graph builds the
+    // photon map of frame F + 1 on a branch of its own, beside F's camera
+    // paths, which gather from the map built during the frame before.  The
+    // photon arrays the camera paths read (stored photons, sorted photons,
+    // grid ranges) and the photon pass's counters exist twice (set 0 is
+    // `ph`'s); the working arrays are shared, since one photon pass runs at a
+    // time.  A frame whose frame count is not the one predicted (or after a
+    // scene change) first builds its own map.
+    struct PipeSet {
+        float4 *photons = nullptr, *sorted = nullptr;
+        uint2* ranges = nullptr;
+        FrameCounters* counters = nullptr;       // the photon pass's
+        srt_camera_uniform* cam = nullptr;       // device: the photon pass's frame count
+    } pipe[2];
+    bool pipe_alloc = false;
+    bool pipe_valid = false;                     // set pipe_cur holds the map of frame pipe_next
+    int pipe_cur = 0;
+    uint32_t pipe_next = 0;
+    uint32_t pipe_scene_version = 0;
+    int last_set = -1;                           // set the last frame gathered from (-1: `ph`, `counters`)
+    cudaGraphExec_t pipe_graph[2] = {nullptr, nullptr};
+    int pipe_launches[2] = {0, 0};
+    cudaStream_t ph_stream = nullptr;
+    cudaEvent_t pfork_ev = nullptr, pjoin_ev = nullptr;
+    srt_camera_uniform* ph_ring = nullptr;       // pinned staging, 4 slots (with cam_ring's events)
+
+    // The photon pass's arguments writing set s, and the camera paths'
+    // arguments gathering from set s.
+    FrameArgs photon_args(int s) const {
+        FrameArgs a = args;
+        a.counters = pipe[s].counters;
+        a.ph_counters = pipe[s].counters;
+        a.cam = pipe[s].cam;
+        a.ph.photons = pipe[s].photons;
+        a.ph.sorted = pipe[s].sorted;
+        a.ph.ranges = pipe[s].ranges;
+        return a;
+    }
+    FrameArgs camera_args(int s) const {
+        FrameArgs a = args;
+        a.ph_counters = pipe[s].counters;
+        a.ph.photons = pipe[s].photons;
+        a.ph.sorted = pipe[s].sorted;
+        a.ph.ranges = pipe[s].ranges;
+        a.gather.photons = pipe[s].sorted;
+        a.gather.ranges = pipe[s].ranges;
+        return a;
+    }
+    // The photon map of the last frame rendered (its counters and stored photons).
+    const FrameCounters* last_photon_counters() const { return last_set >= 0 ? pipe[last_set].counters : counters; }
+    const float4* last_photons() const { return last_set >= 0 ? pipe[last_set].photons : ph.photons; }
+    // The second photon set, both sets' counters and uniforms, the photon
+    // branch's stream and events, the pinned staging (once).
+    cudaError_t ensure_pipe() {
+        if (pipe_alloc) return cudaSuccess;
+        cudaError_t e;
+        const uint32_t cap = ph.capacity;
+        pipe[0].photons = ph.photons;
+        pipe[0].sorted = ph.sorted;
+        pipe[0].ranges = ph.ranges;
+        if ((e = dev_alloc(&pipe[1].photons, 2ull * cap)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&pipe[1].sorted, 2ull * cap)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&pipe[1].ranges, (size_t)1 << p.hash_bits)) != cudaSuccess) return e;
+        if ((e = cudaMemset(pipe[1].ranges, 0, sizeof(uint2) << p.hash_bits)) != cudaSuccess) return e;
+        for (auto& ps : pipe) {
+            if ((e = dev_alloc(&ps.counters, 1)) != cudaSuccess) return e;
+            if ((e = cudaMemset(ps.counters, 0, sizeof(FrameCounters))) != cudaSuccess) return e;
+            if ((e = dev_alloc(&ps.cam, 1)) != cudaSuccess) return e;
+        }
+        if ((e = cudaMallocHost((void**)&ph_ring, 8 * sizeof(srt_camera_uniform))) != cudaSuccess) return e;
+        if ((e = cudaStreamCreateWithFlags(&ph_stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&pfork_ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&pjoin_ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+        pipe_alloc = true;
+        return cudaSuccess;
+    }
+    void drop_pipe_graphs() {
+        for (auto& g : pipe_graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        pipe_valid = false;
+    }
+
     ~srt_renderer() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (auto& g : pipe_graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (ph_stream) cudaStreamDestroy(ph_stream);
+        if (pfork_ev) cudaEventDestroy(pfork_ev);
+        if (pjoin_ev) cudaEventDestroy(pjoin_ev);
+        cudaFreeHost(ph_ring);
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1) {  // set 0's arrays are `ph`'s, freed below
+                cudaFree(pipe[k].photons);
+                cudaFree(pipe[k].sorted);
+                cudaFree(pipe[k].ranges);
+            }
+            cudaFree(pipe[k].counters);
+            cudaFree(pipe[k].cam);
+        }
         if (counts_ev) cudaEventDestroy(counts_ev);
         if (counts_host) cudaFreeHost(counts_host);
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -820,6 +927,7 @@ struct srt_renderer {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
         }
+        drop_pipe_graphs();
     }
     // SRT_TAIL_AUTO: after the first frame, read its path counts back without
     // waiting and, once they are there, choose the tail (the next frame is
@@ -896,7 +1004,11 @@ struct srt_renderer {
     // path radiance, which the shading of b + 1 reads after the join; the
     // closest hits read and write only rays, queues and hits).  The results
     // are those of the serial order.
-    int record_overlapped(cudaStream_t st) {
+    // `set` >= 0: the pipelined frame (SRT_PHOTON_PIPELINE): the camera paths
+    // gather from photon set `set`, built before this frame, while a branch of
+    // its own builds the next frame's map into set `set` ^ 1 (frame count from
+    // pipe[set ^ 1].cam), joined at the frame's end.
+    int record_overlapped(cudaStream_t st, int set = -1) {
         int n = 0;
         cudaStream_t s2 = side_stream;
         auto fork = [&]() {
@@ -907,6 +1019,10 @@ struct srt_renderer {
             cudaEventRecord(join_ev, s2);
             cudaStreamWaitEvent(st, join_ev, 0);
         };
+        const bool pipelined = set >= 0;
+        FrameArgs ca;
+        if (pipelined) ca = camera_args(set);
+        FrameArgs& A = pipelined ? ca : args;
         cudaMemsetAsync(counters, 0, sizeof(FrameCounters), st);
         const bool deferred = args.guiding != 0;
         if (deferred) {
@@ -916,38 +1032,51 @@ struct srt_renderer {
             // frame: no records)
             cudaEventRecord(tfork_ev, st);
             cudaStreamWaitEvent(train_stream, tfork_ev, 0);
-            n += launch_guide_steps(args, train_stream);
+            n += launch_guide_steps(A, train_stream);
             cudaEventRecord(tjoin_ev, train_stream);
         }
-        fork();
-        n += launch_raygen(args, s2);
-        n += launch_bounce(args, 0, s2, 1);
-        if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
-        join();
+        if (pipelined) {
+            const int nx = set ^ 1;
+            cudaEventRecord(pfork_ev, st);
+            cudaStreamWaitEvent(ph_stream, pfork_ev, 0);
+            cudaMemsetAsync(pipe[nx].counters, 0, sizeof(FrameCounters), ph_stream);
+            FrameArgs pa = photon_args(nx);
+            n += launch_photon_pass(pa, ph_stream);
+            cudaEventRecord(pjoin_ev, ph_stream);
+            n += launch_raygen(A, st);
+            n += launch_bounce(A, 0, st, 1);
+        } else {
+            fork();
+            n += launch_raygen(A, s2);
+            n += launch_bounce(A, 0, s2, 1);
+            if (p.photons_per_frame > 0 && scene->n_lights > 0) n += launch_photon_pass(args, st);
+            join();
+        }
         if (deferred) cudaStreamWaitEvent(st, tjoin_ev, 0);
         const uint32_t tail = tail_start();
         for (uint32_t b = 0; b < p.max_depth; ++b) {
-            n += launch_bounce(args, b, st, 2);
+            n += launch_bounce(A, b, st, 2);
             if (b + 1 == tail) {
                 // the tail kernel shades paths whose radiance these shadow rays add to: after them
-                n += launch_bounce(args, b, st, 3);
-                n += launch_tail(args, tail, st);
+                n += launch_bounce(A, b, st, 3);
+                n += launch_tail(A, tail, st);
                 break;
             }
             if (b + 1 < p.max_depth) {
                 fork();
-                n += launch_bounce(args, b, s2, 3);
-                n += launch_bounce(args, b + 1, st, 1);
+                n += launch_bounce(A, b, s2, 3);
+                n += launch_bounce(A, b + 1, st, 1);
                 join();
             } else {
-                n += launch_bounce(args, b, st, 3);
+                n += launch_bounce(A, b, st, 3);
             }
         }
-        n += launch_finalize(args, st);
-        n += launch_frame_stats(args, st);
+        n += launch_finalize(A, st);
+        n += launch_frame_stats(A, st);
         // the training weights read this frame's path radiance: before the
         // next frame's camera rays reset it; the steps run in the next frame
-        if (deferred) n += launch_guide_targets(args, st);
+        if (deferred) n += launch_guide_targets(A, st);
+        if (pipelined) cudaStreamWaitEvent(st, pjoin_ev, 0);
         return n;
     }
 
@@ -1112,6 +1241,7 @@ extern "C" srt_status srt_renderer_create(srt_ctx* c, srt_scene* s, uint32_t w, 
     a.photons_per_frame = p.photons_per_frame;
     a.photon_max_bounces = p.photon_max_bounces;
     a.counters = r->counters;
+    a.ph_counters = r->counters;
     a.stats = r->stats;
     a.err = r->err;
     a.pb = pb;
@@ -1188,10 +1318,51 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
     CUDA_TRY(c, cudaEventSynchronize(r->ring_ev[slot]));
     r->cam_ring[slot] = *cam;
     CUDA_TRY(c, cudaMemcpyAsync(r->cam_dev, &r->cam_ring[slot], sizeof(srt_camera_uniform), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(c, cudaEventRecord(r->ring_ev[slot], st));
     bool timed = (r->p.flags & SRT_FLAG_STAGE_TIMING) != 0;
     bool use_graph = !timed && !(r->p.flags & SRT_FLAG_NO_GRAPH);
-    if (use_graph) {
+    const bool pipelined = SRT_PHOTON_PIPELINE && SRT_FRAME_OVERLAP && !timed && r->p.photons_per_frame > 0 &&
+                           r->scene->n_lights > 0;
+    if (pipelined) {
+        CUDA_TRY(c, r->ensure_pipe());
+        // this frame's photon map: built during the last frame, or now
+        const uint32_t F = cam->frame_count;
+        const int cur = r->pipe_cur;
+        srt_camera_uniform* pr = r->ph_ring + 2 * slot;
+        pr[0] = *cam;
+        pr[1] = *cam;
+        pr[1].frame_count = F + 1u;  // the next frame's photon pass
+        if (!(r->pipe_valid && r->pipe_next == F && r->pipe_scene_version == r->scene->version)) {
+            CUDA_TRY(c, cudaMemcpyAsync(r->pipe[cur].cam, pr, sizeof *pr, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(c, cudaMemsetAsync(r->pipe[cur].counters, 0, sizeof(FrameCounters), st));
+            FrameArgs pa = r->photon_args(cur);
+            r->launches += (uint64_t)launch_photon_pass(pa, st);
+            CUDA_TRY(c, cudaGetLastError());
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(r->pipe[cur ^ 1].cam, pr + 1, sizeof *pr, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(c, cudaEventRecord(r->ring_ev[slot], st));
+        if (use_graph) {
+            if (!r->pipe_graph[cur]) {
+                cudaGraph_t g;
+                CUDA_TRY(c, cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal));
+                r->pipe_launches[cur] = r->record_overlapped(r->cap_stream, cur);
+                CUDA_TRY(c, cudaStreamEndCapture(r->cap_stream, &g));
+                cudaError_t e = cudaGraphInstantiate(&r->pipe_graph[cur], g, 0);
+                cudaGraphDestroy(g);
+                CUDA_TRY(c, e);
+            }
+            CUDA_TRY(c, cudaGraphLaunch(r->pipe_graph[cur], st));
+            r->launches += (uint64_t)r->pipe_launches[cur];
+        } else {
+            r->launches += (uint64_t)r->record_overlapped(st, cur);
+            CUDA_TRY(c, cudaGetLastError());
+        }
+        r->last_set = cur;
+        r->pipe_cur = cur ^ 1;
+        r->pipe_next = F + 1u;
+        r->pipe_valid = true;
+        r->pipe_scene_version = r->scene->version;
+    } else if (use_graph) {
+        CUDA_TRY(c, cudaEventRecord(r->ring_ev[slot], st));
         if (!r->graph) {
             cudaGraph_t g;
             CUDA_TRY(c, cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -1203,7 +1374,10 @@ extern "C" srt_status srt_render_frame(srt_renderer* r, const srt_camera_uniform
         }
         CUDA_TRY(c, cudaGraphLaunch(r->graph, st));
         r->launches += (uint64_t)r->launches_per_frame;
+        r->last_set = -1;
     } else {
+        CUDA_TRY(c, cudaEventRecord(r->ring_ev[slot], st));
+        r->last_set = -1;
         int n = r->record(st, timed);
         r->launches += (uint64_t)n;
         CUDA_TRY(c, cudaGetLastError());
@@ -1430,12 +1604,13 @@ extern "C" srt_status srt_renderer_read_photons(srt_renderer* r, srt_photon* out
     if (!r || !count) return SRT_ERR_INVALID_ARG;
     srt_ctx* c = r->ctx;
     FrameCounters fc;
-    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->counters, sizeof fc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->last_photon_counters(), sizeof fc, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     *count = r->p.photons_per_frame ? fc.photons_stored : 0u;
     uint32_t n = std::min(*count, capacity);
     if (out && n) {
-        CUDA_TRY(c, cudaMemcpyAsync(out, r->ph.photons, (size_t)n * sizeof(srt_photon), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(out, r->last_photons(), (size_t)n * sizeof(srt_photon), cudaMemcpyDeviceToHost,
+                                    c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     }
     return check_device_error(c, r->err);
@@ -1682,10 +1857,7 @@ extern "C" srt_status srt_renderer_guide_configure(srt_renderer* r, float lr, ui
     if (batch > 0) r->guide.batch = batch;
     r->args.guide = r->guide;
     r->args_gen += 1;
-    if (r->graph) {  // both are kernel arguments of the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // both are kernel arguments of the captured frame
     return SRT_OK;
 }
 
@@ -1699,10 +1871,7 @@ extern "C" srt_status srt_renderer_guide_set_steps(srt_renderer* r, uint32_t ste
     r->guide.steps = steps;
     r->args.guide = r->guide;
     r->args_gen += 1;
-    if (r->graph) {  // the step count shapes the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // the step count shapes the captured frame
     return SRT_OK;
 }
 
@@ -1772,10 +1941,7 @@ extern "C" srt_status srt_renderer_guide_set_training(srt_renderer* r, int kind)
     r->guide.tc_train = kind == SRT_GUIDE_TRAIN_TCGEN05 ? 1 : 0;
     r->args.guide = r->guide;
     r->args_gen += 1;
-    if (r->graph) {  // the choice is baked into the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // the choice is baked into the captured frame
     return SRT_OK;
 }
 
@@ -1789,10 +1955,7 @@ extern "C" srt_status srt_renderer_guide_set_inference(srt_renderer* r, int kind
     r->guide.tc = kind == SRT_GUIDE_INFER_TCGEN05 ? 1 : 0;
     r->args.guide = r->guide;
     r->args_gen += 1;
-    if (r->graph) {  // the choice is baked into the captured frame
-        cudaGraphExecDestroy(r->graph);
-        r->graph = nullptr;
-    }
+    r->drop_graph();  // the choice is baked into the captured frame
     return SRT_OK;
 }
 
@@ -1974,7 +2137,7 @@ extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_came
     srt_ctx* c = r->ctx;
     cudaSetDevice(c->device);
     FrameCounters fc;
-    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->counters, sizeof fc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(&fc, r->last_photon_counters(), sizeof fc, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     uint32_t n = r->p.photons_per_frame ? std::min(fc.photons_stored, r->p.photons_per_frame) : 0u;
     DevBufs b;
@@ -1986,7 +2149,7 @@ extern "C" srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_came
     CUDA_TRY(c, b.alloc(&img, (size_t)w * h));
     CUDA_TRY(c, cudaMemcpyAsync(dc, cam, sizeof *cam, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(img, rgba, (size_t)w * h * 4, cudaMemcpyHostToDevice, c->stream));
-    launch_photon_splat(r->ph.photons, n, dc, w, h, counts, img, c->stream);
+    launch_photon_splat(r->last_photons(), n, dc, w, h, counts, img, c->stream);
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaMemcpyAsync(rgba, img, (size_t)w * h * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));

@@ -666,8 +666,8 @@ __global__ void k_frame_stats(FrameArgs a) {
     unsigned long long pr = 0;
     if (a.photons_per_frame > 0u)
         for (uint32_t i = 0; i < a.photon_max_bounces; ++i) {
-            pr += a.counters->photon_paths[i];
-            a.stats->rays_bounce[TRAV_PHOTON][i] += a.counters->photon_paths[i];
+            pr += a.ph_counters->photon_paths[i];
+            a.stats->rays_bounce[TRAV_PHOTON][i] += a.ph_counters->photon_paths[i];
         }
     a.stats->photon_rays += pr;
 }

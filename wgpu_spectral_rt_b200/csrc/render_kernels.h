@@ -85,6 +85,10 @@ struct FrameArgs {
     uint32_t photons_per_frame;
     uint32_t photon_max_bounces;
     FrameCounters* counters;
+    // the counters of the photon pass whose map this frame gathers from (its
+    // photon rays go into the frame's statistics): `counters` unless the
+    // renderer builds the next frame's photon map during this frame
+    const FrameCounters* ph_counters;
     DevStats* stats;
     uint32_t* err;
     PathBuffers pb;
