@@ -21,6 +21,14 @@
 #ifndef SRT_TRACE_MIN_BLOCKS
 #define SRT_TRACE_MIN_BLOCKS 8
 #endif
+// resident blocks of the persistent kernel (k_trace_pt) per SM: 9 caps it at
+// 56 registers without spills of the closest-hit form (a 4-byte spill in the
+// any-hit form); config-2 frame 9.16 vs 9.43 ms with 8 (closest-hit bounces
+// 1-4 6 % faster, photon pass 2.45 vs 2.54 ms).  The one-ray-per-thread
+// kernel stays at 8 (bounce 0 0.44 vs 0.42 ms with 9); 10 blocks spill.
+#ifndef SRT_TRACE_PT_BLOCKS
+#define SRT_TRACE_PT_BLOCKS 9
+#endif
 // idle lanes that trigger a refill of the warp: closest-hit and any-hit
 // kernels (config-2 frame, refill at 4 / 6 / 8 / 12 / 16 / 20 idle lanes for
 // both: 10.01 / 9.96 / 9.94 / 9.97 / 10.10 / 10.31 ms; closest-hit traversal is
@@ -112,7 +120,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
 
 // Persistent form: same inputs and outputs, queue positions from *fetch.
 template <bool ANY, bool COUNT, int STACK>
-__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_PT_BLOCKS)
     k_trace_pt(DevScene S, const uint32_t* __restrict__ queue, const uint32_t* __restrict__ count,
                uint32_t* __restrict__ fetch, const float4* __restrict__ ro, const float4* __restrict__ rd,
                float4* __restrict__ hit, const uint32_t* __restrict__ sh_id, const float4* __restrict__ sh_c,
@@ -280,7 +288,7 @@ template <bool ANY, bool COUNT, int STACK>
 void launch_one(const TraceLaunch& L, cudaStream_t st) {
     size_t smem = trace_smem<STACK>();
     if (SRT_TRACE_PERSISTENT && L.fetch) {
-        uint32_t grid = (uint32_t)(L.sm_count > 0 ? L.sm_count : 148) * SRT_TRACE_MIN_BLOCKS;
+        uint32_t grid = (uint32_t)(L.sm_count > 0 ? L.sm_count : 148) * SRT_TRACE_PT_BLOCKS;
         grid = std::min(grid, std::max(1u, blocks_for(L.max_n, TRACE_BLOCK)));
         k_trace_pt<ANY, COUNT, STACK><<<grid, TRACE_BLOCK, smem, st>>>(L.s, L.queue, L.count, L.fetch, L.ro, L.rd,
                                                                       L.hit, L.sh_id, L.sh_c, L.rad, L.err, L.stats,
