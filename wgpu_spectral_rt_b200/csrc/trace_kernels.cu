@@ -25,7 +25,8 @@
 // 56 registers without spills of the closest-hit form (a 4-byte spill in the
 // any-hit form); config-2 frame 9.16 vs 9.43 ms with 8 (closest-hit bounces
 // 1-4 6 % faster, photon pass 2.45 vs 2.54 ms).  The one-ray-per-thread
-// kernel stays at 8 (bounce 0 0.44 vs 0.42 ms with 9); 10 blocks spill.
+// kernel stays at 8 (bounce 0 0.44 vs 0.42 ms with 9); 10 blocks (48
+// registers) spill: 9.43 ms.
 #ifndef SRT_TRACE_PT_BLOCKS
 #define SRT_TRACE_PT_BLOCKS 9
 #endif
