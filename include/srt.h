@@ -598,12 +598,14 @@ srt_status srt_renderer_splat_photons(srt_renderer* r, const srt_camera_uniform*
 /* of uneven size per iteration.  Per-scene photon passes, ray generation,   */
 /* shading and finalisation run as parallel branches of one CUDA graph; the  */
 /* closest-hit and shadow rays of all scenes are traced in one persistent    */
-/* launch per bounce over per-scene queues.                                  */
+/* launch per bounce over per-scene queues (warps whose finished lanes take  */
+/* the next ray of any scene).                                               */
 /* ------------------------------------------------------------------------ */
 typedef struct srt_batch srt_batch;
 typedef struct srt_batch_tuning {
     uint32_t blocks_per_sm;  /* resident blocks per SM of the batched traversal (1..8) */
-    uint32_t chunk;          /* rays a warp draws from the shared queue at once (32..1024, x32) */
+    uint32_t chunk;          /* rays a warp draws from the shared queue at once (32..1024, x32); the
+                                default persistent traversal hands rays out lane by lane and ignores it */
     float ms_per_iteration;  /* autotune: time of one iteration with this choice */
     uint32_t candidates;     /* autotune: configurations timed */
     uint32_t bvh_width;      /* autotune: children per node of the scenes' trees it kept (it times the
@@ -624,8 +626,9 @@ srt_renderer* srt_batch_renderer(srt_batch* b, uint32_t i);
 srt_status srt_batch_render(srt_batch* b, const srt_camera_uniform* cams, const uint8_t* active);
 srt_status srt_batch_get_tuning(const srt_batch* b, srt_batch_tuning* out);
 srt_status srt_batch_set_tuning(srt_batch* b, const srt_batch_tuning* t);
-/* Times `iterations` iterations of every candidate (blocks per SM x chunk),
- * keeps the fastest, then clears every scene's accumulation and statistics;
+/* Times `iterations` iterations of every candidate (blocks per SM; x chunk
+ * for the chunked traversal), keeps the fastest, then clears every scene's
+ * accumulation and statistics;
  * guided scenes get back the network and Adam state they had before. */
 srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform* cams, uint32_t iterations,
                               srt_batch_tuning* out);

@@ -2633,7 +2633,10 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
     srt_ctx* c = b->ctx;
     cudaSetDevice(c->device);
     static const uint32_t bps[] = {2, 4, 8};
-    static const uint32_t chunks[] = {32, 64, 128};
+    // the persistent traversal (SRT_BATCH_TRACE_PT) takes rays lane by lane:
+    // the chunk is not a knob then
+    static const uint32_t chunk_list[] = {32, 64, 128};
+    const size_t n_chunks = SRT_BATCH_TRACE_PT ? 1 : 3;
     cudaEvent_t e0, e1;
     CUDA_TRY(c, cudaEventCreate(&e0));
     CUDA_TRY(c, cudaEventCreate(&e1));
@@ -2652,7 +2655,8 @@ extern "C" srt_status srt_batch_autotune(srt_batch* b, const srt_camera_uniform*
             }
         }
     for (uint32_t bp : bps)
-        for (uint32_t ch : chunks) {
+        for (size_t ci = 0; ci < n_chunks; ++ci) {
+            const uint32_t ch = chunk_list[ci];
             srt_batch_tuning t{bp, ch, 0.0f, 0, 0};
             srt_batch_set_tuning(b, &t);
             st = b->render(cams, nullptr);  // capture + warm-up

@@ -861,7 +861,9 @@ SRT_DEV bool trav_init(TravState& T, const DevScene& S, float3 o, float3 d, floa
 #ifndef SRT_TRAV_POOL
 #define SRT_TRAV_POOL 1
 #endif
-template <bool ANY>
+// MULTI: the lanes trace rays of different scenes (the batched renderer's
+// persistent launch), so a task reads the triangles of its owner's scene.
+template <bool ANY, bool MULTI = false>
 SRT_DEV void pool_tris(const DevScene& S, TravState& T, bool live, uint32_t& n_tris) {
     constexpr uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
@@ -896,9 +898,13 @@ SRT_DEV void pool_tris(const DevScene& S, TravState& T, bool live, uint32_t& n_t
         const uint32_t axes = __shfl_sync(FULL, T.axes, (int)o);
         uint32_t klo = 0xFFFFFFFFu, khi = 0xFFFFFFFFu;  // (t bits, id) of a hit, else all ones
         float hu = 0.f, hv = 0.f;
+        const TriSlot* tris = S.tris;
+        if (MULTI)
+            tris = reinterpret_cast<const TriSlot*>(
+                __shfl_sync(FULL, reinterpret_cast<unsigned long long>(S.tris), (int)o));
         if (have) {
             const uint32_t bit = __fns(gy, 0u, (int)(task - o_excl + 1u)) & 31u;  // always found: task < incl[o]
-            const TriSlot* ts = S.tris + gx + bit;
+            const TriSlot* ts = tris + gx + bit;
             const float4 a0 = __ldg(&ts->v0), a1 = __ldg(&ts->v1), a2 = __ldg(&ts->v2);
             ++n_tris;
             float t, u, v;

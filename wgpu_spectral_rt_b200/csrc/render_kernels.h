@@ -145,6 +145,13 @@ int launch_photon_splat(const float4* photons, uint32_t n, const srt_camera_unif
 // Batched rendering: the rays of one kind and bounce of many scenes, traced
 // in one launch (trace_kernels.cu).  Visit counting is not available here.
 constexpr int MAX_BATCH = 64;
+// The batch's rays of all scenes in persistent warps with refill
+// (k_trace_multi_pt) instead of chunks of one scene traced lane per ray:
+// 32-scene batch 107.2 vs 116.4 ms per iteration, the same images.  The
+// chunk of srt_batch_tuning then has no effect.
+#ifndef SRT_BATCH_TRACE_PT
+#define SRT_BATCH_TRACE_PT 1
+#endif
 struct MultiTraceItem {
     DevScene s;
     const uint32_t* queue;  // closest: path ids (NULL: identity)

@@ -265,6 +265,98 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
     }
 }
 
+// Persistent form of the batch's traversal (SRT_BATCH_TRACE_PT): the lanes
+// of a warp take rays from one virtual queue over every item's rays (no
+// padding) and keep their own scene, so a finished lane takes the next ray
+// whatever scene it belongs to; the steps are those of k_trace_pt (closest
+// hits with the warp-synchronous node visit, any-hit rays with pooled
+// triangle tests that read the owner's scene).
+template <bool ANY, int STACK>
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+    k_trace_multi_pt(const MultiTraceItem* __restrict__ items, int n_items, uint32_t* __restrict__ fetch) {
+    extern __shared__ uint2 stack_smem[];
+    __shared__ uint32_t pre[MAX_BATCH + 1];
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int i = 0; i < n_items; ++i) {
+            pre[i] = acc;
+            acc += *items[i].count;
+        }
+        pre[n_items] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = pre[n_items];
+    if (total == 0u) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint2* stack = stack_smem + threadIdx.x;
+    DevScene S;  // this lane's scene: the fields traversal reads
+    S.nodes = nullptr;
+    S.tris = nullptr;
+    S.n_nodes = 0u;
+    TravState T{};
+    bool active = false, exhausted = false;
+    uint32_t q = 0, id = 0, n_nodes = 0, n_tris = 0;
+    int s = 0;
+    // a finished ray: the closest hit, or an unoccluded shadow ray's contribution
+    auto finish = [&](const MultiTraceItem& I) {
+        if (ANY) {
+            if (T.best == MISS) {
+                const uint32_t pid = I.sh_id[q];
+                const float4 c = I.sh_c[q], r = I.rad[pid];
+                I.rad[pid] = make_float4(__fadd_rn(r.x, c.x), __fadd_rn(r.y, c.y), __fadd_rn(r.z, c.z),
+                                         __fadd_rn(r.w, c.w));
+            }
+        } else {
+            I.hit[id] = T.best != MISS ? make_float4(T.tbest, __uint_as_float(T.best), T.bu, T.bv)
+                                       : make_float4(0.f, __uint_as_float(MISS), 0.f, 0.f);
+        }
+    };
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
+        if (!exhausted && __popc(idle) >= (ANY ? SRT_TRACE_REFILL_ANY : SRT_TRACE_REFILL)) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
+            if (!active) {
+                const uint32_t my = base + __popc(idle & lt);
+                if (my < total) {
+                    // the item holding virtual index `my`: the last with pre[i] <= my
+                    int lo = 0, hi = n_items - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (pre[mid] <= my) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    s = lo;
+                    const MultiTraceItem& I = items[s];
+                    S.nodes = I.s.nodes;
+                    S.tris = I.s.tris;
+                    S.n_nodes = I.s.n_nodes;
+                    q = my - pre[s];
+                    id = I.queue ? I.queue[q] : q;
+                    const float4 o = I.ro[ANY ? q : id], d = I.rd[ANY ? q : id];
+                    active = trav_init(T, S, xyz(o), xyz(d), o.w, d.w);
+                    if (!active) finish(I);  // degenerate ray: finished without a hit
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
+            if (exhausted) break;
+            continue;
+        }
+        if (kPool && (ANY || SRT_TRAV_POOL >= 2)) {
+            pool_tris<ANY, true>(S, T, active, n_tris);
+            if (ANY && active && T.best != MISS) active = false;  // occluded: nothing to add
+        }
+        if (active && trav_step<ANY, STACK>(S, T, stack, TRACE_BLOCK, items[s].err, n_nodes, n_tris)) {
+            active = false;
+            finish(items[s]);
+        }
+    }
+}
+
 inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 1) / b); }
 
 struct TraceLaunch {
@@ -355,6 +447,17 @@ int launch_trace_multi(const MultiTraceItem* items, int n_items, int any_hit, bo
     uint32_t grid = (uint32_t)(sm_count > 0 ? sm_count : 148) * (uint32_t)std::max(1, blocks_per_sm);
     const int stack = small_stack ? TRAV_STACK_SMALL : TRAV_STACK;
     size_t smem = sizeof(uint2) * stack * TRACE_BLOCK;
+    if (SRT_BATCH_TRACE_PT) {
+        (void)chunk;
+        if (any_hit) {
+            if (small_stack) k_trace_multi_pt<true, TRAV_STACK_SMALL><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch);
+            else k_trace_multi_pt<true, TRAV_STACK><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch);
+        } else {
+            if (small_stack) k_trace_multi_pt<false, TRAV_STACK_SMALL><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch);
+            else k_trace_multi_pt<false, TRAV_STACK><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch);
+        }
+        return 1;
+    }
     if (any_hit) {
         if (small_stack) k_trace_multi<true, TRAV_STACK_SMALL><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
         else k_trace_multi<true, TRAV_STACK><<<grid, TRACE_BLOCK, smem, st>>>(items, n_items, fetch, chunk);
