@@ -71,12 +71,21 @@ SRT_DEV float4 gather(const GatherArgs& g, uint32_t frame, float3 hit_pos, float
 
 // ------------------------------------------------------------------ photon pass
 // The photon pass of photon_emit.wgsl:154-331 as a wavefront: emit every
-// photon path (one thread per emitter id), sort the emitted rays by an
-// octahedral direction key so that a warp traces rays of similar direction,
-// then per bounce: the shared closest-hit kernel over the live queue and a
-// shading kernel for the photon's material logic.  A stored photon lands in
-// its emitter's slot and is flagged; an emitter-ordered compaction afterwards
-// reproduces the order a sequential run of the reference's atomicAdd gives.
+// photon path (one thread per emitter id), then per bounce: the shared
+// closest-hit kernel over the live queue and a shading kernel for the
+// photon's material logic.  A stored photon lands in its emitter's slot and is
+// flagged; an emitter-ordered compaction afterwards reproduces the order a
+// sequential run of the reference's atomicAdd gives.
+//
+// SRT_PHOTON_DIR_SORT sorts the emitted rays by an octahedral direction key
+// first, so that a warp traces rays of similar direction.  It paid while
+// photon rays were traced one per thread; with the persistent warps (refill,
+// warp-synchronous node visits) it no longer does: config-2 photon pass 2.25
+// ms unsorted vs 2.45 ms sorted on 24 bits (2.36 on 16, 2.29 on 8), the same
+// photons.
+#ifndef SRT_PHOTON_DIR_SORT
+#define SRT_PHOTON_DIR_SORT 0
+#endif
 
 // Octahedral 12+12-bit direction code, Morton-interleaved (24 bits).
 SRT_DEV uint32_t dir_key(float3 d) {
@@ -144,8 +153,10 @@ __global__ void k_photon_emit(FrameArgs a) {
     a.ph.ray_d[e] = f4(emit_dir.x, emit_dir.y, emit_dir.z, 100.0f);
     a.ph.state[e] = f4(lambda, energy, __uint_as_float(s), __uint_as_float(0u));
     a.ph.flags[e] = 0u;
-    a.ph.keys[e] = dir_key(emit_dir);
-    a.ph.vals[e] = e;
+    if (SRT_PHOTON_DIR_SORT) {
+        a.ph.keys[e] = dir_key(emit_dir);
+        a.ph.vals[e] = e;
+    }
     if (e == 0) a.counters->photon_paths[0] = a.photons_per_frame;
 }
 
@@ -159,7 +170,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_SHADE_MIN_BLOCKS) k_photon_sh
     const DevScene& S = a.scene;
     const uint32_t* qin = bounce == 0 ? a.ph.sorted_vals : a.ph.queue[bounce & 1];
     bool alive = false;
-    uint32_t e = q < n ? qin[q] : 0u;
+    uint32_t e = q < n ? (qin ? qin[q] : q) : 0u;
     if (q < n) {
         float4 h = a.ph.hit[e];
         uint32_t prim = __float_as_uint(h.y);
@@ -771,12 +782,15 @@ inline uint32_t blocks_for(uint64_t n, uint32_t b) { return (uint32_t)((n + b - 
 int launch_photon_pass(FrameArgs& a, cudaStream_t st) {
     int launches = 0;
     const uint32_t n = a.photons_per_frame;
-    // emit, then order the emitted rays by direction for coherent traversal
+    // emit (with SRT_PHOTON_DIR_SORT, then order the emitted rays by direction)
     k_photon_emit<<<blocks_for(n, 256), 256, 0, st>>>(a);
     ++launches;
-    uint32_t *dir_keys, *order;
-    launches += sort_pairs(a.ph.keys, a.ph.vals, a.ph.keys2, a.ph.vals2, n, nullptr, 0, 24, a.ph.sort_scratch, st,
-                           &dir_keys, &order);
+    uint32_t* order = nullptr;  // bounce-0 queue: emitter order
+    if (SRT_PHOTON_DIR_SORT) {
+        uint32_t* dir_keys;
+        launches += sort_pairs(a.ph.keys, a.ph.vals, a.ph.keys2, a.ph.vals2, n, nullptr, 0, 24, a.ph.sort_scratch,
+                               st, &dir_keys, &order);
+    }
     a.ph.sorted_vals = order;  // bounce-0 queue (read by k_photon_shade at bounce 0)
     for (uint32_t b = 0; b < a.photon_max_bounces; ++b) {
         launches += launch_trace_queue(a.scene, b, b == 0 ? order : a.ph.queue[b & 1], &a.counters->photon_paths[b],

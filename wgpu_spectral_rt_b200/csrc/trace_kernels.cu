@@ -21,6 +21,11 @@
 #ifndef SRT_TRACE_MIN_BLOCKS
 #define SRT_TRACE_MIN_BLOCKS 8
 #endif
+// resident blocks per SM the batch's persistent kernel (k_trace_multi_pt) is
+// compiled for (its launch takes the batch's tuned blocks per SM, at most this)
+#ifndef SRT_TRACE_MULTI_BLOCKS
+#define SRT_TRACE_MULTI_BLOCKS SRT_TRACE_MIN_BLOCKS
+#endif
 // resident blocks of the persistent kernel (k_trace_pt) per SM: 9 caps it at
 // 56 registers without spills of the closest-hit form (a 4-byte spill in the
 // any-hit form); config-2 frame 9.16 vs 9.43 ms with 8 (closest-hit bounces
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
 // hits with the warp-synchronous node visit, any-hit rays with pooled
 // triangle tests that read the owner's scene).
 template <bool ANY, int STACK>
-__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MIN_BLOCKS)
+__global__ void __launch_bounds__(TRACE_BLOCK, SRT_TRACE_MULTI_BLOCKS)
     k_trace_multi_pt(const MultiTraceItem* __restrict__ items, int n_items, uint32_t* __restrict__ fetch) {
     extern __shared__ uint2 stack_smem[];
     __shared__ uint32_t pre[MAX_BATCH + 1];
@@ -433,8 +438,9 @@ int launch_trace_queue(const DevScene& s, uint32_t bounce, const uint32_t* queue
                        uint32_t* fetch, uint32_t max_n, const float4* ro, const float4* rd, float4* hit, int kind,
                        int count_visits, uint32_t* err, DevStats* stats, int sm_count, cudaStream_t st) {
     if (max_n == 0) return 0;
-    // photon rays arrive direction-sorted; persistent warps take them in that
-    // order (SRT_PHOTON_PERSISTENT)
+    // photon rays in emitter order (direction-sorted with
+    // SRT_PHOTON_DIR_SORT); persistent warps take them in that order
+    // (SRT_PHOTON_PERSISTENT)
     TraceLaunch L{s, queue, count, SRT_PHOTON_PERSISTENT ? fetch : nullptr, max_n, ro, rd, hit, nullptr, nullptr,
                   nullptr, err, stats, kind, sm_count, (int)bounce};
     launch_kind<false>(L, count_visits, st);
