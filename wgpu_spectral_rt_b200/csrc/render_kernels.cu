@@ -314,12 +314,38 @@ __global__ void k_grid_ranges(const uint32_t* __restrict__ keys, const uint32_t*
 }
 
 // ------------------------------------------------------------------ camera paths
+// Bounce-0 queue order (SRT_RAYGEN_TILE): queue position q -> pixel, with
+// the pixels of a warp in an 8 x 4 tile (bands of 4 rows, 8-column blocks
+// within a band; narrower blocks and bands at the right and bottom edges)
+// instead of a 32 x 1 strip.  A bijection of [0, w h).  Config-2 camera rays
+// of bounce 0: 0.383 vs 0.428 ms (a warp's rays closer in both directions);
+// a path's result does not depend on its queue position.
+#ifndef SRT_RAYGEN_TILE
+#define SRT_RAYGEN_TILE 1
+#endif
+SRT_DEV void tile_pixel(uint32_t q, uint32_t w, uint32_t h, uint32_t& x, uint32_t& y) {
+    const uint32_t band = q / (4u * w), y0 = 4u * band;
+    const uint32_t hb = min(4u, h - y0);
+    const uint32_t r = q - y0 * w;  // position inside the band
+    const uint32_t blk = r / (8u * hb), x0 = 8u * blk;
+    const uint32_t wb = min(8u, w - x0);
+    const uint32_t t = r - x0 * hb;  // position inside the block
+    x = x0 + t % wb;
+    y = y0 + t / wb;
+}
+
 __global__ void k_raygen(FrameArgs a) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t n = a.width * a.height;
-    if (p >= n) return;
+    if (q >= n) return;
     const srt_camera_uniform& cam = *a.cam;
-    uint32_t x = p % a.width, y = p / a.width;
+    uint32_t x, y;
+    if (SRT_RAYGEN_TILE) tile_pixel(q, a.width, a.height, x, y);
+    else {
+        x = q % a.width;
+        y = q / a.width;
+    }
+    const uint32_t p = x + y * a.width;
     uint32_t s = pcg_hash(x + y * a.width + cam.frame_count * 927163u + a.seed);
     float3 o, d;
     camera_ray(cam, x, y, a.width, a.height, s, o, d);
@@ -330,8 +356,8 @@ __global__ void k_raygen(FrameArgs a) {
     a.pb.wl[p] = wl;
     a.pb.rad[p] = splat4(0.0f);
     a.pb.misc[p] = make_uint4(s, 0u, p, 0u);
-    a.pb.queue[0][p] = p;
-    if (p == 0) a.counters->paths[0] = n;
+    a.pb.queue[0][q] = p;
+    if (q == 0) a.counters->paths[0] = n;
 }
 
 struct LightSample {

@@ -412,7 +412,7 @@ void launch_kind(const TraceLaunch& L, int count_visits, cudaStream_t st) {
 }  // namespace
 
 int launch_trace_closest(const FrameArgs& a, uint32_t bounce, cudaStream_t st) {
-    // primary rays (bounce 0) are pixel-ordered and coherent: one ray per
+    // primary rays (bounce 0) are coherent (8 x 4 pixel tiles): one ray per
     // thread; later bounces are incoherent: persistent warps with refill
     TraceLaunch L{a.scene, a.pb.queue[bounce & 1], &a.counters->paths[bounce],
                   (bounce == 0 && !SRT_PRIMARY_PERSISTENT) ? nullptr : &a.counters->fetch[TRAV_CLOSEST][bounce],
