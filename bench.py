@@ -530,7 +530,8 @@ def main(argv=None):
     # in from pinned memory each step, and each step's RGBA8 image comes back to
     # pinned host memory (srt_read_ldr_async); the host waits for frame k's image
     # after launching frame k + 1, and for the last one before the clock stops
-    e2e_steps = 0 if args.no_e2e else max(8, args.steps // 4)
+    # (at least 48 frames: the host clock over a fraction of a second is jittery)
+    e2e_steps = 0 if args.no_e2e else max(48, args.steps // 2)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
