@@ -217,7 +217,7 @@ class OracleScene:
 
 def device_math(op: int, inp: np.ndarray, aux=None) -> np.ndarray:
     sizes = {0: (4, 4), 1: (4, 12), 2: (8, 4), 3: (28, 16), 4: (36, 16), 5: (4, 20), 6: (96, 40), 7: (20, 4),
-             8: (20, 28)}
+             8: (20, 28), 102: (8, 4), 109: (24, 4), 110: (8, 4)}
     isz, osz = sizes[op]
     a = np.ascontiguousarray(inp)
     n = a.nbytes // isz

@@ -1080,6 +1080,29 @@ orc_scene* orc_scene_create(const srt_scene_arrays* a) {
 }
 
 void orc_scene_destroy(orc_scene* s) { delete s; }
+
+void orc_ray_query(const orc_scene* s, const float o[3], const float d[3], float tmin, float tmax, int any_hit,
+                   orc_query_hit* out) {
+    *out = orc_query_hit{};
+    const f3 of = {o[0], o[1], o[2]}, df = {d[0], d[1], d[2]};
+    if (any_hit) {
+        out->hit = occluded(s, of, df, tmin, tmax, nullptr) ? 1u : 0u;
+        return;
+    }
+    const HitInfo h = query(s, of, df, tmin, tmax, nullptr);
+    if (!h.hit) return;
+    out->hit = 1u;
+    out->inst = h.inst;
+    out->prim = h.prim;
+    out->front = h.front ? 1u : 0u;
+    out->t = h.t;
+    out->u = h.u;
+    out->v = h.v;
+}
+
+void orc_instance_w2o(const orc_scene* s, uint32_t inst, float out[9]) {
+    for (int k = 0; k < 9; ++k) out[k] = s->w2o_f[9 * (size_t)inst + k];
+}
 uint64_t orc_scene_num_tris(const orc_scene* s) { return s->tinst.size(); }
 
 void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit, int brute, double* t_out,
@@ -1174,6 +1197,17 @@ int orc_device_math(int op, uint32_t n, const void* in, void* out, const void* a
             } break;
             case 2:
                 fo[i] = blackbody_radiance(fi[2 * i], fi[2 * i + 1]);
+                break;
+            case 102:  // photon_emit.wgsl:93-105 (the same arithmetic as shader.wgsl's copy)
+                fo[i] = blackbody_radiance(fi[2 * i], fi[2 * i + 1]);
+                break;
+            case 109: {  // fresnel_thin_film_1d, photon_emit.wgsl:107-132
+                const float* a = fi + 6 * i;
+                bool tir;
+                fo[i] = thin_film_1(a[0], a[1], a[2], a[3], a[4], a[5], &tir);
+            } break;
+            case 110:  // reflectance, shader.wgsl:264-269
+                fo[i] = reflectance(fi[2 * i], fi[2 * i + 1]);
                 break;
             case 3: {
                 const float* a = fi + 7 * i;

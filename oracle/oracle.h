@@ -11,12 +11,17 @@
  * driver's ray queries.  Each function cites the reference line it follows.
  *
  * Parity status: the reference has no tests, golden vectors or fixtures, and
- * its code path (wgpu -> Vulkan ray query) cannot run on this machine.  The
- * oracle is pinned by known-answer tests derived from closed forms (PCG
- * values, Planck peak, Fresnel limits, Airy film at zero thickness, hero
- * wavelength pdf normalisation) and by the golden vectors under
- * tests/golden/.  Where a value depends on the driver (traversal order,
- * intersection rounding), parity is unpinned.
+ * its code path (wgpu -> Vulkan ray query) cannot run on this machine.  Its
+ * shader source can: oracle/wgsl_translate.py translates shader.wgsl,
+ * photon_emit.wgsl and build_grid.wgsl mechanically into C++ and
+ * oracle/ref_harness.cpp runs them with their ray queries answered by
+ * orc_ray_query below.  Against that run this restatement is bit-exact —
+ * shading functions, camera rays, stored photons, grid lists, accumulated
+ * frames and images (tests/test_oracle_ref_pin.py, fixtures from
+ * tests/golden/make_ref_golden.py) — besides the closed-form known answers
+ * of tests/golden/golden.json.  What the Vulkan driver decides (traversal
+ * order, intersection rounding, the precision of exp / pow / sin / cos) is
+ * not pinned by either: both runs use this oracle's FP64 queries and libm.
  */
 #ifndef SRT_ORACLE_H
 #define SRT_ORACLE_H
@@ -49,7 +54,10 @@ void orc_trace(const orc_scene* s, const srt_ray* rays, uint32_t n, int any_hit,
 void orc_tri_probe(const orc_scene* s, const srt_ray* rays, const uint32_t* prims, uint32_t n, double* t_out,
                    double* edge_out, double* cos_out);
 
-/* Same op codes and record layouts as srt_test_device_math. */
+/* Same op codes and record layouts as srt_test_device_math, plus
+ * 102 blackbody_radiance of photon_emit.wgsl (in f32[2] -> out f32[1]),
+ * 109 fresnel_thin_film_1d (cos, n1, n2, n3, d, lambda: in f32[6] -> out f32[1]),
+ * 110 reflectance (cos, ior: in f32[2] -> out f32[1]). */
 int orc_device_math(int op, uint32_t n, const void* in, void* out, const void* aux);
 
 /* Photon emission for emitter ids [0, n_photons) (photon_emit.wgsl:154-331).
@@ -85,6 +93,23 @@ void orc_render_frame_photons(const orc_scene* s, const srt_camera_uniform* cam,
                               const srt_params* params, const srt_photon* photons_in, uint32_t n_photons_in,
                               uint32_t row_stride, uint32_t row_phase, float* accum, uint8_t* ldr,
                               float* radiance_out, uint64_t* stats_out, int n_threads);
+
+/* One ray query as the oracle's shading code sees it: the part of a frame that
+ * the Vulkan driver answers in the reference (rayQueryProceed on opaque
+ * triangles).  any_hit = 1 (RAY_FLAG_TERMINATE_ON_FIRST_HIT) fills only hit.
+ * Closest hits: t rounded to FP32, the instance, the primitive within its
+ * mesh, the barycentrics u, v of vertices 1 and 2 and the front-face flag
+ * (counter-clockwise as seen from the ray, in object space).  Used by
+ * oracle/ref_harness.cpp to run the reference's translated shaders. */
+typedef struct orc_query_hit {
+    uint32_t hit, inst, prim, front;
+    float t, u, v, pad;
+} orc_query_hit;
+void orc_ray_query(const orc_scene* s, const float o[3], const float d[3], float tmin, float tmax, int any_hit,
+                   orc_query_hit* out);
+/* The FP32 world-to-object 3x3 (row-major) of instance inst, as the oracle's
+ * shading uses it. */
+void orc_instance_w2o(const orc_scene* s, uint32_t inst, float out[9]);
 
 int orc_max_threads(void);
 
