@@ -234,6 +234,15 @@ srt_status srt_ctx_set_bvh_builder(srt_ctx* ctx, int builder);
  * builder, the width changes speed, never results.  No reference
  * counterpart (the driver builds the reference's BLAS/TLAS). */
 srt_status srt_ctx_set_bvh_width(srt_ctx* ctx, uint32_t width);
+/* Triangles of the largest BVH leaf (1..3, default 2) for the scenes built
+ * next: a collapsed subtree of at most that many triangles is listed in its
+ * parent node, a larger one becomes a node.  Smaller leaves mean more node
+ * visits and fewer triangle tests per ray (config 2: 2 is faster than 3 for
+ * closest hits, slower for shadow rays, faster per frame).  Rebuilds
+ * (srt_scene_rebuild_bvh) keep the scene's leaf size.  Changes speed, never
+ * results.  No reference counterpart (the driver builds the reference's
+ * BLAS/TLAS). */
+srt_status srt_ctx_set_bvh_leaf_size(srt_ctx* ctx, uint32_t max_triangles);
 /* Rebuilds a scene's tree with `width` children per node (same builder).
  * Waits for the device; renderers and batches using the scene pick up the
  * new tree at their next frame (they capture their frame again). */

@@ -140,15 +140,18 @@ def test_config2_closest_hit_ids(srt, orc, config2):
     assert total_bad == 0
 
 
-@pytest.mark.parametrize("builder,width", [("LBVH", 8), ("SAH", 4), ("LBVH", 4)])
-def test_config2_tree_choice_keeps_hits_bit_identical(srt, orc, config2, builder, width):
+@pytest.mark.parametrize("builder,width,leaf", [("LBVH", 8, 2), ("SAH", 4, 2), ("LBVH", 4, 2), ("SAH", 8, 3),
+                                                ("SAH", 8, 1)])
+def test_config2_tree_choice_keeps_hits_bit_identical(srt, orc, config2, builder, width, leaf):
     """The same rays through the default tree (three-axis SAH, 8 children per
-    node) and another tree of the config-2 scene (LBVH, and 4 children per
-    node): identical (t, triangle, u, v) bits."""
+    node, leaves of at most 2 triangles) and another tree of the config-2
+    scene (LBVH, 4 children per node, leaves of 3 or 1): identical (t,
+    triangle, u, v) bits."""
     b, scene, o, cam = config2
     ctx2 = srt.Context(0)
     ctx2.set_bvh_builder(getattr(srt, f"BVH_{builder}"))
     ctx2.set_bvh_width(width)
+    ctx2.set_bvh_leaf_size(leaf)
     scene_l = b.build(ctx2)
     assert scene_l.info()["nodes"] != scene.info()["nodes"]
     rng = np.random.default_rng(22)
@@ -162,7 +165,7 @@ def test_config2_tree_choice_keeps_hits_bit_identical(srt, orc, config2, builder
     a = scene.trace(rays, any_hit=True)
     c = scene_l.trace(rays, any_hit=True)
     assert np.array_equal(a["prim"], c["prim"])
-    print(f"[parity] tree {builder}/{width}: nodes {scene_l.info()['nodes']} depth {scene_l.info()['depth']} "
+    print(f"[parity] tree {builder}/{width}/leaf {leaf}: nodes {scene_l.info()['nodes']} depth {scene_l.info()['depth']} "
           f"(default {scene.info()['nodes']} / {scene.info()['depth']})", flush=True)
     scene_l.close()
     ctx2.close()

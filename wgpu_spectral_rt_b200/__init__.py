@@ -213,6 +213,7 @@ SIGNATURES = {
     "srt_scene_read_bvh": (_I, [_P, _P, C.c_uint64, _P, C.c_uint64]),
     "srt_ctx_set_bvh_builder": (_I, [_P, _I]),
     "srt_ctx_set_bvh_width": (_I, [_P, _U32]),
+    "srt_ctx_set_bvh_leaf_size": (_I, [_P, _U32]),
     "srt_read_ldr_async": (_I, [_P, C.POINTER(_U32)]),
     "srt_ldr_wait": (_I, [_P, _U32, C.POINTER(C.POINTER(C.c_uint8))]),
     "srt_guide_param_count": (_U32, []),
@@ -308,6 +309,10 @@ class Context:
     def set_bvh_width(self, width: int) -> None:
         """Children per BVH node (2..8, default 8) for the scenes built next."""
         _check(lib().srt_ctx_set_bvh_width(self.h, width), self.h)
+
+    def set_bvh_leaf_size(self, max_triangles: int) -> None:
+        """Triangles of the largest BVH leaf (1..3, default 2) for the scenes built next."""
+        _check(lib().srt_ctx_set_bvh_leaf_size(self.h, max_triangles), self.h)
 
     def synchronize(self):
         _check(lib().srt_ctx_synchronize(self.h), self.h)

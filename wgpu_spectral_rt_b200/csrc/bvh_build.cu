@@ -28,6 +28,12 @@ namespace srt {
 namespace {
 
 constexpr uint32_t LEAF = 0x80000000u;
+// A collapsed child with at most leaf_max triangles (BvhInputs) becomes a
+// leaf (its triangles listed in the node); larger ones become 8-wide nodes.
+// At most 3: a node's leaves share a 24-bit triangle mask and a 5-bit offset
+// field.  The closest hit is the minimum of (t, id) and an any-hit answer does
+// not depend on the order, so the choice changes speed, never results.
+constexpr uint32_t LEAF_MAX_LIMIT = 3u;
 
 __device__ __forceinline__ uint32_t float_flip(float f) {
     uint32_t u = __float_as_uint(f);
@@ -706,7 +712,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
                            uint32_t* __restrict__ n_out, Node8* __restrict__ nodes, uint32_t* __restrict__ node_alloc,
                            uint32_t node_cap, TriSlot* __restrict__ tris_out, uint32_t* __restrict__ tri_alloc,
                            uint32_t tri_cap, const TriSlot* __restrict__ flat, const uint32_t* __restrict__ sorted_tri,
-                           uint32_t* __restrict__ err, int width) {
+                           uint32_t* __restrict__ err, int width, uint32_t leaf_max) {
     uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_in) return;
     uint2 q = qin[e];
@@ -750,7 +756,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         ref_range(b, refs[c], cfirst[c], ccount[c]);
         nlo = f3(fminf(nlo.x, clo[c].x), fminf(nlo.y, clo[c].y), fminf(nlo.z, clo[c].z));
         nhi = f3(fmaxf(nhi.x, chi[c].x), fmaxf(nhi.y, chi[c].y), fmaxf(nhi.z, chi[c].z));
-        if (ccount[c] <= 3u) n_tri += ccount[c];
+        if (ccount[c] <= leaf_max) n_tri += ccount[c];
         else ++n_int;
     }
     uint32_t child_base = n_int ? atomicAdd(node_alloc, n_int) : 0u;
@@ -796,7 +802,7 @@ __global__ void k_collapse(Bvh2 b, const uint2* __restrict__ qin, uint32_t n_in,
         slo[s] = clo[c];
         shi[s] = chi[c];
         uint32_t m;
-        if (ccount[c] <= 3u) {
+        if (ccount[c] <= leaf_max) {
             m = (ccount[c] << 5) | tri_off;
             for (uint32_t k = 0; k < ccount[c]; ++k) tris_out[tri_base + tri_off + k] = flat[sorted_tri[cfirst[c] + k]];
             tri_off += ccount[c];
@@ -949,7 +955,8 @@ cudaError_t build_bvh8(const BvhInputs& in, cudaStream_t st, BvhOutputs* out, st
             CK(cudaMemsetAsync(counters + 2, 0, 4, st));
             k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(b, qa, n_in, qb, counters + 2, out->nodes, counters,
                                                            node_cap, out->tris, counters + 1, n, flat, sv, err,
-                                                           in.width < 2 ? 2 : (in.width > 8 ? 8 : in.width));
+                                                           in.width < 2 ? 2 : (in.width > 8 ? 8 : in.width),
+                                                           in.leaf_max < 1u ? 1u : (in.leaf_max > LEAF_MAX_LIMIT ? LEAF_MAX_LIMIT : in.leaf_max));
             ++out->kernel_launches;
             ++depth;
             CK(cudaGetLastError());

@@ -42,6 +42,7 @@ struct BvhInputs {
     uint32_t n_tris;          // flattened triangle count
     int builder;              // BVH_BUILDER_*
     int width = 8;            // children per node, 2..8 (nodes keep the 8-slot format)
+    uint32_t leaf_max = 2;    // triangles of the largest leaf, 1..3 (8 leaves share 24 triangle bits)
 };
 
 struct BvhOutputs {

@@ -46,6 +46,7 @@ struct srt_ctx {
     bool closing = false;
     int bvh_builder = 0;  // SRT_BVH_* for the scenes built next
     int bvh_width = 8;    // children per BVH node for the scenes built next
+    uint32_t bvh_leaf = 2;  // triangles of the largest BVH leaf for the scenes built next
 };
 
 namespace {
@@ -170,6 +171,12 @@ srt_status srt_ctx_set_bvh_builder(srt_ctx* c, int builder) {
 srt_status srt_ctx_set_bvh_width(srt_ctx* c, uint32_t width) {
     if (!c || width < 2 || width > 8) return SRT_ERR_INVALID_ARG;
     c->bvh_width = (int)width;
+    return SRT_OK;
+}
+
+srt_status srt_ctx_set_bvh_leaf_size(srt_ctx* c, uint32_t max_triangles) {
+    if (!c || max_triangles < 1 || max_triangles > 3) return SRT_ERR_INVALID_ARG;
+    c->bvh_leaf = max_triangles;
     return SRT_OK;
 }
 
@@ -326,6 +333,7 @@ struct srt_scene {
     uint32_t version = 0;
     int builder = BVH_BUILDER_SAH;
     int width = 8;
+    uint32_t leaf = 2;  // triangles of the largest leaf (rebuilds keep it)
     uint32_t n_inst = 0;
     ~srt_scene() {
         cudaFree(light_insts);
@@ -440,9 +448,10 @@ srt_status scene_build_impl(srt_ctx* c, const srt_scene_arrays* a,
     CUDA_TRY(c, upload(&s->inst, inst.data(), sizeof(InstDev) * inst.size(), sizeof(InstDev) * inst.size(), st));
     CUDA_TRY(c, upload(&s->fwd, fwd.data(), sizeof(InstFwd) * fwd.size(), sizeof(InstFwd) * fwd.size(), st));
     BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, a->n_instances, (uint32_t)total,
-                 c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH, c->bvh_width};
+                 c->bvh_builder == SRT_BVH_LBVH ? BVH_BUILDER_LBVH : BVH_BUILDER_SAH, c->bvh_width, c->bvh_leaf};
     s->builder = bi.builder;
     s->width = bi.width;
+    s->leaf = bi.leaf_max;
     s->n_inst = a->n_instances;
     std::string msg;
     cudaError_t e = build_bvh8(bi, st, &s->bvh, &msg);
@@ -635,7 +644,7 @@ extern "C" srt_status srt_scene_rebuild_bvh(srt_scene* s, uint32_t width) {
     cudaStream_t st = c->stream;
     CUDA_TRY(c, cudaDeviceSynchronize());  // no frame of any renderer still reads the old tree
     BvhInputs bi{s->vtx, s->idx, s->mesh_infos, s->inst, s->fwd, s->n_inst, (uint32_t)s->n_tris, s->builder,
-                 (int)width};
+                 (int)width, s->leaf};
     BvhOutputs nb{};
     std::string msg;
     cudaError_t e = build_bvh8(bi, st, &nb, &msg);
