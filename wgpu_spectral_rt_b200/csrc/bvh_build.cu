@@ -214,7 +214,8 @@ __global__ void k_refit(const TriSlot* __restrict__ flat, const uint32_t* __rest
 // every resident thread, grows with the count: 3.0 KB at 16, 10.5 KB at 64).
 // Config 2 (1.57M triangles, leaves of <= 2): 16 / 16 bins 7.80 node visits
 // per camera ray, closest hits 3.00 ms per 1080p frame; 64 / 16 7.18 visits,
-// 2.86 ms; 64 / 32 and 64 / 64 within noise of 64 / 16 (2.85, 2.83 ms).  The
+// 2.86 ms; 64 / 32 and 64 / 64 within noise of 64 / 16 (2.85, 2.83 ms), and
+// 128 / 16 of 64 / 16 (2.87 vs 2.88 ms); 96 / 16 7.45 visits, 2.91 ms.  The
 // same hits in every case: the tree changes speed, never results.
 #ifndef SRT_SAH_BINS
 #define SRT_SAH_BINS 64
