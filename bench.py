@@ -212,6 +212,44 @@ def cpu_baseline(cfg, frames=1):
     return out
 
 
+def reference_shaders_sample(cfg, frames=1):
+    """The reference's own WGSL (shader.wgsl, photon_emit.wgsl, build_grid.wgsl),
+    translated mechanically to C++ (oracle/_ref, built from the reference tree by
+    oracle/wgsl_translate.py), timed on whole frames on all host threads: its
+    photon and grid dispatches and its camera pass run their invocations
+    concurrently, ray queries answered by the oracle's FP64 BVH.  Its constants
+    are its own: 2^20 photons per frame (the shaders fix the dispatch and the
+    gather's normalisation) and MAX_DEPTH = the workload's depth; material type
+    5, which the reference lacks, is replaced by its GGX, glass and film types.
+    None of the GPU package is loaded.  A sample beside the arm's value (the
+    oracle port, which takes the workload's photon count), not the value."""
+    orc = _oracle()
+    import ref_binding as ref
+
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libref_wgsl.so not built here (it is built from the reference tree)"}
+    preset, w, h, depth, _photons = cfg
+    scn = orc.Preset(PRESET_IDS[preset], 0)
+    arrays, keep = ref.reference_materials(scn.arrays())
+    rs = ref.RefScene(arrays)
+    pos, yaw, pitch = scn.camera
+    # warm-up (page-in, thread pool): a small crop with few emitters
+    rs.render_frame(orc.camera_uniform(pos, yaw, pitch, w / h, 0), 64, 36, depth, 1 << 14, ordered=False)
+    t_total = 0.0
+    for f in range(frames):
+        u = orc.camera_uniform(pos, yaw, pitch, w / h, 1 + f)
+        t0 = time.perf_counter()
+        rs.render_frame(u, w, h, depth, ref.MAX_PHOTONS, ordered=False)
+        t_total += time.perf_counter() - t0
+    rs.close()
+    del keep
+    return {"value": round(w * h * frames / t_total / 1e6, 4), "unit": "Mpaths/s", "kind": "reference",
+            "cores": orc.max_threads(), "frames": frames, "seconds": round(t_total, 2),
+            "sample": (f"{frames} whole {w}x{h} frame(s) of the reference's own WGSL translated to C++ "
+                       f"(oracle/wgsl_translate.py), its constants: 2^20 photons, MAX_DEPTH {depth}; "
+                       f"type-5 materials as reference types; FP64 ray queries")}
+
+
 def run_reference(args, cfg, rank, world):
     """--impl reference: the CPU port of the reference path (the oracle, with
     its own scene generator and camera; nothing of the GPU package is loaded),
@@ -246,9 +284,11 @@ def run_reference(args, cfg, rank, world):
                                     f"1/16 of a frame")},
         "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
     o.close()
     scn.close()
+    if not args.no_cpu_baseline:
+        line["reference_shaders"] = reference_shaders_sample(cfg)
+    print(json.dumps(line), flush=True)
     return 0
 
 

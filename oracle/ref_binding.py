@@ -56,8 +56,8 @@ def lib() -> C.CDLL:
         L.ref_scene_create.argtypes = [P]
         L.ref_scene_destroy.argtypes = [P]
         L.ref_photon_emit.restype = U32
-        L.ref_photon_emit.argtypes = [P, P, U32, P]
-        L.ref_build_grid.argtypes = [P, P, U32, P, P]
+        L.ref_photon_emit.argtypes = [P, P, U32, P, C.c_int]
+        L.ref_build_grid.argtypes = [P, P, U32, P, P, C.c_int]
         L.ref_camera_pass.argtypes = [P, P, U32, U32, U32, P, P, P, P, P, C.c_int]
         L.ref_camera_rays.argtypes = [P, U32, U32, P, U32, P]
         L.ref_device_math.restype = C.c_int
@@ -68,6 +68,29 @@ def lib() -> C.CDLL:
 
 def _p(a):
     return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def reference_materials(arrays):
+    """The scene with material type 5 (thin-film-coated GGX, this project's own:
+    the reference's shaders do not know it) replaced by reference types, a third
+    each: GGX (roughness from color.w), dispersive glass (A 1.5, B 0.004), Airy
+    film (thickness, n2, n3 kept).  Returns (arrays, materials): keep the second
+    alive while the first is used.  Scenes without type 5 come back unchanged."""
+    mats = np.ctypeslib.as_array(C.cast(arrays.materials, C.POINTER(C.c_float)), (arrays.n_materials, 8)).copy()
+    idx = np.nonzero(mats[:, 4] == 5)[0]
+    if len(idx) == 0:
+        return arrays, None
+    g1, g2, g4 = idx[0::3], idx[1::3], idx[2::3]
+    mats[g1, 4] = 1
+    mats[g1, 5] = mats[g1, 3]
+    mats[g2, 4] = 2
+    mats[g2, 6] = 1.5
+    mats[g2, 7] = 0.004
+    mats[g4, 4] = 4
+    a2 = orc.SceneArrays()
+    C.pointer(a2)[0] = arrays
+    a2.materials = mats.ctypes.data
+    return a2, mats
 
 
 # op -> (input bytes, output bytes) per record; the orc_device_math layouts
@@ -102,19 +125,22 @@ class RefScene:
     def __init__(self, arrays):
         self.h = lib().ref_scene_create(C.byref(arrays))
 
-    def photon_emit(self, cam, n_emit: int = MAX_PHOTONS):
-        """photon_emit.wgsl over emitter ids [0, n_emit) in id order: (the 2^20-record
-        photon buffer, the atomic counter)."""
+    def photon_emit(self, cam, n_emit: int = MAX_PHOTONS, threads: int = 1):
+        """photon_emit.wgsl over emitter ids [0, n_emit): (the 2^20-record photon
+        buffer, the atomic counter).  threads = 1 runs the invocations in id order
+        (the deterministic order the oracle reproduces); more (0 = all) run them
+        concurrently, the photons landing in the order the atomic hands out."""
         buf = np.zeros((MAX_PHOTONS, 8), np.float32)
-        count = lib().ref_photon_emit(self.h, C.byref(cam), n_emit, _p(buf))
+        count = lib().ref_photon_emit(self.h, C.byref(cam), n_emit, _p(buf), threads)
         return buf, int(count)
 
     @staticmethod
-    def build_grid(cam, buf: np.ndarray, count: int):
-        """build_grid.wgsl over the 2^20-id dispatch: (grid_head, grid_next)."""
+    def build_grid(cam, buf: np.ndarray, count: int, threads: int = 1):
+        """build_grid.wgsl over the 2^20-id dispatch: (grid_head, grid_next);
+        threads as for photon_emit."""
         head = np.zeros(HASH_SIZE, np.uint32)
         nxt = np.zeros(MAX_PHOTONS, np.uint32)
-        lib().ref_build_grid(C.byref(cam), _p(buf), count, _p(head), _p(nxt))
+        lib().ref_build_grid(C.byref(cam), _p(buf), count, _p(head), _p(nxt), threads)
         return head, nxt
 
     def camera_pass(self, cam, w: int, h: int, max_depth: int, buf, head, nxt, accum=None, threads: int = 0):
@@ -127,11 +153,14 @@ class RefScene:
         return accum, ldr
 
     def render_frame(self, cam, w: int, h: int, max_depth: int = 12, n_emit: int = MAX_PHOTONS, accum=None,
-                     threads: int = 0):
+                     threads: int = 0, ordered: bool = True):
         """One frame as renderer/mod.rs:168-207 records it: photon pass, grid,
-        camera pass.  Returns (accumulation, rgba8, stored photons)."""
-        buf, count = self.photon_emit(cam, n_emit)
-        head, nxt = self.build_grid(cam, buf, count)
+        camera pass (on `threads` threads, 0 = all).  ordered: the photon and
+        grid dispatches run in id order (deterministic), else concurrently.
+        Returns (accumulation, rgba8, stored photons)."""
+        pt = 1 if ordered else threads
+        buf, count = self.photon_emit(cam, n_emit, pt)
+        head, nxt = self.build_grid(cam, buf, count, pt)
         accum, ldr = self.camera_pass(cam, w, h, max_depth, buf, head, nxt, accum, threads)
         return accum, ldr, buf[:min(count, MAX_PHOTONS)].copy()
 

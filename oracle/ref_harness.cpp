@@ -148,11 +148,15 @@ void ref_scene_destroy(ref_scene* s) {
     delete s;
 }
 
-// Photon pass (photon_emit.wgsl main) for emitter ids [0, n_emit), in id
-// order (the order a sequential run of its atomicAdd gives).  photons must
-// hold 2^20 records (the reference's buffer); returns the atomic counter,
-// which can exceed the number stored.
-uint32_t ref_photon_emit(ref_scene* s, const srt_camera_uniform* cam, uint32_t n_emit, srt_photon* photons) {
+// Photon pass (photon_emit.wgsl main) for emitter ids [0, n_emit).  With
+// n_threads = 1 the invocations run in id order (the order a sequential run
+// of its atomicAdd gives, which the oracle reproduces); with more threads
+// (0 = all) they run concurrently and the stored photons land in the order
+// the atomic hands out, as on a GPU.  photons must hold 2^20 records (the
+// reference's buffer); returns the atomic counter, which can exceed the
+// number stored.
+uint32_t ref_photon_emit(ref_scene* s, const srt_camera_uniform* cam, uint32_t n_emit, srt_photon* photons,
+                         int n_threads) {
     namespace P = wgsl_photon_emit;
     P::tlas = s->tlas;
     P::lights = bind<P::LightInfo>(s->lights);
@@ -163,15 +167,21 @@ uint32_t ref_photon_emit(ref_scene* s, const srt_camera_uniform* cam, uint32_t n
     P::vertices = bind<P::Vertex>(s->vertices);
     P::indices = bind<uint32_t>(s->indices);
     P::mesh_infos = bind<P::MeshInfo>(s->meshes);
-    for (uint32_t i = 0; i < n_emit; ++i) P::cs_main(vec3u(i, 0u, 0u));
+    if (n_threads == 1) {
+        for (uint32_t i = 0; i < n_emit; ++i) P::cs_main(vec3u(i, 0u, 0u));
+    } else {
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+        for (uint32_t i = 0; i < n_emit; ++i) P::cs_main(vec3u(i, 0u, 0u));
+    }
     return P::photon_count.v;
 }
 
 // Grid pass (build_grid.wgsl main) over the dispatch of 2^20 ids, in id
-// order.  grid_head: 2^22 entries (cleared here to 0xFFFFFFFF as
-// renderer/mod.rs:179 does), grid_next: 2^20.
+// order with n_threads = 1, concurrently otherwise (the lists' order then
+// varies as on a GPU).  grid_head: 2^22 entries (cleared here to 0xFFFFFFFF
+// as renderer/mod.rs:179 does), grid_next: 2^20.
 void ref_build_grid(const srt_camera_uniform* cam, srt_photon* photons, uint32_t count, uint32_t* grid_head,
-                    uint32_t* grid_next) {
+                    uint32_t* grid_next, int n_threads) {
     namespace G = wgsl_build_grid;
     for (uint32_t i = 0; i < kHashSize; ++i) grid_head[i] = 0xFFFFFFFFu;
     G::photons = bind<G::Photon>(photons, kMaxPhotons);
@@ -179,7 +189,12 @@ void ref_build_grid(const srt_camera_uniform* cam, srt_photon* photons, uint32_t
     G::grid_head = bind<Atomic<uint32_t>>(grid_head, kHashSize);
     G::grid_next = bind<uint32_t>(grid_next, kMaxPhotons);
     load_camera(G::camera, cam);
-    for (uint32_t i = 0; i < kMaxPhotons; ++i) G::cs_main(vec3u(i, 0u, 0u));
+    if (n_threads == 1) {
+        for (uint32_t i = 0; i < kMaxPhotons; ++i) G::cs_main(vec3u(i, 0u, 0u));
+    } else {
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+        for (uint32_t i = 0; i < kMaxPhotons; ++i) G::cs_main(vec3u(i, 0u, 0u));
+    }
 }
 
 // Camera pass (shader.wgsl main) over a w x h target with MAX_DEPTH

@@ -21,7 +21,10 @@
 //  * float -> integer conversions truncate and saturate;
 //  * ray queries are answered by a callback (ref_harness.cpp answers them with
 //    the oracle's FP64 query, the part a Vulkan driver answers in the
-//    reference); atomics and invocations run one after another.
+//    reference); atomics are real (relaxed) atomics, so a dispatch may run
+//    its invocations on several threads, in which order they land then
+//    varies as on a GPU; run one after another they give the sequential
+//    order.
 #ifndef SRT_REF_RUNTIME_H
 #define SRT_REF_RUNTIME_H
 
@@ -247,19 +250,11 @@ struct Atomic {
 template <class T>
 inline uint32_t wb_arrayLength(const StorageArray<T>* a) { return a->n; }
 template <class T>
-inline T wb_atomicAdd(Atomic<T>* a, T x) {
-    T o = a->v;
-    a->v = (T)(o + x);
-    return o;
-}
+inline T wb_atomicAdd(Atomic<T>* a, T x) { return __atomic_fetch_add(&a->v, x, __ATOMIC_RELAXED); }
 template <class T>
-inline T wb_atomicLoad(Atomic<T>* a) { return a->v; }
+inline T wb_atomicLoad(Atomic<T>* a) { return __atomic_load_n(&a->v, __ATOMIC_RELAXED); }
 template <class T>
-inline T wb_atomicExchange(Atomic<T>* a, T x) {
-    T o = a->v;
-    a->v = x;
-    return o;
-}
+inline T wb_atomicExchange(Atomic<T>* a, T x) { return __atomic_exchange_n(&a->v, x, __ATOMIC_RELAXED); }
 
 // ------------------------------------------------------------ textures
 struct texture_storage_2d {

@@ -29,7 +29,6 @@ Usage: python tests/golden/make_ref_golden.py   (needs the reference tree)
 """
 from __future__ import annotations
 
-import ctypes as C
 import hashlib
 import sys
 import time
@@ -117,18 +116,7 @@ def scene_arrays(preset: int, seed: int, edit: str | None):
     if edit is None:
         return pre, a, None
     assert edit == "config2_mix"
-    mats = np.ctypeslib.as_array(C.cast(a.materials, C.POINTER(C.c_float)), (a.n_materials, 8)).copy()
-    idx = np.nonzero(mats[:, 4] == 5)[0]
-    g1, g2, g4 = idx[0::3], idx[1::3], idx[2::3]
-    mats[g1, 4] = 1
-    mats[g1, 5] = mats[g1, 3]
-    mats[g2, 4] = 2
-    mats[g2, 6] = 1.5
-    mats[g2, 7] = 0.004
-    mats[g4, 4] = 4
-    a2 = orc.SceneArrays()
-    C.pointer(a2)[0] = a
-    a2.materials = mats.ctypes.data
+    a2, mats = ref.reference_materials(a)
     return pre, a2, mats
 
 

@@ -39,6 +39,11 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"].startswith("config2")
+    # beside the port: the reference's own shaders (translated, built from the
+    # reference tree) on whole frames at their own constants, or why not
+    rs = d["reference_shaders"]
+    assert ("unavailable" in rs) or (rs["kind"] == "reference" and rs["value"] > 0 and rs["frames"] >= 1
+                                     and "2^20 photons" in rs["sample"])
 
 
 def test_relmse_and_time_to_reach():
