@@ -87,7 +87,7 @@ def reference_materials(arrays):
     mats[g2, 6] = 1.5
     mats[g2, 7] = 0.004
     mats[g4, 4] = 4
-    a2 = orc.SceneArrays()
+    a2 = type(arrays)()  # the oracle's or the product's srt_scene_arrays record
     C.pointer(a2)[0] = arrays
     a2.materials = mats.ctypes.data
     return a2, mats

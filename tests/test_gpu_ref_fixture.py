@@ -7,7 +7,8 @@ bit for bit (tests/test_oracle_ref_pin.py).  Here the GPU is compared with the
 same fixtures directly, through the C ABI, with the tolerances the GPU-vs-oracle
 tests use: integer work bit-exact; spectral and film math 1e-5 relative;
 frames (the GPU's own FP32 traversal and photon pass, 2^20 emitters, two
-frames) >= 97 % of pixels within 1e-3 relative, image relMSE < 1e-4 and the
+frames; five preset scenes and the config-2 geometry with reference material
+types) >= 97 % of pixels within 1e-3 relative, image relMSE < 1e-4 and the
 rgba8 image within 1 on > 97 % of the channels.
 """
 from __future__ import annotations
@@ -25,6 +26,9 @@ pytestmark = pytest.mark.gpu
 FIX = Path(__file__).resolve().parent / "golden" / "ref_wgsl.npz"
 # frame cases of the fixture whose scenes are the product's presets as they are
 FRAME_CASES = {"cornell": 0, "prism": 1, "config1": 2, "caustic_slab": 4, "indirect_room": 5}
+# and the config-2 geometry (1.57M triangles) with the coated spheres (material
+# type 5, which the reference lacks) as reference GGX, glass and film spheres
+REF_MATERIAL_CASES = {"config2_ref_materials": 3}
 
 
 @pytest.fixture(scope="module")
@@ -59,11 +63,21 @@ def test_camera_rays_match_reference_fixture(ctx, srt, orc, fx):
     assert np.abs(g[:, :6] - fx["camray_out"]).max() < 1e-5
 
 
-@pytest.mark.parametrize("case", sorted(FRAME_CASES))
+@pytest.mark.parametrize("case", sorted(FRAME_CASES) + sorted(REF_MATERIAL_CASES))
 def test_frames_match_reference_fixture(srt, ctx, fx, case):
     b = srt.SceneBuilder()
-    b.add_preset(FRAME_CASES[case], 0)
-    scene = b.build(ctx)
+    if case in FRAME_CASES:
+        b.add_preset(FRAME_CASES[case], 0)
+        scene = b.build(ctx)
+    else:
+        import ref_binding  # the same substitution as the fixture's (oracle/ref_binding.py)
+
+        b.add_preset(REF_MATERIAL_CASES[case], 0)
+        arrays, mats = ref_binding.reference_materials(b.arrays())
+        handle = C.c_void_p()
+        assert srt.lib().srt_scene_build(ctx.h, C.byref(arrays), C.byref(handle)) == 0  # copies the arrays
+        scene = srt.Scene(ctx, handle)
+        del mats
     h, w = fx[f"{case}_f0_accum"].shape[:2]
     r = srt.Renderer(ctx, scene, w, h, srt.default_params())  # MAX_DEPTH 12, 2^20 photons
     n_frames = 0
