@@ -89,7 +89,8 @@ def reference_materials(arrays):
     mats[g4, 4] = 4
     a2 = type(arrays)()  # the oracle's or the product's srt_scene_arrays record
     C.pointer(a2)[0] = arrays
-    a2.materials = mats.ctypes.data
+    field = dict(type(arrays)._fields_)["materials"]  # c_void_p or a typed pointer
+    a2.materials = C.cast(C.c_void_p(mats.ctypes.data), field)
     return a2, mats
 
 
