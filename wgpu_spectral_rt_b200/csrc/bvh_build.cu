@@ -11,9 +11,10 @@
 //   4. binary radix tree over the sorted codes (Karras, HPG 2012)
 //   5. bottom-up bounding boxes (one thread per leaf, atomic visit flags)
 //   6. collapse into 8-wide nodes, level by level: expand the child of
-//      largest surface area until 8 children; subtrees of <= 3 triangles
-//      become leaves; children are placed in slots by ray octant; child
-//      boxes are quantised to 8 bits against the node's box.
+//      largest surface area until 8 children; subtrees of at most leaf_max
+//      triangles (1..3, default 2) become leaves; children are placed in
+//      slots by ray octant; child boxes are quantised to 8 bits against the
+//      node's box.
 #include <array>
 #include <cmath>
 #include <cstdio>
