@@ -5,11 +5,15 @@
 // the reference tree) into C++ under oracle/_ref/; this file binds their
 // buffers the way the reference's passes do (renderer/mod.rs:168-207,
 // photon_emit_pass.rs, build_grid_pass.rs, compute_pass.rs), dispatches
-// their entry points one invocation after another, and answers their ray
+// their entry points (the photon and grid passes one invocation after
+// another for a deterministic order, or concurrently for timing; the camera
+// pass row-parallel, its invocations independent), and answers their ray
 // queries with the oracle's FP64 query (orc_ray_query) — the part that the
 // Vulkan driver answers in the reference.  The oracle's hand restatement
 // (oracle.cpp) is then checked against this run of the reference's code
-// (tests/test_oracle_ref_pin.py, tests/golden/make_ref_golden.py).
+// (tests/test_oracle_ref_pin.py, tests/golden/make_ref_golden.py), and
+// bench.py's reference arm times it.  The entry points bind module-scope
+// state: one call at a time per process.
 //
 // Built by `make -C oracle ref` into oracle/_ref/libref_wgsl.so, only where
 // the reference tree is present; nothing here is committed output.
